@@ -1,0 +1,926 @@
+/*
+ * vf_oracle.c -- FP64 CPU restatement of the VPFHF hot-path arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker and the timed CPU baseline; never
+ * linked into the product).  Every "_ref" function follows the reference's
+ * loop nesting and left-to-right expression order so that it reproduces the
+ * reference's FP64 rounding on a single rank; the "_mf" / fast variants are
+ * algebraically identical reorderings used where speed matters.
+ *
+ * Build: oracle/Makefile (gcc -O2 -fopenmp -ffp-contract=off).
+ */
+#include "vf_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define NODE(P, i, j, k) (((int64_t)(k) * (P)->ny + (j)) * (P)->nx + (i))
+
+/* ------------------------------------------------------------------------ */
+/* Geometry: VFGeometryInitialize builds X[i] = i*lx/(nx-1.) (VFCommon.c:394-399)
+ * and every element loop takes hx = X[ei+1]-X[ei] (e.g. VFMech.c:1557-1559). */
+static double coord(int i, double l, int n) { return i == 0 ? 0. : i * l / (n - 1.); }
+
+static void cell_h(const vfo_problem *P, int ei, int ej, int ek, double *hx, double *hy,
+                   double *hz) {
+  *hx = coord(ei + 1, P->lx, P->nx) - coord(ei, P->lx, P->nx);
+  *hy = coord(ej + 1, P->ly, P->ny) - coord(ej, P->ly, P->ny);
+  *hz = coord(ek + 1, P->lz, P->nz) - coord(ek, P->lz, P->nz);
+}
+
+typedef struct {
+  double lambda, mu, alpha, beta, Gc;
+} cellmat;
+
+/* Lame coefficients as VFMatPropGet computes them (VFCommon.c:583-586); the
+ * optional per-cell E is this build's generalisation of the per-layer table. */
+static cellmat cell_material(const vfo_problem *P, int ei, int ej, int ek) {
+  cellmat m;
+  int l = P->layer ? P->layer[ek] : 0;
+  double E = P->E[l], nu = P->nu[l];
+  if (P->cellE) E = P->cellE[((int64_t)ek * (P->ny - 1) + ej) * (P->nx - 1) + ei];
+  m.lambda = E * nu / (1. + nu) / (1. - 2. * nu);
+  m.mu = E / (1. + nu) * .5;
+  m.alpha = P->alpha[l];
+  m.beta = P->beta[l];
+  m.Gc = P->Gc[l];
+  return m;
+}
+
+static double atCv(const vfo_problem *P) { return P->atnum == 1 ? 2. / 3. : .5; } /* VFCommon.c:482-492 */
+
+/* ------------------------------------------------------------------------ */
+/* VFCartFEElement1DInit (VFCartFE.c:90-116) and VFCartFEElement3DInit
+ * (VFCartFE.c:216-269): 3-point Gauss per axis, tensor product, g = gi+3gj+9gk. */
+typedef struct {
+  double w[27];
+  double phi[8][27];
+  double dphi[8][3][27];
+} etab;
+
+static void tables1d(double l, double w[3], double phi[2][3], double dphi[2][3]) {
+  w[0] = 5. * l / 18.;
+  w[1] = 8. * l / 18.;
+  w[2] = 5. * l / 18.;
+  phi[0][0] = (1. + sqrt(3. / 5.)) * .5;
+  phi[0][1] = .5;
+  phi[0][2] = (1. - sqrt(3. / 5.)) * .5;
+  phi[1][0] = (1. - sqrt(3. / 5.)) * .5;
+  phi[1][1] = .5;
+  phi[1][2] = (1. + sqrt(3. / 5.)) * .5;
+  for (int g = 0; g < 3; g++) {
+    dphi[0][g] = -1. / l;
+    dphi[1][g] = 1. / l;
+  }
+}
+
+static void etab_init(etab *e, double hx, double hy, double hz) {
+  double wx[3], wy[3], wz[3], px[2][3], py[2][3], pz[2][3], dx[2][3], dy[2][3], dz[2][3];
+  tables1d(hx, wx, px, dx);
+  tables1d(hy, wy, py, dy);
+  tables1d(hz, wz, pz, dz);
+  for (int gk = 0, g = 0; gk < 3; gk++)
+    for (int gj = 0; gj < 3; gj++)
+      for (int gi = 0; gi < 3; gi++, g++) e->w[g] = wz[gk] * wy[gj] * wx[gi];
+  for (int gk = 0, g = 0; gk < 3; gk++)
+    for (int gj = 0; gj < 3; gj++)
+      for (int gi = 0; gi < 3; gi++, g++)
+        for (int k = 0; k < 2; k++)
+          for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+              int a = i + 2 * j + 4 * k;
+              e->phi[a][g] = pz[k][gk] * py[j][gj] * px[i][gi];
+              e->dphi[a][0][g] = pz[k][gk] * py[j][gj] * dx[i][gi];
+              e->dphi[a][1][g] = pz[k][gk] * dy[j][gj] * px[i][gi];
+              e->dphi[a][2][g] = dz[k][gk] * py[j][gj] * px[i][gi];
+            }
+}
+
+int vfo_tables(double hx, double hy, double hz, double w[27], double phi[8 * 27],
+               double dphi[8 * 3 * 27]) {
+  etab e;
+  etab_init(&e, hx, hy, hz);
+  memcpy(w, e.w, sizeof e.w);
+  memcpy(phi, e.phi, sizeof e.phi);
+  memcpy(dphi, e.dphi, sizeof e.dphi);
+  return 0;
+}
+
+static void cell_nodes(const vfo_problem *P, int ei, int ej, int ek, int64_t n[8]) {
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) n[i + 2 * j + 4 * k] = NODE(P, ei + i, ej + j, ek + k);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dirichlet BC, VecApplyDirichletBC / ResidualApplyDirichletBC precedence
+ * (VFCartFE.c:493-998): faces X0,X1,Y0,Y1,Z0,Z1 in order (later wins), then the
+ * 8 vertices in the order the reference applies them. */
+int vfo_bc_build(int nx, int ny, int nz, int dof, const int *face, const int *vertex,
+                 const double *bcu, uint8_t *mask, double *value) {
+  int64_t N = (int64_t)nx * ny * nz;
+  memset(mask, 0, (size_t)(N * dof));
+  for (int64_t q = 0; q < N * dof; q++) value[q] = 0.;
+#define SETBC(ii, jj, kk, type)                                                  \
+  do {                                                                           \
+    int64_t q_ = (((int64_t)(kk) * ny + (jj)) * nx + (ii)) * dof + c;            \
+    mask[q_] = 1;                                                                \
+    value[q_] = (type) == VFO_ZERO ? 0. : (type) == VFO_ONE ? 1. : (bcu ? bcu[q_] : 0.); \
+  } while (0)
+  for (int c = 0; c < dof; c++) {
+    const int *f = face + 6 * c;
+    for (int fc = 0; fc < 6; fc++) {
+      int t = f[fc];
+      if (t == VFO_NONE) continue;
+      if (fc < 2) {
+        int i = fc == 0 ? 0 : nx - 1;
+        for (int k = 0; k < nz; k++)
+          for (int j = 0; j < ny; j++) SETBC(i, j, k, t);
+      } else if (fc < 4) {
+        int j = fc == 2 ? 0 : ny - 1;
+        for (int k = 0; k < nz; k++)
+          for (int i = 0; i < nx; i++) SETBC(i, j, k, t);
+      } else {
+        int k = fc == 4 ? 0 : nz - 1;
+        for (int j = 0; j < ny; j++)
+          for (int i = 0; i < nx; i++) SETBC(i, j, k, t);
+      }
+    }
+    /* VERTEX enum: X0Y0Z0,X1Y0Z0,X0Y1Z0,X1Y1Z0,X0Y0Z1,X1Y0Z1,X0Y1Z1,X1Y1Z1 (VFCartFE.h:121-130);
+     * applied in the order X0Y0Z0, X0Y0Z1, X0Y1Z0, X0Y1Z1, X1Y0Z0, X1Y0Z1, X1Y1Z0, X1Y1Z1
+     * (VFCartFE.c:950-972). */
+    static const int order[8] = {0, 4, 2, 6, 1, 5, 3, 7};
+    for (int o = 0; o < 8; o++) {
+      int vtx = order[o];
+      int t = vertex[8 * c + vtx];
+      if (t == VFO_NONE) continue;
+      int i = (vtx & 1) ? nx - 1 : 0, j = (vtx & 2) ? ny - 1 : 0, k = (vtx & 4) ? nz - 1 : 0;
+      SETBC(i, j, k, t);
+    }
+  }
+#undef SETBC
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* VF_BilinearFormU3D_local (VFMech.c:227-290). */
+static void u_element_matrix(const etab *e, const cellmat *m, double eta, const double v8[8],
+                             double K[576]) {
+  double s[27];
+  for (int g = 0; g < 27; g++) s[g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) s[g] += v8[a] * e->phi[a][g];
+  for (int g = 0; g < 27; g++) s[g] = s[g] * s[g] + eta;
+  for (int l = 0; l < 576; l++) K[l] = 0;
+  int l = 0;
+  for (int a = 0; a < 8; a++)
+    for (int c1 = 0; c1 < 3; c1++)
+      for (int b = 0; b < 8; b++)
+        for (int c2 = 0; c2 < 3; c2++, l++)
+          for (int g = 0; g < 27; g++) {
+            double mg = m->lambda * s[g] * e->dphi[a][c1][g] * e->dphi[b][c2][g];
+            mg += m->mu * s[g] * e->dphi[a][c2][g] * e->dphi[b][c1][g];
+            if (c1 == c2)
+              mg += m->mu * s[g] *
+                    (e->dphi[a][0][g] * e->dphi[b][0][g] + e->dphi[a][1][g] * e->dphi[b][1][g] +
+                     e->dphi[a][2][g] * e->dphi[b][2][g]);
+            K[l] += e->w[g] * mg;
+          }
+}
+
+int vfo_u_element_matrix(const vfo_problem *P, int ei, int ej, int ek, const double *v,
+                         double K[576]) {
+  double hx, hy, hz, v8[8];
+  int64_t n[8];
+  etab e;
+  cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+  etab_init(&e, hx, hy, hz);
+  cell_nodes(P, ei, ej, ek, n);
+  for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
+  cellmat m = cell_material(P, ei, ej, ek);
+  u_element_matrix(&e, &m, P->eta, v8, K);
+  return 0;
+}
+
+/* VF_GradientUThermoPoro3D_local (VFMech.c:386-447). */
+static void u_rhs_thermoporo(const etab *e, const cellmat *m, double eta, const double th8[8],
+                             const double p8[8], const double v8[8], double rl[24]) {
+  double coefalpha = (3. * m->lambda + 2. * m->mu) * m->alpha, beta = m->beta;
+  double te[27], pe[27], ve[27];
+  for (int g = 0; g < 27; g++) te[g] = pe[g] = ve[g] = 0.;
+  for (int g = 0; g < 27; g++)
+    for (int a = 0; a < 8; a++) {
+      te[g] += e->phi[a][g] * th8[a];
+      pe[g] += e->phi[a][g] * p8[a];
+      ve[g] += e->phi[a][g] * v8[a];
+    }
+  for (int g = 0; g < 27; g++)
+    for (int a = 0, l = 0; a < 8; a++)
+      for (int c = 0; c < 3; c++, l++)
+        rl[l] += e->w[g] * e->dphi[a][c][g] *
+                 (coefalpha * te[g] * (ve[g] * ve[g] + eta) + beta * pe[g] * ve[g]);
+}
+
+/* VF_GradientUCrackPressure3D_local (VFMech.c:533-589). */
+static void u_rhs_crackpressure(const etab *e, const double p8[8], const double v8[8],
+                                double rl[24]) {
+  double pe[27], gv[3][27];
+  for (int g = 0; g < 27; g++) {
+    pe[g] = 0;
+    for (int c = 0; c < 3; c++) gv[c][g] = 0.;
+  }
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      pe[g] += e->phi[a][g] * p8[a];
+      for (int c = 0; c < 3; c++) gv[c][g] += e->dphi[a][c][g] * v8[a];
+    }
+  for (int a = 0, l = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++, l++)
+      for (int g = 0; g < 27; g++) rl[l] += e->w[g] * pe[g] * gv[c][g] * e->phi[a][g];
+}
+
+static void gather_cell(const vfo_problem *P, int ei, int ej, int ek, const double *v,
+                        const double *theta, const double *thetaRef, const double *p,
+                        double v8[8], double th8[8], double p8[8]) {
+  int64_t n[8];
+  cell_nodes(P, ei, ej, ek, n);
+  for (int a = 0; a < 8; a++) {
+    if (v8) v8[a] = v[n[a]];
+    if (th8) th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+    if (p8) p8[a] = p ? p[n[a]] : 0.;
+  }
+}
+
+/* VF_UResidual (VFMech.c:1456-1887) without in-situ tractions: element loop in
+ * the reference's order, F += K_e u_e then F -= (thermo-poro + crack pressure),
+ * then ResidualApplyDirichletBC (F = u - ubc on BC rows). */
+int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
+                       const double *theta, const double *thetaRef, const double *p,
+                       const uint8_t *bcmask, const double *bcval, double *F) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < 3 * N; q++) F[q] = 0.;
+  double K[576], rl[24], v8[8], th8[8], p8[8], hx, hy, hz;
+  int64_t n[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        cell_nodes(P, ei, ej, ek, n);
+        gather_cell(P, ei, ej, ek, v, theta, thetaRef, p, v8, th8, p8);
+        u_element_matrix(&e, &m, P->eta, v8, K);
+        int l = 0;
+        for (int a = 0; a < 8; a++)
+          for (int c1 = 0; c1 < 3; c1++)
+            for (int b = 0; b < 8; b++)
+              for (int c2 = 0; c2 < 3; c2++, l++) F[3 * n[a] + c1] += K[l] * u[3 * n[b] + c2];
+        for (l = 0; l < 24; l++) rl[l] = 0.;
+        u_rhs_thermoporo(&e, &m, P->eta, th8, p8, v8, rl);
+        if (P->hasCrackPressure) u_rhs_crackpressure(&e, p8, v8, rl);
+        for (int a = 0, l2 = 0; a < 8; a++)
+          for (int c = 0; c < 3; c++, l2++) F[3 * n[a] + c] -= rl[l2];
+      }
+  if (bcmask)
+    for (int64_t q = 0; q < 3 * N; q++)
+      if (bcmask[q]) F[q] = u[q] - bcval[q];
+  return 0;
+}
+
+/* J x with the assembled element matrices (VF_UIJacobian, VFMech.c:1897-2029):
+ * BC rows are identity, BC columns are kept (MatZeroRowsStencil, VFCartFE.c:1293). */
+int vfo_u_apply_ref(const vfo_problem *P, const double *v, const double *x,
+                    const uint8_t *bcmask, double *y) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < 3 * N; q++) y[q] = 0.;
+  double K[576];
+  int64_t n[8];
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        vfo_u_element_matrix(P, ei, ej, ek, v, K);
+        cell_nodes(P, ei, ej, ek, n);
+        int l = 0;
+        for (int a = 0; a < 8; a++)
+          for (int c1 = 0; c1 < 3; c1++)
+            for (int b = 0; b < 8; b++)
+              for (int c2 = 0; c2 < 3; c2++, l++) y[3 * n[a] + c1] += K[l] * x[3 * n[b] + c2];
+      }
+  if (bcmask)
+    for (int64_t q = 0; q < 3 * N; q++)
+      if (bcmask[q]) y[q] = x[q];
+  return 0;
+}
+
+/* Matrix-free J x, per-Gauss-point form of the same bilinear form:
+ * y_(a,c) = sum_g sum_d dphi_a,d(g) sigma_cd(g),
+ * sigma = w s (lambda tr(G) I + mu (G + G^T)),  G_cd = sum_b dphi_b,d u_(b,c).
+ * Elements are visited in 8 parity colours so the OpenMP scatter is race-free
+ * and the result is independent of the thread count. */
+int vfo_u_apply_mf(const vfo_problem *P, const double *v, const double *x,
+                   const uint8_t *bcmask, double *y) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < 3 * N; q++) y[q] = 0.;
+  int nex = P->nx - 1, ney = P->ny - 1, nez = P->nz - 1;
+  if (P->nthreads > 0) {
+#ifdef _OPENMP
+    omp_set_num_threads(P->nthreads);
+#endif
+  }
+  for (int color = 0; color < 8; color++) {
+    int cx = color & 1, cy = (color >> 1) & 1, cz = (color >> 2) & 1;
+    int hx_n = (nex - cx + 1) / 2, hy_n = (ney - cy + 1) / 2, hz_n = (nez - cz + 1) / 2;
+    int64_t total = (int64_t)hx_n * hy_n * hz_n;
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < total; t++) {
+      int ei = cx + 2 * (int)(t % hx_n);
+      int ej = cy + 2 * (int)((t / hx_n) % hy_n);
+      int ek = cz + 2 * (int)(t / ((int64_t)hx_n * hy_n));
+      double hx, hy, hz;
+      etab e;
+      cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+      etab_init(&e, hx, hy, hz);
+      cellmat m = cell_material(P, ei, ej, ek);
+      int64_t n[8];
+      cell_nodes(P, ei, ej, ek, n);
+      double ue[8][3], v8[8], ye[8][3];
+      for (int a = 0; a < 8; a++) {
+        v8[a] = v[n[a]];
+        for (int c = 0; c < 3; c++) {
+          ue[a][c] = x[3 * n[a] + c];
+          ye[a][c] = 0.;
+        }
+      }
+      for (int g = 0; g < 27; g++) {
+        double s = 0., G[3][3] = {{0}};
+        for (int a = 0; a < 8; a++) {
+          s += v8[a] * e.phi[a][g];
+          for (int c = 0; c < 3; c++)
+            for (int d = 0; d < 3; d++) G[c][d] += e.dphi[a][d][g] * ue[a][c];
+        }
+        double ws = e.w[g] * (s * s + P->eta);
+        double tr = G[0][0] + G[1][1] + G[2][2], sg[3][3];
+        for (int c = 0; c < 3; c++)
+          for (int d = 0; d < 3; d++)
+            sg[c][d] = ws * ((c == d ? m.lambda * tr : 0.) + m.mu * (G[c][d] + G[d][c]));
+        for (int a = 0; a < 8; a++)
+          for (int c = 0; c < 3; c++)
+            ye[a][c] += e.dphi[a][0][g] * sg[c][0] + e.dphi[a][1][g] * sg[c][1] +
+                        e.dphi[a][2][g] * sg[c][2];
+      }
+      for (int a = 0; a < 8; a++)
+        for (int c = 0; c < 3; c++) y[3 * n[a] + c] += ye[a][c];
+    }
+  }
+  if (bcmask)
+    for (int64_t q = 0; q < 3 * N; q++)
+      if (bcmask[q]) y[q] = x[q];
+  return 0;
+}
+
+/* f with F = K u - f: the thermo-poro and crack-pressure load vectors of
+ * VF_UResidual (VFMech.c:1600-1626), summed in element order. */
+int vfo_u_rhs(const vfo_problem *P, const double *v, const double *theta,
+              const double *thetaRef, const double *p, double *f) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < 3 * N; q++) f[q] = 0.;
+  double rl[24], v8[8], th8[8], p8[8], hx, hy, hz;
+  int64_t n[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        cell_nodes(P, ei, ej, ek, n);
+        gather_cell(P, ei, ej, ek, v, theta, thetaRef, p, v8, th8, p8);
+        for (int l = 0; l < 24; l++) rl[l] = 0.;
+        u_rhs_thermoporo(&e, &m, P->eta, th8, p8, v8, rl);
+        if (P->hasCrackPressure) u_rhs_crackpressure(&e, p8, v8, rl);
+        for (int a = 0, l = 0; a < 8; a++)
+          for (int c = 0; c < 3; c++, l++) f[3 * n[a] + c] += rl[l];
+      }
+  return 0;
+}
+
+/* Diagonal of K(v) (the Jacobi preconditioner of KSPCG with -U_pc_type jacobi),
+ * BC rows 1 as after MatZeroRowsStencil. */
+int vfo_u_diag(const vfo_problem *P, const double *v, const uint8_t *bcmask, double *d) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < 3 * N; q++) d[q] = 0.;
+  double K[576];
+  int64_t n[8];
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        vfo_u_element_matrix(P, ei, ej, ek, v, K);
+        cell_nodes(P, ei, ej, ek, n);
+        for (int a = 0; a < 8; a++)
+          for (int c = 0; c < 3; c++) d[3 * n[a] + c] += K[(3 * a + c) * 24 + 3 * a + c];
+      }
+  if (bcmask)
+    for (int64_t q = 0; q < 3 * N; q++)
+      if (bcmask[q]) d[q] = 1.;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CSR assembly of the DMDA AIJ matrix (box stencil, 3 dof: up to 81 nnz/row,
+ * columns ascending) -- what PETSc's MatMult runs inside KSPCG. */
+int64_t vfo_u_csr_nnz(const vfo_problem *P) {
+  int64_t nnz = 0;
+  for (int k = 0; k < P->nz; k++)
+    for (int j = 0; j < P->ny; j++)
+      for (int i = 0; i < P->nx; i++) {
+        int cx = (i > 0) + 1 + (i < P->nx - 1), cy = (j > 0) + 1 + (j < P->ny - 1),
+            cz = (k > 0) + 1 + (k < P->nz - 1);
+        nnz += 3 * 3 * (int64_t)cx * cy * cz;
+      }
+  return nnz;
+}
+
+static int64_t csr_pos(const vfo_problem *P, const int64_t *rowptr, int i, int j, int k, int c1,
+                       int di, int dj, int dk, int c2) {
+  /* columns of row (i,j,k,c1): neighbours in (k,j,i) order then component */
+  int x0 = i > 0 ? i - 1 : 0, x1 = i < P->nx - 1 ? i + 1 : i;
+  int y0 = j > 0 ? j - 1 : 0, y1 = j < P->ny - 1 ? j + 1 : j;
+  int z0 = k > 0 ? k - 1 : 0;
+  int cx = x1 - x0 + 1, cy = y1 - y0 + 1;
+  int ox = i + di - x0, oy = j + dj - y0, oz = k + dk - z0;
+  int64_t row = 3 * NODE(P, i, j, k) + c1;
+  return rowptr[row] + ((int64_t)(oz * cy + oy) * cx + ox) * 3 + c2;
+}
+
+int vfo_u_assemble_csr(const vfo_problem *P, const double *v, const uint8_t *bcmask,
+                       int64_t *rowptr, int32_t *colidx, double *vals) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz, r = 0;
+  rowptr[0] = 0;
+  for (int k = 0; k < P->nz; k++)
+    for (int j = 0; j < P->ny; j++)
+      for (int i = 0; i < P->nx; i++)
+        for (int c1 = 0; c1 < 3; c1++, r++) {
+          int64_t pos = rowptr[r];
+          for (int kk = k - 1; kk <= k + 1; kk++)
+            for (int jj = j - 1; jj <= j + 1; jj++)
+              for (int ii = i - 1; ii <= i + 1; ii++) {
+                if (ii < 0 || jj < 0 || kk < 0 || ii >= P->nx || jj >= P->ny || kk >= P->nz)
+                  continue;
+                for (int c2 = 0; c2 < 3; c2++) {
+                  colidx[pos] = (int32_t)(3 * NODE(P, ii, jj, kk) + c2);
+                  vals[pos] = 0.;
+                  pos++;
+                }
+              }
+          rowptr[r + 1] = pos;
+        }
+  int nex = P->nx - 1, ney = P->ny - 1, nez = P->nz - 1;
+  for (int color = 0; color < 8; color++) {
+    int cx = color & 1, cy = (color >> 1) & 1, cz = (color >> 2) & 1;
+    int hx_n = (nex - cx + 1) / 2, hy_n = (ney - cy + 1) / 2, hz_n = (nez - cz + 1) / 2;
+    int64_t total = (int64_t)hx_n * hy_n * hz_n;
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < total; t++) {
+      int ei = cx + 2 * (int)(t % hx_n);
+      int ej = cy + 2 * (int)((t / hx_n) % hy_n);
+      int ek = cz + 2 * (int)(t / ((int64_t)hx_n * hy_n));
+      double K[576];
+      vfo_u_element_matrix(P, ei, ej, ek, v, K);
+      int l = 0;
+      for (int a = 0; a < 8; a++)
+        for (int c1 = 0; c1 < 3; c1++)
+          for (int b = 0; b < 8; b++)
+            for (int c2 = 0; c2 < 3; c2++, l++) {
+              int ai = a & 1, aj = (a >> 1) & 1, ak = a >> 2;
+              int bi = b & 1, bj = (b >> 1) & 1, bk = b >> 2;
+              int64_t pos = csr_pos(P, rowptr, ei + ai, ej + aj, ek + ak, c1, bi - ai, bj - aj,
+                                    bk - ak, c2);
+              vals[pos] += K[l];
+            }
+    }
+  }
+  if (bcmask)
+    for (int64_t q = 0; q < 3 * N; q++)
+      if (bcmask[q])
+        for (int64_t pos = rowptr[q]; pos < rowptr[q + 1]; pos++)
+          vals[pos] = colidx[pos] == q ? 1. : 0.;
+  return 0;
+}
+
+int vfo_csr_spmv(int64_t nrows, const int64_t *rowptr, const int32_t *colidx,
+                 const double *vals, const double *x, double *y, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#endif
+#pragma omp parallel for schedule(static)
+  for (int64_t r = 0; r < nrows; r++) {
+    double s = 0.;
+    for (int64_t pos = rowptr[r]; pos < rowptr[r + 1]; pos++) s += vals[pos] * x[colidx[pos]];
+    y[r] = s;
+  }
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* ElasticEnergyDensity3D_local (VFMech.c:32-106). */
+static void elastic_energy_density(const etab *e, const cellmat *m, const double u8[8][3],
+                                   const double th8[8], double W[27]) {
+  double e11[27], e22[27], e33[27], e12[27], e23[27], e13[27];
+  double lambda = m->lambda, mu = m->mu, alpha = m->alpha;
+  for (int g = 0; g < 27; g++) e11[g] = e22[g] = e33[g] = e12[g] = e23[g] = e13[g] = W[g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      e11[g] += e->dphi[a][0][g] * u8[a][0] - alpha * e->phi[a][g] * th8[a];
+      e22[g] += e->dphi[a][1][g] * u8[a][1] - alpha * e->phi[a][g] * th8[a];
+      e33[g] += e->dphi[a][2][g] * u8[a][2] - alpha * e->phi[a][g] * th8[a];
+      e12[g] += (e->dphi[a][0][g] * u8[a][1] + e->dphi[a][1][g] * u8[a][0]) * .5;
+      e23[g] += (e->dphi[a][1][g] * u8[a][2] + e->dphi[a][2][g] * u8[a][1]) * .5;
+      e13[g] += (e->dphi[a][0][g] * u8[a][2] + e->dphi[a][2][g] * u8[a][0]) * .5;
+    }
+  for (int g = 0; g < 27; g++) {
+    double s11 = (lambda + 2. * mu) * e11[g] + lambda * e22[g] + lambda * e33[g];
+    double s22 = lambda * e11[g] + (lambda + 2. * mu) * e22[g] + lambda * e33[g];
+    double s33 = lambda * e11[g] + lambda * e22[g] + (lambda + 2. * mu) * e33[g];
+    double s12 = 2. * mu * e12[g], s23 = 2. * mu * e23[g], s13 = 2. * mu * e13[g];
+    W[g] = (s11 * e11[g] + s22 * e22[g] + s33 * e33[g]) * .5 + s12 * e12[g] + s23 * e23[g] +
+           s13 * e13[g];
+  }
+}
+
+/* VF_BilinearFormVAT1/AT23D_local + VF_BilinearFormVCoupling3D_local
+ * (VFMech.c:2040-2115), accumulated in the order VF_VResidual uses. */
+static void v_element_matrix(const vfo_problem *P, const etab *e, const cellmat *m,
+                             const double u8[8][3], const double th8[8], double K[64]) {
+  double coef = m->Gc / atCv(P) * .5, eps = P->epsilon, W[27];
+  for (int l = 0; l < 64; l++) K[l] = 0.;
+  for (int a = 0, l = 0; a < 8; a++)
+    for (int b = 0; b < 8; b++, l++)
+      for (int g = 0; g < 27; g++) {
+        double dd = e->dphi[a][0][g] * e->dphi[b][0][g] + e->dphi[a][1][g] * e->dphi[b][1][g] +
+                    e->dphi[a][2][g] * e->dphi[b][2][g];
+        if (P->atnum == 1)
+          K[l] += coef * e->w[g] * dd * eps;
+        else
+          K[l] += coef * e->w[g] * (e->phi[a][g] * e->phi[b][g] / eps + dd * eps);
+      }
+  elastic_energy_density(e, m, u8, th8, W);
+  for (int a = 0, l = 0; a < 8; a++)
+    for (int b = 0; b < 8; b++, l++)
+      for (int g = 0; g < 27; g++) K[l] += e->w[g] * e->phi[a][g] * e->phi[b][g] * W[g] * 2.;
+}
+
+static void gather_u8(const vfo_problem *P, int ei, int ej, int ek, const double *u,
+                      double u8[8][3]) {
+  int64_t n[8];
+  cell_nodes(P, ei, ej, ek, n);
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
+}
+
+int vfo_v_element_matrix(const vfo_problem *P, int ei, int ej, int ek, const double *u,
+                         const double *theta, const double *thetaRef, double K[64]) {
+  double hx, hy, hz, u8[8][3], th8[8];
+  etab e;
+  cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+  etab_init(&e, hx, hy, hz);
+  cellmat m = cell_material(P, ei, ej, ek);
+  gather_u8(P, ei, ej, ek, u, u8);
+  gather_cell(P, ei, ej, ek, NULL, theta, thetaRef, NULL, NULL, th8, NULL);
+  v_element_matrix(P, &e, &m, u8, th8, K);
+  return 0;
+}
+
+/* VF_ResidualVAT1/AT23D_local (VFMech.c:2350-2384). */
+static void v_rhs_at(const vfo_problem *P, const etab *e, const cellmat *m, double rl[8]) {
+  double coef = m->Gc / atCv(P) / P->epsilon * (P->atnum == 1 ? .25 : .5);
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) rl[a] += e->w[g] * e->phi[a][g] * coef;
+}
+
+/* VF_ResidualVCrackPressure3D_local (VFMech.c:2294-2341). */
+static void v_rhs_crackpressure(const etab *e, const double u8[8][3], const double p8[8],
+                                double rl[8]) {
+  double pe[27], ue[3][27];
+  for (int g = 0; g < 27; g++) {
+    pe[g] = 0;
+    for (int c = 0; c < 3; c++) ue[c][g] = 0.;
+  }
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      pe[g] += e->phi[a][g] * p8[a];
+      for (int c = 0; c < 3; c++) ue[c][g] += e->phi[a][g] * u8[a][c];
+    }
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++)
+      for (int g = 0; g < 27; g++) rl[a] += e->w[g] * pe[g] * ue[c][g] * e->dphi[a][c][g];
+}
+
+/* b with F_V = K_V v - b (AT linear term + crack pressure term). */
+int vfo_v_rhs(const vfo_problem *P, const double *u, const double *p, double *b) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < N; q++) b[q] = 0.;
+  double hx, hy, hz, u8[8][3], p8[8], rl[8];
+  int64_t n[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        cell_nodes(P, ei, ej, ek, n);
+        gather_u8(P, ei, ej, ek, u, u8);
+        gather_cell(P, ei, ej, ek, NULL, NULL, NULL, p, NULL, NULL, p8);
+        for (int a = 0; a < 8; a++) rl[a] = 0.;
+        v_rhs_at(P, &e, &m, rl);
+        if (P->hasCrackPressure) v_rhs_crackpressure(&e, u8, p8, rl);
+        for (int a = 0; a < 8; a++) b[n[a]] += rl[a];
+      }
+  return 0;
+}
+
+/* VF_VResidual (VFMech.c:2687-2879), including quirk Q1: the thermo-poro
+ * residual of VF_ResidualVThermoPoro3D_local is overwritten (VFMech.c:2809-2810)
+ * and never reaches F; AT2 irreversibility zeroes F where VIrrev <= irrevtol
+ * (VF_IrrevApplyEQVec, VFMech.c:2597-2628); V BC rows give F = v - bc. */
+int vfo_v_residual_ref(const vfo_problem *P, const double *u, const double *v,
+                       const double *theta, const double *thetaRef, const double *p,
+                       const double *virrev, const uint8_t *bcmask, const double *bcval,
+                       double *F) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < N; q++) F[q] = 0.;
+  double hx, hy, hz, u8[8][3], th8[8], p8[8], rl[8], K[64];
+  int64_t n[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        cell_nodes(P, ei, ej, ek, n);
+        gather_u8(P, ei, ej, ek, u, u8);
+        gather_cell(P, ei, ej, ek, NULL, theta, thetaRef, p, NULL, th8, p8);
+        v_element_matrix(P, &e, &m, u8, th8, K);
+        for (int a = 0; a < 8; a++) {
+          rl[a] = 0.;
+          for (int b = 0; b < 8; b++) rl[a] -= K[a * 8 + b] * v[n[b]];
+        }
+        v_rhs_at(P, &e, &m, rl);
+        if (P->hasCrackPressure) v_rhs_crackpressure(&e, u8, p8, rl);
+        for (int a = 0; a < 8; a++) F[n[a]] -= rl[a];
+      }
+  if (P->atnum == 2 && virrev)
+    for (int64_t q = 0; q < N; q++)
+      if (virrev[q] <= P->irrevtol) F[q] = 0.;
+  if (bcmask)
+    for (int64_t q = 0; q < N; q++)
+      if (bcmask[q]) F[q] = v[q] - bcval[q];
+  return 0;
+}
+
+static uint8_t v_fixed(const vfo_problem *P, const double *virrev, const uint8_t *bcmask,
+                       int64_t q) {
+  if (bcmask && bcmask[q]) return 1;
+  if (P->atnum == 2 && virrev && virrev[q] <= P->irrevtol) return 1;
+  return 0;
+}
+
+/* J_V x: MatApplyDirichletBCRowCol (VFCartFE.c:1305-1454) and, for AT2,
+ * VF_IrrevApplyEQMat (VFMech.c:2637-2682) make those rows and columns identity. */
+int vfo_v_apply(const vfo_problem *P, const double *u, const double *theta,
+                const double *thetaRef, const double *virrev, const uint8_t *bcmask,
+                const double *x, double *y) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < N; q++) y[q] = 0.;
+  int nex = P->nx - 1, ney = P->ny - 1, nez = P->nz - 1;
+  for (int color = 0; color < 8; color++) {
+    int cx = color & 1, cy = (color >> 1) & 1, cz = (color >> 2) & 1;
+    int hx_n = (nex - cx + 1) / 2, hy_n = (ney - cy + 1) / 2, hz_n = (nez - cz + 1) / 2;
+    int64_t total = (int64_t)hx_n * hy_n * hz_n;
+#pragma omp parallel for schedule(static)
+    for (int64_t t = 0; t < total; t++) {
+      int ei = cx + 2 * (int)(t % hx_n);
+      int ej = cy + 2 * (int)((t / hx_n) % hy_n);
+      int ek = cz + 2 * (int)(t / ((int64_t)hx_n * hy_n));
+      double K[64];
+      int64_t n[8];
+      vfo_v_element_matrix(P, ei, ej, ek, u, theta, thetaRef, K);
+      cell_nodes(P, ei, ej, ek, n);
+      double xe[8];
+      for (int b = 0; b < 8; b++) xe[b] = v_fixed(P, virrev, bcmask, n[b]) ? 0. : x[n[b]];
+      for (int a = 0; a < 8; a++) {
+        double s = 0.;
+        for (int b = 0; b < 8; b++) s += K[a * 8 + b] * xe[b];
+        y[n[a]] += s;
+      }
+    }
+  }
+  for (int64_t q = 0; q < N; q++)
+    if (v_fixed(P, virrev, bcmask, q)) y[q] = x[q];
+  return 0;
+}
+
+int vfo_v_diag(const vfo_problem *P, const double *u, const double *theta,
+               const double *thetaRef, const double *virrev, const uint8_t *bcmask,
+               double *d) {
+  int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  for (int64_t q = 0; q < N; q++) d[q] = 0.;
+  double K[64];
+  int64_t n[8];
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        vfo_v_element_matrix(P, ei, ej, ek, u, theta, thetaRef, K);
+        cell_nodes(P, ei, ej, ek, n);
+        for (int a = 0; a < 8; a++) d[n[a]] += K[a * 9];
+      }
+  for (int64_t q = 0; q < N; q++)
+    if (v_fixed(P, virrev, bcmask, q)) d[q] = 1.;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* VF_UEnergy3D (VFMech.c:1111-1427) without in-situ work: per element
+ * VF_ElasticEnergy3D_local (VFMech.c:725-809, quirk Q2: v^2(1+eta) on the
+ * deviatoric part) and VF_PressureWork3D_local (VFMech.c:920-974). */
+int vfo_u_energy(const vfo_problem *P, const double *u, const double *v,
+                 const double *theta, const double *thetaRef, const double *p,
+                 double out[2]) {
+  double myE = 0., myPW = 0., hx, hy, hz, u8[8][3], v8[8], th8[8], p8[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        gather_u8(P, ei, ej, ek, u, u8);
+        gather_cell(P, ei, ej, ek, v, theta, thetaRef, p, v8, th8, p8);
+        double D11[27], D22[27], D33[27], D12[27], D23[27], D13[27], ve[27], pe[27], te[27];
+        double threekappa = 3. * m.lambda + 2. * m.mu, coefbeta = m.beta / threekappa;
+        for (int g = 0; g < 27; g++)
+          D11[g] = D22[g] = D33[g] = D12[g] = D23[g] = D13[g] = ve[g] = pe[g] = te[g] = 0.;
+        for (int a = 0; a < 8; a++)
+          for (int g = 0; g < 27; g++) {
+            D11[g] += e.dphi[a][0][g] * u8[a][0];
+            D22[g] += e.dphi[a][1][g] * u8[a][1];
+            D33[g] += e.dphi[a][2][g] * u8[a][2];
+            D12[g] += (e.dphi[a][0][g] * u8[a][1] + e.dphi[a][1][g] * u8[a][0]) * .5;
+            D23[g] += (e.dphi[a][1][g] * u8[a][2] + e.dphi[a][2][g] * u8[a][1]) * .5;
+            D13[g] += (e.dphi[a][0][g] * u8[a][2] + e.dphi[a][2][g] * u8[a][0]) * .5;
+            ve[g] += e.phi[a][g] * v8[a];
+            pe[g] += e.phi[a][g] * p8[a];
+            te[g] += e.phi[a][g] * th8[a];
+          }
+        double El = 0.;
+        for (int g = 0; g < 27; g++) {
+          double tr = D11[g] + D22[g] + D33[g];
+          D11[g] -= tr / 3.;
+          D22[g] -= tr / 3.;
+          D33[g] -= tr / 3.;
+          El += (D11[g] * D11[g] + D22[g] * D22[g] + D33[g] * D33[g] +
+                 (D12[g] * D12[g] + D23[g] * D23[g] + D13[g] * D13[g]) * 2.) *
+                ve[g] * ve[g] * (1. + P->eta) * m.mu * e.w[g];
+          double WD = (tr / 3. - m.alpha * te[g]) * ve[g] - coefbeta * pe[g];
+          El += 3. * threekappa / 2. * WD * WD * e.w[g];
+          El += threekappa / 6. * tr * tr * P->eta * e.w[g];
+        }
+        myE += El;
+        if (P->hasCrackPressure) {
+          double gv[3][27], ue[3][27], pe2[27];
+          for (int g = 0; g < 27; g++) {
+            pe2[g] = 0;
+            for (int c = 0; c < 3; c++) gv[c][g] = ue[c][g] = 0.;
+          }
+          for (int a = 0; a < 8; a++)
+            for (int g = 0; g < 27; g++) {
+              pe2[g] += e.phi[a][g] * p8[a];
+              for (int c = 0; c < 3; c++) {
+                gv[c][g] += e.dphi[a][c][g] * v8[a];
+                ue[c][g] += e.phi[a][g] * u8[a][c];
+              }
+            }
+          for (int g = 0; g < 27; g++)
+            myPW += e.w[g] * pe2[g] *
+                    (ue[0][g] * gv[0][g] + ue[1][g] * gv[1][g] + ue[2][g] * gv[2][g]);
+        }
+      }
+  out[0] = myE;
+  out[1] = myPW;
+  return 0;
+}
+
+/* VF_VEnergy3D (VFMech.c:2474-2526) with VF_AT1/AT2SurfaceEnergy3D_local
+ * (VFMech.c:2394-2465). */
+int vfo_v_energy(const vfo_problem *P, const double *v, double *surface) {
+  double S = 0., hx, hy, hz, v8[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
+        gather_cell(P, ei, ej, ek, v, NULL, NULL, NULL, v8, NULL, NULL);
+        double coef = m.Gc / atCv(P) * .25, ve[27], gv[3][27];
+        for (int g = 0; g < 27; g++) ve[g] = gv[0][g] = gv[1][g] = gv[2][g] = 0.;
+        for (int a = 0; a < 8; a++)
+          for (int g = 0; g < 27; g++) {
+            ve[g] += v8[a] * e.phi[a][g];
+            gv[0][g] += v8[a] * e.dphi[a][0][g];
+            gv[1][g] += v8[a] * e.dphi[a][1][g];
+            gv[2][g] += v8[a] * e.dphi[a][2][g];
+          }
+        for (int g = 0; g < 27; g++) {
+          double grad2 = gv[0][g] * gv[0][g] + gv[1][g] * gv[1][g] + gv[2][g] * gv[2][g];
+          if (P->atnum == 1)
+            S += e.w[g] * ((1. - ve[g]) / P->epsilon + grad2 * P->epsilon) * coef;
+          else
+            S += e.w[g] * ((1. - ve[g]) * (1. - ve[g]) / P->epsilon + grad2 * P->epsilon) * coef;
+        }
+      }
+  *surface = S;
+  return 0;
+}
+
+/* VolumetricCrackOpening (VFPermfield.c:15-152): COV = sum_e sum_g w (u . grad v). */
+int vfo_cov(const vfo_problem *P, const double *u, const double *v, double *cov,
+            double *cellcov) {
+  double C = 0., hx, hy, hz, u8[8][3], v8[8];
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        gather_u8(P, ei, ej, ek, u, u8);
+        gather_cell(P, ei, ej, ek, v, NULL, NULL, NULL, v8, NULL, NULL);
+        double ud[3][27], dv[3][27];
+        for (int g = 0; g < 27; g++)
+          for (int c = 0; c < 3; c++) ud[c][g] = dv[c][g] = 0.;
+        for (int g = 0; g < 27; g++)
+          for (int a = 0; a < 8; a++)
+            for (int c = 0; c < 3; c++) {
+              ud[c][g] += u8[a][c] * e.phi[a][g];
+              dv[c][g] += v8[a] * e.dphi[a][c][g];
+            }
+        double loc = 0., vol = 0., cell = 0.;
+        for (int g = 0; g < 27; g++) {
+          double t = (ud[0][g] * dv[0][g] + ud[1][g] * dv[1][g] + ud[2][g] * dv[2][g]) * e.w[g];
+          cell += t;
+          vol += e.w[g];
+          loc += t;
+        }
+        if (cellcov) cellcov[((int64_t)ek * (P->ny - 1) + ej) * (P->nx - 1) + ei] = cell / vol;
+        C += loc;
+      }
+  *cov = C;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* VFDistanceToPennyCrack (VFCracks.c:101-126) and VFPennyCrackBuildVAT1/2
+ * (VFCracks.c:136-227). */
+static double penny_distance(const double x[3], const double ctr[3], double r, double th,
+                             double ph) {
+  const double pi = 3.14159265358979323846264338327950288;
+  double n[3], tau[3], l, xdotn;
+  n[0] = cos(th * pi / 180.) * sin(ph * pi / 180.);
+  n[1] = sin(th * pi / 180.) * sin(ph * pi / 180.);
+  n[2] = cos(ph * pi / 180.);
+  xdotn = (x[0] - ctr[0]) * n[0] + (x[1] - ctr[1]) * n[1] + (x[2] - ctr[2]) * n[2];
+  tau[0] = (x[0] - ctr[0]) - xdotn * n[0];
+  tau[1] = (x[1] - ctr[1]) - xdotn * n[1];
+  tau[2] = (x[2] - ctr[2]) - xdotn * n[2];
+  l = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+  if (l <= r) return sqrt(xdotn * xdotn);
+  return sqrt(pow(xdotn, 2) + pow((l - r), 2));
+}
+
+int vfo_penny_crack_v(const vfo_problem *P, const double center[3], double r,
+                      double theta_deg, double phi_deg, double thickness, double *v) {
+  for (int k = 0; k < P->nz; k++)
+    for (int j = 0; j < P->ny; j++)
+      for (int i = 0; i < P->nx; i++) {
+        double x[3] = {coord(i, P->lx, P->nx), coord(j, P->ly, P->ny), coord(k, P->lz, P->nz)};
+        int64_t q = NODE(P, i, j, k);
+        if (r == 0) {
+          v[q] = 1.;
+          continue;
+        }
+        double dist = penny_distance(x, center, r, theta_deg, phi_deg) - thickness / 2.;
+        if (dist <= 0)
+          v[q] = 0.;
+        else if (P->atnum == 1)
+          v[q] = dist < 2. * P->epsilon ? dist / P->epsilon * (1. - .25 * dist / P->epsilon) : 1.;
+        else
+          v[q] = 1. - exp(-dist / 2 / P->epsilon);
+      }
+  return 0;
+}

@@ -1,0 +1,252 @@
+"""Pure-Python model of the CUDA U-apply kernel (vpfhf_b200/csrc/u_apply.{cuh,cu}).
+
+It replays the kernel's schedule -- xy tiles of 32 x TY elements, z-chunks with
+one halo layer, the fixed-order node sums, the register carry between layers,
+the seam partial buffers and the seam fix-up -- with bounds-checked numpy
+indexing, and the modal ("mean/difference") element arithmetic.  The tests use
+it to check the index arithmetic and buffer sizes on the CPU against the
+oracle, independently of any GPU.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+TAU = math.sqrt(0.6) / 2
+GT = (-TAU, 0.0, TAU)
+GW = (5 / 18, 8 / 18, 5 / 18)
+
+
+def modal8(f):
+    a = np.empty(8)
+    b = np.empty(8)
+    m = np.empty(8)
+    for p in range(4):
+        a[2 * p] = 0.5 * (f[2 * p] + f[2 * p + 1])
+        a[2 * p + 1] = f[2 * p + 1] - f[2 * p]
+    for k in range(2):
+        for al in range(2):
+            lo, hi = a[al + 4 * k], a[al + 2 + 4 * k]
+            b[al + 4 * k] = 0.5 * (lo + hi)
+            b[al + 2 + 4 * k] = hi - lo
+    for q in range(4):
+        lo, hi = b[q], b[q + 4]
+        m[q] = 0.5 * (lo + hi)
+        m[q + 4] = hi - lo
+    return m
+
+
+def u_element(xn, vn, lam, mu, eta, h):
+    """xn[8][3], vn[8] -> y[8][3]; same arithmetic as u_element<T> in u_apply.cuh."""
+    ihx, ihy, ihz = 1 / h[0], 1 / h[1], 1 / h[2]
+    vol = h[0] * h[1] * h[2]
+    m = [modal8(xn[:, c]) for c in range(3)]
+    mv = modal8(vn)
+    QX = np.zeros((3, 4))
+    QY = np.zeros((3, 4))
+    QZ = np.zeros((3, 4))
+    SZ = np.zeros((3, 3, 3))
+    for gz in range(3):
+        tz = GT[gz]
+        SY = np.zeros((3, 3))
+        for gy in range(3):
+            ty = GT[gy]
+            SX = np.zeros(3)
+            for gx in range(3):
+                tx = GT[gx]
+                G = np.zeros((3, 3))
+                for c in range(3):
+                    G[c, 0] = (m[c][1] + m[c][3] * ty + m[c][5] * tz + m[c][7] * ty * tz) * ihx
+                    G[c, 1] = (m[c][2] + m[c][3] * tx + m[c][6] * tz + m[c][7] * tx * tz) * ihy
+                    G[c, 2] = (m[c][4] + m[c][5] * tx + m[c][6] * ty + m[c][7] * tx * ty) * ihz
+                vg = (mv[0] + mv[1] * tx + mv[2] * ty + mv[3] * tx * ty + mv[4] * tz
+                      + mv[5] * tx * tz + mv[6] * ty * tz + mv[7] * tx * ty * tz)
+                ws = vol * GW[gx] * GW[gy] * GW[gz] * (vg * vg + eta)
+                tr = G[0, 0] + G[1, 1] + G[2, 2]
+                s = ws * (lam * tr * np.eye(3) + mu * (G + G.T))
+                SX += s[:, 0]
+                SY[:, gx] += s[:, 1]
+                SZ[:, gy, gx] += s[:, 2]
+            for c in range(3):
+                QX[c] += SX[c] * np.array([1, ty, tz, ty * tz])
+        for gx in range(3):
+            tx = GT[gx]
+            for c in range(3):
+                QY[c] += SY[c, gx] * np.array([1, tx, tz, tx * tz])
+    for gy in range(3):
+        for gx in range(3):
+            for c in range(3):
+                QZ[c] += SZ[c, gy, gx] * np.array([1, GT[gx], GT[gy], GT[gx] * GT[gy]])
+
+    def inv(Q, ih):
+        A = np.empty((2, 2))
+        for s1 in range(2):
+            for s2 in range(2):
+                a, b = 2 * s1 - 1, 2 * s2 - 1
+                A[s1, s2] = (Q[0] / 4 + a * Q[1] / 2 + b * Q[2] / 2 + a * b * Q[3]) * ih
+        return A
+
+    y = np.zeros((8, 3))
+    for c in range(3):
+        Ax, Ay, Az = inv(QX[c], ihx), inv(QY[c], ihy), inv(QZ[c], ihz)
+        for k in range(2):
+            for j in range(2):
+                for i in range(2):
+                    y[i + 2 * j + 4 * k, c] = ((Ax[j, k] if i else -Ax[j, k])
+                                               + (Ay[i, k] if j else -Ay[i, k])
+                                               + (Az[i, j] if k else -Az[i, j]))
+    return y
+
+
+def plan(nx, ny, nz, TY, zc):
+    ntx = -(-(nx - 1) // 32)
+    nty = -(-(ny - 1) // TY)
+    nzc = -(-nz // zc)
+    return dict(ntx=ntx, nty=nty, zc=zc, nzc=nzc,
+                seamX=(ntx - 1) * nz * ny * 12, seamY=(nty - 1) * nz * nx * 6)
+
+
+def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None):
+    """Replays u_apply_kernel + u_seam_fixup_kernel; returns y (3N)."""
+    nx, ny, nz = n
+    nex, ney = nx - 1, ny - 1
+    P = plan(nx, ny, nz, TY, zc)
+    ntx, nty = P["ntx"], P["nty"]
+    N = nx * ny * nz
+    y = np.full(3 * N, np.nan)
+    seamX = np.full(max(P["seamX"], 1), np.nan)
+    seamY = np.full(max(P["seamY"], 1), np.nan)
+    written = np.zeros(3 * N, int)
+    el_fn = element or (lambda xn, vn: u_element(xn, vn, lam, mu, eta, h))
+    BX, BY = 33, TY + 1
+    nslot = -(-(BX * BY) // (32 * TY))
+
+    def nid(i, j, k):
+        assert 0 <= i < nx and 0 <= j < ny and 0 <= k < nz
+        return (k * ny + j) * nx + i
+
+    for bz in range(P["nzc"]):
+        for by in range(nty):
+            for bx in range(ntx):
+                X0, Y0, z0 = 32 * bx, TY * by, bz * zc
+                if z0 >= nz:
+                    continue
+                z1 = min(z0 + zc, nz)
+                kf, kl = max(z0 - 1, 0), min(z1, nz - 1) - 1
+                carry = np.zeros((32 * TY, nslot, 3))
+
+                def emit(l, w, X, Y, z, val):
+                    left, right = (l == 0 and bx > 0), (l == 32 and bx < ntx - 1)
+                    bot, top = (w == 0 and by > 0), (w == TY and by < nty - 1)
+                    nn = nid(X, Y, z)
+                    if not (left or right or bot or top):
+                        for c in range(3):
+                            y[3 * nn + c] = x[3 * nn + c] if (bcbits[nn] >> c) & 1 else val[c]
+                            written[3 * nn + c] += 1
+                    elif left or right:
+                        i = bx if left else bx + 1
+                        slot = (2 if bot else 0) + (1 if left else 0)
+                        base = ((((i - 1) * nz + z) * ny + Y) * 4 + slot) * 3
+                        assert 0 <= base and base + 3 <= P["seamX"]
+                        assert np.isnan(seamX[base:base + 3]).all()
+                        seamX[base:base + 3] = val
+                    else:
+                        j = by if bot else by + 1
+                        base = ((((j - 1) * nz + z) * nx + X) * 2 + (1 if bot else 0)) * 3
+                        assert 0 <= base and base + 3 <= P["seamY"]
+                        assert np.isnan(seamY[base:base + 3]).all()
+                        seamY[base:base + 3] = val
+
+                def plane(kz):
+                    sx = np.zeros((4, BY, BX))
+                    for w in range(BY):
+                        for l in range(BX):
+                            X, Y = X0 + l, Y0 + w
+                            if X < nx and Y < ny:
+                                nn = nid(X, Y, kz)
+                                sx[0:3, w, l] = x[3 * nn:3 * nn + 3]
+                                sx[3, w, l] = v[nn]
+                    return sx
+
+                buf = {kf: plane(kf)}
+                for k in range(kf, kl + 1):
+                    buf[k + 1] = plane(k + 1)
+                    sc = np.zeros((24, TY, 32))
+                    for wy in range(TY):
+                        for lane in range(32):
+                            ex, ey = X0 + lane, Y0 + wy
+                            if ex < nex and ey < ney:
+                                xn = np.zeros((8, 3))
+                                vn = np.zeros(8)
+                                for kk in range(2):
+                                    for j in range(2):
+                                        for i in range(2):
+                                            a = i + 2 * j + 4 * kk
+                                            xn[a] = buf[k + kk][0:3, wy + j, lane + i]
+                                            vn[a] = buf[k + kk][3, wy + j, lane + i]
+                                yc = el_fn(xn, vn)
+                                sc[:, wy, lane] = yc.reshape(24)
+                    for tid in range(32 * TY):
+                        for si in range(nslot):
+                            s = tid + si * 32 * TY
+                            if s >= BX * BY:
+                                continue
+                            l, w = s % BX, s // BX
+                            X, Y = X0 + l, Y0 + w
+                            if X >= nx or Y >= ny:
+                                continue
+                            p0 = np.zeros(3)
+                            p1 = np.zeros(3)
+                            for dw in range(2):
+                                ew, j = w - 1 + dw, 1 - dw
+                                if ew < 0 or ew >= TY:
+                                    continue
+                                for dl in range(2):
+                                    el, i = l - 1 + dl, 1 - dl
+                                    if el < 0 or el >= 32:
+                                        continue
+                                    p0 += sc[(i + 2 * j) * 3:(i + 2 * j) * 3 + 3, ew, el]
+                                    p1 += sc[(i + 2 * j + 4) * 3:(i + 2 * j + 4) * 3 + 3, ew, el]
+                            if k >= z0:
+                                emit(l, w, X, Y, k, carry[tid, si] + p0)
+                            carry[tid, si] = p1
+                if z1 == nz:
+                    for tid in range(32 * TY):
+                        for si in range(nslot):
+                            s = tid + si * 32 * TY
+                            if s >= BX * BY:
+                                continue
+                            l, w = s % BX, s // BX
+                            X, Y = X0 + l, Y0 + w
+                            if X < nx and Y < ny:
+                                emit(l, w, X, Y, nz - 1, carry[tid, si])
+    # seam fix-up
+    nxs = (ntx - 1) * nz * ny
+    nys = (nty - 1) * nz * nx
+    for t in range(nxs + nys):
+        if t < nxs:
+            Y = t % ny
+            r = t // ny
+            z, i = r % nz, r // nz + 1
+            onY = (Y % TY == 0) and Y > 0 and (Y // TY < nty)
+            p = seamX[t * 12:t * 12 + 12]
+            val = ((p[0:3] + p[3:6]) + p[6:9]) + p[9:12] if onY else p[0:3] + p[3:6]
+            X = 32 * i
+        else:
+            u = t - nxs
+            X = u % nx
+            r = u // nx
+            z, j = r % nz, r // nz + 1
+            if X % 32 == 0 and X > 0 and X // 32 < ntx:
+                continue
+            p = seamY[u * 6:u * 6 + 6]
+            val = p[0:3] + p[3:6]
+            Y = TY * j
+        assert not np.isnan(val).any(), "seam slot never written"
+        nn = nid(X, Y, z)
+        for c in range(3):
+            y[3 * nn + c] = x[3 * nn + c] if (bcbits[nn] >> c) & 1 else val[c]
+            written[3 * nn + c] += 1
+    assert (written == 1).all(), "every dof must be written exactly once"
+    return y

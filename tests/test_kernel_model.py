@@ -1,0 +1,31 @@
+"""CPU check of the U-apply kernel's schedule (tiling, seams, carries) and modal
+element arithmetic, replayed in Python against the oracle."""
+import numpy as np
+import pytest
+
+import kernel_model as km
+
+
+def test_modal_element_matches_element_matrix(oracle_mod):
+    rng = np.random.default_rng(3)
+    o = oracle_mod.Oracle((2, 2, 2), (0.3, 0.5, 0.7), E=2.0, nu=0.3, eta=1e-3)
+    lam, mu = 2.0 * 0.3 / 1.3 / 0.4, 2.0 / 1.3 * 0.5
+    for _ in range(4):
+        v, x = rng.uniform(0, 1, 8), rng.standard_normal(24)
+        yref = o.u_element_matrix(0, 0, 0, v) @ x
+        y = km.u_element(x.reshape(8, 3), v, lam, mu, 1e-3, (0.3, 0.5, 0.7)).reshape(24)
+        assert np.abs(y - yref).max() <= 1e-14 * np.abs(yref).max()
+
+
+@pytest.mark.parametrize("n,TY,zc", [((37, 21, 13), 8, 5), ((34, 10, 7), 4, 3), ((3, 2, 4), 8, 2)])
+def test_tiled_schedule_matches_oracle(oracle_mod, n, TY, zc):
+    rng = np.random.default_rng(sum(n))
+    o = oracle_mod.Oracle(n, (1.1, 0.9, 0.7), E=3.0, nu=0.2, eta=1e-2)
+    lam, mu = 3.0 * 0.2 / 1.2 / 0.6, 3.0 / 1.2 * 0.5
+    v, x = rng.uniform(0, 1, o.N), rng.standard_normal(3 * o.N)
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    bits = (mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)
+    yref = o.u_apply(v, x, mask)
+    h = tuple(L / (k - 1) for L, k in zip((1.1, 0.9, 0.7), n))
+    y = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, zc=zc)
+    assert np.abs(y - yref).max() <= 1e-13 * np.abs(yref).max()

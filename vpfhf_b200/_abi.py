@@ -1,0 +1,103 @@
+"""ctypes binding of libvfgpu.so (include/vfgpu.h).
+
+The library is required: on a machine with a CUDA GPU, loading fails loudly if
+libvfgpu.so is missing or does not load; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(HERE, "libvfgpu.so")
+
+OK, NOT_CONVERGED, DIVERGED = 0, 1, 2
+ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_STATE = -1, -2, -3, -4
+FP64, MIXED = 0, 1
+BC_NONE, BC_ZERO, BC_ONE, BC_FIXED = 0, 1, 2, 3
+FIELD_U, FIELD_V, FIELD_VIRREV, FIELD_BCU, FIELD_THETA, FIELD_THETAREF, FIELD_PRESSURE = range(7)
+FIELD_NAMES = {"U": FIELD_U, "V": FIELD_V, "VIrrev": FIELD_VIRREV, "BCU": FIELD_BCU,
+               "theta": FIELD_THETA, "thetaRef": FIELD_THETAREF, "pressure": FIELD_PRESSURE}
+
+
+class Grid(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("lx", C.c_double), ("ly", C.c_double), ("lz", C.c_double)]
+
+
+class MatProp(C.Structure):
+    _fields_ = [("E", C.c_double), ("nu", C.c_double), ("alpha", C.c_double),
+                ("beta", C.c_double), ("Gc", C.c_double)]
+
+
+class VFProp(C.Structure):
+    _fields_ = [("epsilon", C.c_double), ("eta", C.c_double), ("irrevtol", C.c_double),
+                ("atnum", C.c_int), ("hasCrackPressure", C.c_int)]
+
+
+class BC(C.Structure):
+    _fields_ = [("face", C.c_int * 6), ("faceValue", C.c_double * 6),
+                ("vertex", C.c_int * 8), ("vertexValue", C.c_double * 8)]
+
+
+class VFGPUError(RuntimeError):
+    def __init__(self, code, fn, msg):
+        super().__init__(f"{fn} failed with status {code}: {msg}")
+        self.code = code
+
+
+_LIB = None
+
+# name -> argtypes (all return int)
+_SIGS = {
+    "vfgpu_create": [C.POINTER(Grid), C.POINTER(C.c_void_p)],
+    "vfgpu_destroy": [C.c_void_p],
+    "vfgpu_set_matprop": [C.c_void_p, C.c_int, C.POINTER(MatProp), C.c_void_p],
+    "vfgpu_set_cell_modulus": [C.c_void_p, C.c_void_p],
+    "vfgpu_set_vfprop": [C.c_void_p, C.POINTER(VFProp)],
+    "vfgpu_set_bc": [C.c_void_p, C.POINTER(BC), C.POINTER(BC)],
+    "vfgpu_set_field": [C.c_void_p, C.c_int, C.c_void_p],
+    "vfgpu_get_field": [C.c_void_p, C.c_int, C.c_void_p],
+    "vfgpu_u_apply": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
+}
+
+
+def lib():
+    """Loads libvfgpu.so (building it first if the sources are present and it is missing)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIBPATH):
+        from . import build as _build
+        _build.build()
+    L = C.CDLL(LIBPATH)
+    L.vfgpu_last_error.restype = C.c_char_p
+    L.vfgpu_last_error.argtypes = []
+    for name, args in _SIGS.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    _LIB = L
+    return L
+
+
+def exported_symbols():
+    return ["vfgpu_last_error"] + list(_SIGS)
+
+
+def check(code, fn):
+    if code < 0:
+        raise VFGPUError(code, fn, lib().vfgpu_last_error().decode())
+    return code
+
+
+def ptr(a):
+    """Raw address of a numpy array (host) or a torch tensor (host or device)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a.data_ptr()  # torch.Tensor

@@ -1,0 +1,15 @@
+// abi_util.h -- helpers shared by the C-ABI translation units.
+#pragma once
+
+#include "ctx.h"
+
+namespace vfgpu {
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+bool is_device_ptr(const void* p);
+cudaError_t copy_in(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
+cudaError_t copy_out(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
+int ensure_v32(vfgpu_ctx* c);
+template <typename T>
+UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const UPlan& p);
+}  // namespace vfgpu

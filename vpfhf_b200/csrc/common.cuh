@@ -1,0 +1,35 @@
+// common.cuh -- shared helpers for the vfgpu kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vfgpu {
+
+// 1-D 3-point Gauss rule on the reference interval t in [-1/2, 1/2]
+// (VFCartFE.c:100-107: nodes (1 -+ sqrt(3/5))/2 on [0,1], weights 5/18, 8/18, 5/18).
+#define VF_TAU 0.38729833462074168852   /* sqrt(3/5)/2 */
+#define VF_W0 0.27777777777777777778    /* 5/18 */
+#define VF_W1 0.44444444444444444444    /* 8/18 */
+
+// Element-layer material table (per-layer VFMatProp, VFCommon.h:69-80).
+#define VF_MAXLAYER 16
+struct LayerTable {
+  double lambda[VF_MAXLAYER];   // Lame lambda (VFCommon.c:584)
+  double mu[VF_MAXLAYER];       // Lame mu     (VFCommon.c:585)
+  double lamfac[VF_MAXLAYER];   // lambda / E  (for per-cell E)
+  double mufac[VF_MAXLAYER];    // mu / E
+  double alpha[VF_MAXLAYER];    // thermal expansion
+  double beta[VF_MAXLAYER];     // Biot coefficient
+  double Gc[VF_MAXLAYER];
+};
+
+template <typename T> struct Vec3 { T x, y, z; };
+
+__host__ __device__ inline int64_t node_index(int i, int j, int k, int nx, int ny) {
+  return ((int64_t)k * ny + j) * nx + i;
+}
+
+inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+}  // namespace vfgpu

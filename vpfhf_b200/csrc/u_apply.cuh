@@ -1,0 +1,242 @@
+// u_apply.cuh -- matrix-free apply of the phase-field-degraded Q1-hex elasticity
+// operator K(v) (VF_BilinearFormU3D_local, VFMech.c:227-290, applied as in
+// VF_UResidual, VFMech.c:1555-1596) on sm_100a.
+//
+// Element math ("modal" sum factorisation).  On the uniform DMDA grid every
+// element is the same box, so in local coordinates t in [-1/2,1/2]^3 a
+// trilinear field is f(t) = sum_{abc} m_abc P_a(tx) P_b(ty) P_c(tz) with
+// P_0 = 1, P_1 = t; the 8 modal coefficients come from 3 butterfly passes
+// ((lo+hi)/2, hi-lo) over the nodal values.  Then
+//   d/dx f = (1/hx) (m_100 + m_110 ty + m_101 tz + m_111 ty tz)
+// does not depend on tx, and similarly for y and z, so the 3x3 gradient at the
+// 27 Gauss points of the reference's rule (t = -tau, 0, tau, tau = sqrt(3/5)/2,
+// weights 5/18, 8/18, 5/18) costs a few FMAs per point.  The stress
+//   sigma = w (v^2 + eta) (lambda tr(G) I + mu (G + G^T))
+// is accumulated into 4 bilinear moments per (component, direction), and the
+// transpose y_(a,c) = sum_g sum_d dphi_a,d(g) sigma_cd(g) is rebuilt from those
+// moments with the inverse butterfly.  About 1.4k operations per element,
+// against 8,856 for the per-Gauss-point form and ~233k for the element-matrix
+// form the reference uses.
+//
+// Tiling.  A CTA owns a tile of 32 (x, one warp) x TY (y, TY warps) elements
+// and marches up a chunk of node planes in z.  Each layer: the next node plane
+// of the tile's node box (33 x (TY+1) nodes: u and v) is staged in shared
+// memory, every thread computes its element, the 8x3 corner contributions go to
+// shared memory, and node-owner threads sum the (up to 4) xy-contributions in a
+// fixed order -- deterministic, no atomics.  The z-direction sum is carried in
+// registers from one layer to the next.  A z-chunk recomputes the one element
+// layer below it (halo).  Nodes on the seam lines between xy-tiles receive
+// partial sums from 2 or 4 tiles; those partials go to a seam buffer and a
+// second kernel (seam_fixup) adds them in a fixed order.
+//
+// Dirichlet rows (MatZeroRowsStencil, VFCartFE.c:1293, quirk: rows only): on a
+// BC dof the output is y = x; BC columns are kept.
+#pragma once
+
+#include "common.cuh"
+
+namespace vfgpu {
+
+template <typename T> struct UApplyArgs {
+  const T* __restrict__ x;            // 3N interlaced input
+  const T* __restrict__ v;            // N phase field
+  T* __restrict__ y;                  // 3N output
+  const uint8_t* __restrict__ bc;     // N: bit c => dof (node,c) is Dirichlet
+  const uint8_t* __restrict__ elayer; // nz-1: material layer of element layer ek (or null)
+  const float* __restrict__ cellE;    // per-cell Young's modulus (or null)
+  T* __restrict__ seamX;              // x-seam partials [(ntx-1)][nz][ny][4][3]
+  T* __restrict__ seamY;              // y-seam partials [(nty-1)][nz][nx][2][3]
+  int nx, ny, nz;
+  int ntx, nty, zc;                   // tiles in x, y; owned node planes per z-chunk
+  T ihx, ihy, ihz, vol, eta;
+};
+
+// Modal transform of nodal values f[a], a = i + 2j + 4k, into m[p], p = a + 2b + 4c
+// with 0 = mean, 1 = difference along each axis.
+template <typename T>
+__device__ __forceinline__ void modal8(const T (&f)[8], T (&m)[8]) {
+  T a[8], b[8];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    a[2 * p] = T(0.5) * (f[2 * p] + f[2 * p + 1]);
+    a[2 * p + 1] = f[2 * p + 1] - f[2 * p];
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int al = 0; al < 2; al++) {
+      T lo = a[al + 4 * k], hi = a[al + 2 + 4 * k];
+      b[al + 4 * k] = T(0.5) * (lo + hi);
+      b[al + 2 + 4 * k] = hi - lo;
+    }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    T lo = b[q], hi = b[q + 4];
+    m[q] = T(0.5) * (lo + hi);
+    m[q + 4] = hi - lo;
+  }
+}
+
+// a + b*t_g for Gauss index g (t_1 = 0 is folded at compile time).
+template <typename T> __device__ __forceinline__ T lin(int g, T a, T b) {
+  return g == 1 ? a : (g == 0 ? fma(b, T(-VF_TAU), a) : fma(b, T(VF_TAU), a));
+}
+template <typename T> __device__ __forceinline__ T gw(int g) { return g == 1 ? T(VF_W1) : T(VF_W0); }
+template <typename T> __device__ __forceinline__ T gt(int g) {
+  return g == 1 ? T(0) : (g == 0 ? T(-VF_TAU) : T(VF_TAU));
+}
+
+// Moment update q[0..3] += s * {1, t1, t2, t1 t2} for Gauss indices (g1, g2).
+template <typename T>
+__device__ __forceinline__ void moment4(T (&q)[4], int g1, int g2, T s) {
+  q[0] += s;
+  if (g1 != 1) q[1] = fma(gt<T>(g1), s, q[1]);
+  if (g2 != 1) q[2] = fma(gt<T>(g2), s, q[2]);
+  if (g1 != 1 && g2 != 1) q[3] = fma(gt<T>(g1) * gt<T>(g2), s, q[3]);
+}
+
+// A[s1][s2] = (Q0/4 + s1 Q1/2 + s2 Q2/2 + s1 s2 Q3) / h, s = -1 (index 0) or +1 (index 1).
+template <typename T>
+__device__ __forceinline__ void inv_butterfly(const T (&Q)[4], T ih, T (&A)[2][2]) {
+  const T q0 = Q[0] * (T(0.25) * ih), q1 = Q[1] * (T(0.5) * ih);
+  const T q2 = Q[2] * (T(0.5) * ih), q3 = Q[3] * ih;
+  const T r0m = q0 - q2, r0p = q0 + q2, r1m = q1 - q3, r1p = q1 + q3;
+  A[0][0] = r0m - r1m;
+  A[1][0] = r0m + r1m;
+  A[0][1] = r0p - r1p;
+  A[1][1] = r0p + r1p;
+}
+
+// y[a][c] = (K_e(v) x_e)[a][c] for one element.
+template <typename T>
+__device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
+                                          T eta, T ihx, T ihy, T ihz, T vol, T (&y)[8][3]) {
+  T m[3][8], mv[8];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    T f[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) f[a] = xn[a][c];
+    modal8(f, m[c]);
+  }
+  modal8(vn, mv);
+  // Gradient coefficient sets: d/dx u_c = Ax + Bx ty + Cx tz + Dx ty tz, etc.
+  T Ax[3], Bx[3], Cx[3], Dx[3], Ay[3], By[3], Cy[3], Dy[3], Az[3], Bz[3], Cz[3], Dz[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    Ax[c] = m[c][1] * ihx; Bx[c] = m[c][3] * ihx; Cx[c] = m[c][5] * ihx; Dx[c] = m[c][7] * ihx;
+    Ay[c] = m[c][2] * ihy; By[c] = m[c][3] * ihy; Cy[c] = m[c][6] * ihy; Dy[c] = m[c][7] * ihy;
+    Az[c] = m[c][4] * ihz; Bz[c] = m[c][5] * ihz; Cz[c] = m[c][6] * ihz; Dz[c] = m[c][7] * ihz;
+  }
+  T QX[3][4], QY[3][4], QZ[3][4], SZ[3][3][3];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) QX[c][q] = QY[c][q] = QZ[c][q] = T(0);
+  const T mu2 = T(2) * mu;
+
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++) {
+    const T volw = vol * gw<T>(gz);
+    T ax[3], bx[3], ay[3], by[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      ax[c] = lin(gz, Ax[c], Cx[c]);
+      bx[c] = lin(gz, Bx[c], Dx[c]);
+      ay[c] = lin(gz, Ay[c], Cy[c]);
+      by[c] = lin(gz, By[c], Dy[c]);
+    }
+    const T p0 = lin(gz, mv[0], mv[4]), p1 = lin(gz, mv[1], mv[5]);
+    const T p2 = lin(gz, mv[2], mv[6]), p3 = lin(gz, mv[3], mv[7]);
+    T SY[3][3];
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++) {
+      T Gx[3], al[3], be[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        Gx[c] = lin(gy, ax[c], bx[c]);
+        al[c] = lin(gy, Az[c], Cz[c]);
+        be[c] = lin(gy, Bz[c], Dz[c]);
+      }
+      const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
+      T SX[3];
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        T Gy[3], Gz[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          Gy[c] = lin(gx, ay[c], by[c]);
+          Gz[c] = lin(gx, al[c], be[c]);
+        }
+        const T vg = lin(gx, q0, q1);
+        const T ws = (volw * (gw<T>(gx) * gw<T>(gy))) * fma(vg, vg, eta);
+        const T tr = Gx[0] + Gy[1] + Gz[2];
+        const T L = (ws * lam) * tr, m2 = ws * mu2, m1 = ws * mu;
+        const T s00 = fma(m2, Gx[0], L), s11 = fma(m2, Gy[1], L), s22 = fma(m2, Gz[2], L);
+        const T s01 = m1 * (Gy[0] + Gx[1]);
+        const T s02 = m1 * (Gz[0] + Gx[2]);
+        const T s12 = m1 * (Gz[1] + Gy[2]);
+        if (gx == 0) {
+          SX[0] = s00; SX[1] = s01; SX[2] = s02;
+        } else {
+          SX[0] += s00; SX[1] += s01; SX[2] += s02;
+        }
+        if (gy == 0) {
+          SY[0][gx] = s01; SY[1][gx] = s11; SY[2][gx] = s12;
+        } else {
+          SY[0][gx] += s01; SY[1][gx] += s11; SY[2][gx] += s12;
+        }
+        if (gz == 0) {
+          SZ[0][gy][gx] = s02; SZ[1][gy][gx] = s12; SZ[2][gy][gx] = s22;
+        } else {
+          SZ[0][gy][gx] += s02; SZ[1][gy][gx] += s12; SZ[2][gy][gx] += s22;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) moment4(QX[c], gy, gz, SX[c]);
+    }
+#pragma unroll
+    for (int gx = 0; gx < 3; gx++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) moment4(QY[c], gx, gz, SY[c][gx]);
+  }
+#pragma unroll
+  for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+    for (int gx = 0; gx < 3; gx++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) moment4(QZ[c], gx, gy, SZ[c][gy][gx]);
+
+  // Inverse butterfly: direction-d part of node (i,j,k) is
+  //   s_d/h_d * (Q0/4 + s_1 Q1/2 + s_2 Q2/2 + s_1 s_2 Q3), s = -1 (node 0) or +1 (node 1).
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    T A[3][2][2];
+    inv_butterfly(QX[c], ihx, A[0]);
+    inv_butterfly(QY[c], ihy, A[1]);
+    inv_butterfly(QZ[c], ihz, A[2]);
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int i = 0; i < 2; i++) {
+          const T ax_ = i ? A[0][j][k] : -A[0][j][k];
+          const T ay_ = j ? A[1][i][k] : -A[1][i][k];
+          const T az_ = k ? A[2][i][j] : -A[2][i][j];
+          y[i + 2 * j + 4 * k][c] = (ax_ + ay_) + az_;
+        }
+  }
+}
+
+// Launch geometry shared by the host launcher and the kernels.
+template <int TY> struct UTile {
+  static constexpr int BX = 33, BY = TY + 1, NT = 32 * TY;
+  static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
+};
+
+template <typename T, int TY> constexpr size_t u_apply_smem_bytes() {
+  return sizeof(T) * (2 * 4 * UTile<TY>::BX * UTile<TY>::BY + 24 * 32 * TY);
+}
+
+}  // namespace vfgpu
