@@ -81,6 +81,29 @@ typedef struct {
   double vertexValue[8];
 } vfgpu_bc;
 
+/* Solver options.  Defaults (vfgpu_default_solve_opts) are the reference's:
+ * SNES atol = rtol = stol = 1e-8 (VFCommon.c:1024, 1071), KSPCG rtol 1e-8,
+ * atol 1e-10 (VFCommon.c:1039, 1081) with a Jacobi preconditioner. */
+typedef struct {
+  int precision;          /* VFGPU_FP64 or VFGPU_MIXED                                  */
+  double ksp_rtol, ksp_atol, ksp_dtol;
+  int ksp_maxit;          /* per linear solve (per inner solve for VFGPU_MIXED)         */
+  double snes_rtol, snes_atol, snes_stol;
+  int snes_maxit;
+  double inner_rtol;      /* VFGPU_MIXED: relative tolerance of each FP32 inner solve   */
+  int max_refine;         /* VFGPU_MIXED: cap on FP64 refinement steps per Newton step  */
+  double time_limit;      /* wall-clock watchdog in seconds (0 = none)                  */
+} vfgpu_solve_opts;
+
+typedef struct {
+  int newton_its;         /* SNES iterations                                            */
+  int ksp_its;            /* total CG iterations (all inner solves)                     */
+  int refine_its;         /* VFGPU_MIXED: FP64 refinement steps                         */
+  int reason;             /* SNESConvergedReason numbering; -100 = watchdog             */
+  double fnorm0, fnorm;   /* residual norm before / after (inactive-set norm for V)     */
+  double seconds;
+} vfgpu_solve_stats;
+
 /* Message of the last failed call on this thread ("" if none). */
 const char* vfgpu_last_error(void);
 
@@ -109,6 +132,52 @@ int vfgpu_get_field(vfgpu_ctx* ctx, int field, double* data);
  * with the resident V.  x, y: 3N.  precision: VFGPU_FP64 or VFGPU_MIXED (FP32
  * kernel; x is rounded to FP32, y returned in FP64). */
 int vfgpu_u_apply(vfgpu_ctx* ctx, int precision, const double* x, double* y);
+
+/* Stream-ordered variant for device-resident data: x, y are device arrays of
+ * the precision's type (double for VFGPU_FP64, float for VFGPU_MIXED); the
+ * work is queued on the ctx's stream and the call returns without waiting. */
+int vfgpu_u_apply_dev(vfgpu_ctx* ctx, int precision, const void* x, void* y);
+
+/* The cudaStream_t every call of this ctx runs on (for event timing / ordering). */
+int vfgpu_get_stream(vfgpu_ctx* ctx, void** stream);
+
+void vfgpu_default_solve_opts(vfgpu_solve_opts* opts);
+
+/* VF_StepU (VFMech.c:1436-1452): SNESSolve(snesU) on the resident U with the
+ * resident V, theta, thetaRef, pressure; Newton + L2 line search, PCG(Jacobi),
+ * the residual of VF_UResidual (VFMech.c:1456-1887, no in-situ tractions).
+ * Returns VFGPU_OK when converged, VFGPU_NOT_CONVERGED (iteration cap or
+ * watchdog) or VFGPU_DIVERGED; the reference's VF_StepU returns 0 in all three
+ * cases and only prints (VFMech.c:1445-1450).  opts may be NULL (defaults). */
+int vfgpu_step_u(vfgpu_ctx* ctx, const vfgpu_solve_opts* opts, vfgpu_solve_stats* stats);
+
+/* VF_StepV (VFMech.c:3057-3082): SNESSolve(snesV) with SNESVINEWTONRSLS on the
+ * resident V: bounds [0,1] (AT2) or [0,VIrrev] (AT1, VFCommon.c:1149-1154),
+ * residual of VF_VResidual (VFMech.c:2687-2879, thermo-poro term discarded as in
+ * the reference), AT2 irreversibility where VIrrev <= irrevtol. */
+int vfgpu_step_v(vfgpu_ctx* ctx, const vfgpu_solve_opts* opts, vfgpu_solve_stats* stats);
+
+/* VFTimeStepPrepare (VFCommon.c:1132-1157): VIrrev := V; Dirichlet values into U
+ * (from BCU for FIXED) and V. */
+int vfgpu_time_step_prepare(vfgpu_ctx* ctx);
+
+/* One alternate-minimisation iteration (VFCommon.c:1183-1202 loop body):
+ * StepU, StepV, errV = ||V - Vold||_inf. */
+int vfgpu_am_step(vfgpu_ctx* ctx, const vfgpu_solve_opts* opts, double* errV,
+                  vfgpu_solve_stats* statsU, vfgpu_solve_stats* statsV);
+
+/* VF_UEnergy3D (VFMech.c:1111-1427): elastic energy and pressure work (the in-situ
+ * work is 0: in-situ tractions are not on this path). */
+int vfgpu_u_energy(vfgpu_ctx* ctx, double* elastic, double* insitu, double* pressurework);
+/* VF_VEnergy3D (VFMech.c:2474-2526): AT1/AT2 surface energy. */
+int vfgpu_v_energy(vfgpu_ctx* ctx, double* surface);
+/* VolumetricCrackOpening (VFPermfield.c:75-152): total and, if cellcov is not
+ * NULL, the per-cell average ((nx-1)(ny-1)(nz-1)). */
+int vfgpu_crack_opening(vfgpu_ctx* ctx, double* cov, double* cellcov);
+
+/* The SNES residuals at the resident fields: VF_UResidual (3N) and VF_VResidual (N). */
+int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);
+int vfgpu_v_residual(vfgpu_ctx* ctx, double* F);
 
 #ifdef __cplusplus
 }

@@ -250,3 +250,64 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None):
             written[3 * nn + c] += 1
     assert (written == 1).all(), "every dof must be written exactly once"
     return y
+
+
+def v_element(xn, cg, aeps, h):
+    """xn[8], cg[27] (weight-premultiplied mass coefficient) -> y[8]; the arithmetic of
+    v_element<T> in ops.cuh."""
+    ihx, ihy, ihz = 1 / h[0], 1 / h[1], 1 / h[2]
+    vol = h[0] * h[1] * h[2]
+    m = modal8(xn)
+    QX, QY, QZ = np.zeros(4), np.zeros(4), np.zeros(4)
+    M = np.zeros(8)
+    SZ = np.zeros((3, 3))
+    for gz in range(3):
+        tz = GT[gz]
+        SY = np.zeros(3)
+        for gy in range(3):
+            ty = GT[gy]
+            SX = 0.0
+            for gx in range(3):
+                tx = GT[gx]
+                g = gx + 3 * gy + 9 * gz
+                Gx = (m[1] + m[3] * ty + m[5] * tz + m[7] * ty * tz) * ihx
+                Gy = (m[2] + m[3] * tx + m[6] * tz + m[7] * tx * tz) * ihy
+                Gz = (m[4] + m[5] * tx + m[6] * ty + m[7] * tx * ty) * ihz
+                xg = (m[0] + m[1] * tx + m[2] * ty + m[3] * tx * ty + m[4] * tz + m[5] * tx * tz
+                      + m[6] * ty * tz + m[7] * tx * ty * tz)
+                wa = aeps * vol * GW[gx] * GW[gy] * GW[gz]
+                SX += wa * Gx
+                SY[gx] += wa * Gy
+                SZ[gy, gx] += wa * Gz
+                psi = cg[g] * xg
+                M += psi * np.array([1, tx, ty, tx * ty, tz, tx * tz, ty * tz, tx * ty * tz])
+            QX += SX * np.array([1, ty, tz, ty * tz])
+        for gx in range(3):
+            QY += SY[gx] * np.array([1, GT[gx], tz, GT[gx] * tz])
+    for gy in range(3):
+        for gx in range(3):
+            QZ += SZ[gy, gx] * np.array([1, GT[gx], GT[gy], GT[gx] * GT[gy]])
+
+    def inv(Q, ih):
+        A = np.empty((2, 2))
+        for s1 in range(2):
+            for s2 in range(2):
+                a, b = 2 * s1 - 1, 2 * s2 - 1
+                A[s1, s2] = (Q[0] / 4 + a * Q[1] / 2 + b * Q[2] / 2 + a * b * Q[3]) * ih
+        return A
+
+    AX, AY, AZ = inv(QX, ihx), inv(QY, ihy), inv(QZ, ihz)
+    y = np.zeros(8)
+    for k in range(2):
+        for j in range(2):
+            for i in range(2):
+                sgn = np.array([2 * i - 1, 2 * j - 1, 2 * k - 1])
+                val = 0.0
+                for p in range(8):  # value part: prod_d (1/2 + s_d t_d) moments
+                    al, be, ga = p & 1, (p >> 1) & 1, p >> 2
+                    f = 1.0
+                    for d, mode in enumerate((al, be, ga)):
+                        f *= sgn[d] if mode else 0.5
+                    val += f * M[p]
+                y[i + 2 * j + 4 * k] = ((AX[j, k] * sgn[0] + AY[i, k] * sgn[1]) + AZ[i, j] * sgn[2]) + val
+    return y

@@ -1,0 +1,171 @@
+"""GPU parity of the residuals, the U/V solves, energies and the AM loop."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _penny(oracle_mod, n, atnum=1, alpha=0.0, beta=0.0, seed=0):
+    import vpfhf_b200 as vg
+    L = 4.0
+    h = L / (n - 1)
+    kw = dict(E=1e10, nu=0.25, Gc=100.0, epsilon=2 * h, eta=1e-8, atnum=atnum)
+    o = oracle_mod.Oracle((n, n, n), (L, L, L), alpha=alpha, beta=beta, pressurize=True, **kw)
+    ctx = vg.VFContext((n, n, n), (L, L, L),
+                       dict(E=kw["E"], nu=kw["nu"], Gc=kw["Gc"], alpha=alpha, beta=beta),
+                       epsilon=kw["epsilon"], eta=kw["eta"], atnum=atnum, pressurize=True)
+    ctx.set_bc(vg.rollers())
+    v = o.penny_v((2.0, 2.0, 2.0), 0.8)
+    ctx.set_field("V", v)
+    ctx.set_field("VIrrev", v)
+    p = np.full(o.N, 1e6)
+    ctx.set_field("pressure", p)
+    mask, val = o.bc(oracle_mod.rollers_face())
+    return o, ctx, v, p, mask, val
+
+
+def test_u_residual(cuda, oracle_mod):
+    rng = np.random.default_rng(1)
+    o, ctx, v, p, mask, val = _penny(oracle_mod, 17, alpha=1e-5, beta=0.7)
+    u = rng.standard_normal(3 * o.N) * 1e-4
+    u[mask == 1] = 0.0
+    theta = rng.uniform(0, 10, o.N)
+    ctx.set_field("U", u)
+    ctx.set_field("theta", theta)
+    p = p * (1 + 0.1 * rng.standard_normal(o.N))
+    ctx.set_field("pressure", p)
+    F = ctx.u_residual()
+    Fr = o.u_residual_ref(u, v, theta, None, p, mask, val)
+    assert np.abs(F - Fr).max() <= 1e-12 * np.abs(Fr).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("atnum", [1, 2])
+def test_v_residual(cuda, oracle_mod, atnum):
+    import vpfhf_b200 as vg
+    rng = np.random.default_rng(2)
+    o, ctx, v, p, mask, val = _penny(oracle_mod, 17, atnum=atnum, alpha=1e-5, beta=0.7)
+    u = rng.standard_normal(3 * o.N) * 1e-4
+    theta = rng.uniform(0, 10, o.N)
+    virrev = np.clip(v + 0.02 * rng.standard_normal(o.N), 0, 1)
+    ctx.set_field("U", u)
+    ctx.set_field("theta", theta)
+    ctx.set_field("VIrrev", virrev)
+    bcv = vg.BCSpec(X0=vg.BC_ONE, Z1=vg.BC_ZERO)
+    ctx.set_bc(vg.rollers(), bcv)
+    face = np.zeros((1, 6), np.int32)
+    face[0, 0], face[0, 5] = oracle_mod.ONE, oracle_mod.ZERO
+    vmask, vval = o.bc(face, dof=1)
+    F = ctx.v_residual()
+    Fr = o.v_residual_ref(u, v, theta, None, p, virrev, vmask, vval)
+    assert np.abs(F - Fr).max() <= 1e-11 * np.abs(Fr).max()
+    ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_step_u_and_v(cuda, oracle_mod, precision):
+    o, ctx, v, p, mask, val = _penny(oracle_mod, 17)
+    u = np.zeros(3 * o.N)
+    rc, st = ctx.step_u(dict(precision=precision))
+    assert rc == 0 and st["reason"] > 0, st
+    so = o.step_u(u, v, p=p, mask=mask, value=val)
+    ug = ctx.get_field("U")
+    assert np.linalg.norm(ug - u) <= 1e-6 * np.linalg.norm(u)
+    el, _, pw = ctx.u_energy()
+    el_o, pw_o = o.u_energy(u, v, p=p)
+    assert el == pytest.approx(el_o, rel=1e-7) and pw == pytest.approx(pw_o, rel=1e-7)
+    # V solve from the same U (AT1: bounds [0, VIrrev])
+    rc, sv = ctx.step_v(dict(precision=precision))
+    assert rc == 0 and sv["reason"] > 0, sv
+    vo_ = v.copy()
+    o.step_v(vo_, u, np.zeros(o.N), v.copy(), p=p)
+    vg_ = ctx.get_field("V")
+    assert np.abs(vg_ - vo_).max() <= 1e-6
+    assert ctx.v_energy() == pytest.approx(o.v_energy(vo_), rel=1e-7)
+    assert ctx.crack_opening() == pytest.approx(o.cov(ug, vg_), rel=1e-10)
+    ctx.close()
+
+
+def runtest1_gpu(vg, precision, steps=11, altmintol=1e-3):
+    """ValidationTests/test1.c (make runtest1 arguments) through the product path."""
+    n = (101, 5, 5)
+    ctx = vg.VFContext(n, (10., 1., 1.), dict(E=1.0, nu=0.0, Gc=0.1), epsilon=0.5, eta=1e-8,
+                       atnum=1, pressurize=False)
+    bcU = [vg.BCSpec(X0=(vg.BC_FIXED, -1.0), X1=(vg.BC_FIXED, 1.0)),
+           vg.BCSpec(X0=vg.BC_ZERO, X1=vg.BC_ZERO), vg.BCSpec(X0=vg.BC_ZERO, X1=vg.BC_ZERO)]
+    ctx.set_bc(bcU, vg.BCSpec(X0=vg.BC_ONE, X1=vg.BC_ONE))
+    bcu1 = vg.bc_vector(n, bcU)
+    out = []
+    for ts in range(steps):
+        t = 0.4 * ts
+        ctx.set_field("BCU", bcu1 * t)
+        ctx.time_step_prepare()
+        it = 0
+        while True:
+            rc, err, su, sv = ctx.am_step(dict(precision=precision))
+            assert rc == 0, (su, sv)
+            it += 1
+            if not (err >= altmintol and it <= 10000):
+                break
+        cov = ctx.crack_opening()
+        el, _, _ = ctx.u_energy()
+        out.append(dict(t=t, am_its=it, cov=cov, elastic=el, surface=ctx.v_energy()))
+    ctx.close()
+    return out
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_runtest1_on_gpu(cuda, precision):
+    """The reference's golden ValidationTests/results/runtest1.out, through vfgpu."""
+    import vpfhf_b200 as vg
+    gold = json.load(open(os.path.join(HERE, "golden", "runtest1.json")))["steps"]
+    mine = runtest1_gpu(vg, precision)
+    rel = 2e-6 if precision == "fp64" else 2e-5
+    for m, r in zip(mine, gold):
+        t = r["t"]
+        if t <= 2.0 + 1e-9:
+            if precision == "fp64":
+                assert m["am_its"] == r["am_its"], t
+            assert m["cov"] == pytest.approx(r["cov"], rel=rel, abs=1e-6), t
+            assert m["elastic"] == pytest.approx(r["elastic"], rel=rel, abs=1e-12), t
+            assert m["surface"] == pytest.approx(r["surface"], rel=rel, abs=1e-12), t
+        else:
+            assert m["cov"] == pytest.approx(r["cov"], rel=2e-4), t
+            assert m["surface"] == pytest.approx(r["surface"], rel=2e-4), t
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_penny41_am_loop(cuda, precision):
+    """5 AM iterations of the 41^3 pressurized penny crack against the oracle fixture:
+    relative energy error <= 1e-6 and v L-inf <= 1e-4 (the parity bar)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import vpfhf_b200 as vg
+    from make_penny41 import PARAMS as P
+    fx = np.load(os.path.join(HERE, "golden", "penny41.npz"))
+    rec = fx["rec"]
+    n = P["n"]
+    # the initial V is built on the host exactly as the oracle does (VFCracks.c:185-227)
+    import vforacle as vo
+    ov = vo.Oracle(n, P["l"], E=P["E"], nu=P["nu"], Gc=P["Gc"], epsilon=P["epsilon"],
+                   eta=P["eta"], atnum=P["atnum"])
+    v0 = ov.penny_v(P["center"], P["r"])
+    ctx = vg.VFContext(n, P["l"], dict(E=P["E"], nu=P["nu"], Gc=P["Gc"]), epsilon=P["epsilon"],
+                       eta=P["eta"], atnum=P["atnum"], pressurize=True)
+    ctx.set_bc(vg.rollers())
+    ctx.set_field("V", v0)
+    ctx.set_field("pressure", np.full(ctx.N, P["p"]))
+    ctx.time_step_prepare()
+    for it in range(P["am_its"]):
+        rc, err, su, sv = ctx.am_step(dict(precision=precision))
+        assert rc == 0, (su, sv)
+        el, _, pw = ctx.u_energy()
+        s, cov = ctx.v_energy(), ctx.crack_opening()
+        for got, ref in zip((el, pw, s, cov), rec[it, :4]):
+            assert got == pytest.approx(ref, rel=1e-6), (it, got, ref)
+    assert np.abs(ctx.get_field("V") - fx["V"]).max() <= 1e-4
+    ctx.close()

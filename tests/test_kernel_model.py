@@ -29,3 +29,17 @@ def test_tiled_schedule_matches_oracle(oracle_mod, n, TY, zc):
     h = tuple(L / (k - 1) for L, k in zip((1.1, 0.9, 0.7), n))
     y = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, zc=zc)
     assert np.abs(y - yref).max() <= 1e-13 * np.abs(yref).max()
+
+
+def test_modal_v_element_matches_gauss_sum(oracle_mod):
+    """K_V,e x = sum_g [aeps w grad(phi_a).grad(x) + c_g phi_a x] from the element tables."""
+    rng = np.random.default_rng(5)
+    h = (0.3, 0.5, 0.7)
+    w, phi, dphi = np.zeros(27), np.zeros(216), np.zeros(648)
+    oracle_mod.lib().vfo_tables(*h, w, phi, dphi)
+    phi, dphi = phi.reshape(8, 27), dphi.reshape(8, 3, 27)
+    for _ in range(3):
+        x, cg, aeps = rng.standard_normal(8), rng.uniform(0, 2, 27), rng.uniform(0.5, 2)
+        K = np.einsum("g,adg,bdg->ab", w * aeps, dphi, dphi) + np.einsum("g,ag,bg->ab", cg, phi, phi)
+        y = km.v_element(x, cg, aeps, h)
+        assert np.abs(y - K @ x).max() <= 1e-13 * np.abs(K @ x).max()

@@ -16,7 +16,9 @@ import numpy as np
 from . import _abi
 from ._abi import (BC_FIXED, BC_NONE, BC_ONE, BC_ZERO, FP64, MIXED, VFGPUError)  # noqa: F401
 
-__all__ = ["VFContext", "BCSpec", "rollers", "FP64", "MIXED", "VFGPUError"]
+__all__ = ["VFContext", "BCSpec", "rollers", "solve_opts", "bc_vector", "FP64", "MIXED",
+           "VFGPUError", "VF_StepU", "VF_StepV", "VF_UEnergy3D", "VF_VEnergy3D",
+           "VolumetricCrackOpening", "VFTimeStepPrepare"]
 
 
 class BCSpec:
@@ -142,3 +144,149 @@ class VFContext:
         _abi.check(self.L.vfgpu_u_apply(self.h, int(precision), _abi.ptr(x), _abi.ptr(out)),
                    "vfgpu_u_apply")
         return out
+
+    def u_apply_dev(self, x, y, precision=FP64):
+        """Queues y = J_U x on the ctx stream; x, y are device tensors (float64 for FP64,
+        float32 for MIXED).  Returns immediately."""
+        _abi.check(self.L.vfgpu_u_apply_dev(self.h, int(precision), x.data_ptr(), y.data_ptr()),
+                   "vfgpu_u_apply_dev")
+
+    @property
+    def stream_handle(self):
+        s = C.c_void_p()
+        _abi.check(self.L.vfgpu_get_stream(self.h, C.byref(s)), "vfgpu_get_stream")
+        return s.value
+
+    def torch_stream(self):
+        """The ctx stream as a torch.cuda.ExternalStream (for events / ordering)."""
+        import torch
+        return torch.cuda.ExternalStream(self.stream_handle)
+
+    # -- solves ---------------------------------------------------------------------
+    def step_u(self, opts=None):
+        """VF_StepU: returns (status, stats dict); status 0 converged, 1 not converged,
+        2 diverged."""
+        st = _abi.SolveStats()
+        o = solve_opts(**(opts or {}))
+        rc = _abi.check(self.L.vfgpu_step_u(self.h, C.byref(o), C.byref(st)), "vfgpu_step_u")
+        return rc, st.as_dict()
+
+    def step_v(self, opts=None):
+        """VF_StepV (VI Newton with bounds [0,1] or [0,VIrrev])."""
+        st = _abi.SolveStats()
+        o = solve_opts(**(opts or {}))
+        rc = _abi.check(self.L.vfgpu_step_v(self.h, C.byref(o), C.byref(st)), "vfgpu_step_v")
+        return rc, st.as_dict()
+
+    def am_step(self, opts=None):
+        """StepU + StepV; returns (status, errV, statsU, statsV)."""
+        su, sv, err = _abi.SolveStats(), _abi.SolveStats(), C.c_double()
+        o = solve_opts(**(opts or {}))
+        rc = _abi.check(self.L.vfgpu_am_step(self.h, C.byref(o), C.byref(err), C.byref(su),
+                                             C.byref(sv)), "vfgpu_am_step")
+        return rc, err.value, su.as_dict(), sv.as_dict()
+
+    def time_step_prepare(self):
+        _abi.check(self.L.vfgpu_time_step_prepare(self.h), "vfgpu_time_step_prepare")
+
+    def u_energy(self):
+        """(elastic energy, in-situ work, pressure work) as VF_UEnergy3D."""
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        _abi.check(self.L.vfgpu_u_energy(self.h, C.byref(a), C.byref(b), C.byref(c)),
+                   "vfgpu_u_energy")
+        return a.value, b.value, c.value
+
+    def v_energy(self):
+        s = C.c_double()
+        _abi.check(self.L.vfgpu_v_energy(self.h, C.byref(s)), "vfgpu_v_energy")
+        return s.value
+
+    def crack_opening(self, cell=False):
+        cov = C.c_double()
+        n = self.n
+        cc = np.empty((n[0] - 1) * (n[1] - 1) * (n[2] - 1)) if cell else None
+        _abi.check(self.L.vfgpu_crack_opening(self.h, C.byref(cov), _abi.ptr(cc)),
+                   "vfgpu_crack_opening")
+        return (cov.value, cc) if cell else cov.value
+
+    def u_residual(self):
+        F = np.empty(3 * self.N)
+        _abi.check(self.L.vfgpu_u_residual(self.h, _abi.ptr(F)), "vfgpu_u_residual")
+        return F
+
+    def v_residual(self):
+        F = np.empty(self.N)
+        _abi.check(self.L.vfgpu_v_residual(self.h, _abi.ptr(F)), "vfgpu_v_residual")
+        return F
+
+
+def solve_opts(**kw):
+    """SolveOpts with the reference's defaults (vfgpu_default_solve_opts), overridden by kw;
+    `precision` accepts FP64 / MIXED or "fp64" / "mixed"."""
+    o = _abi.SolveOpts()
+    _abi.lib().vfgpu_default_solve_opts(C.byref(o))
+    for k, v in kw.items():
+        if k == "precision" and isinstance(v, str):
+            v = {"fp64": FP64, "mixed": MIXED}[v.lower()]
+        setattr(o, k, v)
+    return o
+
+
+def bc_vector(n, bcs):
+    """VecSetFromBC (VFCartFE.c:279-491): the vector of Dirichlet values of a VFBC array
+    (face values in face order X0,X1,Y0,Y1,Z0,Z1, then vertex values); dof = len(bcs)."""
+    nx, ny, nz = n
+    dof = len(bcs)
+    out = np.zeros((nz, ny, nx, dof))
+    for c, b in enumerate(bcs):
+        for f in range(6):
+            t = b.face[f]
+            if t == BC_NONE:
+                continue
+            val = 0.0 if t == BC_ZERO else 1.0 if t == BC_ONE else b.faceValue[f]
+            sl = [slice(None)] * 3
+            axis = 2 - f // 2          # X -> last array axis
+            sl[axis] = 0 if f % 2 == 0 else n[f // 2] - 1
+            out[tuple(sl) + (c,)] = val
+        for o in (0, 4, 2, 6, 1, 5, 3, 7):
+            t = b.vertex[o]
+            if t == BC_NONE:
+                continue
+            val = 0.0 if t == BC_ZERO else 1.0 if t == BC_ONE else b.vertexValue[o]
+            i = nx - 1 if o & 1 else 0
+            j = ny - 1 if o & 2 else 0
+            k = nz - 1 if o & 4 else 0
+            out[k, j, i, c] = val
+    return out.reshape(-1)
+
+
+# -- the reference's entry points over a VFContext ---------------------------------
+def VF_StepU(ctx, opts=None):
+    """VF_StepU (VFMech.c:1436): returns the SNES converged reason's stats."""
+    return ctx.step_u(opts)
+
+
+def VF_StepV(ctx, opts=None):
+    """VF_StepV (VFMech.c:3057): returns 0 or the negative SNES reason, as the reference."""
+    rc, st = ctx.step_v(opts)
+    return st["reason"] if st["reason"] < 0 else 0
+
+
+def VF_UEnergy3D(ctx):
+    """(ElasticEnergy, InsituWork, PressureWork) (VFMech.c:1111)."""
+    return ctx.u_energy()
+
+
+def VF_VEnergy3D(ctx):
+    """SurfaceEnergy (VFMech.c:2474)."""
+    return ctx.v_energy()
+
+
+def VolumetricCrackOpening(ctx):
+    """Crack opening volume (VFPermfield.c:75)."""
+    return ctx.crack_opening()
+
+
+def VFTimeStepPrepare(ctx):
+    """VFCommon.c:1132."""
+    ctx.time_step_prepare()

@@ -42,6 +42,22 @@ class BC(C.Structure):
                 ("vertex", C.c_int * 8), ("vertexValue", C.c_double * 8)]
 
 
+class SolveOpts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("ksp_rtol", C.c_double), ("ksp_atol", C.c_double),
+                ("ksp_dtol", C.c_double), ("ksp_maxit", C.c_int), ("snes_rtol", C.c_double),
+                ("snes_atol", C.c_double), ("snes_stol", C.c_double), ("snes_maxit", C.c_int),
+                ("inner_rtol", C.c_double), ("max_refine", C.c_int), ("time_limit", C.c_double)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("newton_its", C.c_int), ("ksp_its", C.c_int), ("refine_its", C.c_int),
+                ("reason", C.c_int), ("fnorm0", C.c_double), ("fnorm", C.c_double),
+                ("seconds", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class VFGPUError(RuntimeError):
     def __init__(self, code, fn, msg):
         super().__init__(f"{fn} failed with status {code}: {msg}")
@@ -61,7 +77,21 @@ _SIGS = {
     "vfgpu_set_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_get_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_u_apply": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
+    "vfgpu_u_apply_dev": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],
+    "vfgpu_get_stream": [C.c_void_p, C.POINTER(C.c_void_p)],
+    "vfgpu_step_u": [C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)],
+    "vfgpu_step_v": [C.c_void_p, C.POINTER(SolveOpts), C.POINTER(SolveStats)],
+    "vfgpu_time_step_prepare": [C.c_void_p],
+    "vfgpu_am_step": [C.c_void_p, C.POINTER(SolveOpts), C.POINTER(C.c_double),
+                      C.POINTER(SolveStats), C.POINTER(SolveStats)],
+    "vfgpu_u_energy": [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                       C.POINTER(C.c_double)],
+    "vfgpu_v_energy": [C.c_void_p, C.POINTER(C.c_double)],
+    "vfgpu_crack_opening": [C.c_void_p, C.POINTER(C.c_double), C.c_void_p],
+    "vfgpu_u_residual": [C.c_void_p, C.c_void_p],
+    "vfgpu_v_residual": [C.c_void_p, C.c_void_p],
 }
+_VOID_SIGS = {"vfgpu_default_solve_opts": [C.POINTER(SolveOpts)]}
 
 
 def lib():
@@ -79,12 +109,16 @@ def lib():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
+    for name, args in _VOID_SIGS.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = None
     _LIB = L
     return L
 
 
 def exported_symbols():
-    return ["vfgpu_last_error"] + list(_SIGS)
+    return ["vfgpu_last_error"] + list(_SIGS) + list(_VOID_SIGS)
 
 
 def check(code, fn):

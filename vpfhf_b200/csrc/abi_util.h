@@ -10,6 +10,7 @@ bool is_device_ptr(const void* p);
 cudaError_t copy_in(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
 cudaError_t copy_out(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
 int ensure_v32(vfgpu_ctx* c);
+void free_solver(vfgpu_ctx* c);
 template <typename T>
-UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const UPlan& p);
+UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
 }  // namespace vfgpu

@@ -5,6 +5,8 @@
 #include <vector>
 
 #include "../../include/vfgpu.h"
+#include "cg.cuh"
+#include "elem.h"
 #include "kernels.h"
 
 struct vfgpu_ctx {
@@ -36,11 +38,26 @@ struct vfgpu_ctx {
   bool v32_stale = true;
 
   // scratch
-  vfgpu::UPlan plan64{}, plan32{};
-  double* seam64 = nullptr;
+  vfgpu::TilePlan plan64{}, plan32{}, vplan64{}, vplan32{};
+  double* seam64 = nullptr;  // U seams FP64 (V seams use the same buffer: they are smaller)
   float* seam32 = nullptr;
   double *t64a = nullptr, *t64b = nullptr;
   float *t32a = nullptr, *t32b = nullptr;
+
+  // solver work space, allocated at the first solve (see solve_buffers in step.cu)
+  static constexpr int NP64 = 9, NP32 = 5;
+  double* p64[NP64] = {nullptr};  // 3N doubles each
+  float* p32[NP32] = {nullptr};   // 3N floats each
+  double* coef64 = nullptr;       // 27 per cell: V coupling coefficient
+  float* coef32 = nullptr;
+  uint8_t* vmask = nullptr;       // N
+  vfgpu::ETab* d_tab = nullptr;   // element tables of the uniform element
+  vfgpu::CGState* d_cg = nullptr; // device CG scalars
+  vfgpu::CGState* h_cg = nullptr; // pinned host mirror
+  double* d_red = nullptr;        // reduction partials (RED_BLOCKS * 4 + energy blocks * 4)
+  double* d_out = nullptr;        // small device results (16 doubles)
+  double* h_out = nullptr;        // pinned host mirror of d_out
+  bool have_solver = false;
 };
 
 namespace vfgpu {

@@ -1,0 +1,447 @@
+// elem.cu -- once-per-solve element kernels, written per Gauss point after the
+// reference's element routines (they run once per StepU / StepV, so clarity wins
+// over speed here).  Scatter to nodes is done in 8 parity colours of elements so
+// that no two threads of a launch touch the same node: deterministic, no atomics.
+#include <cmath>
+
+#include "elem.h"
+
+namespace vfgpu {
+
+void etab_host(double hx, double hy, double hz, ETab* e) {
+  // VFCartFEElement1DInit (VFCartFE.c:90-116), tensor product as VFCartFEElement3DInit.
+  auto t1 = [](double l, double w[3], double phi[2][3], double dphi[2][3]) {
+    w[0] = 5. * l / 18.;
+    w[1] = 8. * l / 18.;
+    w[2] = 5. * l / 18.;
+    phi[0][0] = (1. + sqrt(3. / 5.)) * .5;
+    phi[0][1] = .5;
+    phi[0][2] = (1. - sqrt(3. / 5.)) * .5;
+    phi[1][0] = (1. - sqrt(3. / 5.)) * .5;
+    phi[1][1] = .5;
+    phi[1][2] = (1. + sqrt(3. / 5.)) * .5;
+    for (int g = 0; g < 3; g++) {
+      dphi[0][g] = -1. / l;
+      dphi[1][g] = 1. / l;
+    }
+  };
+  double wx[3], wy[3], wz[3], px[2][3], py[2][3], pz[2][3], dx[2][3], dy[2][3], dz[2][3];
+  t1(hx, wx, px, dx);
+  t1(hy, wy, py, dy);
+  t1(hz, wz, pz, dz);
+  for (int gk = 0, g = 0; gk < 3; gk++)
+    for (int gj = 0; gj < 3; gj++)
+      for (int gi = 0; gi < 3; gi++, g++) {
+        e->w[g] = wz[gk] * wy[gj] * wx[gi];
+        for (int k = 0; k < 2; k++)
+          for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+              const int a = i + 2 * j + 4 * k;
+              e->phi[a][g] = pz[k][gk] * py[j][gj] * px[i][gi];
+              e->dphi[a][0][g] = pz[k][gk] * py[j][gj] * dx[i][gi];
+              e->dphi[a][1][g] = pz[k][gk] * dy[j][gj] * px[i][gi];
+              e->dphi[a][2][g] = dz[k][gk] * py[j][gj] * px[i][gi];
+            }
+      }
+}
+
+namespace {
+
+struct CellMat {
+  double lambda, mu, alpha, beta, Gc;
+};
+
+__device__ __forceinline__ CellMat cell_mat(const ElemArgs& E, int ei, int ej, int ek) {
+  const int l = E.elayer ? E.elayer[ek] : 0;
+  CellMat m;
+  if (E.cellE) {
+    const double Ec = (double)E.cellE[((int64_t)ek * (E.ny - 1) + ej) * (E.nx - 1) + ei];
+    m.lambda = Ec * E.L.lamfac[l];
+    m.mu = Ec * E.L.mufac[l];
+  } else {
+    m.lambda = E.L.lambda[l];
+    m.mu = E.L.mu[l];
+  }
+  m.alpha = E.L.alpha[l];
+  m.beta = E.L.beta[l];
+  m.Gc = E.L.Gc[l];
+  return m;
+}
+
+__device__ __forceinline__ void cell_nodes(const ElemArgs& E, int ei, int ej, int ek,
+                                           int64_t (&n)[8]) {
+#pragma unroll
+  for (int a = 0; a < 8; a++)
+    n[a] = node_index(ei + (a & 1), ej + ((a >> 1) & 1), ek + (a >> 2), E.nx, E.ny);
+}
+
+// Element (ei,ej,ek) of colour (cx,cy,cz) for the linear thread index t, or false.
+__device__ __forceinline__ bool colour_cell(const ElemArgs& E, int color, int64_t t, int& ei,
+                                            int& ej, int& ek) {
+  const int cx = color & 1, cy = (color >> 1) & 1, cz = color >> 2;
+  const int hx = (E.nx - 1 - cx + 1) / 2, hy = (E.ny - 1 - cy + 1) / 2, hz = (E.nz - 1 - cz + 1) / 2;
+  if (t >= (int64_t)hx * hy * hz) return false;
+  ei = cx + 2 * (int)(t % hx);
+  ej = cy + 2 * (int)((t / hx) % hy);
+  ek = cz + 2 * (int)(t / ((int64_t)hx * hy));
+  return true;
+}
+
+__global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restrict__ v,
+                             const double* __restrict__ theta, const double* __restrict__ thetaRef,
+                             const double* __restrict__ p, double* __restrict__ f) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  const ETab& e = *E.tab;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double v8[8], th8[8], p8[8], rl[24];
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    v8[a] = v[n[a]];
+    th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+    p8[a] = p ? p[n[a]] : 0.;
+  }
+  for (int l = 0; l < 24; l++) rl[l] = 0.;
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  // VF_GradientUThermoPoro3D_local (VFMech.c:386-447)
+  const double coefalpha = (3. * m.lambda + 2. * m.mu) * m.alpha, beta = m.beta;
+  for (int g = 0; g < 27; g++) {
+    double te = 0., pe = 0., ve = 0.;
+    for (int a = 0; a < 8; a++) {
+      te += e.phi[a][g] * th8[a];
+      pe += e.phi[a][g] * p8[a];
+      ve += e.phi[a][g] * v8[a];
+    }
+    const double s = coefalpha * te * (ve * ve + E.eta) + beta * pe * ve;
+    for (int a = 0; a < 8; a++)
+      for (int c = 0; c < 3; c++) rl[3 * a + c] += e.w[g] * e.dphi[a][c][g] * s;
+  }
+  // VF_GradientUCrackPressure3D_local (VFMech.c:533-589)
+  if (E.hasCrackPressure) {
+    for (int g = 0; g < 27; g++) {
+      double pe = 0., gv[3] = {0., 0., 0.};
+      for (int a = 0; a < 8; a++) {
+        pe += e.phi[a][g] * p8[a];
+        for (int c = 0; c < 3; c++) gv[c] += e.dphi[a][c][g] * v8[a];
+      }
+      for (int a = 0; a < 8; a++)
+        for (int c = 0; c < 3; c++) rl[3 * a + c] += e.w[g] * pe * gv[c] * e.phi[a][g];
+    }
+  }
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) f[3 * n[a] + c] += rl[3 * a + c];
+}
+
+__global__ void u_diag_kernel(const ElemArgs E, int color, const double* __restrict__ v,
+                              double* __restrict__ d) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  const ETab& e = *E.tab;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double v8[8], dg[24];
+#pragma unroll
+  for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
+  for (int l = 0; l < 24; l++) dg[l] = 0.;
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  for (int g = 0; g < 27; g++) {
+    double s = 0.;
+    for (int a = 0; a < 8; a++) s += v8[a] * e.phi[a][g];
+    const double ws = e.w[g] * (s * s + E.eta);
+    for (int a = 0; a < 8; a++) {
+      const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
+      const double g2 = d0 * d0 + d1 * d1 + d2 * d2;
+      dg[3 * a + 0] += ws * ((m.lambda + m.mu) * d0 * d0 + m.mu * g2);
+      dg[3 * a + 1] += ws * ((m.lambda + m.mu) * d1 * d1 + m.mu * g2);
+      dg[3 * a + 2] += ws * ((m.lambda + m.mu) * d2 * d2 + m.mu * g2);
+    }
+  }
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) d[3 * n[a] + c] += dg[3 * a + c];
+}
+
+__global__ void bc_diag_kernel(const uint8_t* __restrict__ bcbits, double* __restrict__ d, int64_t N) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned b = bcbits[i];
+    for (int c = 0; c < 3; c++)
+      if ((b >> c) & 1u) d[3 * i + c] = 1.;
+  }
+}
+
+// ElasticEnergyDensity3D_local (VFMech.c:32-106) at every Gauss point, times 2 and
+// the Gauss weight, plus the AT2 mass coefficient (VFMech.c:2040-2058).
+__global__ void v_coef_kernel(const ElemArgs E, const double* __restrict__ u,
+                              const double* __restrict__ theta, const double* __restrict__ thetaRef,
+                              double* __restrict__ coef, float* __restrict__ coef32) {
+  const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= NCELL) return;
+  const int ei = (int)(cell % (E.nx - 1));
+  const int ej = (int)((cell / (E.nx - 1)) % (E.ny - 1));
+  const int ek = (int)(cell / ((int64_t)(E.nx - 1) * (E.ny - 1)));
+  const ETab& e = *E.tab;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double u8[8][3], th8[8];
+  for (int a = 0; a < 8; a++) {
+    for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
+    th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+  }
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  const double mass = E.atnum == 2 ? m.Gc / E.atcv * .5 / E.epsilon : 0.;
+  for (int g = 0; g < 27; g++) {
+    double e11 = 0, e22 = 0, e33 = 0, e12 = 0, e23 = 0, e13 = 0;
+    for (int a = 0; a < 8; a++) {
+      const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
+      const double at = m.alpha * e.phi[a][g] * th8[a];
+      e11 += d0 * u8[a][0] - at;
+      e22 += d1 * u8[a][1] - at;
+      e33 += d2 * u8[a][2] - at;
+      e12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
+      e23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
+      e13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
+    }
+    const double l = m.lambda, mu = m.mu;
+    const double s11 = (l + 2. * mu) * e11 + l * e22 + l * e33;
+    const double s22 = l * e11 + (l + 2. * mu) * e22 + l * e33;
+    const double s33 = l * e11 + l * e22 + (l + 2. * mu) * e33;
+    const double W = (s11 * e11 + s22 * e22 + s33 * e33) * .5 + 2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
+    const double cgv = e.w[g] * (2. * W + mass);
+    coef[27 * cell + g] = cgv;
+    if (coef32) coef32[27 * cell + g] = (float)cgv;
+  }
+}
+
+__global__ void v_rhs_kernel(const ElemArgs E, int color, const double* __restrict__ u,
+                             const double* __restrict__ p, double* __restrict__ b) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  const ETab& e = *E.tab;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  double rl[8];
+  // VF_ResidualVAT1/AT23D_local (VFMech.c:2350-2384)
+  const double coef = m.Gc / E.atcv / E.epsilon * (E.atnum == 1 ? .25 : .5);
+  for (int a = 0; a < 8; a++) {
+    rl[a] = 0.;
+    for (int g = 0; g < 27; g++) rl[a] += e.w[g] * e.phi[a][g] * coef;
+  }
+  // VF_ResidualVCrackPressure3D_local (VFMech.c:2294-2341)
+  if (E.hasCrackPressure && p) {
+    double u8[8][3], p8[8];
+    for (int a = 0; a < 8; a++) {
+      for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
+      p8[a] = p[n[a]];
+    }
+    for (int g = 0; g < 27; g++) {
+      double pe = 0., ue[3] = {0., 0., 0.};
+      for (int a = 0; a < 8; a++) {
+        pe += e.phi[a][g] * p8[a];
+        for (int c = 0; c < 3; c++) ue[c] += e.phi[a][g] * u8[a][c];
+      }
+      for (int a = 0; a < 8; a++)
+        rl[a] += e.w[g] * pe * (ue[0] * e.dphi[a][0][g] + ue[1] * e.dphi[a][1][g] + ue[2] * e.dphi[a][2][g]);
+    }
+  }
+  for (int a = 0; a < 8; a++) b[n[a]] += rl[a];
+}
+
+__global__ void v_diag_kernel(const ElemArgs E, int color, const double* __restrict__ coef,
+                              double* __restrict__ d) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  const ETab& e = *E.tab;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  const double aeps = m.Gc / E.atcv * .5 * E.epsilon;
+  const int64_t cell = ((int64_t)ek * (E.ny - 1) + ej) * (E.nx - 1) + ei;
+  for (int a = 0; a < 8; a++) {
+    double s = 0.;
+    for (int g = 0; g < 27; g++) {
+      const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
+      s += aeps * e.w[g] * (d0 * d0 + d1 * d1 + d2 * d2) + coef[27 * cell + g] * e.phi[a][g] * e.phi[a][g];
+    }
+    d[n[a]] += s;
+  }
+}
+
+// Neumaier-compensated accumulation.
+struct KSum {
+  double s = 0., c = 0.;
+  __device__ void add(double x) {
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  __device__ double value() const { return s + c; }
+};
+
+constexpr int EN_THREADS = 256, EN_BLOCKS = 592;
+
+// One thread per element (grid-stride, fixed assignment), per-thread compensated
+// sums, pairwise tree in shared memory, per-block partials: deterministic.
+__global__ void __launch_bounds__(EN_THREADS) energy_kernel(
+    const ElemArgs E, const double* __restrict__ u, const double* __restrict__ v,
+    const double* __restrict__ theta, const double* __restrict__ thetaRef,
+    const double* __restrict__ p, double* __restrict__ partial, double* __restrict__ cellcov) {
+  __shared__ double red[4][EN_THREADS];
+  const ETab& e = *E.tab;
+  const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  KSum acc[4];
+  for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < NCELL;
+       cell += (int64_t)gridDim.x * blockDim.x) {
+    const int ei = (int)(cell % (E.nx - 1));
+    const int ej = (int)((cell / (E.nx - 1)) % (E.ny - 1));
+    const int ek = (int)(cell / ((int64_t)(E.nx - 1) * (E.ny - 1)));
+    int64_t n[8];
+    cell_nodes(E, ei, ej, ek, n);
+    const CellMat m = cell_mat(E, ei, ej, ek);
+    double u8[8][3], v8[8], th8[8], p8[8];
+    for (int a = 0; a < 8; a++) {
+      for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
+      v8[a] = v[n[a]];
+      th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+      p8[a] = p ? p[n[a]] : 0.;
+    }
+    const double threekappa = 3. * m.lambda + 2. * m.mu, coefbeta = m.beta / threekappa;
+    const double scoef = m.Gc / E.atcv * .25;
+    double el = 0., pw = 0., se = 0., cv = 0.;
+    for (int g = 0; g < 27; g++) {
+      double D11 = 0, D22 = 0, D33 = 0, D12 = 0, D23 = 0, D13 = 0, ve = 0, pe = 0, te = 0;
+      double gv[3] = {0, 0, 0}, ue[3] = {0, 0, 0};
+      for (int a = 0; a < 8; a++) {
+        const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
+        const double ph = e.phi[a][g];
+        D11 += d0 * u8[a][0];
+        D22 += d1 * u8[a][1];
+        D33 += d2 * u8[a][2];
+        D12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
+        D23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
+        D13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
+        ve += ph * v8[a];
+        pe += ph * p8[a];
+        te += ph * th8[a];
+        gv[0] += d0 * v8[a];
+        gv[1] += d1 * v8[a];
+        gv[2] += d2 * v8[a];
+        for (int c = 0; c < 3; c++) ue[c] += ph * u8[a][c];
+      }
+      // VF_ElasticEnergy3D_local (VFMech.c:725-809), quirk Q2: v^2 (1+eta) on the deviator
+      const double tr = D11 + D22 + D33;
+      D11 -= tr / 3.;
+      D22 -= tr / 3.;
+      D33 -= tr / 3.;
+      el += (D11 * D11 + D22 * D22 + D33 * D33 + (D12 * D12 + D23 * D23 + D13 * D13) * 2.) * ve * ve *
+            (1. + E.eta) * m.mu * e.w[g];
+      const double WD = (tr / 3. - m.alpha * te) * ve - coefbeta * pe;
+      el += 3. * threekappa / 2. * WD * WD * e.w[g];
+      el += threekappa / 6. * tr * tr * E.eta * e.w[g];
+      const double udv = ue[0] * gv[0] + ue[1] * gv[1] + ue[2] * gv[2];
+      // VF_PressureWork3D_local (VFMech.c:920-974)
+      if (E.hasCrackPressure) pw += e.w[g] * pe * udv;
+      // VF_AT1/AT2SurfaceEnergy3D_local (VFMech.c:2394-2465)
+      const double g2 = gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
+      const double om = 1. - ve;
+      se += e.w[g] * ((E.atnum == 1 ? om : om * om) / E.epsilon + g2 * E.epsilon) * scoef;
+      // VolumetricCrackOpening3D_local (VFPermfield.c:15-73)
+      cv += udv * e.w[g];
+    }
+    if (cellcov) {
+      double vol = 0.;
+      for (int g = 0; g < 27; g++) vol += e.w[g];
+      cellcov[cell] = cv / vol;
+    }
+    acc[0].add(el);
+    acc[1].add(pw);
+    acc[2].add(se);
+    acc[3].add(cv);
+  }
+  for (int q = 0; q < 4; q++) red[q][threadIdx.x] = acc[q].value();
+  __syncthreads();
+  for (int st = EN_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int q = 0; q < 4; q++) red[q][threadIdx.x] += red[q][threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) partial[blockIdx.x * 4 + threadIdx.x] = red[threadIdx.x][0];
+}
+
+__global__ void energy_final_kernel(const double* __restrict__ partial, int nblocks,
+                                    double* __restrict__ out) {
+  if (threadIdx.x >= 4) return;
+  KSum s;
+  for (int b = 0; b < nblocks; b++) s.add(partial[b * 4 + threadIdx.x]);
+  out[threadIdx.x] = s.value();
+}
+
+template <typename K, typename... Args>
+cudaError_t colours(const ElemArgs& E, K kernel, cudaStream_t s, Args... args) {
+  for (int color = 0; color < 8; color++) {
+    const int cx = color & 1, cy = (color >> 1) & 1, cz = color >> 2;
+    const int64_t cnt = (int64_t)((E.nx - 1 - cx + 1) / 2) * ((E.ny - 1 - cy + 1) / 2) *
+                        ((E.nz - 1 - cz + 1) / 2);
+    if (cnt == 0) continue;
+    kernel<<<(int)((cnt + 127) / 128), 128, 0, s>>>(E, color, args...);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_u_rhs(const ElemArgs& E, const double* v, const double* theta,
+                         const double* thetaRef, const double* p, double* f, cudaStream_t s) {
+  const int64_t N = (int64_t)E.nx * E.ny * E.nz;
+  cudaError_t e = cudaMemsetAsync(f, 0, 3 * N * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  return colours(E, u_rhs_kernel, s, v, theta, thetaRef, p, f);
+}
+
+cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcbits, double* d,
+                          cudaStream_t s) {
+  const int64_t N = (int64_t)E.nx * E.ny * E.nz;
+  cudaError_t e = cudaMemsetAsync(d, 0, 3 * N * sizeof(double), s);
+  if (e == cudaSuccess) e = colours(E, u_diag_kernel, s, v, d);
+  if (e == cudaSuccess && bcbits) {
+    bc_diag_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 2368), 256, 0, s>>>(bcbits, d, N);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+cudaError_t launch_v_coef(const ElemArgs& E, const double* u, const double* theta,
+                          const double* thetaRef, double* coef, float* coef32, cudaStream_t s) {
+  const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  v_coef_kernel<<<(int)((NCELL + 127) / 128), 128, 0, s>>>(E, u, theta, thetaRef, coef, coef32);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v_rhs(const ElemArgs& E, const double* u, const double* p, double* b,
+                         cudaStream_t s) {
+  const int64_t N = (int64_t)E.nx * E.ny * E.nz;
+  cudaError_t e = cudaMemsetAsync(b, 0, N * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  return colours(E, v_rhs_kernel, s, u, p, b);
+}
+
+cudaError_t launch_v_diag(const ElemArgs& E, const double* coef, double* d, cudaStream_t s) {
+  const int64_t N = (int64_t)E.nx * E.ny * E.nz;
+  cudaError_t e = cudaMemsetAsync(d, 0, N * sizeof(double), s);
+  if (e != cudaSuccess) return e;
+  return colours(E, v_diag_kernel, s, coef, d);
+}
+
+int energy_blocks() { return EN_BLOCKS; }
+
+cudaError_t launch_energies(const ElemArgs& E, const double* u, const double* v,
+                            const double* theta, const double* thetaRef, const double* p,
+                            double* partial, double* out, double* cellcov, cudaStream_t s) {
+  energy_kernel<<<EN_BLOCKS, EN_THREADS, 0, s>>>(E, u, v, theta, thetaRef, p, partial, cellcov);
+  energy_final_kernel<<<1, 32, 0, s>>>(partial, EN_BLOCKS, out);
+  return cudaGetLastError();
+}
+
+}  // namespace vfgpu

@@ -1,0 +1,51 @@
+// elem.h -- once-per-solve element kernels (FP64): load vectors, Jacobi diagonals,
+// the V coupling coefficient, energies and crack opening.
+#pragma once
+
+#include "common.cuh"
+
+namespace vfgpu {
+
+// VFCartFEElement3DInit tables (VFCartFE.c:216-269) of the uniform element.
+struct ETab {
+  double w[27];
+  double phi[8][27];
+  double dphi[8][3][27];
+};
+void etab_host(double hx, double hy, double hz, ETab* e);
+
+struct ElemArgs {
+  const ETab* __restrict__ tab;
+  int nx, ny, nz;
+  const uint8_t* __restrict__ elayer;
+  const float* __restrict__ cellE;
+  LayerTable L;
+  double eta, epsilon, atcv;
+  int atnum, hasCrackPressure;
+};
+
+// f (3N) = thermo-poro + crack-pressure load (VFMech.c:386-447, 533-589), so that
+// F_U = K u - f.  Overwrites f.
+cudaError_t launch_u_rhs(const ElemArgs& E, const double* v, const double* theta,
+                         const double* thetaRef, const double* p, double* f, cudaStream_t s);
+// d (3N) = diag K(v), Dirichlet rows 1.  Overwrites d.
+cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcbits, double* d,
+                          cudaStream_t s);
+// coef (27 per cell) = w_g (2 W_g(u,theta) [+ Gc/(2c_w)/eps for AT2]) in FP64 and,
+// if coef32 is not null, FP32.
+cudaError_t launch_v_coef(const ElemArgs& E, const double* u, const double* theta,
+                          const double* thetaRef, double* coef, float* coef32, cudaStream_t s);
+// b (N) = AT linear term + crack pressure term (VFMech.c:2294-2384).  Overwrites b.
+cudaError_t launch_v_rhs(const ElemArgs& E, const double* u, const double* p, double* b,
+                         cudaStream_t s);
+// d (N) = diag K_V.  Overwrites d.
+cudaError_t launch_v_diag(const ElemArgs& E, const double* coef, double* d, cudaStream_t s);
+
+// Energies: out[0] elastic, out[1] pressure work, out[2] surface, out[3] crack
+// opening volume.  partial must hold 2*4*nblocks doubles; out is device memory.
+int energy_blocks();
+cudaError_t launch_energies(const ElemArgs& E, const double* u, const double* v,
+                            const double* theta, const double* thetaRef, const double* p,
+                            double* partial, double* out, double* cellcov, cudaStream_t s);
+
+}  // namespace vfgpu

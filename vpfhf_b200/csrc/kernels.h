@@ -4,21 +4,18 @@
 #include <algorithm>
 
 #include "common.cuh"
-#include "u_apply.cuh"
+#include "ops.cuh"
 
 namespace vfgpu {
 
-// Launch plan of the U apply: xy tiles of 32 x ty elements, z-chunks of zc planes,
-// seam buffer sizes (elements of the working precision).
-struct UPlan {
-  int ty, ntx, nty, zc, nzc;
-  size_t seamX, seamY;
-};
-
-UPlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms);
+TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms);
+TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms);
 
 template <typename T>
-cudaError_t launch_u_apply(const UApplyArgs<T>& A, const UPlan& p, const LayerTable& L,
+cudaError_t launch_u_apply(const UApplyArgs<T>& A, const TilePlan& p, const LayerTable& L,
+                           cudaStream_t s);
+template <typename T>
+cudaError_t launch_v_apply(const VApplyArgs<T>& A, const TilePlan& p, const LayerTable& L,
                            cudaStream_t s);
 
 }  // namespace vfgpu

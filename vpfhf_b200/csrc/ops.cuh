@@ -1,0 +1,189 @@
+// ops.cuh -- element operators plugged into the tile engine.
+//
+//   UOp: y = K(v) x, the degraded elasticity operator of VF_BilinearFormU3D_local
+//        (VFMech.c:227-290) with Dirichlet rows identity (VFCartFE.c:1147-1296).
+//   VOp: y = K_V x, the damage operator of VF_BilinearFormVAT1/AT23D_local +
+//        VF_BilinearFormVCoupling3D_local (VFMech.c:2040-2115):
+//        (Gc/(2 c_w)) eps int grad(phi_a).grad(phi_b) + int c(x) phi_a phi_b,
+//        c = 2 W(u) [+ Gc/(2 c_w)/eps for AT2], with c premultiplied by the Gauss
+//        weight and stored per element and Gauss point (vfgpu v_coef kernel).
+//        An optional mask removes dofs (row and column) for the reduced-space
+//        solves of the VI Newton method and the rows+columns Dirichlet/irreversibility
+//        treatment (VFCartFE.c:1305-1454, VFMech.c:2637-2682).
+#pragma once
+
+#include "tile_engine.cuh"
+#include "u_apply.cuh"
+
+namespace vfgpu {
+
+template <typename T_> struct UOp {
+  using T = T_;
+  using Args = UApplyArgs<T>;
+  static constexpr int NC = 3, NIN = 4;
+  __device__ __forceinline__ static void load_node(const Args& A, int64_t n, T (&v)[NIN]) {
+    v[0] = A.x[3 * n];
+    v[1] = A.x[3 * n + 1];
+    v[2] = A.x[3 * n + 2];
+    v[3] = A.v[n];
+  }
+  __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
+                                                 int ey, int ez, const T (&in)[8][NIN],
+                                                 T (&out)[8][NC]) {
+    T xn[8][3], vn[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      xn[a][0] = in[a][0];
+      xn[a][1] = in[a][1];
+      xn[a][2] = in[a][2];
+      vn[a] = in[a][3];
+    }
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    T lam, mu;
+    if (A.cellE) {
+      const T E = T(A.cellE[((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex]);
+      lam = E * T(L.lamfac[layer]);
+      mu = E * T(L.mufac[layer]);
+    } else {
+      lam = T(L.lambda[layer]);
+      mu = T(L.mu[layer]);
+    }
+    u_element<T>(xn, vn, lam, mu, A.eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+  }
+  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    const unsigned b = A.bc ? A.bc[n] : 0u;
+#pragma unroll
+    for (int c = 0; c < 3; c++) A.y[3 * n + c] = ((b >> c) & 1u) ? A.x[3 * n + c] : val[c];
+  }
+};
+
+template <typename T> struct VApplyArgs {
+  const T* __restrict__ x;            // N input
+  T* __restrict__ y;                  // N output
+  const uint8_t* __restrict__ mask;   // N: nonzero => dof removed (x -> 0, y = 0); or null
+  const T* __restrict__ coef;         // 27 per cell: w_g (2 W_g [+ A/eps]), cell-major
+  const uint8_t* __restrict__ elayer; // nz-1 or null
+  T* __restrict__ seamX;
+  T* __restrict__ seamY;
+  const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
+  int nx, ny, nz, ntx, nty, zc;
+  T ihx, ihy, ihz, vol;
+  T aeps[VF_MAXLAYER];                // Gc/(2 c_w) * eps per layer
+};
+
+// y[a] = (K_V,e x_e)[a] for one element (same modal scheme as u_element).
+template <typename T>
+__device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict__ cg, T aeps,
+                                          T ihx, T ihy, T ihz, T vol, T (&y)[8]) {
+  T m[8];
+  modal8(xn, m);
+  const T Ax = m[1] * ihx, Bx = m[3] * ihx, Cx = m[5] * ihx, Dx = m[7] * ihx;
+  const T Ay = m[2] * ihy, By = m[3] * ihy, Cy = m[6] * ihy, Dy = m[7] * ihy;
+  const T Az = m[4] * ihz, Bz = m[5] * ihz, Cz = m[6] * ihz, Dz = m[7] * ihz;
+  T QX[4] = {0, 0, 0, 0}, QY[4] = {0, 0, 0, 0}, QZ[4] = {0, 0, 0, 0}, SZ[3][3];
+  T M[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // value moments sum psi P_a(tx) P_b(ty) P_c(tz)
+  const T av = aeps * vol;
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++) {
+    const T ax = lin(gz, Ax, Cx), bx = lin(gz, Bx, Dx), ay = lin(gz, Ay, Cy), by = lin(gz, By, Dy);
+    const T p0 = lin(gz, m[0], m[4]), p1 = lin(gz, m[1], m[5]);
+    const T p2 = lin(gz, m[2], m[6]), p3 = lin(gz, m[3], m[7]);
+    T SY[3];
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++) {
+      const T Gx = lin(gy, ax, bx), al = lin(gy, Az, Cz), be = lin(gy, Bz, Dz);
+      const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
+      T SX = T(0);
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        const int g = gx + 3 * gy + 9 * gz;
+        const T Gy = lin(gx, ay, by), Gz = lin(gx, al, be), xg = lin(gx, q0, q1);
+        const T wa = av * (gw<T>(gx) * gw<T>(gy) * gw<T>(gz));
+        const T fx = wa * Gx, fy = wa * Gy, fz = wa * Gz;
+        const T psi = cg[g] * xg;
+        SX = gx == 0 ? fx : SX + fx;
+        SY[gx] = gy == 0 ? fy : SY[gx] + fy;
+        SZ[gy][gx] = gz == 0 ? fz : SZ[gy][gx] + fz;
+        // value moments
+        const T tx = gt<T>(gx), ty = gt<T>(gy), tz = gt<T>(gz);
+        M[0] += psi;
+        if (gx != 1) M[1] = fma(tx, psi, M[1]);
+        if (gy != 1) M[2] = fma(ty, psi, M[2]);
+        if (gx != 1 && gy != 1) M[3] = fma(tx * ty, psi, M[3]);
+        if (gz != 1) M[4] = fma(tz, psi, M[4]);
+        if (gx != 1 && gz != 1) M[5] = fma(tx * tz, psi, M[5]);
+        if (gy != 1 && gz != 1) M[6] = fma(ty * tz, psi, M[6]);
+        if (gx != 1 && gy != 1 && gz != 1) M[7] = fma(tx * ty * tz, psi, M[7]);
+      }
+      moment4(QX, gy, gz, SX);
+    }
+#pragma unroll
+    for (int gx = 0; gx < 3; gx++) moment4(QY, gx, gz, SY[gx]);
+  }
+#pragma unroll
+  for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+    for (int gx = 0; gx < 3; gx++) moment4(QZ, gx, gy, SZ[gy][gx]);
+  T AX[2][2], AY[2][2], AZ[2][2];
+  inv_butterfly(QX, ihx, AX);
+  inv_butterfly(QY, ihy, AY);
+  inv_butterfly(QZ, ihz, AZ);
+  // value part: sum_g psi prod_d (1/2 + s_d t_d) -> 3 inverse butterflies over M
+  T b1[8], b2[8], b3[8];
+#pragma unroll
+  for (int q = 0; q < 4; q++) {  // z: M[q] (mode 0), M[q+4] (mode 1) -> k = 0,1
+    b1[q] = T(0.5) * M[q] - M[q + 4];
+    b1[q + 4] = T(0.5) * M[q] + M[q + 4];
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int al = 0; al < 2; al++) {  // y
+      const T lo = b1[al + 4 * k], hi = b1[al + 2 + 4 * k];
+      b2[al + 4 * k] = T(0.5) * lo - hi;
+      b2[al + 2 + 4 * k] = T(0.5) * lo + hi;
+    }
+#pragma unroll
+  for (int p = 0; p < 4; p++) {  // x
+    const T lo = b2[2 * p], hi = b2[2 * p + 1];
+    b3[2 * p] = T(0.5) * lo - hi;
+    b3[2 * p + 1] = T(0.5) * lo + hi;
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const T ax_ = i ? AX[j][k] : -AX[j][k];
+        const T ay_ = j ? AY[i][k] : -AY[i][k];
+        const T az_ = k ? AZ[i][j] : -AZ[i][j];
+        y[i + 2 * j + 4 * k] = ((ax_ + ay_) + az_) + b3[i + 2 * j + 4 * k];
+      }
+}
+
+template <typename T_> struct VOp {
+  using T = T_;
+  using Args = VApplyArgs<T>;
+  static constexpr int NC = 1, NIN = 1;
+  __device__ __forceinline__ static void load_node(const Args& A, int64_t n, T (&v)[NIN]) {
+    v[0] = (A.mask && A.mask[n]) ? T(0) : A.x[n];
+  }
+  __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
+                                                 int ey, int ez, const T (&in)[8][NIN],
+                                                 T (&out)[8][NC]) {
+    T xn[8], yn[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) xn[a] = in[a][0];
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    const int64_t cell = ((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex;
+    v_element<T>(xn, A.coef + 27 * cell, A.aeps[layer], A.ihx, A.ihy, A.ihz, A.vol, yn);
+#pragma unroll
+    for (int a = 0; a < 8; a++) out[a][0] = yn[a];
+  }
+  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    A.y[n] = (A.mask && A.mask[n]) ? T(0) : val[0];
+  }
+};
+
+}  // namespace vfgpu

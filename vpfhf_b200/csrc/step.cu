@@ -1,0 +1,635 @@
+// step.cu -- the U and V solves (VF_StepU / VF_StepV), the time-step preparation
+// and the energy / crack-opening reductions behind the C ABI.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+#include "abi_util.h"
+#include "solver.h"
+#include "vec.h"
+
+using namespace vfgpu;
+
+namespace vfgpu {
+
+void free_solver(vfgpu_ctx* c) {
+  for (auto& p : c->p64) cudaFree(p), p = nullptr;
+  for (auto& p : c->p32) cudaFree(p), p = nullptr;
+  cudaFree(c->coef64);
+  cudaFree(c->coef32);
+  cudaFree(c->vmask);
+  cudaFree(c->d_tab);
+  cudaFree(c->d_cg);
+  cudaFree(c->d_red);
+  cudaFree(c->d_out);
+  if (c->h_cg) cudaFreeHost(c->h_cg);
+  if (c->h_out) cudaFreeHost(c->h_out);
+  c->coef64 = nullptr;
+  c->coef32 = nullptr;
+  c->vmask = nullptr;
+  c->d_tab = nullptr;
+  c->d_cg = nullptr;
+  c->d_red = nullptr;
+  c->d_out = nullptr;
+  c->h_cg = nullptr;
+  c->h_out = nullptr;
+  c->have_solver = false;
+}
+
+static int solve_buffers(vfgpu_ctx* c) {
+  if (c->have_solver) return VFGPU_OK;
+  cudaError_t e = cudaSuccess;
+  const size_t n3 = 3 * (size_t)c->N;
+  for (auto& p : c->p64)
+    if (e == cudaSuccess) e = cudaMalloc((void**)&p, n3 * sizeof(double));
+  for (auto& p : c->p32)
+    if (e == cudaSuccess) e = cudaMalloc((void**)&p, n3 * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef64, 27 * (size_t)c->NC * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef32, 27 * (size_t)c->NC * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->vmask, (size_t)c->N);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_tab, sizeof(ETab));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cg, sizeof(CGState));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&c->d_red, (size_t)(RED_BLOCKS + energy_blocks()) * 4 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_out, 16 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_cg, sizeof(CGState));
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_out, 16 * sizeof(double));
+  if (e == cudaSuccess) {
+    ETab t;
+    etab_host(c->hx, c->hy, c->hz, &t);
+    e = cudaMemcpyAsync(c->d_tab, &t, sizeof t, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  }
+  if (e != cudaSuccess) {
+    free_solver(c);
+    return cuda_fail(e, "solver work space");
+  }
+  c->have_solver = true;
+  return VFGPU_OK;
+}
+
+static ElemArgs elem_args(vfgpu_ctx* c) {
+  ElemArgs E{};
+  E.tab = c->d_tab;
+  E.nx = c->nx;
+  E.ny = c->ny;
+  E.nz = c->nz;
+  E.elayer = c->d_elayer;
+  E.cellE = c->d_cellE;
+  E.L = c->layers;
+  E.eta = c->vf.eta;
+  E.epsilon = c->vf.epsilon;
+  E.atcv = c->vf.atnum == 1 ? 2. / 3. : .5;  // VFCommon.c:482-492
+  E.atnum = c->vf.atnum;
+  E.hasCrackPressure = c->vf.hasCrackPressure;
+  return E;
+}
+
+template <typename T>
+static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask, const T* coef,
+                            T* seam, const TilePlan& p) {
+  VApplyArgs<T> A{};
+  A.x = x;
+  A.y = y;
+  A.mask = mask;
+  A.coef = coef;
+  A.elayer = c->d_elayer;
+  A.seamX = seam;
+  A.seamY = seam + p.seamX;
+  A.nx = c->nx;
+  A.ny = c->ny;
+  A.nz = c->nz;
+  A.ihx = T(1.0 / c->hx);
+  A.ihy = T(1.0 / c->hy);
+  A.ihz = T(1.0 / c->hz);
+  A.vol = T(c->hx * c->hy * c->hz);
+  const double atcv = c->vf.atnum == 1 ? 2. / 3. : .5;
+  for (int l = 0; l < VF_MAXLAYER; l++) A.aeps[l] = T(c->layers.Gc[l] / atcv * .5 * c->vf.epsilon);
+  return A;
+}
+
+// Reads n doubles of d_out into h_out (synchronising the stream).
+static cudaError_t fetch(vfgpu_ctx* c, int n) {
+  cudaError_t e = cudaMemcpyAsync(c->h_out, c->d_out, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
+}
+
+static double dot_host(vfgpu_ctx* c, const double* a, const double* b, int64_t n, cudaError_t& e) {
+  const double* pa[1] = {a};
+  const double* pb[1] = {b};
+  if (e == cudaSuccess) e = dev_dots(pa, pb, 1, n, c->d_red, c->d_out, c->stream);
+  if (e == cudaSuccess) e = fetch(c, 1);
+  return e == cudaSuccess ? c->h_out[0] : NAN;
+}
+
+using clk = std::chrono::steady_clock;
+
+struct Watch {
+  clk::time_point t0 = clk::now();
+  double limit = 0;
+  bool expired() const {
+    return limit > 0 && std::chrono::duration<double>(clk::now() - t0).count() > limit;
+  }
+  double seconds() const { return std::chrono::duration<double>(clk::now() - t0).count(); }
+};
+
+// PCG with device-side convergence: queues batches of iterations (every kernel of a
+// converged solve is a no-op), checks the flag between batches.
+template <typename T, class Apply>
+static int run_cg(vfgpu_ctx* c, const CGVecs<T>& v, Apply apply, double rtol, double atol,
+                  double dtol, int maxit, const Watch& w, int* its, int* reason, bool* timeout) {
+  cudaError_t e = cg_init<T>(v, c->d_cg, c->d_red, rtol, atol, dtol, maxit, c->stream);
+  int batch = 4;
+  *timeout = false;
+  while (e == cudaSuccess) {
+    e = cudaMemcpyAsync(c->h_cg, c->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess || c->h_cg->done) break;
+    if (w.expired()) {
+      *timeout = true;
+      break;
+    }
+    for (int b = 0; b < batch && e == cudaSuccess; b++) {
+      e = apply(v.p, v.w, &c->d_cg->done);
+      if (e == cudaSuccess) e = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream);
+    }
+    batch = std::min(batch * 2, 64);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "CG");
+  *its = c->h_cg->its;
+  *reason = c->h_cg->reason;
+  return VFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------- U
+static cudaError_t u_apply64(vfgpu_ctx* c, const double* x, double* y, const int* skip) {
+  UApplyArgs<double> A = u_args<double>(c, x, c->f[VFGPU_FIELD_V], y, c->seam64, c->plan64);
+  A.skip = skip;
+  return launch_u_apply<double>(A, c->plan64, c->layers, c->stream);
+}
+static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* skip) {
+  UApplyArgs<float> A = u_args<float>(c, x, c->V32, y, c->seam32, c->plan32);
+  A.skip = skip;
+  return launch_u_apply<float>(A, c->plan32, c->layers, c->stream);
+}
+
+// F = K(V) U - f, Dirichlet rows U - ubc (VF_UResidual, VFMech.c:1456-1887).
+static cudaError_t u_residual(vfgpu_ctx* c, const double* u, const double* f, double* tmp,
+                              double* F) {
+  cudaError_t e = u_apply64(c, u, tmp, nullptr);
+  if (e == cudaSuccess)
+    e = dev_u_residual(tmp, f, u, c->bcU_kind, c->f[VFGPU_FIELD_BCU], F, 3 * c->N, c->stream);
+  return e;
+}
+
+}  // namespace vfgpu
+
+extern "C" {
+
+void vfgpu_default_solve_opts(vfgpu_solve_opts* o) {
+  if (!o) return;
+  // VFCommon.c:1024 (SNES atol = rtol = 1e-8) and :1039 (KSP rtol 1e-8, atol 1e-10)
+  o->precision = VFGPU_FP64;
+  o->ksp_rtol = 1e-8;
+  o->ksp_atol = 1e-10;
+  o->ksp_dtol = 1e5;
+  o->ksp_maxit = 10000;
+  o->snes_rtol = 1e-8;
+  o->snes_atol = 1e-8;
+  o->snes_stol = 1e-8;
+  o->snes_maxit = 50;
+  o->inner_rtol = 1e-4;
+  o->max_refine = 12;
+  o->time_limit = 0.;
+}
+
+int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: null ctx");
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "vfgpu_step_u: material not set");
+  vfgpu_solve_opts o;
+  if (o_) o = *o_; else vfgpu_default_solve_opts(&o);
+  if (o.precision != VFGPU_FP64 && o.precision != VFGPU_MIXED)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad precision");
+  vfgpu_solve_stats S{};
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  Watch w;
+  w.limit = o.time_limit;
+  const int64_t n3 = 3 * c->N;
+  double *f = c->p64[0], *dinv = c->p64[1], *F = c->p64[2], *Y = c->p64[3], *JY = c->p64[4];
+  double *R = c->p64[5], *P = c->p64[6], *W = c->p64[7];
+  double* U = c->f[VFGPU_FIELD_U];
+  const bool mixed = o.precision == VFGPU_MIXED;
+  ElemArgs E = elem_args(c);
+  cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
+                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+  if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream);
+  if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
+  if (mixed && e == cudaSuccess) {
+    rc = ensure_v32(c);
+    if (rc) return rc;
+  }
+  if (e == cudaSuccess) e = u_residual(c, U, f, JY, F);
+  double fnorm = dot_host(c, F, F, n3, e);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+  fnorm = sqrt(fnorm);
+  S.fnorm0 = fnorm;
+  const double ttol = o.snes_rtol * fnorm;
+  int reason = 0;
+  if (fnorm < o.snes_atol) reason = 2;  // SNES_CONVERGED_FNORM_ABS
+  auto apply64 = [&](const double* x, double* y, const int* skip) { return u_apply64(c, x, y, skip); };
+  auto apply32 = [&](const float* x, float* y, const int* skip) { return u_apply32(c, x, y, skip); };
+  for (int it = 0; !reason && it < o.snes_maxit; it++) {
+    int kits = 0, kreason = 0;
+    bool tmo = false;
+    if (!mixed) {
+      CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3};
+      rc = run_cg<double>(c, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
+                          &kreason, &tmo);
+      if (rc) return rc;
+      S.ksp_its += kits;
+    } else {
+      // Iterative refinement: FP32 PCG corrections, FP64 residual F - J Y.
+      e = cudaMemsetAsync(Y, 0, n3 * sizeof(double), c->stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(R, F, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+      if (e == cudaSuccess) e = dev_znorm2(F, dinv, n3, c->d_red, c->d_out, c->stream);
+      if (e == cudaSuccess) e = fetch(c, 1);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+      const double z0 = sqrt(c->h_out[0]), target = std::max(o.ksp_rtol * z0, o.ksp_atol);
+      double zr = z0;
+      kreason = CG_DIVERGED_ITS;
+      for (int k = 0; k < o.max_refine && zr > target; k++) {
+        float *x32 = c->p32[0], *r32 = c->p32[1], *pp32 = c->p32[2], *w32 = c->p32[3];
+        float* b32 = reinterpret_cast<float*>(P);  // FP32 right-hand side staged in P
+        e = dev_to_f32(R, b32, n3, c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+        CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3};
+        const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
+        int its32 = 0, r32reason = 0;
+        rc = run_cg<float>(c, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
+                           &r32reason, &tmo);
+        if (rc) return rc;
+        S.ksp_its += its32;
+        S.refine_its += 1;
+        if (r32reason < 0 && r32reason != CG_DIVERGED_ITS && its32 == 0) break;
+        e = dev_add_f32(Y, x32, n3, c->stream);
+        if (e == cudaSuccess) e = u_apply64(c, Y, JY, nullptr);            // J Y (FP64)
+        if (e == cudaSuccess) e = dev_axpby(R, F, -1.0, JY, n3, c->stream);  // R = F - J Y
+        if (e == cudaSuccess) e = dev_znorm2(R, dinv, n3, c->d_red, c->d_out, c->stream);
+        if (e == cudaSuccess) e = fetch(c, 1);
+        if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+        zr = sqrt(c->h_out[0]);
+        if (!(zr == zr)) {
+          kreason = CG_DIVERGED_NAN;
+          break;
+        }
+        if (tmo) break;
+      }
+      if (zr <= target) kreason = CG_CONVERGED_RTOL;
+    }
+    if (tmo) {
+      reason = -100;  // wall-clock watchdog
+      break;
+    }
+    if (kreason < 0 && kreason != CG_DIVERGED_ITS) {
+      reason = -3;  // SNES_DIVERGED_LINEAR_SOLVE
+      break;
+    }
+    // L2 line search.  F is affine in U, so ||F(U - l Y)||^2 is an exact quadratic in l
+    // whose minimiser (what SNESLINESEARCHL2's secant step lands on) is
+    // l* = (F . JY) / (JY . JY).
+    e = u_apply64(c, Y, JY, nullptr);
+    const double* pa[3] = {F, JY, Y};
+    const double* pb[3] = {JY, JY, Y};
+    if (e == cudaSuccess) e = dev_dots(pa, pb, 3, n3, c->d_red, c->d_out, c->stream);
+    if (e == cudaSuccess) e = fetch(c, 3);
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+    double lambda = 1.0;
+    if (c->h_out[1] > 0) {
+      const double l = c->h_out[0] / c->h_out[1];
+      if (l == l && l > 1e-12) lambda = l;
+    }
+    const double ynorm = lambda * sqrt(c->h_out[2]);
+    e = dev_axpy(U, -lambda, Y, n3, c->stream);
+    if (e == cudaSuccess) e = u_residual(c, U, f, JY, F);
+    const double* qa[2] = {F, U};
+    const double* qb[2] = {F, U};
+    if (e == cudaSuccess) e = dev_dots(qa, qb, 2, n3, c->d_red, c->d_out, c->stream);
+    if (e == cudaSuccess) e = fetch(c, 2);
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+    fnorm = sqrt(c->h_out[0]);
+    const double xnorm = sqrt(c->h_out[1]);
+    S.newton_its = it + 1;
+    if (!(fnorm == fnorm)) reason = -4;                 // SNES_DIVERGED_FNORM_NAN
+    else if (fnorm < o.snes_atol) reason = 2;           // SNES_CONVERGED_FNORM_ABS
+    else if (fnorm <= ttol) reason = 3;                 // SNES_CONVERGED_FNORM_RELATIVE
+    else if (ynorm < o.snes_stol * xnorm) reason = 4;   // SNES_CONVERGED_SNORM_RELATIVE
+    if (w.expired() && !reason) reason = -100;
+  }
+  if (!reason) reason = -5;  // SNES_DIVERGED_MAX_IT
+  S.reason = reason;
+  S.fnorm = fnorm;
+  S.seconds = w.seconds();
+  if (st) *st = S;
+  if (reason > 0) return VFGPU_OK;
+  if (reason == -5 || reason == -100) return VFGPU_NOT_CONVERGED;
+  return VFGPU_DIVERGED;
+}
+
+}  // extern "C"
+
+namespace vfgpu {
+
+// ---------------------------------------------------------------------------- V
+static cudaError_t v_apply64(vfgpu_ctx* c, const double* x, double* y, const uint8_t* mask,
+                             const int* skip) {
+  VApplyArgs<double> A = v_args<double>(c, x, y, mask, c->coef64, c->seam64, c->vplan64);
+  A.skip = skip;
+  return launch_v_apply<double>(A, c->vplan64, c->layers, c->stream);
+}
+static cudaError_t v_apply32(vfgpu_ctx* c, const float* x, float* y, const uint8_t* mask,
+                             const int* skip) {
+  VApplyArgs<float> A = v_args<float>(c, x, y, mask, c->coef32, c->seam32, c->vplan32);
+  A.skip = skip;
+  return launch_v_apply<float>(A, c->vplan32, c->layers, c->stream);
+}
+
+// F_V (VF_VResidual, VFMech.c:2687-2879) at v.
+static cudaError_t v_residual(vfgpu_ctx* c, const double* v, const double* b, double* tmp,
+                              double* F) {
+  cudaError_t e = v_apply64(c, v, tmp, nullptr, nullptr);
+  if (e == cudaSuccess)
+    e = dev_v_residual(tmp, b, v, c->f[VFGPU_FIELD_VIRREV], c->bcV_kind, c->vf.irrevtol,
+                       c->vf.atnum == 2, F, c->N, c->stream);
+  return e;
+}
+
+}  // namespace vfgpu
+
+extern "C" {
+
+int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_step_v: null ctx");
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "vfgpu_step_v: material not set");
+  vfgpu_solve_opts o;
+  if (o_) o = *o_; else vfgpu_default_solve_opts(&o);
+  if (o.precision != VFGPU_FP64 && o.precision != VFGPU_MIXED)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_step_v: bad precision");
+  vfgpu_solve_stats S{};
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  Watch w;
+  w.limit = o.time_limit;
+  const int64_t N = c->N;
+  const bool mixed = o.precision == VFGPU_MIXED, at2 = c->vf.atnum == 2;
+  // N-sized work vectors carved from the 3N pool
+  double *lb = c->p64[0], *ub = c->p64[0] + N, *b = c->p64[0] + 2 * N;
+  double *dinv = c->p64[1], *F = c->p64[1] + N, *Y = c->p64[1] + 2 * N;
+  double *Wt = c->p64[2], *Fw = c->p64[2] + N, *tmp = c->p64[2] + 2 * N;
+  double *R = c->p64[3], *P = c->p64[3] + N, *Wv = c->p64[3] + 2 * N;
+  double* Vy = c->p64[4];  // N: accumulated correction of the mixed solve
+  float *dinv32 = c->p32[4], *x32 = c->p32[0], *r32 = c->p32[1], *pp32 = c->p32[2], *w32 = c->p32[3];
+  float* b32 = c->p32[4] + N;
+  double* V = c->f[VFGPU_FIELD_V];
+  uint8_t* mask = c->vmask;
+  ElemArgs E = elem_args(c);
+  cudaError_t e = dev_v_bounds(c->f[VFGPU_FIELD_VIRREV], c->vf.atnum == 1, lb, ub, V, N, c->stream);
+  if (e == cudaSuccess)
+    e = launch_v_coef(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_THETA], c->f[VFGPU_FIELD_THETAREF],
+                      c->coef64, mixed ? c->coef32 : nullptr, c->stream);
+  if (e == cudaSuccess) e = launch_v_rhs(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_PRESSURE], b, c->stream);
+  if (e == cudaSuccess) e = launch_v_diag(E, c->coef64, tmp, c->stream);
+  if (e == cudaSuccess) e = dev_inv(tmp, dinv, mixed ? dinv32 : nullptr, N, c->stream);
+  if (e == cudaSuccess) e = v_residual(c, V, b, tmp, F);
+  if (e == cudaSuccess) e = dev_vi_norm2(F, V, lb, ub, N, c->d_red, c->d_out, c->stream);
+  if (e == cudaSuccess) e = fetch(c, 1);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+  double fnorm = sqrt(c->h_out[0]);
+  S.fnorm0 = fnorm;
+  const double ttol = o.snes_rtol * fnorm;
+  int reason = 0;
+  if (fnorm < o.snes_atol) reason = 2;
+  auto apply64 = [&](const double* x, double* y, const int* skip) { return v_apply64(c, x, y, mask, skip); };
+  auto apply32 = [&](const float* x, float* y, const int* skip) { return v_apply32(c, x, y, mask, skip); };
+  for (int it = 0; !reason && it < o.snes_maxit; it++) {
+    e = dev_v_mask(F, V, lb, ub, c->f[VFGPU_FIELD_VIRREV], c->bcV_kind, c->vf.irrevtol, at2, mask, N,
+                   c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+    int kits = 0, kreason = 0;
+    bool tmo = false;
+    if (!mixed) {
+      CGVecs<double> v{Y, R, P, Wv, dinv, F, mask, N};
+      rc = run_cg<double>(c, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
+                          &kreason, &tmo);
+      if (rc) return rc;
+      S.ksp_its += kits;
+    } else {
+      e = cudaMemsetAsync(Vy, 0, N * sizeof(double), c->stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(R, F, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+      if (e == cudaSuccess) e = dev_v_fix_step(R, F, mask, nullptr, N, c->stream);  // R = 0 on removed dofs
+      if (e == cudaSuccess) e = dev_znorm2(R, dinv, N, c->d_red, c->d_out, c->stream);
+      if (e == cudaSuccess) e = fetch(c, 1);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+      const double z0 = sqrt(c->h_out[0]), target = std::max(o.ksp_rtol * z0, o.ksp_atol);
+      double zr = z0;
+      kreason = zr <= target ? CG_CONVERGED_ATOL : CG_DIVERGED_ITS;
+      for (int k = 0; k < o.max_refine && zr > target; k++) {
+        e = dev_to_f32(R, b32, N, c->stream);
+        if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+        CGVecs<float> v{x32, r32, pp32, w32, dinv32, b32, mask, N};
+        const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
+        int its32 = 0, r32reason = 0;
+        rc = run_cg<float>(c, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
+                           &r32reason, &tmo);
+        if (rc) return rc;
+        S.ksp_its += its32;
+        S.refine_its += 1;
+        e = dev_add_f32(Vy, x32, N, c->stream);
+        if (e == cudaSuccess) e = v_apply64(c, Vy, tmp, mask, nullptr);
+        if (e == cudaSuccess) e = dev_axpby(R, F, -1.0, tmp, N, c->stream);
+        if (e == cudaSuccess) e = dev_v_fix_step(R, F, mask, nullptr, N, c->stream);
+        if (e == cudaSuccess) e = dev_znorm2(R, dinv, N, c->d_red, c->d_out, c->stream);
+        if (e == cudaSuccess) e = fetch(c, 1);
+        if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+        zr = sqrt(c->h_out[0]);
+        if (!(zr == zr)) {
+          kreason = CG_DIVERGED_NAN;
+          break;
+        }
+        if (tmo) break;
+      }
+      if (zr <= target) kreason = CG_CONVERGED_RTOL;
+      e = cudaMemcpyAsync(Y, Vy, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+    }
+    if (tmo) {
+      reason = -100;
+      break;
+    }
+    if (kreason < 0 && kreason != CG_DIVERGED_ITS) {
+      reason = -3;
+      break;
+    }
+    e = dev_v_fix_step(Y, F, mask, c->bcV_kind, N, c->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+    // projected back-tracking line search (SNESLINESEARCHBT with alpha = 0): accept the
+    // first lambda = 1, 1/2, ... that does not increase the inactive-set norm.
+    double lambda = 1.0, gnorm = 0.0, ynorm2 = 0.0;
+    for (int bt = 0; bt < 30; bt++) {
+      e = dev_v_project(V, Y, lambda, lb, ub, Wt, N, c->d_red, c->d_out, c->stream);
+      if (e == cudaSuccess) e = fetch(c, 1);
+      ynorm2 = c->h_out[0];
+      if (e == cudaSuccess) e = v_residual(c, Wt, b, tmp, Fw);
+      if (e == cudaSuccess) e = dev_vi_norm2(Fw, Wt, lb, ub, N, c->d_red, c->d_out, c->stream);
+      if (e == cudaSuccess) e = fetch(c, 1);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+      gnorm = sqrt(c->h_out[0]);
+      if (gnorm <= fnorm || lambda < 1e-12) break;
+      lambda *= 0.5;
+    }
+    e = cudaMemcpyAsync(V, Wt, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F, Fw, N * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    const double xnorm = sqrt(dot_host(c, V, V, N, e));
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+    fnorm = gnorm;
+    const double ynorm = sqrt(ynorm2);
+    S.newton_its = it + 1;
+    if (!(fnorm == fnorm)) reason = -4;
+    else if (fnorm < o.snes_atol) reason = 2;
+    else if (fnorm <= ttol) reason = 3;
+    else if (ynorm < o.snes_stol * xnorm) reason = 4;
+    if (w.expired() && !reason) reason = -100;
+  }
+  if (!reason) reason = -5;
+  c->v32_stale = true;
+  S.reason = reason;
+  S.fnorm = fnorm;
+  S.seconds = w.seconds();
+  if (st) *st = S;
+  if (reason > 0) return VFGPU_OK;
+  if (reason == -5 || reason == -100) return VFGPU_NOT_CONVERGED;
+  return VFGPU_DIVERGED;
+}
+
+// VFTimeStepPrepare (VFCommon.c:1132-1157): VIrrev := V, U and V take their
+// Dirichlet values; the AT1 upper bound is VIrrev (applied inside vfgpu_step_v).
+int vfgpu_time_step_prepare(vfgpu_ctx* c) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_time_step_prepare: null ctx");
+  cudaSetDevice(c->dev);
+  cudaError_t e = cudaMemcpyAsync(c->f[VFGPU_FIELD_VIRREV], c->f[VFGPU_FIELD_V], c->N * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, c->stream);
+  if (e == cudaSuccess) e = dev_apply_bc(c->f[VFGPU_FIELD_U], c->bcU_kind, c->f[VFGPU_FIELD_BCU], 3 * c->N, c->stream);
+  if (e == cudaSuccess) e = dev_apply_bc(c->f[VFGPU_FIELD_V], c->bcV_kind, nullptr, c->N, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_time_step_prepare");
+  c->v32_stale = true;
+  return VFGPU_OK;
+}
+
+// One alternate-minimisation iteration: VF_StepU then VF_StepV, and ||V - Vold||_inf
+// (the loop body of VFFractureTimeStep, VFCommon.c:1183-1202).
+int vfgpu_am_step(vfgpu_ctx* c, const vfgpu_solve_opts* o, double* errV, vfgpu_solve_stats* su,
+                  vfgpu_solve_stats* sv) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_am_step: null ctx");
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  double* vold = c->p64[8];
+  cudaError_t e = cudaMemcpyAsync(vold, c->f[VFGPU_FIELD_V], c->N * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_am_step");
+  int ru = vfgpu_step_u(c, o, su);
+  if (ru < 0) return ru;
+  int rv = vfgpu_step_v(c, o, sv);
+  if (rv < 0) return rv;
+  e = dev_absmax_diff(c->f[VFGPU_FIELD_V], vold, c->N, c->d_red, c->d_out, c->stream);
+  if (e == cudaSuccess) e = fetch(c, 1);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_am_step");
+  if (errV) *errV = c->h_out[0];
+  return std::max(ru, rv);
+}
+
+static int energies(vfgpu_ctx* c, double* cellcov) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "null ctx");
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "material not set");
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  double* cc = cellcov;
+  const bool stage = cellcov && !is_device_ptr(cellcov);
+  if (stage) cc = c->p64[8];
+  ElemArgs E = elem_args(c);
+  cudaError_t e = launch_energies(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
+                                  c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE],
+                                  c->d_red + RED_BLOCKS * 4, c->d_out, cc, c->stream);
+  if (e == cudaSuccess && stage)
+    e = cudaMemcpyAsync(cellcov, cc, c->NC * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = fetch(c, 4);
+  if (e != cudaSuccess) return cuda_fail(e, "energies");
+  return VFGPU_OK;
+}
+
+int vfgpu_u_energy(vfgpu_ctx* c, double* elastic, double* insitu, double* pressurework) {
+  int rc = energies(c, nullptr);
+  if (rc) return rc;
+  if (elastic) *elastic = c->h_out[0];
+  if (insitu) *insitu = 0.0;  // in-situ tractions are not part of this path (hasInsitu = false)
+  if (pressurework) *pressurework = c->h_out[1];
+  return VFGPU_OK;
+}
+
+int vfgpu_v_energy(vfgpu_ctx* c, double* surface) {
+  int rc = energies(c, nullptr);
+  if (rc) return rc;
+  if (surface) *surface = c->h_out[2];
+  return VFGPU_OK;
+}
+
+int vfgpu_crack_opening(vfgpu_ctx* c, double* cov, double* cellcov) {
+  int rc = energies(c, cellcov);
+  if (rc) return rc;
+  if (cov) *cov = c->h_out[3];
+  return VFGPU_OK;
+}
+
+int vfgpu_u_residual(vfgpu_ctx* c, double* F) {
+  if (!c || !F) return fail(VFGPU_ERR_INVALID, "vfgpu_u_residual: null argument");
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "vfgpu_u_residual: material not set");
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  ElemArgs E = elem_args(c);
+  double *f = c->p64[0], *tmp = c->p64[1], *Fd = c->p64[2];
+  cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
+                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+  if (e == cudaSuccess) e = u_residual(c, c->f[VFGPU_FIELD_U], f, tmp, Fd);
+  if (e == cudaSuccess) e = copy_out(c, F, Fd, 3 * c->N);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_residual");
+  return VFGPU_OK;
+}
+
+int vfgpu_v_residual(vfgpu_ctx* c, double* F) {
+  if (!c || !F) return fail(VFGPU_ERR_INVALID, "vfgpu_v_residual: null argument");
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "vfgpu_v_residual: material not set");
+  cudaSetDevice(c->dev);
+  int rc = solve_buffers(c);
+  if (rc) return rc;
+  ElemArgs E = elem_args(c);
+  const int64_t N = c->N;
+  double *b = c->p64[0], *tmp = c->p64[0] + N, *Fd = c->p64[0] + 2 * N;
+  cudaError_t e = launch_v_coef(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_THETA],
+                                c->f[VFGPU_FIELD_THETAREF], c->coef64, nullptr, c->stream);
+  if (e == cudaSuccess) e = launch_v_rhs(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_PRESSURE], b, c->stream);
+  if (e == cudaSuccess) e = v_residual(c, c->f[VFGPU_FIELD_V], b, tmp, Fd);
+  if (e == cudaSuccess) e = copy_out(c, F, Fd, N);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_v_residual");
+  return VFGPU_OK;
+}
+
+}  // extern "C"

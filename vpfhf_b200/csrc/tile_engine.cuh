@@ -1,0 +1,271 @@
+// tile_engine.cuh -- the z-marching tile schedule shared by the matrix-free
+// operators (U: 3 dofs per node, V: 1 dof per node).
+//
+// A CTA owns 32 (x, one warp) x TY (y, TY warps) elements and marches up a chunk
+// of node planes in z.  Per element layer: the next node plane of the tile's
+// 33 x (TY+1) node box is staged in shared memory, each thread computes its
+// element's 8 x NC corner contributions (Op::element), those go to shared
+// memory, and node-owner threads sum the (up to 4) xy-contributions in a fixed
+// order; the z-direction sum is carried in registers.  A z-chunk recomputes the
+// element layer below its first plane.  Nodes on the seams between xy-tiles get
+// partial sums from 2 or 4 tiles, written to a seam buffer and summed in a
+// fixed order by seam_fixup_kernel.  The result is deterministic (no atomics)
+// and independent of the chunking in z.
+//
+// Op supplies:  NC, NIN (per-node inputs staged in smem), the Args type with
+//   x/y/seamX/seamY/nx/ny/nz/ntx/nty/zc members, and
+//   load_node(A, n, vals[NIN]), element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]),
+//   finish_node(A, n, val[NC]) (writes y, applying Dirichlet rows / masks), and an
+//   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
+//   so that a queued batch of iterations costs nothing once it is done).
+#pragma once
+
+#include "common.cuh"
+
+namespace vfgpu {
+
+template <int TY> struct Tile {
+  static constexpr int BX = 33, BY = TY + 1, NT = 32 * TY;
+  static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
+};
+
+template <class Op, int TY> constexpr size_t tile_smem_bytes() {
+  using T = typename Op::T;
+  return sizeof(T) * (2 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + 8 * Op::NC * 32 * TY);
+}
+
+template <class Op, int TY, int MINB>
+__global__ void __launch_bounds__(32 * TY, MINB)
+    tile_apply_kernel(const typename Op::Args A, const LayerTable L) {
+  using T = typename Op::T;
+  using G = Tile<TY>;
+  constexpr int NC = Op::NC, NIN = Op::NIN;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sx = reinterpret_cast<T*>(smem_raw);  // [2 buf][NIN][BY][BX]
+  T* sc = sx + 2 * NIN * G::BY * G::BX;    // [8*NC][TY][32]
+  const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
+  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
+  const int X0 = bx * 32, Y0 = by * TY;
+  const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
+  const int z0 = bz * A.zc;
+  if (z0 >= nz) return;
+  if (A.skip && *A.skip) return;  // converged solve: uniform early exit, before any barrier
+  const int z1 = min(z0 + A.zc, nz);
+  const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
+
+#define SXA(buf, comp, w, l) sx[(((buf) * NIN + (comp)) * G::BY + (w)) * G::BX + (l)]
+#define SCA(q, w, l) sc[((q) * TY + (w)) * 32 + (l)]
+
+  auto load_plane = [&](int buf, int kz) {
+    for (int s = tid; s < G::BX * G::BY; s += G::NT) {
+      const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
+      T vals[NIN];
+#pragma unroll
+      for (int q = 0; q < NIN; q++) vals[q] = T(0);
+      if (X < nx && Y < ny) Op::load_node(A, node_index(X, Y, kz, nx, ny), vals);
+#pragma unroll
+      for (int q = 0; q < NIN; q++) SXA(buf, q, w, l) = vals[q];
+    }
+  };
+
+  auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC]) {
+    const bool left = (l == 0 && bx > 0), right = (l == 32 && bx < A.ntx - 1);
+    const bool bot = (w == 0 && by > 0), top = (w == TY && by < A.nty - 1);
+    if (!(left || right || bot || top)) {
+      Op::finish_node(A, node_index(X, Y, z, nx, ny), val);
+    } else if (left || right) {
+      const int i = left ? bx : bx + 1;
+      const int slot = (bot ? 2 : 0) + (left ? 1 : 0);
+      T* p = A.seamX + ((((int64_t)(i - 1) * nz + z) * ny + Y) * 4 + slot) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; c++) p[c] = val[c];
+    } else {
+      const int j = bot ? by : by + 1;
+      T* p = A.seamY + ((((int64_t)(j - 1) * nz + z) * nx + X) * 2 + (bot ? 1 : 0)) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; c++) p[c] = val[c];
+    }
+  };
+
+  T carry[G::NSLOT][NC];
+#pragma unroll
+  for (int si = 0; si < G::NSLOT; si++)
+#pragma unroll
+    for (int c = 0; c < NC; c++) carry[si][c] = T(0);
+
+  load_plane(0, kf);
+  int cur = 0;
+  for (int k = kf; k <= kl; k++) {
+    load_plane(cur ^ 1, k + 1);
+    __syncthreads();
+    const int ex = X0 + lane, ey = Y0 + wy;
+    T yc[8][NC];
+    if (ex < nex && ey < ney) {
+      T in[8][NIN];
+#pragma unroll
+      for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+          for (int i = 0; i < 2; i++) {
+            const int a = i + 2 * j + 4 * kk, buf = kk ? cur ^ 1 : cur;
+#pragma unroll
+            for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
+          }
+      Op::element(A, L, ex, ey, k, in, yc);
+    } else {
+#pragma unroll
+      for (int a = 0; a < 8; a++)
+#pragma unroll
+        for (int c = 0; c < NC; c++) yc[a][c] = T(0);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) SCA(a * NC + c, wy, lane) = yc[a][c];
+    __syncthreads();
+#pragma unroll
+    for (int si = 0; si < G::NSLOT; si++) {
+      const int s = tid + si * G::NT;
+      if (s >= G::BX * G::BY) continue;
+      const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
+      if (X >= nx || Y >= ny) continue;
+      T p0[NC], p1[NC];
+#pragma unroll
+      for (int c = 0; c < NC; c++) p0[c] = p1[c] = T(0);
+#pragma unroll
+      for (int dw = 0; dw < 2; dw++) {
+        const int ew = w - 1 + dw, j = 1 - dw;
+        if (ew < 0 || ew >= TY) continue;
+#pragma unroll
+        for (int dl = 0; dl < 2; dl++) {
+          const int el = l - 1 + dl, i = 1 - dl;
+          if (el < 0 || el >= 32) continue;
+#pragma unroll
+          for (int c = 0; c < NC; c++) {
+            p0[c] += SCA((i + 2 * j) * NC + c, ew, el);
+            p1[c] += SCA((i + 2 * j + 4) * NC + c, ew, el);
+          }
+        }
+      }
+      if (k >= z0) {
+        T val[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) val[c] = carry[si][c] + p0[c];
+        emit(l, w, X, Y, k, val);
+      }
+#pragma unroll
+      for (int c = 0; c < NC; c++) carry[si][c] = p1[c];
+    }
+    cur ^= 1;
+  }
+  if (z1 == nz) {
+#pragma unroll
+    for (int si = 0; si < G::NSLOT; si++) {
+      const int s = tid + si * G::NT;
+      if (s >= G::BX * G::BY) continue;
+      const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
+      if (X >= nx || Y >= ny) continue;
+      emit(l, w, X, Y, nz - 1, carry[si]);
+    }
+  }
+#undef SXA
+#undef SCA
+}
+
+// Sums the 2 (or 4 where an x-seam crosses a y-seam) tile partials of every
+// seam node in a fixed order and finishes the node (Op::finish_node).
+template <class Op>
+__global__ void seam_fixup_kernel(const typename Op::Args A, int TY) {
+  using T = typename Op::T;
+  constexpr int NC = Op::NC;
+  const int nx = A.nx, ny = A.ny, nz = A.nz;
+  if (A.skip && *A.skip) return;
+  const int64_t nxs = (int64_t)(A.ntx - 1) * nz * ny;
+  const int64_t nys = (int64_t)(A.nty - 1) * nz * nx;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nxs + nys;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    T val[NC];
+    int64_t n;
+    if (t < nxs) {
+      const int Y = (int)(t % ny);
+      const int64_t r = t / ny;
+      const int z = (int)(r % nz), i = (int)(r / nz) + 1;
+      const bool onY = (Y % TY == 0) && (Y > 0) && (Y / TY < A.nty);
+      const T* p = A.seamX + t * 4 * NC;
+#pragma unroll
+      for (int c = 0; c < NC; c++)
+        val[c] = onY ? ((p[c] + p[NC + c]) + p[2 * NC + c]) + p[3 * NC + c] : p[c] + p[NC + c];
+      n = node_index(32 * i, Y, z, nx, ny);
+    } else {
+      const int64_t u = t - nxs;
+      const int X = (int)(u % nx);
+      const int64_t r = u / nx;
+      const int z = (int)(r % nz), j = (int)(r / nz) + 1;
+      if (X % 32 == 0 && X > 0 && X / 32 < A.ntx) continue;
+      const T* p = A.seamY + u * 2 * NC;
+#pragma unroll
+      for (int c = 0; c < NC; c++) val[c] = p[c] + p[NC + c];
+      n = node_index(X, TY * j, z, nx, ny);
+    }
+    Op::finish_node(A, n, val);
+  }
+}
+
+// Launch plan: xy tiles of 32 x ty elements, z-chunks of zc planes (chosen to fill
+// the SMs in whole waves), and the seam buffer sizes in elements of T.
+struct TilePlan {
+  int ty, ntx, nty, zc, nzc;
+  size_t seamX, seamY;
+};
+
+inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_sm, int num_sms) {
+  TilePlan p;
+  p.ty = ty;
+  p.ntx = (nx - 1 + 31) / 32;
+  p.nty = (ny - 1 + ty - 1) / ty;
+  const int slots = num_sms * ctas_per_sm, tiles = p.ntx * p.nty;
+  double best = 1e300;
+  p.zc = nz;
+  for (int nzc = 1; nzc <= nz; nzc++) {
+    const int zc = (nz + nzc - 1) / nzc, chunks = (nz + zc - 1) / zc;
+    const int waves = (tiles * chunks + slots - 1) / slots;
+    const double cost = (double)waves * (zc + 1 + 2);  // +1 halo layer, +2 fill/drain
+    if (cost < best - 1e-9) {
+      best = cost;
+      p.zc = zc;
+    }
+  }
+  p.nzc = (nz + p.zc - 1) / p.zc;
+  p.seamX = (size_t)(p.ntx - 1) * nz * ny * 4 * nc;
+  p.seamY = (size_t)(p.nty - 1) * nz * nx * 2 * nc;
+  return p;
+}
+
+template <class Op, int TY, int MINB>
+cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const LayerTable& L,
+                              cudaStream_t s) {
+  A.ntx = p.ntx;
+  A.nty = p.nty;
+  A.zc = p.zc;
+  constexpr size_t smem = tile_smem_bytes<Op, TY>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY);
+  tile_apply_kernel<Op, TY, MINB><<<grid, block, smem, s>>>(A, L);
+  const int64_t nseam = (int64_t)(p.ntx - 1) * A.nz * A.ny + (int64_t)(p.nty - 1) * A.nz * A.nx;
+  if (nseam > 0) {
+    const int threads = 256;
+    const int blocks = (int)((nseam + threads - 1) / threads < 148 * 8 ? (nseam + threads - 1) / threads
+                                                                       : 148 * 8);
+    seam_fixup_kernel<Op><<<blocks, threads, 0, s>>>(A, TY);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace vfgpu

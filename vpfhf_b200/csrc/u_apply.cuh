@@ -18,16 +18,8 @@
 // against 8,856 for the per-Gauss-point form and ~233k for the element-matrix
 // form the reference uses.
 //
-// Tiling.  A CTA owns a tile of 32 (x, one warp) x TY (y, TY warps) elements
-// and marches up a chunk of node planes in z.  Each layer: the next node plane
-// of the tile's node box (33 x (TY+1) nodes: u and v) is staged in shared
-// memory, every thread computes its element, the 8x3 corner contributions go to
-// shared memory, and node-owner threads sum the (up to 4) xy-contributions in a
-// fixed order -- deterministic, no atomics.  The z-direction sum is carried in
-// registers from one layer to the next.  A z-chunk recomputes the one element
-// layer below it (halo).  Nodes on the seam lines between xy-tiles receive
-// partial sums from 2 or 4 tiles; those partials go to a seam buffer and a
-// second kernel (seam_fixup) adds them in a fixed order.
+// The schedule (tiles, z-march, seams) is in tile_engine.cuh, the operator
+// policy in ops.cuh.
 //
 // Dirichlet rows (MatZeroRowsStencil, VFCartFE.c:1293, quirk: rows only): on a
 // BC dof the output is y = x; BC columns are kept.
@@ -46,6 +38,7 @@ template <typename T> struct UApplyArgs {
   const float* __restrict__ cellE;    // per-cell Young's modulus (or null)
   T* __restrict__ seamX;              // x-seam partials [(ntx-1)][nz][ny][4][3]
   T* __restrict__ seamY;              // y-seam partials [(nty-1)][nz][nx][2][3]
+  const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   int nx, ny, nz;
   int ntx, nty, zc;                   // tiles in x, y; owned node planes per z-chunk
   T ihx, ihy, ihz, vol, eta;
@@ -227,16 +220,6 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
           y[i + 2 * j + 4 * k][c] = (ax_ + ay_) + az_;
         }
   }
-}
-
-// Launch geometry shared by the host launcher and the kernels.
-template <int TY> struct UTile {
-  static constexpr int BX = 33, BY = TY + 1, NT = 32 * TY;
-  static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
-};
-
-template <typename T, int TY> constexpr size_t u_apply_smem_bytes() {
-  return sizeof(T) * (2 * 4 * UTile<TY>::BX * UTile<TY>::BY + 24 * 32 * TY);
 }
 
 }  // namespace vfgpu

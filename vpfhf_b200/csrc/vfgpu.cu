@@ -103,7 +103,7 @@ int ensure_v32(vfgpu_ctx* c) {
 }
 
 template <typename T>
-UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const UPlan& p) {
+UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p) {
   UApplyArgs<T> A{};
   A.x = x;
   A.v = v;
@@ -124,9 +124,9 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   return A;
 }
 template UApplyArgs<double> u_args<double>(vfgpu_ctx*, const double*, const double*, double*,
-                                           double*, const UPlan&);
+                                           double*, const TilePlan&);
 template UApplyArgs<float> u_args<float>(vfgpu_ctx*, const float*, const float*, float*, float*,
-                                         const UPlan&);
+                                         const TilePlan&);
 
 }  // namespace vfgpu
 
@@ -139,6 +139,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   if (!c) return VFGPU_OK;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  free_solver(c);
   for (auto& p : c->f) cudaFree(p);
   void* bufs[] = {c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
@@ -178,6 +179,8 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   c->NC = (int64_t)(g->nx - 1) * (g->ny - 1) * (g->nz - 1);
   c->plan64 = u_plan(c->nx, c->ny, c->nz, 8, c->nsm);
   c->plan32 = u_plan(c->nx, c->ny, c->nz, 4, c->nsm);
+  c->vplan64 = v_plan(c->nx, c->ny, c->nz, 8, c->nsm);
+  c->vplan32 = v_plan(c->nx, c->ny, c->nz, 4, c->nsm);
 #define ALLOC(ptr, bytes)                                  \
   do {                                                     \
     e = cudaMalloc((void**)&(ptr), (size_t)(bytes));       \
@@ -377,6 +380,36 @@ int vfgpu_u_apply(vfgpu_ctx* c, int precision, const double* x, double* y) {
   if (e == cudaSuccess && !ydev) e = copy_out(c, y, yd, n3);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply");
+  return VFGPU_OK;
+}
+
+int vfgpu_u_apply_dev(vfgpu_ctx* c, int precision, const void* x, void* y) {
+  if (!c || !x || !y) return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_dev: null argument");
+  if (precision != VFGPU_FP64 && precision != VFGPU_MIXED)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_dev: bad precision %d", precision);
+  if (!c->have_mat) return fail(VFGPU_ERR_STATE, "vfgpu_u_apply_dev: material not set");
+  if (!is_device_ptr(x) || !is_device_ptr(y))
+    return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_dev: x and y must be device pointers");
+  cudaSetDevice(c->dev);
+  cudaError_t e;
+  if (precision == VFGPU_FP64) {
+    e = launch_u_apply<double>(u_args<double>(c, (const double*)x, c->f[VFGPU_FIELD_V], (double*)y,
+                                              c->seam64, c->plan64),
+                               c->plan64, c->layers, c->stream);
+  } else {
+    int st = ensure_v32(c);
+    if (st) return st;
+    e = launch_u_apply<float>(u_args<float>(c, (const float*)x, c->V32, (float*)y, c->seam32,
+                                            c->plan32),
+                              c->plan32, c->layers, c->stream);
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_dev");
+  return VFGPU_OK;
+}
+
+int vfgpu_get_stream(vfgpu_ctx* c, void** stream) {
+  if (!c || !stream) return fail(VFGPU_ERR_INVALID, "vfgpu_get_stream: null argument");
+  *stream = (void*)c->stream;
   return VFGPU_OK;
 }
 
