@@ -1,0 +1,353 @@
+"""Benchmark of the U operator (matvec GDOF/s) and the AM step on the 129^3
+pressurized penny crack (the FP64-vs-mixed configuration), one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A "step" is one application of the degraded elasticity operator K(v) to a
+3N-vector (3 x 129^3 = 6,440,067 dofs) with the inputs resident in HBM; the L2
+is flushed between timed steps.  `e2e` times the same step through the C ABI
+(vfgpu_u_apply) from pinned host memory, copies included.  The AM-step rate
+(StepU + StepV to tolerance, FP64 and mixed) is reported beside it.
+
+Multi-GPU: the operator does not shard in this build ("replicas only"): every
+rank runs its own copy of the workload and `value` is the total over ranks.
+
+--impl reference times the reference's CPU algorithm for the same metric: the
+assembled AIJ (CSR, 81 nnz/row) sparse matrix-vector product that KSPCG runs
+(restated in the oracle, oracle/vf_oracle.c) on all host cores, on a bounded
+sample (the 65^3 grid, whose matrix is far larger than the host caches).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_EDGE, L_BOX = 129, 4.0
+WORKLOAD = "penny crack 129^3 (6.44M U dofs), E=1e10 nu=0.25 Gc=100 AT1 eps=2h eta=1e-8 p=1e6"
+
+
+def _rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while active."""
+
+    def __init__(self, gpu):
+        self.gpu, self.proc, self.path = gpu, None, None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9:
+                    rows.append(f)
+        except Exception:
+            pass
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def setup_problem(vg, n):
+    """The 129^3 penny crack at its first AM iterate (v from VFPennyCrackBuildVAT1)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    h = L_BOX / (n - 1)
+    ctx = vg.VFContext((n, n, n), (L_BOX,) * 3, dict(E=1e10, nu=0.25, Gc=100.0), epsilon=2 * h,
+                       eta=1e-8, atnum=1, pressurize=True)
+    ctx.set_bc(vg.rollers())
+    v0 = vg.penny_crack_v((n, n, n), (L_BOX,) * 3, (L_BOX / 2,) * 3, 0.4, epsilon=2 * h)
+    ctx.set_field("V", v0)
+    ctx.set_field("pressure", np.full(ctx.N, 1e6))
+    ctx.time_step_prepare()
+    return ctx, v0
+
+
+def fp_peak_tflops(torch, dtype):
+    """Measured FMA throughput of the CUDA cores (a dependent-chain-free FMA kernel)."""
+    from vpfhf_b200 import _abi
+    import ctypes as C
+    L = _abi.lib()
+    if not hasattr(L, "vfgpu_fma_peak"):
+        return None
+    L.vfgpu_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
+    L.vfgpu_fma_peak.restype = C.c_int
+    out = C.c_double()
+    if L.vfgpu_fma_peak(8 if dtype == "f64" else 4, C.byref(out)) != 0:
+        return None
+    return out.value
+
+
+def run_gpu(args):
+    import torch
+    import vpfhf_b200 as vg
+
+    rank, world, local = _rank()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    n = args.grid
+    ctx, v0 = setup_problem(vg, n)
+    N3 = 3 * ctx.N
+    s = ctx.torch_stream()
+    rng = np.random.default_rng(1000 + rank)
+    x_host = rng.standard_normal(N3) * 1e-4
+    x = torch.from_numpy(x_host).cuda()
+    y = torch.empty_like(x)
+    x32, y32 = x.float(), torch.empty(N3, dtype=torch.float32, device="cuda")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    torch.cuda.synchronize()
+
+    def timed_applies(prec, xi, yi, K, W):
+        for _ in range(W):
+            ctx.u_apply_dev(xi, yi, prec)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(K)]
+        barrier()
+        for a, b in ev:
+            with torch.cuda.stream(s):
+                flush.zero_()
+            a.record(s)
+            ctx.u_apply_dev(xi, yi, prec)
+            b.record(s)
+        torch.cuda.synchronize()
+        barrier()
+        return [a.elapsed_time(b) for a, b in ev]
+
+    with ClockSampler(local) as clk:
+        t64 = timed_applies(vg.FP64, x, y, args.steps, args.warmup)
+    clocks = clk.summary()
+    t32 = timed_applies(vg.MIXED, x32, y32, args.steps, args.warmup)
+    ms64 = float(np.mean(t64))
+    ms32 = float(np.mean(t32))
+    if dist:
+        m = torch.tensor([ms64, ms32], dtype=torch.float64, device="cuda")
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms64, ms32 = m.tolist()
+
+    if args.only_apply:
+        if rank == 0:
+            print(json.dumps({"grid": n, "ms_fp64": ms64, "ms_fp32": ms32, "clocks": clocks}))
+        ctx.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    # e2e through the C ABI from pinned host memory (H2D of x, D2H of y every step)
+    xp = torch.empty(N3, dtype=torch.float64, pin_memory=True)
+    xp.numpy()[:] = x_host
+    yp = torch.empty(N3, dtype=torch.float64, pin_memory=True)
+    xpn, ypn = xp.numpy(), yp.numpy()
+    for _ in range(args.warmup):
+        ctx.u_apply(xpn, vg.FP64, out=ypn)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.u_apply(xpn, vg.FP64, out=ypn)
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    if dist:
+        m = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        e2e_ms = m.item()
+
+    # AM steps (StepU + StepV to tolerance) from the penny-crack start, FP64 and mixed
+    am = {}
+    for prec in ("fp64", "mixed"):
+        ctx.set_field("U", np.zeros(N3))
+        ctx.set_field("V", v0)
+        ctx.time_step_prepare()
+        times, energies = [], []
+        for it in range(args.am_steps):
+            barrier()
+            t0 = time.perf_counter()
+            rc, err, su, sv = ctx.am_step(dict(precision=prec))
+            barrier()
+            times.append(time.perf_counter() - t0)
+            el, _, pw = ctx.u_energy()
+            energies.append((el, pw, ctx.v_energy(), ctx.crack_opening()))
+        am[prec] = dict(s_per_step=float(np.mean(times[1:] if len(times) > 1 else times)),
+                        energies=energies, last_kspU=su["ksp_its"], last_kspV=sv["ksp_its"])
+    rel = max(abs(a - b) / abs(b) for ea, eb in zip(am["mixed"]["energies"], am["fp64"]["energies"])
+              for a, b in zip(ea, eb))
+
+    if rank != 0:
+        ctx.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peaks = _peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    nodes, cells = ctx.N, (n - 1) ** 3
+    # algorithmic traffic per apply: read u (24 B) + v (8 B), write y (24 B) per node
+    alg_bytes = 56.0 * nodes
+    ops_el = 1400  # arithmetic operations per element of the modal apply (u_apply.cuh)
+    f64_peak = fp_peak_tflops(torch, "f64")
+    value = N3 * world / (ms64 * 1e-3) / 1e9
+    line = {
+        "metric": "GDOF/s matvec",
+        "value": round(value, 3),
+        "unit": "GDOF/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms64, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded random u; v from the penny-crack construction)",
+        "config": {"workload": WORKLOAD, "grid": [n, n, n], "u_dofs": N3,
+                   "parallelism": f"replicas x{world}", "l2": "flushed between timed steps"},
+        "e2e": {"value": round(N3 * world / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GDOF/s",
+                "h2d_bytes_per_step": N3 * 8, "d2h_bytes_per_step": N3 * 8},
+        "gpu_launches": 2 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (ms64 * 1e-3) / 1e9, 1),
+                     "peak": hbm, "unit": "GB/s",
+                     "frac": round(alg_bytes / (ms64 * 1e-3) / 1e9 / hbm, 4),
+                     "traffic": None,
+                     "note": "compute-bound operator; see compute_roofline"},
+        "compute_roofline": {
+            "pipe": "fp64 CUDA cores",
+            "ops_per_element": ops_el,
+            "achieved_tops": round(cells * ops_el / (ms64 * 1e-3) / 1e12, 3),
+            "peak_tops_measured": f64_peak,
+            "frac": (round(cells * ops_el / (ms64 * 1e-3) / 1e12 / f64_peak, 3)
+                     if f64_peak else None),
+            "per_gauss_point_equiv_tflops": round(cells * 8856 / (ms64 * 1e-3) / 1e12, 2)},
+        "mixed": {"value": round(N3 * world / (ms32 * 1e-3) / 1e9, 3), "unit": "GDOF/s",
+                  "ms_per_step": round(ms32, 4), "dtype": "f32"},
+        "am_steps_per_s": {"fp64": round(1.0 / am["fp64"]["s_per_step"], 3),
+                           "mixed": round(1.0 / am["mixed"]["s_per_step"], 3),
+                           "mixed_vs_fp64_max_rel_energy_diff": rel,
+                           "steps": args.am_steps,
+                           "kspU_last": {k: am[k]["last_kspU"] for k in am}},
+        "clocks": clocks,
+    }
+    if args.cpu_baseline:
+        line["cpu_baseline"] = cpu_reference(args, quick=True)
+    print(json.dumps(line))
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def cpu_reference(args, quick=False):
+    """The reference's KSP matvec (AIJ SpMV, restated in the oracle) on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import vforacle as vo
+    n = 65
+    h = L_BOX / (n - 1)
+    cores = os.cpu_count() or 1
+    o = vo.Oracle((n, n, n), (L_BOX,) * 3, E=1e10, nu=0.25, Gc=100.0, epsilon=2 * h, eta=1e-8,
+                  atnum=1, nthreads=cores)
+    v = o.penny_v((L_BOX / 2,) * 3, 0.4)
+    mask, _ = o.bc(vo.rollers_face())
+    csr = o.u_csr(v, mask)
+    x = np.random.default_rng(7).standard_normal(3 * o.N)
+    reps = 3 if quick else max(3, args.steps)
+    o.csr_spmv(csr, x, cores)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        o.csr_spmv(csr, x, cores)
+    dt = (time.perf_counter() - t0) / reps
+    return {"value": round(3 * o.N / dt / 1e9, 4), "unit": "GDOF/s", "cores": cores,
+            "kind": "port",
+            "sample": f"AIJ (CSR, 81 nnz/row) SpMV of K(v) on the 65^3 penny-crack grid "
+                      f"({3 * o.N} dofs, {len(csr[1])} nonzeros), {reps} products"}
+
+
+def run_reference(args):
+    rank, world, _ = _rank()
+    if rank != 0:
+        return
+    cb = cpu_reference(args)
+    print(json.dumps({
+        "impl": "reference", "metric": "GDOF/s matvec", "value": cb["value"], "unit": "GDOF/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "GDOF/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--am-steps", type=int, default=3)
+    ap.add_argument("--impl", default="vfgpu", choices=["vfgpu", "reference"])
+    ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--grid", type=int, default=N_EDGE, help="nodes per axis (profiling runs)")
+    ap.add_argument("--only-apply", action="store_true",
+                    help="time the operator applications only (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

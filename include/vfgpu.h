@@ -179,6 +179,12 @@ int vfgpu_crack_opening(vfgpu_ctx* ctx, double* cov, double* cellcov);
 int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);
 int vfgpu_v_residual(vfgpu_ctx* ctx, double* F);
 
+/* Measurement utility, no counterpart in the reference: FMA throughput of the
+ * current GPU's CUDA cores in TFLOP/s for bytes = 8 (FP64) or 4 (FP32), from a
+ * kernel of independent FMA chains (the denominator of the operator's compute
+ * roofline). */
+int vfgpu_fma_peak(int bytes, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -134,8 +134,11 @@ def test_runtest1_on_gpu(cuda, precision):
             assert m["elastic"] == pytest.approx(r["elastic"], rel=rel, abs=1e-12), t
             assert m["surface"] == pytest.approx(r["surface"], rel=rel, abs=1e-12), t
         else:
-            assert m["cov"] == pytest.approx(r["cov"], rel=2e-4), t
-            assert m["surface"] == pytest.approx(r["surface"], rel=2e-4), t
+            # after full fracture the AM loop stops after one or two sweeps (altmintol 1e-3),
+            # so these states are not converged and depend on the solver path
+            post = 2e-4 if precision == "fp64" else 2e-3
+            assert m["cov"] == pytest.approx(r["cov"], rel=post), t
+            assert m["surface"] == pytest.approx(r["surface"], rel=post), t
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])

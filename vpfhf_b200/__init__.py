@@ -232,6 +232,33 @@ def solve_opts(**kw):
     return o
 
 
+def penny_crack_v(n, l, center, r, theta=0.0, phi=0.0, thickness=0.0, epsilon=0.2, atnum=1):
+    """Initial phase field of one penny-shaped crack, VFPennyCrackBuildVAT1/2
+    (VFCracks.c:136-227) with the distance of VFDistanceToPennyCrack (VFCracks.c:101-126):
+    disk normal (cos th sin ph, sin th sin ph, cos ph) in degrees; v = 0 within
+    thickness/2 of the disk; AT1 profile d/eps (1 - d/(4 eps)) for d < 2 eps, AT2
+    1 - exp(-d/(2 eps)).  Several cracks combine by pointwise minimum
+    (VFFieldsInitialize, VFCommon.c:829-857)."""
+    nx, ny, nz = n
+    x = [np.arange(k) * (L / (k - 1)) for k, L in zip(n, l)]
+    Z, Y, X = np.meshgrid(x[2], x[1], x[0], indexing="ij")
+    t, p = np.deg2rad(theta), np.deg2rad(phi)
+    nrm = (np.cos(t) * np.sin(p), np.sin(t) * np.sin(p), np.cos(p))
+    dx, dy, dz = X - center[0], Y - center[1], Z - center[2]
+    xn = dx * nrm[0] + dy * nrm[1] + dz * nrm[2]
+    tx, ty, tz = dx - xn * nrm[0], dy - xn * nrm[1], dz - xn * nrm[2]
+    lt = np.sqrt(tx * tx + ty * ty + tz * tz)
+    d = np.where(lt <= r, np.abs(xn), np.sqrt(xn ** 2 + (lt - r) ** 2)) - thickness / 2.0
+    if r == 0:
+        return np.ones(nx * ny * nz)
+    if atnum == 1:
+        v = np.where(d <= 0, 0.0, np.where(d < 2 * epsilon, d / epsilon * (1 - 0.25 * d / epsilon),
+                                          1.0))
+    else:
+        v = np.where(d <= 0, 0.0, 1.0 - np.exp(-np.maximum(d, 0) / 2 / epsilon))
+    return np.ascontiguousarray(v).reshape(-1)
+
+
 def bc_vector(n, bcs):
     """VecSetFromBC (VFCartFE.c:279-491): the vector of Dirichlet values of a VFBC array
     (face values in face order X0,X1,Y0,Y1,Z0,Z1, then vertex values); dof = len(bcs)."""

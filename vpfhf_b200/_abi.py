@@ -90,6 +90,7 @@ _SIGS = {
     "vfgpu_crack_opening": [C.c_void_p, C.POINTER(C.c_double), C.c_void_p],
     "vfgpu_u_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_v_residual": [C.c_void_p, C.c_void_p],
+    "vfgpu_fma_peak": [C.c_int, C.POINTER(C.c_double)],
 }
 _VOID_SIGS = {"vfgpu_default_solve_opts": [C.POINTER(SolveOpts)]}
 
