@@ -179,6 +179,29 @@ int vfgpu_crack_opening(vfgpu_ctx* ctx, double* cov, double* cellcov);
 int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);
 int vfgpu_v_residual(vfgpu_ctx* ctx, double* F);
 
+/* No counterpart in the reference.  y = K(v) x like vfgpu_u_apply (FP64, one
+ * homogeneous material, Dirichlet rows from bcbits), for callers that cannot
+ * allocate device memory while they run -- e.g. a matrix-shell callback inside
+ * an external solver whose host program owns every device buffer, or a loop
+ * that cannot afford cudaMalloc's device-wide synchronisation.  No ctx is
+ * needed and nothing is allocated: v (N), x and y (3N) and bcbits (N bytes,
+ * bit c set = component c of the node is Dirichlet; may be NULL) are device
+ * arrays of the current device, the work is queued on `stream` (a
+ * cudaStream_t, NULL = legacy default stream) and the call returns without
+ * waiting.  The only scratch (the seam partial sums) is a fixed 32 MiB array
+ * inside the library (VFGPU_NOALLOC_SCRATCH_DOUBLES doubles; every GPU that
+ * loads the library holds it until exit); grids whose seams need more are
+ * rejected with VFGPU_ERR_INVALID (129^3 fits, 161^3 does not).  The first call
+ * on a device looks up the array's device address (cudaGetSymbolAddress): make
+ * that first call before any stream capture.  All calls share the one array, so
+ * calls whose work overlaps on the GPU (different streams, different threads)
+ * race; serialise them.  Every scratch slot read is written earlier in the same
+ * call, so no clearing is needed between calls. */
+#define VFGPU_NOALLOC_SCRATCH_DOUBLES 4194304
+int vfgpu_u_apply_noalloc(const vfgpu_grid* grid, const vfgpu_matprop* mp, double eta,
+                          const double* v, const unsigned char* bcbits, const double* x,
+                          double* y, void* stream);
+
 /* Measurement utility, no counterpart in the reference: FMA throughput of the
  * current GPU's CUDA cores in TFLOP/s for bytes = 8 (FP64) or 4 (FP32), from a
  * kernel of independent FMA chains (the denominator of the operator's compute

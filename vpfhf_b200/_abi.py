@@ -91,6 +91,8 @@ _SIGS = {
     "vfgpu_u_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_v_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_fma_peak": [C.c_int, C.POINTER(C.c_double)],
+    "vfgpu_u_apply_noalloc": [C.POINTER(Grid), C.POINTER(MatProp), C.c_double, C.c_void_p,
+                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
 }
 _VOID_SIGS = {"vfgpu_default_solve_opts": [C.POINTER(SolveOpts)]}
 
