@@ -15,17 +15,29 @@
 #include "tile_engine.cuh"
 #include "u_apply.cuh"
 
+// Per-precision choice of the z-moment accumulation in u_element (see u_apply.cuh).
+#ifndef VFGPU_UZDIRECT_F64
+#define VFGPU_UZDIRECT_F64 0
+#endif
+#ifndef VFGPU_UZDIRECT_F32
+#define VFGPU_UZDIRECT_F32 0
+#endif
+
 namespace vfgpu {
+
+template <typename T> constexpr bool uzdirect() {
+  return sizeof(T) == 8 ? VFGPU_UZDIRECT_F64 != 0 : VFGPU_UZDIRECT_F32 != 0;
+}
 
 template <typename T_> struct UOp {
   using T = T_;
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4;
-  __device__ __forceinline__ static void load_node(const Args& A, int64_t n, T (&v)[NIN]) {
-    v[0] = A.x[3 * n];
-    v[1] = A.x[3 * n + 1];
-    v[2] = A.x[3 * n + 2];
-    v[3] = A.v[n];
+  __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
+    src[0] = A.x + 3 * n;
+    src[1] = A.x + 3 * n + 1;
+    src[2] = A.x + 3 * n + 2;
+    src[3] = A.v + n;
   }
   __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
                                                  int ey, int ez, const T (&in)[8][NIN],
@@ -48,7 +60,7 @@ template <typename T_> struct UOp {
       lam = T(L.lambda[layer]);
       mu = T(L.mu[layer]);
     }
-    u_element<T>(xn, vn, lam, mu, A.eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+    u_element<T, uzdirect<T>()>(xn, vn, lam, mu, A.eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
     const unsigned b = A.bc ? A.bc[n] : 0u;
@@ -58,9 +70,11 @@ template <typename T_> struct UOp {
 };
 
 template <typename T> struct VApplyArgs {
-  const T* __restrict__ x;            // N input
+  const T* __restrict__ x;            // N input; must be 0 on masked dofs (the reduced-space
+                                      // CG keeps its directions 0 there), which makes the
+                                      // masked columns drop out
   T* __restrict__ y;                  // N output
-  const uint8_t* __restrict__ mask;   // N: nonzero => dof removed (x -> 0, y = 0); or null
+  const uint8_t* __restrict__ mask;   // N: nonzero => dof removed (y = 0); or null
   const T* __restrict__ coef;         // 27 per cell: w_g (2 W_g [+ A/eps]), cell-major
   const uint8_t* __restrict__ elayer; // nz-1 or null
   T* __restrict__ seamX;
@@ -166,8 +180,8 @@ template <typename T_> struct VOp {
   using T = T_;
   using Args = VApplyArgs<T>;
   static constexpr int NC = 1, NIN = 1;
-  __device__ __forceinline__ static void load_node(const Args& A, int64_t n, T (&v)[NIN]) {
-    v[0] = (A.mask && A.mask[n]) ? T(0) : A.x[n];
+  __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
+    src[0] = A.x + n;
   }
   __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
                                                  int ey, int ez, const T (&in)[8][NIN],

@@ -2,8 +2,9 @@
 // operators (U: 3 dofs per node, V: 1 dof per node).
 //
 // A CTA owns 32 (x, one warp) x TY (y, TY warps) elements and marches up a chunk
-// of node planes in z.  Per element layer: the next node plane of the tile's
-// 33 x (TY+1) node box is staged in shared memory, each thread computes its
+// of node planes in z.  Per element layer: node planes of the tile's 33 x (TY+1)
+// node box stream through a 3-slot shared-memory ring by asynchronous copies
+// (cp.async, two planes ahead), each thread computes its
 // element's 8 x NC corner contributions (Op::element), those go to shared
 // memory, and node-owner threads sum the (up to 4) xy-contributions in a fixed
 // order; the z-direction sum is carried in registers.  A z-chunk recomputes the
@@ -14,7 +15,8 @@
 //
 // Op supplies:  NC, NIN (per-node inputs staged in smem), the Args type with
 //   x/y/seamX/seamY/nx/ny/nz/ntx/nty/zc members, and
-//   load_node(A, n, vals[NIN]), element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]),
+//   node_src(A, n, src[NIN]) (global addresses of a node's inputs),
+//   element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]),
 //   finish_node(A, n, val[NC]) (writes y, applying Dirichlet rows / masks), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
 //   so that a queued batch of iterations costs nothing once it is done).
@@ -29,10 +31,28 @@ template <int TY> struct Tile {
   static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
 };
 
+// Shared memory: a ring of 3 node planes [3][NIN][BY][BX] (planes k, k+1 in use,
+// k+2 in flight) and 2 buffers of element corner contributions [2][8*NC][TY][32].
 template <class Op, int TY> constexpr size_t tile_smem_bytes() {
   using T = typename Op::T;
-  return sizeof(T) * (2 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + 8 * Op::NC * 32 * TY);
+  return sizeof(T) * (3 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + 2 * 8 * Op::NC * 32 * TY);
 }
+
+// Asynchronous global -> shared copy of one 4- or 8-byte value (LDGSTS); with
+// valid == false nothing is read and the destination is zero-filled.
+template <typename T>
+__device__ __forceinline__ void cp_async_val(T* smem, const T* gmem, bool valid) {
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "4- or 8-byte values");
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  if constexpr (sizeof(T) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 8 : 0) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gmem),
+                 "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <class Op, int TY, int MINB>
 __global__ void __launch_bounds__(32 * TY, MINB)
@@ -41,8 +61,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   using G = Tile<TY>;
   constexpr int NC = Op::NC, NIN = Op::NIN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sx = reinterpret_cast<T*>(smem_raw);  // [2 buf][NIN][BY][BX]
-  T* sc = sx + 2 * NIN * G::BY * G::BX;    // [8*NC][TY][32]
+  T* sx = reinterpret_cast<T*>(smem_raw);  // [3 ring][NIN][BY][BX]
+  T* sc = sx + 3 * NIN * G::BY * G::BX;    // [2][8*NC][TY][32]
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
   const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
   const int X0 = bx * 32, Y0 = by * TY;
@@ -54,18 +74,19 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
 
 #define SXA(buf, comp, w, l) sx[(((buf) * NIN + (comp)) * G::BY + (w)) * G::BX + (l)]
-#define SCA(q, w, l) sc[((q) * TY + (w)) * 32 + (l)]
+#define SCA(b, q, w, l) sc[(((b) * 8 * NC + (q)) * TY + (w)) * 32 + (l)]
 
-  auto load_plane = [&](int buf, int kz) {
+  // issue the asynchronous copies of node plane kz into ring slot buf (one group)
+  auto fetch_plane = [&](int buf, int kz) {
     for (int s = tid; s < G::BX * G::BY; s += G::NT) {
       const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
-      T vals[NIN];
+      const bool in = X < nx && Y < ny;
+      const T* src[NIN];
+      Op::node_src(A, in ? node_index(X, Y, kz, nx, ny) : 0, src);
 #pragma unroll
-      for (int q = 0; q < NIN; q++) vals[q] = T(0);
-      if (X < nx && Y < ny) Op::load_node(A, node_index(X, Y, kz, nx, ny), vals);
-#pragma unroll
-      for (int q = 0; q < NIN; q++) SXA(buf, q, w, l) = vals[q];
+      for (int q = 0; q < NIN; q++) cp_async_val(&SXA(buf, q, w, l), src[q], in);
     }
+    cp_async_commit();
   };
 
   auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC]) {
@@ -93,11 +114,16 @@ __global__ void __launch_bounds__(32 * TY, MINB)
 #pragma unroll
     for (int c = 0; c < NC; c++) carry[si][c] = T(0);
 
-  load_plane(0, kf);
-  int cur = 0;
+  // Pipeline: planes kf, kf+1 resident before the first layer; during layer k the
+  // copy of plane k+2 is in flight; one barrier per layer publishes plane k+2 and
+  // the corner contributions of layer k together.
+  fetch_plane(0, kf);
+  fetch_plane(1, kf + 1);
+  cp_async_wait_all();
+  __syncthreads();
+  if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
   for (int k = kf; k <= kl; k++) {
-    load_plane(cur ^ 1, k + 1);
-    __syncthreads();
+    const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = (k - kf) & 1;
     const int ex = X0 + lane, ey = Y0 + wy;
     T yc[8][NC];
     if (ex < nex && ey < ney) {
@@ -108,7 +134,7 @@ __global__ void __launch_bounds__(32 * TY, MINB)
         for (int j = 0; j < 2; j++)
 #pragma unroll
           for (int i = 0; i < 2; i++) {
-            const int a = i + 2 * j + 4 * kk, buf = kk ? cur ^ 1 : cur;
+            const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
 #pragma unroll
             for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
           }
@@ -122,8 +148,10 @@ __global__ void __launch_bounds__(32 * TY, MINB)
 #pragma unroll
     for (int a = 0; a < 8; a++)
 #pragma unroll
-      for (int c = 0; c < NC; c++) SCA(a * NC + c, wy, lane) = yc[a][c];
-    __syncthreads();
+      for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, wy, lane) = yc[a][c];
+    cp_async_wait_all();  // this thread's copies of plane k+2 have landed
+    __syncthreads();      // ... and everyone's; corner contributions of layer k visible
+    if (k + 3 <= kl + 1) fetch_plane(r0, k + 3);  // plane k is no longer read
 #pragma unroll
     for (int si = 0; si < G::NSLOT; si++) {
       const int s = tid + si * G::NT;
@@ -143,8 +171,8 @@ __global__ void __launch_bounds__(32 * TY, MINB)
           if (el < 0 || el >= 32) continue;
 #pragma unroll
           for (int c = 0; c < NC; c++) {
-            p0[c] += SCA((i + 2 * j) * NC + c, ew, el);
-            p1[c] += SCA((i + 2 * j + 4) * NC + c, ew, el);
+            p0[c] += SCA(sb, (i + 2 * j) * NC + c, ew, el);
+            p1[c] += SCA(sb, (i + 2 * j + 4) * NC + c, ew, el);
           }
         }
       }
@@ -157,7 +185,6 @@ __global__ void __launch_bounds__(32 * TY, MINB)
 #pragma unroll
       for (int c = 0; c < NC; c++) carry[si][c] = p1[c];
     }
-    cur ^= 1;
   }
   if (z1 == nz) {
 #pragma unroll
