@@ -113,6 +113,11 @@ const char* vfgpu_last_error(void);
 int vfgpu_create(const vfgpu_grid* grid, vfgpu_ctx** out);
 int vfgpu_destroy(vfgpu_ctx* ctx);
 
+/* Device bytes a ctx of this grid holds once it has solved (fields + solver work
+ * space); no counterpart in the reference.  Used for memory-based admission of
+ * problems in the serving loop. */
+int vfgpu_memory_estimate(const vfgpu_grid* grid, long long* bytes);
+
 /* Per-layer material (VFMatPropGet, VFCommon.c:506-588); layer[ek] for the
  * nz-1 element layers (VFLayerInit, VFCommon.c:1099-1120), NULL = all layer 0. */
 int vfgpu_set_matprop(vfgpu_ctx* ctx, int nlayer, const vfgpu_matprop* mp, const int* layer);

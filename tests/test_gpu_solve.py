@@ -176,3 +176,39 @@ def test_penny41_am_loop(cuda, precision):
             assert got == pytest.approx(ref, rel=1e-6), (it, got, ref)
     assert np.abs(ctx.get_field("V") - fx["V"]).max() <= 1e-4
     ctx.close()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_context_reuse_across_problems(cuda, precision):
+    """A context reused for a second problem (new E, nu, Gc, epsilon, AT model; the captured
+    CG graphs stay in place) gives bit-identical results to a fresh context."""
+    import vpfhf_b200 as vg
+    n, L = (17, 17, 17), (4.0, 4.0, 4.0)
+
+    def problem(ctx, mp, eps, atnum):
+        ctx.set_matprop(mp)
+        ctx.set_vfprop(epsilon=eps, eta=1e-8, atnum=atnum, pressurize=True)
+        ctx.set_bc(vg.rollers())
+        v = vg.penny_crack_v(n, L, (2.0, 2.0, 2.0), 0.9, epsilon=eps, atnum=atnum)
+        for f in ("U",):
+            ctx.set_field(f, np.zeros(3 * ctx.N))
+        ctx.set_field("V", v)
+        ctx.set_field("VIrrev", v)
+        ctx.set_field("pressure", np.full(ctx.N, 2e6))
+        ctx.time_step_prepare()
+        for _ in range(2):
+            rc, err, su, sv = ctx.am_step(dict(precision=precision))
+            assert rc == 0, (su, sv)
+        return ctx.get_field("U"), ctx.get_field("V"), ctx.u_energy(), ctx.v_energy()
+
+    pa = (dict(E=1e10, nu=0.25, Gc=100.0), 0.5, 1)
+    pb = (dict(E=2.5e10, nu=0.3, Gc=40.0), 0.6, 2)
+    reused = vg.VFContext(n, L, pa[0])
+    problem(reused, *pa)
+    got = problem(reused, *pb)
+    fresh = vg.VFContext(n, L, pb[0])
+    ref = problem(fresh, *pb)
+    assert np.array_equal(got[0], ref[0]) and np.array_equal(got[1], ref[1])
+    assert got[2] == ref[2] and got[3] == ref[3]
+    reused.close()
+    fresh.close()

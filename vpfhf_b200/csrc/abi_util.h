@@ -11,6 +11,7 @@ cudaError_t copy_in(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
 cudaError_t copy_out(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
 int ensure_v32(vfgpu_ctx* c);
 void free_solver(vfgpu_ctx* c);
+int upload_params(vfgpu_ctx* c);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
 }  // namespace vfgpu

@@ -6,6 +6,14 @@ namespace vfgpu {
 
 constexpr int U_TY = 8, V_TY = 8;
 
+cudaError_t apply_kernel_attributes() {
+  cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOp<float>, U_TY, 2>();
+  if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();
+  if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, 3>();
+  return e;
+}
+
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   return tile_plan(nx, ny, nz, U_TY, 3, prec_bytes == 8 ? 1 : 2, num_sms);
 }

@@ -24,6 +24,15 @@ struct LayerTable {
   double Gc[VF_MAXLAYER];
 };
 
+// Per-problem parameters the operator kernels read through a device pointer, so
+// that captured CUDA graphs stay valid when a ctx is re-used for another problem
+// (set-up calls rewrite this block instead of the kernels' by-value arguments).
+struct DevParams {
+  LayerTable L;
+  double eta;                  // eta (VFProp.eta)
+  double aeps[VF_MAXLAYER];    // Gc/(2 c_w) * eps per layer (V operator gradient term)
+};
+
 template <typename T> struct Vec3 { T x, y, z; };
 
 __host__ __device__ inline int64_t node_index(int i, int j, int k, int nx, int ny) {

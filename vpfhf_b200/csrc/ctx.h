@@ -21,6 +21,7 @@ struct vfgpu_ctx {
   int nlayer = 0;
   vfgpu::LayerTable layers{};
   uint8_t* d_elayer = nullptr;  // nz-1
+  vfgpu::DevParams* d_params = nullptr;  // device copy of layers / eta / aeps
   float* d_cellE = nullptr;     // NC or null
   bool have_mat = false;
   vfgpu_vfprop vf{0.2, 1e-5, 5e-2, 2, 0};  // VFPropGet defaults (VFCommon.c:468-480)
@@ -58,6 +59,20 @@ struct vfgpu_ctx {
   double* d_out = nullptr;        // small device results (16 doubles)
   double* h_out = nullptr;        // pinned host mirror of d_out
   bool have_solver = false;
+
+  // Captured CUDA graphs of CG iteration batches, keyed by (call site, batch size).
+  // Kernels read the material table, eta and the AT gradient weights through
+  // d_params, so new material / vfprop values leave the graphs valid; a set-up call
+  // that changes a captured pointer (the cell-modulus array) bumps `gen` and stale
+  // graphs are re-captured.
+  struct Graph {
+    int kind, batch;
+    uint64_t gen;
+    cudaGraphExec_t exec;
+  };
+  std::vector<Graph> graphs;
+  uint64_t gen = 1;
+  bool use_graphs = true;
 };
 
 namespace vfgpu {

@@ -8,6 +8,7 @@
 
 namespace vfgpu {
 
+cudaError_t apply_kernel_attributes();
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms);
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms);
 

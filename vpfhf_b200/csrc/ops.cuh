@@ -51,16 +51,18 @@ template <typename T_> struct UOp {
       vn[a] = in[a][3];
     }
     const int layer = A.elayer ? A.elayer[ez] : 0;
+    const LayerTable& LT = A.P ? A.P->L : L;
+    const T eta = A.P ? T(A.P->eta) : A.eta;
     T lam, mu;
     if (A.cellE) {
       const T E = T(A.cellE[((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex]);
-      lam = E * T(L.lamfac[layer]);
-      mu = E * T(L.mufac[layer]);
+      lam = E * T(LT.lamfac[layer]);
+      mu = E * T(LT.mufac[layer]);
     } else {
-      lam = T(L.lambda[layer]);
-      mu = T(L.mu[layer]);
+      lam = T(LT.lambda[layer]);
+      mu = T(LT.mu[layer]);
     }
-    u_element<T, uzdirect<T>()>(xn, vn, lam, mu, A.eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+    u_element<T, uzdirect<T>()>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
     const unsigned b = A.bc ? A.bc[n] : 0u;
@@ -80,9 +82,9 @@ template <typename T> struct VApplyArgs {
   T* __restrict__ seamX;
   T* __restrict__ seamY;
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
+  const DevParams* __restrict__ P;    // Gc/(2 c_w) eps per layer
   int nx, ny, nz, ntx, nty, zc;
   T ihx, ihy, ihz, vol;
-  T aeps[VF_MAXLAYER];                // Gc/(2 c_w) * eps per layer
 };
 
 // y[a] = (K_V,e x_e)[a] for one element (same modal scheme as u_element).
@@ -191,7 +193,7 @@ template <typename T_> struct VOp {
     for (int a = 0; a < 8; a++) xn[a] = in[a][0];
     const int layer = A.elayer ? A.elayer[ez] : 0;
     const int64_t cell = ((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex;
-    v_element<T>(xn, A.coef + 27 * cell, A.aeps[layer], A.ihx, A.ihy, A.ihz, A.vol, yn);
+    v_element<T>(xn, A.coef + 27 * cell, T(A.P->aeps[layer]), A.ihx, A.ihy, A.ihz, A.vol, yn);
 #pragma unroll
     for (int a = 0; a < 8; a++) out[a][0] = yn[a];
   }

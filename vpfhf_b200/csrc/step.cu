@@ -103,8 +103,7 @@ static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask,
   A.ihy = T(1.0 / c->hy);
   A.ihz = T(1.0 / c->hz);
   A.vol = T(c->hx * c->hy * c->hz);
-  const double atcv = c->vf.atnum == 1 ? 2. / 3. : .5;
-  for (int l = 0; l < VF_MAXLAYER; l++) A.aeps[l] = T(c->layers.Gc[l] / atcv * .5 * c->vf.epsilon);
+  A.P = c->d_params;
   return A;
 }
 
@@ -137,12 +136,57 @@ struct Watch {
 
 // PCG with device-side convergence: queues batches of iterations (every kernel of a
 // converged solve is a no-op), checks the flag between batches.
+// Graph of `batch` CG iterations for call site `kind`, captured on first use (the
+// kernels' pointers are fixed per call site; see vfgpu_ctx::Graph).
+template <class Body>
+static cudaGraphExec_t cg_graph(vfgpu_ctx* c, int kind, int batch, Body body) {
+  for (auto& g : c->graphs)
+    if (g.kind == kind && g.batch == batch) {
+      if (g.gen == c->gen) return g.exec;
+      cudaGraphExecDestroy(g.exec);
+      g.exec = nullptr;
+    }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  const cudaError_t eb = body();
+  const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+  if (eb != cudaSuccess || ec != cudaSuccess || !graph ||
+      cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return nullptr;
+  }
+  cudaGraphDestroy(graph);
+  bool stored = false;
+  for (auto& g : c->graphs)
+    if (g.kind == kind && g.batch == batch) {
+      g.exec = exec;
+      g.gen = c->gen;
+      stored = true;
+    }
+  if (!stored) c->graphs.push_back({kind, batch, c->gen, exec});
+  return exec;
+}
+
 template <typename T, class Apply>
-static int run_cg(vfgpu_ctx* c, const CGVecs<T>& v, Apply apply, double rtol, double atol,
-                  double dtol, int maxit, const Watch& w, int* its, int* reason, bool* timeout) {
+static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, double rtol,
+                  double atol, double dtol, int maxit, const Watch& w, int* its, int* reason,
+                  bool* timeout) {
   cudaError_t e = cg_init<T>(v, c->d_cg, c->d_red, rtol, atol, dtol, maxit, c->stream);
   int batch = 4;
   *timeout = false;
+  auto body = [&](int nb) {
+    cudaError_t eb = cudaSuccess;
+    for (int b = 0; b < nb && eb == cudaSuccess; b++) {
+      eb = apply(v.p, v.w, &c->d_cg->done);
+      if (eb == cudaSuccess) eb = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream);
+    }
+    return eb;
+  };
   while (e == cudaSuccess) {
     e = cudaMemcpyAsync(c->h_cg, c->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
@@ -151,10 +195,8 @@ static int run_cg(vfgpu_ctx* c, const CGVecs<T>& v, Apply apply, double rtol, do
       *timeout = true;
       break;
     }
-    for (int b = 0; b < batch && e == cudaSuccess; b++) {
-      e = apply(v.p, v.w, &c->d_cg->done);
-      if (e == cudaSuccess) e = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream);
-    }
+    cudaGraphExec_t g = c->use_graphs ? cg_graph(c, kind, batch, [&] { return body(batch); }) : nullptr;
+    e = g ? cudaGraphLaunch(g, c->stream) : body(batch);
     batch = std::min(batch * 2, 64);
   }
   if (e != cudaSuccess) return cuda_fail(e, "CG");
@@ -247,7 +289,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     bool tmo = false;
     if (!mixed) {
       CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3};
-      rc = run_cg<double>(c, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
+      rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
       S.ksp_its += kits;
@@ -269,7 +311,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3};
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
-        rc = run_cg<float>(c, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
+        rc = run_cg<float>(c, 2, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
                            &r32reason, &tmo);
         if (rc) return rc;
         S.ksp_its += its32;
@@ -423,7 +465,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     bool tmo = false;
     if (!mixed) {
       CGVecs<double> v{Y, R, P, Wv, dinv, F, mask, N};
-      rc = run_cg<double>(c, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
+      rc = run_cg<double>(c, 3, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
       S.ksp_its += kits;
@@ -443,7 +485,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         CGVecs<float> v{x32, r32, pp32, w32, dinv32, b32, mask, N};
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
-        rc = run_cg<float>(c, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
+        rc = run_cg<float>(c, 4, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
                            &r32reason, &tmo);
         if (rc) return rc;
         S.ksp_its += its32;
@@ -593,6 +635,25 @@ int vfgpu_crack_opening(vfgpu_ctx* c, double* cov, double* cellcov) {
   int rc = energies(c, cellcov);
   if (rc) return rc;
   if (cov) *cov = c->h_out[3];
+  return VFGPU_OK;
+}
+
+int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
+  if (!g || !bytes) return fail(VFGPU_ERR_INVALID, "vfgpu_memory_estimate: null argument");
+  if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_memory_estimate: bad grid");
+  const long long N = (long long)g->nx * g->ny * g->nz;
+  const long long NC = (long long)(g->nx - 1) * (g->ny - 1) * (g->nz - 1);
+  const TilePlan p64 = u_plan(g->nx, g->ny, g->nz, 8, 148), p32 = u_plan(g->nx, g->ny, g->nz, 4, 148);
+  long long b = 0;
+  b += (2 * 3 * N + 5 * N) * 8;                          // fields U, BCU, V, VIrrev, theta, thetaRef, p
+  b += N * 4 + (g->nz - 1) + 3 * N + 3 * N;              // V32, layers, BC kinds and bits
+  b += (long long)(p64.seamX + p64.seamY) * 8 + (long long)(p32.seamX + p32.seamY) * 4;
+  b += 2 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
+  b += vfgpu_ctx::NP64 * 3 * N * 8 + vfgpu_ctx::NP32 * 3 * N * 4;  // solver work space
+  b += 27 * NC * 12 + N;                                 // V coefficient (FP64 + FP32), mask
+  b += (RED_BLOCKS + energy_blocks()) * 4 * 8 + 4096;    // reductions, scalars
+  *bytes = b;
   return VFGPU_OK;
 }
 

@@ -269,6 +269,18 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
   return p;
 }
 
+// Opt-in to the dynamic shared memory the kernel needs; done once per process (and
+// up front, from vfgpu_create, so that no attribute call happens inside a capture).
+template <class Op, int TY, int MINB> inline bool g_tile_attr_set = false;
+template <class Op, int TY, int MINB> cudaError_t set_tile_attributes() {
+  if (g_tile_attr_set<Op, TY, MINB>) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)tile_smem_bytes<Op, TY>());
+  if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB> = true;
+  return e;
+}
+
 template <class Op, int TY, int MINB>
 cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const LayerTable& L,
                               cudaStream_t s) {
@@ -276,13 +288,8 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
   A.nty = p.nty;
   A.zc = p.zc;
   constexpr size_t smem = tile_smem_bytes<Op, TY>();
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
+  if (ea != cudaSuccess) return ea;
   dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY);
   tile_apply_kernel<Op, TY, MINB><<<grid, block, smem, s>>>(A, L);
   const int64_t nseam = (int64_t)(p.ntx - 1) * A.nz * A.ny + (int64_t)(p.nty - 1) * A.nz * A.nx;

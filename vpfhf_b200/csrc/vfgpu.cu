@@ -102,6 +102,19 @@ int ensure_v32(vfgpu_ctx* c) {
   return VFGPU_OK;
 }
 
+// Rewrites the device parameter block from the host-side material and vfprop.
+int upload_params(vfgpu_ctx* c) {
+  DevParams P{};
+  P.L = c->layers;
+  P.eta = c->vf.eta;
+  const double atcv = c->vf.atnum == 1 ? 2. / 3. : .5;  // VFCommon.c:482-492
+  for (int l = 0; l < VF_MAXLAYER; l++) P.aeps[l] = c->layers.Gc[l] / atcv * .5 * c->vf.epsilon;
+  cudaError_t e = cudaMemcpyAsync(c->d_params, &P, sizeof P, cudaMemcpyHostToDevice, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "parameter upload");
+  return VFGPU_OK;
+}
+
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p) {
   UApplyArgs<T> A{};
@@ -121,6 +134,7 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   A.ihz = T(1.0 / c->hz);
   A.vol = T(c->hx * c->hy * c->hz);
   A.eta = T(c->vf.eta);
+  A.P = c->d_params;
   return A;
 }
 template UApplyArgs<double> u_args<double>(vfgpu_ctx*, const double*, const double*, double*,
@@ -139,9 +153,12 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   if (!c) return VFGPU_OK;
   cudaSetDevice(c->dev);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (auto& g : c->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  c->graphs.clear();
   free_solver(c);
   for (auto& p : c->f) cudaFree(p);
-  void* bufs[] = {c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_params, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -189,6 +206,11 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
       return cuda_fail(e, "vfgpu_create: cudaMalloc");     \
     }                                                      \
   } while (0)
+  e = apply_kernel_attributes();
+  if (e != cudaSuccess) {
+    delete c;
+    return cuda_fail(e, "vfgpu_create: kernel attributes");
+  }
   e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) {
     vfgpu_destroy(c);
@@ -197,6 +219,7 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   for (int fi = 0; fi < 7; fi++) ALLOC(c->f[fi], field_len(c, fi) * sizeof(double));
   ALLOC(c->V32, c->N * sizeof(float));
   ALLOC(c->d_elayer, std::max(1, c->nz - 1));
+  ALLOC(c->d_params, sizeof(DevParams));
   ALLOC(c->bcU_kind, 3 * c->N);
   ALLOC(c->bcU_bits, c->N);
   ALLOC(c->bcV_kind, c->N);
@@ -226,6 +249,10 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   if (e != cudaSuccess) {
     vfgpu_destroy(c);
     return cuda_fail(e, "vfgpu_create");
+  }
+  if (upload_params(c) != VFGPU_OK) {
+    vfgpu_destroy(c);
+    return VFGPU_ERR_CUDA;
   }
   *out = c;
   return VFGPU_OK;
@@ -265,19 +292,25 @@ int vfgpu_set_matprop(vfgpu_ctx* c, int nlayer, const vfgpu_matprop* mp, const i
   c->layers = L;
   c->nlayer = nlayer;
   c->have_mat = true;
-  return VFGPU_OK;
+  return upload_params(c);
 }
 
 int vfgpu_set_cell_modulus(vfgpu_ctx* c, const double* cellE) {
   if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_set_cell_modulus: null ctx");
   cudaSetDevice(c->dev);
+  // The cell-modulus pointer is captured by CG graphs: they are re-captured whenever it
+  // appears, disappears or moves.
   if (!cellE) {
+    if (c->d_cellE) c->gen++;
     cudaFree(c->d_cellE);
     c->d_cellE = nullptr;
     return VFGPU_OK;
   }
   cudaError_t e = cudaSuccess;
-  if (!c->d_cellE) e = cudaMalloc((void**)&c->d_cellE, c->NC * sizeof(float));
+  if (!c->d_cellE) {
+    c->gen++;
+    e = cudaMalloc((void**)&c->d_cellE, c->NC * sizeof(float));
+  }
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_set_cell_modulus");
   // staged through t64a (>= 3N >= NC doubles)
   e = copy_in(c, c->t64a, cellE, c->NC);
@@ -294,7 +327,7 @@ int vfgpu_set_vfprop(vfgpu_ctx* c, const vfgpu_vfprop* vf) {
   if (!(vf->epsilon > 0) || !(vf->eta >= 0))
     return fail(VFGPU_ERR_INVALID, "vfgpu_set_vfprop: need epsilon > 0 and eta >= 0");
   c->vf = *vf;
-  return VFGPU_OK;
+  return upload_params(c);
 }
 
 int vfgpu_set_bc(vfgpu_ctx* c, const vfgpu_bc bcU[3], const vfgpu_bc* bcV) {
