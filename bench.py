@@ -7,7 +7,10 @@ A "step" is one application of the degraded elasticity operator K(v) to a
 3N-vector (3 x 129^3 = 6,440,067 dofs) with the inputs resident in HBM; the L2
 is flushed between timed steps.  `e2e` times the same step through the C ABI
 (vfgpu_u_apply) from pinned host memory, copies included.  The AM-step rate
-(StepU + StepV to tolerance, FP64 and mixed) is reported beside it.
+(StepU + StepV to tolerance, FP64 and mixed, 10 iterations from the penny-crack
+start) is reported beside it with the mixed-vs-FP64 differences of the energies,
+the crack opening and V, and so is the serving stream (p50 / p99 latency and
+throughput of independent problems through the library's request loop).
 
 Multi-GPU: the operator does not shard in this build ("replicas only"): every
 rank runs its own copy of the workload and `value` is the total over ranks.
@@ -208,7 +211,7 @@ def run_gpu(args):
         e2e_ms = m.item()
 
     # AM steps (StepU + StepV to tolerance) from the penny-crack start, FP64 and mixed
-    am = {}
+    am, vfin = {}, {}
     for prec in ("fp64", "mixed"):
         ctx.set_field("U", np.zeros(N3))
         ctx.set_field("V", v0)
@@ -224,8 +227,15 @@ def run_gpu(args):
             energies.append((el, pw, ctx.v_energy(), ctx.crack_opening()))
         am[prec] = dict(s_per_step=float(np.mean(times[1:] if len(times) > 1 else times)),
                         energies=energies, last_kspU=su["ksp_its"], last_kspV=sv["ksp_its"])
+        vfin[prec] = ctx.get_field("V")
     rel = max(abs(a - b) / abs(b) for ea, eb in zip(am["mixed"]["energies"], am["fp64"]["energies"])
               for a, b in zip(ea, eb))
+    names = ("elastic", "pressure_work", "surface", "cov")
+    rel_last = {k: abs(a - b) / abs(b) for k, a, b in
+                zip(names, am["mixed"]["energies"][-1], am["fp64"]["energies"][-1])}
+    v_linf = float(np.abs(vfin["mixed"] - vfin["fp64"]).max())
+
+    serving = run_serving(args) if args.serve_problems > 0 else None
 
     if rank != 0:
         ctx.close()
@@ -277,16 +287,47 @@ def run_gpu(args):
         "am_steps_per_s": {"fp64": round(1.0 / am["fp64"]["s_per_step"], 3),
                            "mixed": round(1.0 / am["mixed"]["s_per_step"], 3),
                            "mixed_vs_fp64_max_rel_energy_diff": rel,
+                           "mixed_vs_fp64_rel_at_last_step": rel_last,
+                           "mixed_vs_fp64_v_linf": v_linf,
                            "steps": args.am_steps,
                            "kspU_last": {k: am[k]["last_kspU"] for k in am}},
         "clocks": clocks,
     }
+    if serving:
+        line["serving"] = serving
     if args.cpu_baseline:
         line["cpu_baseline"] = cpu_reference(args, quick=True)
     print(json.dumps(line))
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def run_serving(args):
+    """The serving stream: independent pressurised-crack problems (grid edge uniform over
+    {17, 33, 65, 97}, 1-4 random penny cracks, E ~ U[5,30] GPa, nu ~ U[0.15,0.35], AT1/AT2,
+    5 AM iterations each) through the library's request loop.  The FP64 capacity is
+    measured closed-loop on the first 128 problems; the full stream then arrives as a
+    seeded Poisson process at 0.8x that capacity, once in FP64 and once mixed (same
+    arrival times).  Latency = completion - arrival."""
+    from vpfhf_b200.serve import poisson_arrivals, run_stream, serving_stream
+    count, workers = args.serve_problems, args.serve_workers
+    cal = serving_stream(count=min(128, count), precision="fp64")
+    _, cap = run_stream(cal, None, workers=workers)
+    rate = 0.8 * cap["throughput"]
+    arr = poisson_arrivals(count, rate)
+    out = {"problems": count, "workers": workers, "am_its_per_problem": 5,
+           "capacity_fp64_per_s": round(cap["throughput"], 3),
+           "arrival_rate_per_s": round(rate, 3),
+           "grids": "edge uniform over {17,33,65,97}, cube [0,4]^3"}
+    keys = ("throughput", "p50_s", "p99_s", "mean_s", "max_s", "failed", "reused",
+            "contexts_created", "evictions", "peak_reserved_gb", "span_s")
+    for prec in ("fp64", "mixed"):
+        _, summ = run_stream(serving_stream(count=count, precision=prec), arr, workers=workers)
+        out[prec] = {k: (round(summ[k], 4) if isinstance(summ[k], float) else summ[k])
+                     for k in keys}
+        out[prec]["throughput_unit"] = "problems/s"
+    return out
 
 
 def cpu_reference(args, quick=False):
@@ -334,7 +375,10 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--am-steps", type=int, default=3)
+    ap.add_argument("--am-steps", type=int, default=10)
+    ap.add_argument("--serve-problems", type=int, default=512,
+                    help="problems in the serving stream (0 skips it)")
+    ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--impl", default="vfgpu", choices=["vfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--grid", type=int, default=N_EDGE, help="nodes per axis (profiling runs)")

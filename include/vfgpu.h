@@ -184,6 +184,94 @@ int vfgpu_crack_opening(vfgpu_ctx* ctx, double* cov, double* cellcov);
 int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);
 int vfgpu_v_residual(vfgpu_ctx* ctx, double* F);
 
+/* ---- crack initialisers ------------------------------------------------------ */
+/* VFPennyCrack (VFCracks.h): disk of radius r around center, normal
+ * (cos theta sin phi, sin theta sin phi, cos phi) with the angles in degrees. */
+typedef struct {
+  double center[3];
+  double r, theta, phi, thickness;
+} vfgpu_penny;
+/* VFRectangularCrack (VFCracks.h): corners P1 = corners[0..2], P2 = [3..5],
+ * P3 = [6..8]; the fourth corner is P2 + P3 - P1. */
+typedef struct {
+  double corners[9];
+  double thickness;
+} vfgpu_rect;
+
+/* The crack part of VFFieldsInitialize (VFCommon.c:823-857) on the device:
+ * V = VIrrev = pointwise minimum over the penny cracks (VFPennyCrackBuildVAT1/2,
+ * VFCracks.c:136-227) and the rectangular cracks (VFRectangularCrackBuildVAT1/2,
+ * VFCracks.c:436-513) with the profile of the ctx's atnum and epsilon; 1 where
+ * there are none.  Any number of cracks. */
+int vfgpu_init_cracks(vfgpu_ctx* ctx, int npenny, const vfgpu_penny* penny, int nrect,
+                      const vfgpu_rect* rect);
+
+/* ---- serving: a request loop over independent problems ------------------------
+ * No counterpart in the reference (one problem per process there).  A server owns
+ * worker threads on one GPU.  Each request is a whole fracture problem: grid,
+ * material, phase-field parameters, BCs, cracks, a uniform crack pressure and a
+ * number of AM iterations.  Requests are admitted in arrival order as workers and
+ * device memory free up (vfgpu_memory_estimate against the server's budget).  Each
+ * admitted problem runs on a ctx of its grid size taken from a pool: contexts
+ * (fields, solver work space, captured CUDA graphs) are kept after a problem ends
+ * and reused by the next problem of the same size; idle contexts of other sizes
+ * are evicted when memory is short.  Problems on different workers overlap on the
+ * device through their own streams.  The kernels are deterministic, so a problem
+ * gives the same bits alone and in any mix. */
+#define VFGPU_SERVE_MAX_PENNY 16
+#define VFGPU_SERVE_MAX_RECT 16
+typedef struct {
+  vfgpu_grid grid;
+  vfgpu_matprop mp;            /* one layer */
+  vfgpu_vfprop vf;
+  vfgpu_bc bcU[3], bcV;
+  double pressure;             /* uniform crack pressure (used when vf.hasCrackPressure) */
+  int npenny, nrect;
+  vfgpu_penny penny[VFGPU_SERVE_MAX_PENNY];
+  vfgpu_rect rect[VFGPU_SERVE_MAX_RECT];
+  int am_its;                  /* AM iterations: exactly am_its if > 0 ...              */
+  double altmintol;            /* ... else until ||V - Vold||_inf < altmintol           */
+  int max_am_its;              /*     or max_am_its iterations                          */
+  vfgpu_solve_opts opts;       /* precision and tolerances of both solves               */
+  double* out_u;               /* optional host buffers filled at the end: 3N, N, N     */
+  double* out_v;
+  double* out_cellcov;         /* optional ((nx-1)(ny-1)(nz-1)) */
+  unsigned long long tag;      /* caller's id, returned in the result */
+} vfgpu_request;
+
+typedef struct {
+  unsigned long long ticket, tag;
+  int status;                  /* VFGPU_OK, or the first failing call's code            */
+  int am_its, ksp_its_u, ksp_its_v;
+  double am_err;               /* last ||V - Vold||_inf */
+  double elastic, pressure_work, surface, cov;
+  double t_submit, t_start, t_done;  /* seconds on the server clock */
+  int worker;
+  int reused_ctx;              /* 1 if the problem ran on a pooled ctx */
+  char error[160];             /* message of the failing call, "" if status == VFGPU_OK */
+} vfgpu_result;
+
+typedef struct {
+  long long budget_bytes, reserved_bytes, peak_reserved_bytes;
+  int workers, contexts, contexts_created, evictions;
+  long long submitted, completed, queued, running;
+} vfgpu_server_info;
+
+typedef struct vfgpu_server vfgpu_server;
+/* workers >= 1 threads on CUDA device `device`; budget_bytes <= 0 means 85% of the
+ * device memory free at creation. */
+int vfgpu_server_create(int device, int workers, long long budget_bytes, vfgpu_server** out);
+/* Copies the request and queues it; *ticket identifies its result.  Never blocks. */
+int vfgpu_server_submit(vfgpu_server* s, const vfgpu_request* req, unsigned long long* ticket);
+/* Waits up to timeout_s (< 0: for ever) for the next finished problem, in completion
+ * order.  Returns VFGPU_OK with *res filled, or VFGPU_NOT_CONVERGED on timeout. */
+int vfgpu_server_next(vfgpu_server* s, double timeout_s, vfgpu_result* res);
+/* Seconds since the server was created (the clock of the result time stamps). */
+double vfgpu_server_clock(vfgpu_server* s);
+int vfgpu_server_info_get(vfgpu_server* s, vfgpu_server_info* info);
+/* Finishes the queued and running problems, joins the workers, frees every ctx. */
+int vfgpu_server_destroy(vfgpu_server* s);
+
 /* No counterpart in the reference.  y = K(v) x like vfgpu_u_apply (FP64, one
  * homogeneous material, Dirichlet rows from bcbits), for callers that cannot
  * allocate device memory while they run -- e.g. a matrix-shell callback inside

@@ -924,3 +924,106 @@ int vfo_penny_crack_v(const vfo_problem *P, const double center[3], double r,
       }
   return 0;
 }
+
+/* VFDistanceToRectangularCrack (VFCracks.c:331-427): the crack is the parallelogram with
+ * corners P1 = c[0..2], P2 = c[3..5], P3 = c[6..8] and P4 = 2C - P1, C = (P2 + P3)/2.
+ * The in-plane distance from C to the edge along the direction of the projected point
+ * is found from the angles the direction makes with C->P3 and C->P4; the operation
+ * order (and the NaN that a point on the normal through C produces, which makes the
+ * final test pick the plane distance) follows the reference. */
+static void unit3(double a[3]) {
+  double nn = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  a[0] = a[0] / nn;
+  a[1] = a[1] / nn;
+  a[2] = a[2] / nn;
+}
+static double dot3(const double a[3], const double b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+double vfo_rect_distance(const double x[3], const double c[9]) {
+  const double pi = 3.14159265358979323846264338327950288;
+  double C[3], P4[3], a[3], b[3], n[3], tau[3], p[3], q[3], e1[3], e2[3], nq[3], side[3];
+  for (int d = 0; d < 3; d++) {
+    C[d] = (c[6 + d] + c[3 + d]) / 2.;
+    P4[d] = 2. * C[d] - c[d];
+    a[d] = c[3 + d] - c[d];
+    b[d] = c[6 + d] - c[d];
+  }
+  n[0] = a[1] * b[2] - a[2] * b[1];
+  n[1] = a[2] * b[0] - a[0] * b[2];
+  n[2] = a[0] * b[1] - a[1] * b[0];
+  unit3(n);
+  double s = (x[0] - C[0]) * n[0] + (x[1] - C[1]) * n[1] + (x[2] - C[2]) * n[2];
+  for (int d = 0; d < 3; d++) {
+    tau[d] = (x[d] - C[d]) - s * n[d];
+    p[d] = C[d] + s * n[d];
+    q[d] = x[d] + C[d] - p[d];
+    e1[d] = c[6 + d] - C[d];
+    e2[d] = P4[d] - C[d];
+  }
+  unit3(e1);
+  unit3(e2);
+  const double theta_side = pi - acos(dot3(e2, e1));
+  for (int d = 0; d < 3; d++) nq[d] = q[d] - C[d];
+  unit3(nq);
+  const double theta = acos(dot3(e2, nq)) + acos(-e1[0] * nq[0] - e1[1] * nq[1] - e1[2] * nq[2]);
+  const int k = ((theta - theta_side) < 1e-6 || (2. * pi - theta_side - theta) < 1e-6) ? 3 : 6;
+  for (int d = 0; d < 3; d++) side[d] = P4[d] - c[k + d];
+  unit3(side);
+  const double da = sqrt((P4[0] - C[0]) * (P4[0] - C[0]) + (P4[1] - C[1]) * (P4[1] - C[1]) +
+                         (P4[2] - C[2]) * (P4[2] - C[2]));
+  double db = fabs((P4[0] - C[0]) * side[0] + (P4[1] - C[1]) * side[1] + (P4[2] - C[2]) * side[2]);
+  db = sqrt(da * da - db * db);
+  const double to_side = db / sin(acos(dot3(side, nq)));
+  const double l = sqrt(tau[0] * tau[0] + tau[1] * tau[1] + tau[2] * tau[2]);
+  if (l > to_side) return sqrt((l - to_side) * (l - to_side) + s * s);
+  return sqrt(s * s);
+}
+
+/* VFRectangularCrackBuildVAT1/AT2 (VFCracks.c:436-513).  AT1 subtracts half the
+ * thickness from the distance; AT2 compares the raw distance with the full
+ * thickness and uses it unshifted in the profile. */
+int vfo_rect_crack_v(const vfo_problem *P, const double corners[9], double thickness,
+                     double *v) {
+  for (int k = 0; k < P->nz; k++)
+    for (int j = 0; j < P->ny; j++)
+      for (int i = 0; i < P->nx; i++) {
+        double x[3] = {coord(i, P->lx, P->nx), coord(j, P->ly, P->ny), coord(k, P->lz, P->nz)};
+        int64_t q = NODE(P, i, j, k);
+        double dist = vfo_rect_distance(x, corners);
+        if (P->atnum == 1) {
+          dist -= thickness / 2.;
+          if (dist <= 0)
+            v[q] = 0.;
+          else
+            v[q] = dist < 2. * P->epsilon ? dist / P->epsilon * (1. - .25 * dist / P->epsilon) : 1.;
+        } else {
+          v[q] = dist <= thickness ? 0. : 1. - exp(-dist / 2 / P->epsilon);
+        }
+      }
+  return 0;
+}
+
+/* VFFieldsInitialize (VFCommon.c:823-857): V = VIrrev = pointwise minimum over the
+ * penny cracks (7 doubles each: center[3], r, theta, phi, thickness) and the
+ * rectangular cracks (10 doubles each: corners[9], thickness), 1 where there is none. */
+int vfo_cracks_v(const vfo_problem *P, int npenny, const double *penny, int nrect,
+                 const double *rect, double *v) {
+  const int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  double *w = (double *)malloc(N * sizeof(double));
+  if (!w) return -1;
+  for (int64_t q = 0; q < N; q++) v[q] = 1.;
+  for (int c = 0; c < npenny + nrect; c++) {
+    if (c < npenny) {
+      const double *pc = penny + 7 * c;
+      vfo_penny_crack_v(P, pc, pc[3], pc[4], pc[5], pc[6], w);
+    } else {
+      const double *rc = rect + 10 * (c - npenny);
+      vfo_rect_crack_v(P, rc, rc[9], w);
+    }
+    for (int64_t q = 0; q < N; q++) v[q] = w[q] < v[q] ? w[q] : v[q];
+  }
+  free(w);
+  return 0;
+}

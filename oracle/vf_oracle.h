@@ -124,6 +124,11 @@ int vfo_cov(const vfo_problem *P, const double *u, const double *v, double *cov,
 /* ---- penny crack initial V (VFCracks.c:101-227) ---- */
 int vfo_penny_crack_v(const vfo_problem *P, const double center[3], double r,
                       double theta_deg, double phi_deg, double thickness, double *v);
+/* rectangular crack (VFCracks.c:331-513) and the several-crack minimum (VFCommon.c:823-857) */
+double vfo_rect_distance(const double x[3], const double corners[9]);
+int vfo_rect_crack_v(const vfo_problem *P, const double corners[9], double thickness, double *v);
+int vfo_cracks_v(const vfo_problem *P, int npenny, const double *penny, int nrect,
+                 const double *rect, double *v);
 
 /* ---- solvers (PETSc semantics restated: VFCommon.c:1005-1088) ---- */
 int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *theta,

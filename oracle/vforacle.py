@@ -113,6 +113,8 @@ def _declare(L):
         "vfo_v_energy": [_P, _dp, C.POINTER(C.c_double)],
         "vfo_cov": [_P, _dp, _dp, C.POINTER(C.c_double), odp],
         "vfo_penny_crack_v": [_P, _dp, C.c_double, C.c_double, C.c_double, C.c_double, _dp],
+        "vfo_rect_crack_v": [_P, _dp, C.c_double, _dp],
+        "vfo_cracks_v": [_P, C.c_int, odp, C.c_int, odp, _dp],
         "vfo_step_u": [_P, _dp, _dp, odp, odp, odp, ou8, odp, C.POINTER(SolverOpts),
                        C.POINTER(Stats)],
         "vfo_step_v": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
@@ -122,6 +124,8 @@ def _declare(L):
         f = getattr(L, name)
         f.argtypes = args
         f.restype = C.c_int
+    L.vfo_rect_distance.argtypes = [_dp, _dp]
+    L.vfo_rect_distance.restype = C.c_double
     L.vfo_u_csr_nnz.argtypes = [_P]
     L.vfo_u_csr_nnz.restype = C.c_int64
 
@@ -266,6 +270,24 @@ class Oracle:
         v = np.zeros(self.N)
         self.L.vfo_penny_crack_v(C.byref(self.P), np.asarray(center, np.float64), float(r),
                                  float(theta), float(phi), float(thickness), v)
+        return v
+
+    def rect_v(self, corners, thickness=0.0):
+        v = np.zeros(self.N)
+        self.L.vfo_rect_crack_v(C.byref(self.P), np.asarray(corners, np.float64), float(thickness), v)
+        return v
+
+    def rect_distance(self, x, corners):
+        return self.L.vfo_rect_distance(np.asarray(x, np.float64), np.asarray(corners, np.float64))
+
+    def cracks_v(self, pennies=(), rects=()):
+        """pennies: rows (cx, cy, cz, r, theta, phi, thickness); rects: rows (9 corners,
+        thickness).  V = VIrrev = the pointwise minimum (VFCommon.c:823-857)."""
+        pa = np.ascontiguousarray(np.asarray(pennies, np.float64).reshape(-1, 7))
+        ra = np.ascontiguousarray(np.asarray(rects, np.float64).reshape(-1, 10))
+        v = np.zeros(self.N)
+        self.L.vfo_cracks_v(C.byref(self.P), len(pa), pa if len(pa) else None, len(ra),
+                            ra if len(ra) else None, v)
         return v
 
     # -- solvers -------------------------------------------------------------

@@ -162,6 +162,15 @@ class VFContext:
         import torch
         return torch.cuda.ExternalStream(self.stream_handle)
 
+    def init_cracks(self, pennies=(), rects=()):
+        """Device crack initialisation (VFFieldsInitialize, VFCommon.c:823-857): V = VIrrev =
+        min over the cracks.  pennies: dicts (center, r, theta, phi, thickness) or rows
+        (cx, cy, cz, r, theta, phi, thickness); rects: dicts (corners, thickness) or rows
+        (9 corners, thickness)."""
+        pa, ra = penny_array(pennies), rect_array(rects)
+        _abi.check(self.L.vfgpu_init_cracks(self.h, len(pa), pa if len(pa) else None, len(ra),
+                                            ra if len(ra) else None), "vfgpu_init_cracks")
+
     # -- solves ---------------------------------------------------------------------
     def step_u(self, opts=None):
         """VF_StepU: returns (status, stats dict); status 0 converged, 1 not converged,
@@ -257,6 +266,27 @@ def penny_crack_v(n, l, center, r, theta=0.0, phi=0.0, thickness=0.0, epsilon=0.
     else:
         v = np.where(d <= 0, 0.0, 1.0 - np.exp(-np.maximum(d, 0) / 2 / epsilon))
     return np.ascontiguousarray(v).reshape(-1)
+
+
+def _penny(p):
+    if isinstance(p, dict):
+        return _abi.Penny((C.c_double * 3)(*p["center"]), p["r"], p.get("theta", 0.0),
+                          p.get("phi", 0.0), p.get("thickness", 0.0))
+    return _abi.Penny((C.c_double * 3)(*p[:3]), *p[3:7])
+
+
+def _rect(r):
+    if isinstance(r, dict):
+        return _abi.Rect((C.c_double * 9)(*r["corners"]), r.get("thickness", 0.0))
+    return _abi.Rect((C.c_double * 9)(*r[:9]), r[9])
+
+
+def penny_array(pennies):
+    return (_abi.Penny * len(pennies))(*[_penny(p) for p in pennies])
+
+
+def rect_array(rects):
+    return (_abi.Rect * len(rects))(*[_rect(r) for r in rects])
 
 
 def bc_vector(n, bcs):

@@ -58,6 +58,53 @@ class SolveStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Penny(C.Structure):
+    _fields_ = [("center", C.c_double * 3), ("r", C.c_double), ("theta", C.c_double),
+                ("phi", C.c_double), ("thickness", C.c_double)]
+
+
+class Rect(C.Structure):
+    _fields_ = [("corners", C.c_double * 9), ("thickness", C.c_double)]
+
+
+SERVE_MAX_PENNY = 16
+SERVE_MAX_RECT = 16
+
+
+class Request(C.Structure):
+    _fields_ = [("grid", Grid), ("mp", MatProp), ("vf", VFProp), ("bcU", BC * 3), ("bcV", BC),
+                ("pressure", C.c_double), ("npenny", C.c_int), ("nrect", C.c_int),
+                ("penny", Penny * SERVE_MAX_PENNY), ("rect", Rect * SERVE_MAX_RECT),
+                ("am_its", C.c_int), ("altmintol", C.c_double), ("max_am_its", C.c_int),
+                ("opts", SolveOpts), ("out_u", C.c_void_p), ("out_v", C.c_void_p),
+                ("out_cellcov", C.c_void_p), ("tag", C.c_ulonglong)]
+
+
+class Result(C.Structure):
+    _fields_ = [("ticket", C.c_ulonglong), ("tag", C.c_ulonglong), ("status", C.c_int),
+                ("am_its", C.c_int), ("ksp_its_u", C.c_int), ("ksp_its_v", C.c_int),
+                ("am_err", C.c_double), ("elastic", C.c_double), ("pressure_work", C.c_double),
+                ("surface", C.c_double), ("cov", C.c_double), ("t_submit", C.c_double),
+                ("t_start", C.c_double), ("t_done", C.c_double), ("worker", C.c_int),
+                ("reused_ctx", C.c_int), ("error", C.c_char * 160)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_}
+        d["error"] = self.error.decode(errors="replace")
+        return d
+
+
+class ServerInfo(C.Structure):
+    _fields_ = [("budget_bytes", C.c_longlong), ("reserved_bytes", C.c_longlong),
+                ("peak_reserved_bytes", C.c_longlong), ("workers", C.c_int),
+                ("contexts", C.c_int), ("contexts_created", C.c_int), ("evictions", C.c_int),
+                ("submitted", C.c_longlong), ("completed", C.c_longlong),
+                ("queued", C.c_longlong), ("running", C.c_longlong)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class VFGPUError(RuntimeError):
     def __init__(self, code, fn, msg):
         super().__init__(f"{fn} failed with status {code}: {msg}")
@@ -91,6 +138,12 @@ _SIGS = {
     "vfgpu_crack_opening": [C.c_void_p, C.POINTER(C.c_double), C.c_void_p],
     "vfgpu_u_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_v_residual": [C.c_void_p, C.c_void_p],
+    "vfgpu_init_cracks": [C.c_void_p, C.c_int, C.POINTER(Penny), C.c_int, C.POINTER(Rect)],
+    "vfgpu_server_create": [C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_void_p)],
+    "vfgpu_server_submit": [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_ulonglong)],
+    "vfgpu_server_next": [C.c_void_p, C.c_double, C.POINTER(Result)],
+    "vfgpu_server_info_get": [C.c_void_p, C.POINTER(ServerInfo)],
+    "vfgpu_server_destroy": [C.c_void_p],
     "vfgpu_fma_peak": [C.c_int, C.POINTER(C.c_double)],
     "vfgpu_u_apply_noalloc": [C.POINTER(Grid), C.POINTER(MatProp), C.c_double, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
@@ -117,12 +170,14 @@ def lib():
         f = getattr(L, name)
         f.argtypes = args
         f.restype = None
+    L.vfgpu_server_clock.argtypes = [C.c_void_p]
+    L.vfgpu_server_clock.restype = C.c_double
     _LIB = L
     return L
 
 
 def exported_symbols():
-    return ["vfgpu_last_error"] + list(_SIGS) + list(_VOID_SIGS)
+    return ["vfgpu_last_error", "vfgpu_server_clock"] + list(_SIGS) + list(_VOID_SIGS)
 
 
 def check(code, fn):

@@ -21,6 +21,8 @@ LIB = os.path.join(HERE, "libvfgpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+# Per-file extra flags: the crack initialisers round like the reference's C code.
+FILE_FLAGS = {"cracks.cu": ["-fmad=false"]}
 
 
 def _flags(debug: bool) -> list[str]:
@@ -37,7 +39,7 @@ def _deps_mtime() -> float:
 
 
 def _compile(src: str, obj: str, debug: bool) -> tuple[str, int, str]:
-    cmd = [NVCC] + _flags(debug) + ["-c", src, "-o", obj]
+    cmd = [NVCC] + _flags(debug) + FILE_FLAGS.get(os.path.basename(src), []) + ["-c", src, "-o", obj]
     p = subprocess.run(cmd, capture_output=True, text=True)
     return src, p.returncode, p.stdout + p.stderr
 

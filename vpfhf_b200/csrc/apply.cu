@@ -1,4 +1,6 @@
 // apply.cu -- instantiations of the tile engine for the U and V operators.
+#include <mutex>
+
 #include "kernels.h"
 #include "ops.cuh"
 
@@ -7,6 +9,8 @@ namespace vfgpu {
 constexpr int U_TY = 8, V_TY = 8;
 
 cudaError_t apply_kernel_attributes() {
+  static std::mutex m;  // contexts may be created from several threads
+  std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<UOp<float>, U_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();

@@ -269,15 +269,19 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
   return p;
 }
 
-// Opt-in to the dynamic shared memory the kernel needs; done once per process (and
+// Opt-in to the dynamic shared memory the kernel needs; done once per device (and
 // up front, from vfgpu_create, so that no attribute call happens inside a capture).
-template <class Op, int TY, int MINB> inline bool g_tile_attr_set = false;
+// Callers serialise (apply_kernel_attributes holds a mutex).
+template <class Op, int TY, int MINB> inline unsigned long long g_tile_attr_set = 0;  // device bits
 template <class Op, int TY, int MINB> cudaError_t set_tile_attributes() {
-  if (g_tile_attr_set<Op, TY, MINB>) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)tile_smem_bytes<Op, TY>());
-  if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB> = true;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (g_tile_attr_set<Op, TY, MINB> & bit) return cudaSuccess;
+  e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)tile_smem_bytes<Op, TY>());
+  if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB> |= bit;
   return e;
 }
 
