@@ -184,6 +184,36 @@ def run_gpu(args):
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         ms64, ms32 = m.tolist()
 
+    if args.only_am:
+        out = {}
+        for prec in ("fp64", "mixed"):
+            ctx.set_field("U", np.zeros(N3))
+            ctx.set_field("V", v0)
+            ctx.time_step_prepare()
+            steps = []
+            for it in range(args.am_steps):
+                last = it == args.am_steps - 1
+                barrier()
+                if last and prec == args.profile_precision:
+                    torch.cuda.profiler.start()
+                t0 = time.perf_counter()
+                rc, err, su, sv = ctx.am_step(dict(precision=prec))
+                barrier()
+                dt = time.perf_counter() - t0
+                if last and prec == args.profile_precision:
+                    torch.cuda.profiler.stop()
+                steps.append(dict(s=dt, u_s=su["seconds"], v_s=sv["seconds"],
+                                  u_newton=su["newton_its"], u_ksp=su["ksp_its"],
+                                  u_refine=su["refine_its"], v_newton=sv["newton_its"],
+                                  v_ksp=sv["ksp_its"], v_refine=sv["refine_its"], err=err))
+            out[prec] = steps
+        if rank == 0:
+            print(json.dumps({"grid": n, "am": out}))
+        ctx.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
     if args.only_apply:
         if rank == 0:
             print(json.dumps({"grid": n, "ms_fp64": ms64, "ms_fp32": ms32, "clocks": clocks}))
@@ -384,6 +414,10 @@ def main():
     ap.add_argument("--grid", type=int, default=N_EDGE, help="nodes per axis (profiling runs)")
     ap.add_argument("--only-apply", action="store_true",
                     help="time the operator applications only (profiling runs)")
+    ap.add_argument("--only-am", action="store_true",
+                    help="run the AM steps only, with a per-solve breakdown; the last step of "
+                         "--profile-precision is bracketed by cudaProfilerStart/Stop")
+    ap.add_argument("--profile-precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
