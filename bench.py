@@ -360,6 +360,87 @@ def run_serving(args):
     return out
 
 
+def _am_run(ctx, prob, prec, its, altmintol=0.0, reset=True):
+    """AM iterations on `ctx`: exactly `its` (altmintol 0) or until ||V - Vold||_inf <
+    altmintol; returns per-iteration records."""
+    import torch
+    if reset:
+        ctx.set_field("U", np.zeros(3 * ctx.N))
+        ctx.init_cracks(prob["pennies"])
+        ctx.time_step_prepare()
+    recs = []
+    for it in range(its):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc, err, su, sv = ctx.am_step(dict(precision=prec))
+        dt = time.perf_counter() - t0
+        recs.append(dict(s=dt, err=err, rc=rc, kspU=su["ksp_its"], kspV=sv["ksp_its"]))
+        if altmintol > 0 and err < altmintol:
+            break
+    return recs
+
+
+def _energies(ctx):
+    el, _, pw = ctx.u_energy()
+    return dict(elastic=el, pressure_work=pw, surface=ctx.v_energy(), cov=ctx.crack_opening())
+
+
+def run_large(args):
+    """The large single-GPU set-ups: `c5` (321^3, heterogeneous E, 8 cracks, 10 AM
+    iterations, FP64 and mixed from the same start) and `c3` (257x257x129 poroelastic,
+    16 cracks, 20 quasi-static pressure steps in mixed precision, AM to 1e-3)."""
+    import torch
+    import vpfhf_b200 as vg
+    from vpfhf_b200 import workloads as wl
+    rank, world, local = _rank()
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    prob = wl.c5_problem() if args.config == "c5" else wl.c3_problem()
+    if args.grid != N_EDGE:  # smaller instance of the same set-up (tests, probes)
+        scale = args.grid / prob["n"][0]
+        n = tuple(max(9, int(round((k - 1) * scale)) + 1) for k in prob["n"])
+        prob = (wl.c5_problem(n=n) if args.config == "c5" else wl.c3_problem(n=n))
+    gen_s = time.perf_counter() - t0
+    ctx = wl.make_context(vg, prob)
+    n = prob["n"]
+    out = {"config": args.config, "grid": list(n), "u_dofs": 3 * ctx.N, "setup_s": round(gen_s, 2),
+           "cracks": len(prob["pennies"])}
+    if args.config == "c5":
+        res, fields = {}, {}
+        for prec in ("fp64", "mixed"):
+            recs = _am_run(ctx, prob, prec, args.am_steps)
+            res[prec] = dict(s_per_step=float(np.mean([r["s"] for r in recs[1:]])),
+                             kspU=[r["kspU"] for r in recs], kspV=[r["kspV"] for r in recs],
+                             **_energies(ctx))
+            fields[prec] = ctx.get_field("V")
+        out.update({
+            "am_its": args.am_steps,
+            "am_steps_per_s": {k: round(1.0 / res[k]["s_per_step"], 4) for k in res},
+            "mixed_over_fp64": round(res["fp64"]["s_per_step"] / res["mixed"]["s_per_step"], 3),
+            "mixed_vs_fp64_rel": {k: abs(res["mixed"][k] - res["fp64"][k]) / abs(res["fp64"][k])
+                                  for k in ("elastic", "pressure_work", "surface", "cov")},
+            "mixed_vs_fp64_v_linf": float(np.abs(fields["mixed"] - fields["fp64"]).max()),
+            "fp64": res["fp64"], "mixed": res["mixed"]})
+    else:
+        pfull = prob["pressure"]
+        steps, am_total, t_total = [], 0, 0.0
+        for k in range(1, args.load_steps + 1):
+            ctx.set_field("pressure", pfull * (k / args.load_steps))
+            ctx.time_step_prepare()
+            recs = _am_run(ctx, prob, "mixed", args.max_am, altmintol=1e-3, reset=False)
+            am_total += len(recs)
+            t_total += sum(r["s"] for r in recs)
+            steps.append(dict(step=k, am_its=len(recs), last_err=recs[-1]["err"],
+                              s=round(sum(r["s"] for r in recs), 3), **_energies(ctx)))
+        out.update({"precision": "mixed", "load_steps": args.load_steps, "altmintol": 1e-3,
+                    "max_am_per_step": args.max_am, "am_steps": am_total,
+                    "am_steps_per_s": round(am_total / t_total, 4), "solve_s": round(t_total, 2),
+                    "steps": steps})
+    ctx.close()
+    if rank == 0:
+        print(json.dumps(out))
+
+
 def cpu_reference(args, quick=False):
     """The reference's KSP matvec (AIJ SpMV, restated in the oracle) on the host cores."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -414,6 +495,10 @@ def main():
     ap.add_argument("--grid", type=int, default=N_EDGE, help="nodes per axis (profiling runs)")
     ap.add_argument("--only-apply", action="store_true",
                     help="time the operator applications only (profiling runs)")
+    ap.add_argument("--config", default="c2", choices=["c2", "c3", "c5"],
+                    help="c2: the headline line; c3 / c5: the large set-ups (one JSON line)")
+    ap.add_argument("--load-steps", type=int, default=20, help="c3 quasi-static steps")
+    ap.add_argument("--max-am", type=int, default=25, help="c3 AM cap per load step")
     ap.add_argument("--only-am", action="store_true",
                     help="run the AM steps only, with a per-solve breakdown; the last step of "
                          "--profile-precision is bracketed by cudaProfilerStart/Stop")
@@ -423,6 +508,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.config in ("c3", "c5"):
+        run_large(args)
     else:
         run_gpu(args)
 

@@ -212,3 +212,34 @@ def test_context_reuse_across_problems(cuda, precision):
     assert got[2] == ref[2] and got[3] == ref[3]
     reused.close()
     fresh.close()
+
+
+def test_sneddon_penny_crack_opening(cuda):
+    """Sneddon's crack opening volume 16 (1 - nu^2) p a^3 / (3 E) of a pressurised penny
+    crack, with a band of fully broken elements (thickness 2h) as the crack: the
+    computed COV converges to it at first order in h; the Richardson extrapolation of
+    the two finest grids is within 10 %.  Clapeyron W_p = 2 E_el holds throughout."""
+    import vpfhf_b200 as vg
+    E, nu, p, a, L = 1e10, 0.25, 1e6, 0.8, 4.0
+    sneddon = 16 * (1 - nu ** 2) * p * a ** 3 / (3 * E)
+    hs, ratios = [], []
+    for n in (97, 129, 161):
+        h = L / (n - 1)
+        ctx = vg.VFContext((n, n, n), (L, L, L), dict(E=E, nu=nu, Gc=100.0), epsilon=2 * h,
+                           eta=1e-8, atnum=1, pressurize=True)
+        ctx.set_bc(vg.rollers())
+        ctx.set_field("pressure", np.full(ctx.N, p))
+        ctx.init_cracks([dict(center=(2.0, 2.0, 2.0), r=a, theta=0.0, phi=0.0, thickness=2 * h)])
+        ctx.time_step_prepare()
+        rc, st = ctx.step_u()
+        assert rc == 0, st
+        el, _, pw = ctx.u_energy()
+        assert pw == pytest.approx(2 * el, rel=1e-3)
+        hs.append(h)
+        ratios.append(ctx.crack_opening() / sneddon)
+        ctx.close()
+    assert ratios[0] > ratios[1] > ratios[2] > 1.0
+    for h, r in zip(hs, ratios):  # first order: (ratio - 1) a / h roughly constant
+        assert 4.0 < (r - 1) * a / h < 8.0
+    extrap = (ratios[2] * hs[1] - ratios[1] * hs[2]) / (hs[1] - hs[2])
+    assert abs(extrap - 1) < 0.1

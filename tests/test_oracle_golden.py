@@ -92,3 +92,19 @@ def test_clapeyron_penny_crack(oracle_mod):
     assert st.reason > 0
     el, pw = o.u_energy(u, v, p=p)
     assert pw == pytest.approx(2 * el, rel=1e-4)
+
+
+def test_penny_surface_energy_converges_to_gc_area(oracle_mod):
+    """AT1 surface energy of the initial penny profile (VFCracks.c:185-227 through
+    VF_VEnergy3D) tends to Gc pi r^2 at first order in eps: the excess over Gc pi r^2,
+    divided by Gc 2 pi r eps (the crack front's share), stays ~0.83 as eps halves."""
+    r, Gc = 1.2, 100.0
+    excess = []
+    for n, eps in ((81, 0.1), (121, 0.0667)):
+        o = oracle_mod.Oracle((n, n, n), (4.0, 4.0, 4.0), E=1e10, nu=0.25, Gc=Gc, epsilon=eps,
+                              eta=1e-8, atnum=1)
+        s = o.v_energy(o.penny_v((2.0, 2.0, 2.0), r))
+        excess.append((s - Gc * np.pi * r * r) / (Gc * 2 * np.pi * r * eps))
+        assert abs(s / (Gc * np.pi * r * r) - 1) < 1.8 * eps / r
+    assert 0.7 < excess[0] < 0.95 and 0.7 < excess[1] < 0.95
+    assert abs(excess[0] - excess[1]) < 0.05

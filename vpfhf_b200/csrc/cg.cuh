@@ -21,8 +21,12 @@ struct CGState {
   int its, maxit, done, reason;
 };
 
-constexpr int RED_THREADS = 256, RED_BLOCKS = 296;
+// Fixed reduction grid (4 blocks per SM of a B200): the block partials are summed in
+// a fixed order, so every reduction is deterministic.
+constexpr int RED_THREADS = 256, RED_BLOCKS = 592;
 
+// The vectors are whole device allocations (16-byte aligned: the kernels use 16-byte
+// loads and stores).
 template <typename T> struct CGVecs {
   T* x;              // solution
   T* r;              // residual

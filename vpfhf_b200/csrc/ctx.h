@@ -47,8 +47,8 @@ struct vfgpu_ctx {
 
   // solver work space, allocated at the first solve (see solve_buffers in step.cu)
   static constexpr int NP64 = 9, NP32 = 5;
-  double* p64[NP64] = {nullptr};  // 3N doubles each
-  float* p32[NP32] = {nullptr};   // 3N floats each
+  double* p64[NP64] = {nullptr};  // 3N + kPoolSlack doubles each
+  float* p32[NP32] = {nullptr};   // 3N + kPoolSlack floats each
   double* coef64 = nullptr;       // 27 per cell: V coupling coefficient
   float* coef32 = nullptr;
   uint8_t* vmask = nullptr;       // N
@@ -77,4 +77,9 @@ struct vfgpu_ctx {
 
 namespace vfgpu {
 int64_t field_len(const vfgpu_ctx* c, int field);
+// Solver pools hold 3N + kPoolSlack values; N-vectors carved from them start at
+// multiples of pool_stride(N) (a multiple of 4 values: 16-byte aligned for float
+// and double).
+constexpr int64_t kPoolSlack = 16;
+inline int64_t pool_stride(int64_t n) { return (n + 3) & ~int64_t(3); }
 }

@@ -51,6 +51,49 @@ __device__ __forceinline__ void final_sum(const double* __restrict__ partial, do
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n);              \
        i += (int64_t)gridDim.x * blockDim.x)
 
+// 16-byte packets for the bandwidth-bound CG kernels: W values of T per load/store.
+// The CG vectors are whole cudaMalloc allocations (256-byte aligned); the n % W tail
+// is done with scalar accesses by the first threads of the grid.
+template <typename T> struct Pack {
+  static constexpr int W = 16 / sizeof(T);
+  T e[W];
+};
+template <typename T>
+__device__ __forceinline__ Pack<T> ld16(const T* __restrict__ a, int64_t c) {
+  Pack<T> p;
+  if constexpr (sizeof(T) == 8) {
+    const double2 q = reinterpret_cast<const double2*>(a)[c];
+    p.e[0] = q.x;
+    p.e[1] = q.y;
+  } else {
+    const float4 q = reinterpret_cast<const float4*>(a)[c];
+    p.e[0] = q.x;
+    p.e[1] = q.y;
+    p.e[2] = q.z;
+    p.e[3] = q.w;
+  }
+  return p;
+}
+template <typename T>
+__device__ __forceinline__ void st16(T* __restrict__ a, int64_t c, const Pack<T>& p) {
+  if constexpr (sizeof(T) == 8) {
+    reinterpret_cast<double2*>(a)[c] = make_double2(p.e[0], p.e[1]);
+  } else {
+    reinterpret_cast<float4*>(a)[c] = make_float4(p.e[0], p.e[1], p.e[2], p.e[3]);
+  }
+}
+// Visits the n values as 16-byte packets (fp(packet index)), then the tail of
+// n % W values one by one (ft(element index)).
+template <typename T, class FP, class FT>
+__device__ __forceinline__ void pack_loop(int64_t n, FP fp, FT ft) {
+  constexpr int W = Pack<T>::W;
+  const int64_t np = n / W;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t c = t0; c < np; c += st) fp(c);
+  for (int64_t i = np * W + t0; i < n; i += st) ft(i);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) cg_init_kernel(CGVecs<T> v, double* partial) {
   double acc[2] = {0., 0.};
@@ -99,7 +142,14 @@ __global__ void __launch_bounds__(RED_THREADS) cg_pw_kernel(CGVecs<T> v, const C
                                                             double* partial) {
   if (st->done) return;
   double acc[1] = {0.};
-  GRID_LOOP(i, v.n) acc[0] += (double)v.p[i] * (double)v.w[i];
+  pack_loop<T>(
+      v.n,
+      [&](int64_t c) {
+        const Pack<T> p = ld16(v.p, c), w = ld16(v.w, c);
+#pragma unroll
+        for (int k = 0; k < Pack<T>::W; k++) acc[0] += (double)p.e[k] * (double)w.e[k];
+      },
+      [&](int64_t i) { acc[0] += (double)v.p[i] * (double)v.w[i]; });
   block_sum<1>(acc, partial);
 }
 
@@ -124,15 +174,31 @@ __global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, con
   if (st->done) return;
   const T a = (T)st->alpha;
   double acc[2] = {0., 0.};
-  GRID_LOOP(i, v.n) {
-    const T x = v.x[i] + a * v.p[i];
-    const T r = v.r[i] - a * v.w[i];
-    const T z = r * v.dinv[i];
-    v.x[i] = x;
-    v.r[i] = r;
-    acc[0] += (double)z * (double)r;
-    acc[1] += (double)z * (double)z;
-  }
+  pack_loop<T>(
+      v.n,
+      [&](int64_t c) {
+        Pack<T> x = ld16(v.x, c), r = ld16(v.r, c);
+        const Pack<T> p = ld16(v.p, c), w = ld16(v.w, c), d = ld16(v.dinv, c);
+#pragma unroll
+        for (int k = 0; k < Pack<T>::W; k++) {
+          x.e[k] = x.e[k] + a * p.e[k];
+          r.e[k] = r.e[k] - a * w.e[k];
+          const T z = r.e[k] * d.e[k];
+          acc[0] += (double)z * (double)r.e[k];
+          acc[1] += (double)z * (double)z;
+        }
+        st16(v.x, c, x);
+        st16(v.r, c, r);
+      },
+      [&](int64_t i) {
+        const T x = v.x[i] + a * v.p[i];
+        const T r = v.r[i] - a * v.w[i];
+        const T z = r * v.dinv[i];
+        v.x[i] = x;
+        v.r[i] = r;
+        acc[0] += (double)z * (double)r;
+        acc[1] += (double)z * (double)z;
+      });
   block_sum<2>(acc, partial);
 }
 
@@ -171,7 +237,16 @@ template <typename T>
 __global__ void cg_p_kernel(CGVecs<T> v, const CGState* st) {
   if (st->done) return;
   const T b = (T)st->beta;
-  GRID_LOOP(i, v.n) v.p[i] = v.r[i] * v.dinv[i] + b * v.p[i];
+  pack_loop<T>(
+      v.n,
+      [&](int64_t c) {
+        Pack<T> p = ld16(v.p, c);
+        const Pack<T> r = ld16(v.r, c), d = ld16(v.dinv, c);
+#pragma unroll
+        for (int k = 0; k < Pack<T>::W; k++) p.e[k] = r.e[k] * d.e[k] + b * p.e[k];
+        st16(v.p, c, p);
+      },
+      [&](int64_t i) { v.p[i] = v.r[i] * v.dinv[i] + b * v.p[i]; });
 }
 
 // ---- generic vector kernels ----
@@ -348,8 +423,16 @@ cudaError_t cg_init(const CGVecs<T>& v, CGState* st, double* partial, double rto
   return cudaGetLastError();
 }
 
+template <typename T> static bool aligned16(const CGVecs<T>& v) {
+  const void* ps[] = {v.x, v.r, v.p, v.w, v.dinv};
+  for (const void* p : ps)
+    if (reinterpret_cast<uintptr_t>(p) % 16) return false;
+  return true;
+}
+
 template <typename T>
 cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s) {
+  if (!aligned16(v)) return cudaErrorMisalignedAddress;  // caught on the host, nothing launched
   cg_pw_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);
   cg_alpha_final<<<1, RED_THREADS, 0, s>>>(st, partial);
   cg_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);

@@ -39,7 +39,8 @@ void free_solver(vfgpu_ctx* c) {
 static int solve_buffers(vfgpu_ctx* c) {
   if (c->have_solver) return VFGPU_OK;
   cudaError_t e = cudaSuccess;
-  const size_t n3 = 3 * (size_t)c->N;
+  // 3N values plus slack, so that three N-vectors carved at 16-byte aligned offsets fit
+  const size_t n3 = 3 * (size_t)c->N + kPoolSlack;
   for (auto& p : c->p64)
     if (e == cudaSuccess) e = cudaMalloc((void**)&p, n3 * sizeof(double));
   for (auto& p : c->p32)
@@ -428,14 +429,16 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   w.limit = o.time_limit;
   const int64_t N = c->N;
   const bool mixed = o.precision == VFGPU_MIXED, at2 = c->vf.atnum == 2;
-  // N-sized work vectors carved from the 3N pool
-  double *lb = c->p64[0], *ub = c->p64[0] + N, *b = c->p64[0] + 2 * N;
-  double *dinv = c->p64[1], *F = c->p64[1] + N, *Y = c->p64[1] + 2 * N;
-  double *Wt = c->p64[2], *Fw = c->p64[2] + N, *tmp = c->p64[2] + 2 * N;
-  double *R = c->p64[3], *P = c->p64[3] + N, *Wv = c->p64[3] + 2 * N;
+  // N-sized work vectors carved from the 3N pools at 16-byte aligned offsets (the CG
+  // kernels use 16-byte accesses)
+  const int64_t Na = pool_stride(N);
+  double *lb = c->p64[0], *ub = c->p64[0] + Na, *b = c->p64[0] + 2 * Na;
+  double *dinv = c->p64[1], *F = c->p64[1] + Na, *Y = c->p64[1] + 2 * Na;
+  double *Wt = c->p64[2], *Fw = c->p64[2] + Na, *tmp = c->p64[2] + 2 * Na;
+  double *R = c->p64[3], *P = c->p64[3] + Na, *Wv = c->p64[3] + 2 * Na;
   double* Vy = c->p64[4];  // N: accumulated correction of the mixed solve
   float *dinv32 = c->p32[4], *x32 = c->p32[0], *r32 = c->p32[1], *pp32 = c->p32[2], *w32 = c->p32[3];
-  float* b32 = c->p32[4] + N;
+  float* b32 = c->p32[4] + Na;
   double* V = c->f[VFGPU_FIELD_V];
   uint8_t* mask = c->vmask;
   ElemArgs E = elem_args(c);
@@ -650,7 +653,7 @@ int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
   b += N * 4 + (g->nz - 1) + 3 * N + 3 * N;              // V32, layers, BC kinds and bits
   b += (long long)(p64.seamX + p64.seamY) * 8 + (long long)(p32.seamX + p32.seamY) * 4;
   b += 2 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
-  b += vfgpu_ctx::NP64 * 3 * N * 8 + vfgpu_ctx::NP32 * 3 * N * 4;  // solver work space
+  b += vfgpu_ctx::NP64 * (3 * N + kPoolSlack) * 8 + vfgpu_ctx::NP32 * (3 * N + kPoolSlack) * 4;
   b += 27 * NC * 12 + N;                                 // V coefficient (FP64 + FP32), mask
   b += (RED_BLOCKS + energy_blocks()) * 4 * 8 + 4096;    // reductions, scalars
   *bytes = b;
@@ -682,7 +685,8 @@ int vfgpu_v_residual(vfgpu_ctx* c, double* F) {
   if (rc) return rc;
   ElemArgs E = elem_args(c);
   const int64_t N = c->N;
-  double *b = c->p64[0], *tmp = c->p64[0] + N, *Fd = c->p64[0] + 2 * N;
+  const int64_t Na = pool_stride(N);
+  double *b = c->p64[0], *tmp = c->p64[0] + Na, *Fd = c->p64[0] + 2 * Na;
   cudaError_t e = launch_v_coef(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_THETA],
                                 c->f[VFGPU_FIELD_THETAREF], c->coef64, nullptr, c->stream);
   if (e == cudaSuccess) e = launch_v_rhs(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_PRESSURE], b, c->stream);
