@@ -13,8 +13,9 @@ def test_modal_element_matches_element_matrix(oracle_mod):
     for _ in range(4):
         v, x = rng.uniform(0, 1, 8), rng.standard_normal(24)
         yref = o.u_element_matrix(0, 0, 0, v) @ x
-        y = km.u_element(x.reshape(8, 3), v, lam, mu, 1e-3, (0.3, 0.5, 0.7)).reshape(24)
-        assert np.abs(y - yref).max() <= 1e-14 * np.abs(yref).max()
+        for f in (km.u_element, km.u_element_points):
+            y = f(x.reshape(8, 3), v, lam, mu, 1e-3, (0.3, 0.5, 0.7)).reshape(24)
+            assert np.abs(y - yref).max() <= 1e-14 * np.abs(yref).max()
 
 
 @pytest.mark.parametrize("n,TY,zc", [((37, 21, 13), 8, 5), ((34, 10, 7), 4, 3), ((3, 2, 4), 8, 2)])

@@ -1,5 +1,6 @@
 // apply.cu -- instantiations of the tile engine for the U and V operators.
 #include <mutex>
+#include <type_traits>
 
 #include "kernels.h"
 #include "ops.cuh"
@@ -7,19 +8,35 @@
 namespace vfgpu {
 
 constexpr int U_TY = 8, V_TY = 8;
+// FP32 U operator: scalar UOp<float> (2 CTAs of 8 warps per SM) by default.  The
+// packed two-lane variant (UOpF2: two elements per thread, half the arithmetic
+// instructions) is kept as a build option; it needs 255 registers, so one CTA of
+// 8 warps per SM, and measured slower on B200: 0.210 ms against 0.197 ms at 129^3,
+// 0.405 ms against 0.354 ms at 161^3 (16 element rows; 0.219 / 0.395 ms with 8).
+#ifndef VFGPU_U32_PACKED
+#define VFGPU_U32_PACKED 0
+#endif
+#ifndef VFGPU_U32_PACKED_TY
+#define VFGPU_U32_PACKED_TY 16
+#endif
+constexpr bool kU32Packed = VFGPU_U32_PACKED != 0;
+constexpr int U32_TY = kU32Packed ? VFGPU_U32_PACKED_TY : U_TY;
+constexpr int U32_MINB = kU32Packed ? (VFGPU_U32_PACKED_TY == 16 ? 1 : 2) : 2;
+using U32Op = std::conditional_t<kU32Packed, UOpF2, UOp<float>>;
 
 cudaError_t apply_kernel_attributes() {
   static std::mutex m;  // contexts may be created from several threads
   std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOp<float>, U_TY, 2>();
+  if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, 3>();
   return e;
 }
 
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
-  return tile_plan(nx, ny, nz, U_TY, 3, prec_bytes == 8 ? 1 : 2, num_sms);
+  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U_TY, 3, 1, num_sms);
+  return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
 }
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   return tile_plan(nx, ny, nz, V_TY, 1, prec_bytes == 8 ? 2 : 3, num_sms);
@@ -33,7 +50,7 @@ cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& 
 template <>
 cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
                                   const LayerTable& L, cudaStream_t s) {
-  return launch_tile_apply<UOp<float>, U_TY, 2>(A, p, L, s);
+  return launch_tile_apply<U32Op, U32_TY, U32_MINB>(A, p, L, s);
 }
 template <>
 cudaError_t launch_v_apply<double>(const VApplyArgs<double>& A, const TilePlan& p,

@@ -12,27 +12,16 @@
 //        treatment (VFCartFE.c:1305-1454, VFMech.c:2637-2682).
 #pragma once
 
+#include "f2.cuh"
 #include "tile_engine.cuh"
 #include "u_apply.cuh"
 
-// Per-precision choice of the z-moment accumulation in u_element (see u_apply.cuh).
-#ifndef VFGPU_UZDIRECT_F64
-#define VFGPU_UZDIRECT_F64 0
-#endif
-#ifndef VFGPU_UZDIRECT_F32
-#define VFGPU_UZDIRECT_F32 0
-#endif
-
 namespace vfgpu {
-
-template <typename T> constexpr bool uzdirect() {
-  return sizeof(T) == 8 ? VFGPU_UZDIRECT_F64 != 0 : VFGPU_UZDIRECT_F32 != 0;
-}
 
 template <typename T_> struct UOp {
   using T = T_;
   using Args = UApplyArgs<T>;
-  static constexpr int NC = 3, NIN = 4;
+  static constexpr int NC = 3, NIN = 4, EPT = 1;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + 3 * n;
     src[1] = A.x + 3 * n + 1;
@@ -62,12 +51,63 @@ template <typename T_> struct UOp {
       lam = T(LT.lambda[layer]);
       mu = T(LT.mu[layer]);
     }
-    u_element<T, uzdirect<T>()>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+    u_element<T>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
     const unsigned b = A.bc ? A.bc[n] : 0u;
 #pragma unroll
     for (int c = 0; c < 3; c++) A.y[3 * n + c] = ((b >> c) & 1u) ? A.x[3 * n + c] : val[c];
+  }
+};
+
+// The FP32 U operator on two y-adjacent elements per thread, one per lane of the
+// packed FP32 instructions (f2): the same arithmetic as UOp<float> with half the
+// instructions.
+struct UOpF2 {
+  using T = float;
+  using Args = UApplyArgs<float>;
+  static constexpr int NC = 3, NIN = 4, EPT = 2;
+  __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
+    UOp<float>::node_src(A, n, src);
+  }
+  __device__ __forceinline__ static void element_multi(const Args& A, const LayerTable& L, int ex,
+                                                       const int (&ey)[2], int ez, const bool (&ok)[2],
+                                                       const T (&in)[2][8][NIN], T (&out)[2][8][NC]) {
+    f2 xn[8][3], vn[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) xn[a][c] = f2(in[0][a][c], in[1][a][c]);
+      vn[a] = f2(in[0][a][3], in[1][a][3]);
+    }
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    const LayerTable& LT = A.P ? A.P->L : L;
+    const float eta = A.P ? float(A.P->eta) : A.eta;
+    f2 lam, mu;
+    if (A.cellE) {
+      float E[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++)
+        E[e] = ok[e] ? A.cellE[((int64_t)ez * (A.ny - 1) + ey[e]) * (A.nx - 1) + ex] : 0.f;
+      const f2 Ep(E[0], E[1]);
+      lam = Ep * f2(float(LT.lamfac[layer]));
+      mu = Ep * f2(float(LT.mufac[layer]));
+    } else {
+      lam = f2(float(LT.lambda[layer]));
+      mu = f2(float(LT.mu[layer]));
+    }
+    f2 y[8][3];
+    u_element<f2>(xn, vn, lam, mu, f2(eta), f2(A.ihx), f2(A.ihy), f2(A.ihz), f2(A.vol), y);
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        out[0][a][c] = ok[0] ? y[a][c].v.x : 0.f;
+        out[1][a][c] = ok[1] ? y[a][c].v.y : 0.f;
+      }
+  }
+  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    UOp<float>::finish_node(A, n, val);
   }
 };
 
@@ -181,7 +221,7 @@ __device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict_
 template <typename T_> struct VOp {
   using T = T_;
   using Args = VApplyArgs<T>;
-  static constexpr int NC = 1, NIN = 1;
+  static constexpr int NC = 1, NIN = 1, EPT = 1;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + n;
   }

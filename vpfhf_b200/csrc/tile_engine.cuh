@@ -13,10 +13,14 @@
 // fixed order by seam_fixup_kernel.  The result is deterministic (no atomics)
 // and independent of the chunking in z.
 //
-// Op supplies:  NC, NIN (per-node inputs staged in smem), the Args type with
+// Op supplies:  NC, NIN (per-node inputs staged in smem), EPT (elements per
+//   thread: 1, or 2 for an operator that evaluates two y-adjacent elements at once
+//   in the two lanes of packed FP32 instructions), the Args type with
 //   x/y/seamX/seamY/nx/ny/nz/ntx/nty/zc members, and
 //   node_src(A, n, src[NIN]) (global addresses of a node's inputs),
-//   element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]),
+//   element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]) (EPT = 1) or
+//   element_multi(A, L, ex, ey[EPT], ez, ok[EPT], in[EPT][8][NIN], out[EPT][8][NC])
+//   (EPT > 1; out[e] must be 0 where ok[e] is false),
 //   finish_node(A, n, val[NC]) (writes y, applying Dirichlet rows / masks), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
 //   so that a queued batch of iterations costs nothing once it is done).
@@ -26,8 +30,11 @@
 
 namespace vfgpu {
 
-template <int TY> struct Tile {
-  static constexpr int BX = 33, BY = TY + 1, NT = 32 * TY;
+// TY element rows per tile; an Op with EPT = 2 gives every thread two y-adjacent
+// elements (TY / EPT thread rows).
+template <int TY, int EPT = 1> struct Tile {
+  static_assert(TY % EPT == 0, "element rows must split evenly over thread rows");
+  static constexpr int BX = 33, BY = TY + 1, TR = TY / EPT, NT = 32 * TR;
   static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
 };
 
@@ -55,10 +62,11 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 template <class Op, int TY, int MINB>
-__global__ void __launch_bounds__(32 * TY, MINB)
+__global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     tile_apply_kernel(const typename Op::Args A, const LayerTable L) {
   using T = typename Op::T;
-  using G = Tile<TY>;
+  using G = Tile<TY, Op::EPT>;
+  constexpr int EPT = Op::EPT;
   constexpr int NC = Op::NC, NIN = Op::NIN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sx = reinterpret_cast<T*>(smem_raw);  // [3 ring][NIN][BY][BX]
@@ -124,31 +132,74 @@ __global__ void __launch_bounds__(32 * TY, MINB)
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
   for (int k = kf; k <= kl; k++) {
     const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = (k - kf) & 1;
-    const int ex = X0 + lane, ey = Y0 + wy;
-    T yc[8][NC];
-    if (ex < nex && ey < ney) {
-      T in[8][NIN];
+    const int ex = X0 + lane;
+    if constexpr (EPT == 1) {
+      const int ey = Y0 + wy;
+      T yc[8][NC];
+      if (ex < nex && ey < ney) {
+        T in[8][NIN];
 #pragma unroll
-      for (int kk = 0; kk < 2; kk++)
+        for (int kk = 0; kk < 2; kk++)
 #pragma unroll
-        for (int j = 0; j < 2; j++)
+          for (int j = 0; j < 2; j++)
 #pragma unroll
-          for (int i = 0; i < 2; i++) {
-            const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
+            for (int i = 0; i < 2; i++) {
+              const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
 #pragma unroll
-            for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
-          }
-      Op::element(A, L, ex, ey, k, in, yc);
-    } else {
+              for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
+            }
+        Op::element(A, L, ex, ey, k, in, yc);
+      } else {
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) yc[a][c] = T(0);
+      }
 #pragma unroll
       for (int a = 0; a < 8; a++)
 #pragma unroll
-        for (int c = 0; c < NC; c++) yc[a][c] = T(0);
+        for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, wy, lane) = yc[a][c];
+    } else {
+      // element rows EPT*wy + e, e < EPT (node rows EPT*wy .. EPT*wy + EPT)
+      int ey[EPT];
+      bool ok[EPT], any = false;
+#pragma unroll
+      for (int e = 0; e < EPT; e++) {
+        ey[e] = Y0 + EPT * wy + e;
+        ok[e] = ex < nex && ey[e] < ney;
+        any = any || ok[e];
+      }
+      T yc[EPT][8][NC];
+      if (any) {
+        T in[EPT][8][NIN];
+#pragma unroll
+        for (int e = 0; e < EPT; e++)
+#pragma unroll
+          for (int kk = 0; kk < 2; kk++)
+#pragma unroll
+            for (int j = 0; j < 2; j++)
+#pragma unroll
+              for (int i = 0; i < 2; i++) {
+                const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
+#pragma unroll
+                for (int q = 0; q < NIN; q++) in[e][a][q] = SXA(buf, q, EPT * wy + e + j, lane + i);
+              }
+        Op::element_multi(A, L, ex, ey, k, ok, in, yc);
+      } else {
+#pragma unroll
+        for (int e = 0; e < EPT; e++)
+#pragma unroll
+          for (int a = 0; a < 8; a++)
+#pragma unroll
+            for (int c = 0; c < NC; c++) yc[e][a][c] = T(0);
+      }
+#pragma unroll
+      for (int e = 0; e < EPT; e++)
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+          for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, EPT * wy + e, lane) = yc[e][a][c];
     }
-#pragma unroll
-    for (int a = 0; a < 8; a++)
-#pragma unroll
-      for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, wy, lane) = yc[a][c];
     cp_async_wait_all();  // this thread's copies of plane k+2 have landed
     __syncthreads();      // ... and everyone's; corner contributions of layer k visible
     if (k + 3 <= kl + 1) fetch_plane(r0, k + 3);  // plane k is no longer read
@@ -294,7 +345,7 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
   constexpr size_t smem = tile_smem_bytes<Op, TY>();
   cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
   if (ea != cudaSuccess) return ea;
-  dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY);
+  dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY / Op::EPT);
   tile_apply_kernel<Op, TY, MINB><<<grid, block, smem, s>>>(A, L);
   const int64_t nseam = (int64_t)(p.ntx - 1) * A.nz * A.ny + (int64_t)(p.nty - 1) * A.nz * A.nx;
   if (nseam > 0) {

@@ -75,10 +75,12 @@ __device__ __forceinline__ void modal8(const T (&f)[8], T (&m)[8]) {
 template <typename T> __device__ __forceinline__ T lin(int g, T a, T b) {
   return g == 1 ? a : (g == 0 ? fma(b, T(-VF_TAU), a) : fma(b, T(VF_TAU), a));
 }
-template <typename T> __device__ __forceinline__ T gw(int g) { return g == 1 ? T(VF_W1) : T(VF_W0); }
-template <typename T> __device__ __forceinline__ T gt(int g) {
-  return g == 1 ? T(0) : (g == 0 ? T(-VF_TAU) : T(VF_TAU));
-}
+// Gauss weights and points as double constants (products of them fold at compile
+// time before the conversion to T).
+__device__ __forceinline__ constexpr double gwd(int g) { return g == 1 ? VF_W1 : VF_W0; }
+__device__ __forceinline__ constexpr double gtd(int g) { return g == 1 ? 0.0 : (g == 0 ? -VF_TAU : VF_TAU); }
+template <typename T> __device__ __forceinline__ T gw(int g) { return T(gwd(g)); }
+template <typename T> __device__ __forceinline__ T gt(int g) { return T(gtd(g)); }
 
 // Moment update q[0..3] += s * {1, t1, t2, t1 t2} for Gauss indices (g1, g2).
 template <typename T>
@@ -86,7 +88,7 @@ __device__ __forceinline__ void moment4(T (&q)[4], int g1, int g2, T s) {
   q[0] += s;
   if (g1 != 1) q[1] = fma(gt<T>(g1), s, q[1]);
   if (g2 != 1) q[2] = fma(gt<T>(g2), s, q[2]);
-  if (g1 != 1 && g2 != 1) q[3] = fma(gt<T>(g1) * gt<T>(g2), s, q[3]);
+  if (g1 != 1 && g2 != 1) q[3] = fma(T(gtd(g1) * gtd(g2)), s, q[3]);
 }
 
 // A[s1][s2] = (Q0/4 + s1 Q1/2 + s2 Q2/2 + s1 s2 Q3) / h, s = -1 (index 0) or +1 (index 1).
@@ -101,10 +103,29 @@ __device__ __forceinline__ void inv_butterfly(const T (&Q)[4], T ih, T (&A)[2][2
   A[1][1] = r0p + r1p;
 }
 
-// y[a][c] = (K_e(v) x_e)[a][c] for one element.  ZDIRECT accumulates the z-direction
-// moments at every Gauss point instead of summing over gz first (fewer live
-// registers, ~8% more arithmetic).
-template <typename T, bool ZDIRECT = false>
+// (s0 a0 + s1 a1) + s2 a2 with s = -1 for index 0 and +1 for index 1, written with
+// subtractions instead of negations (bit-identical: negation is exact and rounding
+// is sign-symmetric).
+template <typename T>
+__device__ __forceinline__ T signed_sum3(T a0, T a1, T a2, int i, int j, int k) {
+  if (i && j) return k ? (a0 + a1) + a2 : (a0 + a1) - a2;
+  if (i) return k ? (a0 - a1) + a2 : (a0 - a1) - a2;
+  if (j) return k ? (a1 - a0) + a2 : (a1 - a0) - a2;
+  return k ? a2 - (a0 + a1) : -((a0 + a1) + a2);
+}
+
+// y[a][c] = (K_e(v) x_e)[a][c] for one element.
+//
+// Along a Gauss row (fixed gy, gz) the gradient is G(t) = G0 + t G1 in t = tx, with
+// G1 having no x column, and v(t)^2 + eta = a0 + a1 t + a2 t^2, so the stress of
+// every point is (a0 + a1 t + a2 t^2)(D0 + t D1), D = lambda tr(G) I + mu (G + G^T).
+// The two sums over the row's three points that the moments need,
+//   M0 = sum_gx w_x s = Wr [(a0 + a2/12) D0 + (a1/12) D1],
+//   M1 = sum_gx w_x t s = Wr [(a1/12) D0 + ((a0 + 0.15 a2)/12) D1],
+// follow from sum w_x = 1, sum w_x t^2 = 1/12, sum w_x t^4 = 1/80 (the odd sums
+// vanish): the same 3-point Gauss sum as point by point, in about 2/3 of the
+// operations.  Wr = vol w_y w_z.
+template <typename T>
 __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
                                           T eta, T ihx, T ihy, T ihz, T vol, T (&y)[8][3]) {
   T m[3][8], mv[8];
@@ -120,7 +141,10 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
   //   d/dx u_c = (m1 + m3 ty + m5 tz + m7 ty tz)/hx, d/dy u_c = (m2 + m3 tx + m6 tz + m7 tx tz)/hy,
   //   d/dz u_c = (m4 + m5 tx + m6 ty + m7 tx ty)/hz; the 1/h scaling is applied per plane/row
   //   so only 21 coefficients stay live.
-  T QX[3][4], QY[3][4], QZ[3][4], SZ[3][3][ZDIRECT ? 1 : 3];
+  // QX, QY, QZ: the 4 bilinear moments per component of the x, y, z stress columns.
+  // SY0/SY1: M0/M1 of the y column summed over the rows of a plane; SZ0/SZ1[c][gy]:
+  // M0/M1 of the z column summed over the planes, per row index.
+  T QX[3][4], QY[3][4], QZ[3][4], SZ0[3][3], SZ1[3][3];
 #pragma unroll
   for (int c = 0; c < 3; c++)
 #pragma unroll
@@ -141,7 +165,9 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
     }
     const T p0 = lin(gz, mv[0], mv[4]), p1 = lin(gz, mv[1], mv[5]);
     const T p2 = lin(gz, mv[2], mv[6]), p3 = lin(gz, mv[3], mv[7]);
-    T SY[3][3];
+    // D1 = D(G1), G1 = [0 | by | be]: the y part is constant over the plane
+    const T e01y = mu * by[0];
+    T SY0[3], SY1[3];
 #pragma unroll
     for (int gy = 0; gy < 3; gy++) {
       T Gx[3], al[3], be[3];
@@ -152,59 +178,68 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
         be[c] = lin(gy, m[c][5], m[c][7]) * ihz;
       }
       const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
-      T SX[3];
-#pragma unroll
-      for (int gx = 0; gx < 3; gx++) {
-        T Gy[3], Gz[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-          Gy[c] = lin(gx, ay[c], by[c]);
-          Gz[c] = lin(gx, al[c], be[c]);
-        }
-        const T vg = lin(gx, q0, q1);
-        const T ws = (volw * (gw<T>(gx) * gw<T>(gy))) * fma(vg, vg, eta);
-        const T tr = Gx[0] + Gy[1] + Gz[2];
-        const T L = (ws * lam) * tr, m2 = ws * mu2, m1 = ws * mu;
-        const T s00 = fma(m2, Gx[0], L), s11 = fma(m2, Gy[1], L), s22 = fma(m2, Gz[2], L);
-        const T s01 = m1 * (Gy[0] + Gx[1]);
-        const T s02 = m1 * (Gz[0] + Gx[2]);
-        const T s12 = m1 * (Gz[1] + Gy[2]);
-        if (gx == 0) {
-          SX[0] = s00; SX[1] = s01; SX[2] = s02;
-        } else {
-          SX[0] += s00; SX[1] += s01; SX[2] += s02;
-        }
-        if (gy == 0) {
-          SY[0][gx] = s01; SY[1][gx] = s11; SY[2][gx] = s12;
-        } else {
-          SY[0][gx] += s01; SY[1][gx] += s11; SY[2][gx] += s12;
-        }
-        if constexpr (ZDIRECT) {
-          moment4(QZ[0], gx, gy, s02);
-          moment4(QZ[1], gx, gy, s12);
-          moment4(QZ[2], gx, gy, s22);
-        } else if (gz == 0) {
-          SZ[0][gy][gx] = s02; SZ[1][gy][gx] = s12; SZ[2][gy][gx] = s22;
-        } else {
-          SZ[0][gy][gx] += s02; SZ[1][gy][gx] += s12; SZ[2][gy][gx] += s22;
-        }
+      // v^2 + eta = a0 + 2 h1 t + a2 t^2 along the row; row weights
+      const T Wr = volw * gw<T>(gy);
+      const T a0 = fma(q0, q0, eta), a2 = q1 * q1, h1 = q0 * q1;
+      const T C0 = Wr * fma(a2, T(1.0 / 12.0), a0);
+      const T C1 = Wr * (h1 * T(1.0 / 6.0));
+      const T E1 = Wr * (fma(a2, T(0.15), a0) * T(1.0 / 12.0));
+      // D0 = D(G0), G0 = [Gx | ay | al]
+      const T L0 = lam * ((Gx[0] + ay[1]) + al[2]);
+      const T d00 = fma(mu2, Gx[0], L0), d11 = fma(mu2, ay[1], L0), d22 = fma(mu2, al[2], L0);
+      const T d01 = mu * (ay[0] + Gx[1]), d02 = mu * (al[0] + Gx[2]), d12 = mu * (al[1] + ay[2]);
+      // D1 = D(G1)
+      const T L1 = lam * (by[1] + be[2]);
+      const T e11 = fma(mu2, by[1], L1), e22 = fma(mu2, be[2], L1);
+      const T e02 = mu * be[0], e12 = mu * (be[1] + by[2]);
+      // M0 of the 6 stress components, M1 of the 5 the y and z columns need
+      const T n00 = fma(C0, d00, C1 * L1), n01 = fma(C0, d01, C1 * e01y);
+      const T n02 = fma(C0, d02, C1 * e02), n11 = fma(C0, d11, C1 * e11);
+      const T n12 = fma(C0, d12, C1 * e12), n22 = fma(C0, d22, C1 * e22);
+      const T o01 = fma(C1, d01, E1 * e01y), o02 = fma(C1, d02, E1 * e02);
+      const T o11 = fma(C1, d11, E1 * e11), o12 = fma(C1, d12, E1 * e12);
+      const T o22 = fma(C1, d22, E1 * e22);
+      moment4(QX[0], gy, gz, n00);
+      moment4(QX[1], gy, gz, n01);
+      moment4(QX[2], gy, gz, n02);
+      if (gy == 0) {
+        SY0[0] = n01; SY0[1] = n11; SY0[2] = n12;
+        SY1[0] = o01; SY1[1] = o11; SY1[2] = o12;
+      } else {
+        SY0[0] += n01; SY0[1] += n11; SY0[2] += n12;
+        SY1[0] += o01; SY1[1] += o11; SY1[2] += o12;
       }
-#pragma unroll
-      for (int c = 0; c < 3; c++) moment4(QX[c], gy, gz, SX[c]);
+      if (gz == 0) {
+        SZ0[0][gy] = n02; SZ0[1][gy] = n12; SZ0[2][gy] = n22;
+        SZ1[0][gy] = o02; SZ1[1][gy] = o12; SZ1[2][gy] = o22;
+      } else {
+        SZ0[0][gy] += n02; SZ0[1][gy] += n12; SZ0[2][gy] += n22;
+        SZ1[0][gy] += o02; SZ1[1][gy] += o12; SZ1[2][gy] += o22;
+      }
     }
+    // QY moments {1, tx, tz, tx tz}: the tx moment is M1
 #pragma unroll
-    for (int gx = 0; gx < 3; gx++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) moment4(QY[c], gx, gz, SY[c][gx]);
+    for (int c = 0; c < 3; c++) {
+      QY[c][0] += SY0[c];
+      QY[c][1] += SY1[c];
+      if (gz != 1) {
+        QY[c][2] = fma(gt<T>(gz), SY0[c], QY[c][2]);
+        QY[c][3] = fma(gt<T>(gz), SY1[c], QY[c][3]);
+      }
+    }
   }
-  if constexpr (!ZDIRECT) {
+  // QZ moments {1, tx, ty, tx ty}
 #pragma unroll
-    for (int gy = 0; gy < 3; gy++)
+  for (int gy = 0; gy < 3; gy++)
 #pragma unroll
-      for (int gx = 0; gx < 3; gx++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) moment4(QZ[c], gx, gy, SZ[c][gy][gx]);
-  }
+    for (int c = 0; c < 3; c++) {
+      QZ[c][0] += SZ0[c][gy];
+      QZ[c][1] += SZ1[c][gy];
+      if (gy != 1) {
+        QZ[c][2] = fma(gt<T>(gy), SZ0[c][gy], QZ[c][2]);
+        QZ[c][3] = fma(gt<T>(gy), SZ1[c][gy], QZ[c][3]);
+      }
+    }
 
   // Inverse butterfly: direction-d part of node (i,j,k) is
   //   s_d/h_d * (Q0/4 + s_1 Q1/2 + s_2 Q2/2 + s_1 s_2 Q3), s = -1 (node 0) or +1 (node 1).
@@ -219,12 +254,8 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
 #pragma unroll
       for (int j = 0; j < 2; j++)
 #pragma unroll
-        for (int i = 0; i < 2; i++) {
-          const T ax_ = i ? A[0][j][k] : -A[0][j][k];
-          const T ay_ = j ? A[1][i][k] : -A[1][i][k];
-          const T az_ = k ? A[2][i][j] : -A[2][i][j];
-          y[i + 2 * j + 4 * k][c] = (ax_ + ay_) + az_;
-        }
+        for (int i = 0; i < 2; i++)
+          y[i + 2 * j + 4 * k][c] = signed_sum3(A[0][j][k], A[1][i][k], A[2][i][j], i, j, k);
   }
 }
 
