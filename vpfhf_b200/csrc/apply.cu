@@ -10,9 +10,9 @@ namespace vfgpu {
 constexpr int U_TY = 8, V_TY = 8;
 // FP32 U operator: scalar UOp<float> (2 CTAs of 8 warps per SM) by default.  The
 // packed two-lane variant (UOpF2: two elements per thread, half the arithmetic
-// instructions) is kept as a build option; it needs 255 registers, so one CTA of
-// 8 warps per SM, and measured slower on B200: 0.210 ms against 0.197 ms at 129^3,
-// 0.405 ms against 0.354 ms at 161^3 (16 element rows; 0.219 / 0.395 ms with 8).
+// instructions) is kept as a build option; it needs 242 registers, so one CTA of
+// 8 warps per SM, and measured slower on B200: 0.185 ms against 0.161 ms at 129^3,
+// 0.353 ms against 0.298 ms at 161^3 (16 element rows; 0.189 / 0.339 ms with 8).
 #ifndef VFGPU_U32_PACKED
 #define VFGPU_U32_PACKED 0
 #endif
