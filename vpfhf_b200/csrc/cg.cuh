@@ -19,6 +19,7 @@ enum { CG_RUNNING = 0, CG_CONVERGED_RTOL = 2, CG_CONVERGED_ATOL = 3, CG_DIVERGED
 struct CGState {
   double rz, rz_new, pw, zz, alpha, beta, rnorm0, ttol, dtol;
   int its, maxit, done, reason;
+  unsigned int arrive;  // blocks of the running update kernel that have finished
 };
 
 // Fixed reduction grid (4 blocks per SM of a B200): the block partials are summed in
@@ -36,9 +37,13 @@ template <typename T> struct CGVecs {
   const T* b;        // right-hand side
   const uint8_t* mask;  // nonzero => dof removed from the system (or null)
   int64_t n;
+  const double* dotp;   // the operator's block partials of p.w (written by the apply), or
+  int ndot;             // null: cg_after_apply computes p.w in a separate pass
 };
 
-// Host-side driver pieces (solver.cu).
+// Host-side driver pieces (solver.cu).  One iteration is: the operator apply
+// w = A p, which also writes the block partials of p.w to v.dotp (the tile
+// engine's A.dot), then cg_after_apply.
 template <typename T>
 cudaError_t cg_init(const CGVecs<T>& v, CGState* st, double* partial, double rtol, double atol,
                     double dtol, int maxit, cudaStream_t s);

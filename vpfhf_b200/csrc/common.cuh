@@ -41,4 +41,21 @@ __host__ __device__ inline int64_t node_index(int i, int j, int k, int nx, int n
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
 
+// Deterministic sum of one double per thread over a block (any 1-3D shape with a
+// multiple of 32 threads): warp shuffle trees, then warp 0 sums the warp totals in
+// order.  `scratch` is shared memory for >= 32 doubles; every thread must call
+// (it contains a barrier); the result is valid in thread 0.
+__device__ __forceinline__ double block_sum_dbl(double v, double* scratch) {
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int nw = (blockDim.x * blockDim.y * blockDim.z) >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((tid & 31) == 0) scratch[tid >> 5] = v;
+  __syncthreads();
+  double s = 0.;
+  if (tid == 0)
+    for (int w = 0; w < nw; w++) s += scratch[w];
+  return s;
+}
+
 }  // namespace vfgpu

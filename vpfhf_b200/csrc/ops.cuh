@@ -53,10 +53,19 @@ template <typename T_> struct UOp {
     }
     u_element<T>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
-  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+  // Writes y of node n (Dirichlet rows: y = x); with DOT, returns x.y over its dofs
+  // (the launch accumulates the CG dot into A.dot).
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
     const unsigned b = A.bc ? A.bc[n] : 0u;
+    double d = 0.;
 #pragma unroll
-    for (int c = 0; c < 3; c++) A.y[3 * n + c] = ((b >> c) & 1u) ? A.x[3 * n + c] : val[c];
+    for (int c = 0; c < 3; c++) {
+      const T y = ((b >> c) & 1u) ? A.x[3 * n + c] : val[c];
+      A.y[3 * n + c] = y;
+      if constexpr (DOT) d += (double)A.x[3 * n + c] * (double)y;
+    }
+    return d;
   }
 };
 
@@ -106,8 +115,9 @@ struct UOpF2 {
         out[1][a][c] = ok[1] ? y[a][c].v.y : 0.f;
       }
   }
-  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
-    UOp<float>::finish_node(A, n, val);
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    return UOp<float>::finish_node<DOT>(A, n, val);
   }
 };
 
@@ -123,6 +133,7 @@ template <typename T> struct VApplyArgs {
   T* __restrict__ seamY;
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   const DevParams* __restrict__ P;    // Gc/(2 c_w) eps per layer
+  double* __restrict__ dot;           // if non-null: per-block partials of x.y
   int nx, ny, nz, ntx, nty, zc;
   T ihx, ihy, ihz, vol;
 };
@@ -237,8 +248,12 @@ template <typename T_> struct VOp {
 #pragma unroll
     for (int a = 0; a < 8; a++) out[a][0] = yn[a];
   }
-  __device__ __forceinline__ static void finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
-    A.y[n] = (A.mask && A.mask[n]) ? T(0) : val[0];
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    const T y = (A.mask && A.mask[n]) ? T(0) : val[0];
+    A.y[n] = y;
+    if constexpr (DOT) return (double)A.x[n] * (double)y;
+    return 0.;
   }
 };
 

@@ -122,6 +122,7 @@ __global__ void cg_init_final(CGState* st, const double* partial, double rtol, d
     st->dtol = dtol;
     st->its = 0;
     st->maxit = maxit;
+    st->arrive = 0;
     st->done = 0;
     st->reason = CG_RUNNING;
     if (!(st->rnorm0 == st->rnorm0)) {
@@ -137,6 +138,53 @@ __global__ void cg_init_final(CGState* st, const double* partial, double rtol, d
   }
 }
 
+// Fixed-order sum of n block partials by one block; every thread gets the result
+// (identical in every block that calls it).  L1 is bypassed: the partials were
+// written by other blocks or by an earlier kernel.
+__device__ __forceinline__ double sum_partials(const double* __restrict__ p, int n) {
+  __shared__ double red[RED_THREADS];
+  double v = 0.;
+  for (int b = threadIdx.x; b < n; b += RED_THREADS) v += __ldcg(p + b);
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int st = RED_THREADS / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  const double s = red[0];
+  __syncthreads();
+  return s;
+}
+
+// End of a CG iteration from the new (r, z) and (z, z): iteration count,
+// convergence tests (KSPConvergedDefault on the preconditioned norm) and beta.
+__device__ __forceinline__ void cg_finish_iteration(CGState* st, double rz, double zz) {
+  st->its += 1;
+  st->zz = zz;
+  const double dp = sqrt(zz);
+  if (!(dp == dp)) {
+    st->done = 1;
+    st->reason = CG_DIVERGED_NAN;
+  } else if (dp <= st->ttol) {
+    st->done = 1;
+    st->reason = CG_CONVERGED_RTOL;
+  } else if (dp >= st->dtol * st->rnorm0) {
+    st->done = 1;
+    st->reason = CG_DIVERGED_DTOL;
+  } else if (st->its >= st->maxit) {
+    st->done = 1;
+    st->reason = CG_DIVERGED_ITS;
+  } else {
+    st->beta = rz / st->rz;
+    st->rz = rz;
+    if (rz == 0.) {
+      st->done = 1;
+      st->reason = CG_CONVERGED_ATOL;
+    }
+  }
+}
+
+// p.w by blocks (for an operator apply that did not produce it).
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) cg_pw_kernel(CGVecs<T> v, const CGState* st,
                                                             double* partial) {
@@ -153,26 +201,30 @@ __global__ void __launch_bounds__(RED_THREADS) cg_pw_kernel(CGVecs<T> v, const C
   block_sum<1>(acc, partial);
 }
 
-__global__ void cg_alpha_final(CGState* st, const double* partial) {
-  if (st->done) return;
-  double s[1];
-  final_sum<1>(partial, s);
-  if (threadIdx.x == 0) {
-    st->pw = s[0];
-    if (!(s[0] > 0.)) {
-      st->done = 1;
-      st->reason = (s[0] == s[0]) ? CG_DIVERGED_INDEFINITE : CG_DIVERGED_NAN;
-    } else {
-      st->alpha = st->rz / s[0];
-    }
-  }
-}
-
+// One CG step after w = A p: every block sums the operator's p.w partials (written
+// by the tile and seam kernels of the apply) to the same alpha = (r,z)/(p,w), updates
+// x and r, and adds its share of (r,z), (z,z) with z = D^-1 r; the last block to
+// finish sums those partials and ends the iteration (cg_finish_iteration).  The
+// arrival counter is the only atomic; every sum has a fixed order.
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, const CGState* st,
+__global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, CGState* st,
                                                                 double* partial) {
   if (st->done) return;
-  const T a = (T)st->alpha;
+  const double pw = sum_partials(v.dotp, v.ndot);
+  if (!(pw > 0.)) {  // same value in every block: all of them stop here
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->pw = pw;
+      st->done = 1;
+      st->reason = (pw == pw) ? CG_DIVERGED_INDEFINITE : CG_DIVERGED_NAN;
+    }
+    return;
+  }
+  const double alpha = st->rz / pw;  // st->rz changes only after every block has arrived
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    st->pw = pw;
+    st->alpha = alpha;
+  }
+  const T a = (T)alpha;
   double acc[2] = {0., 0.};
   pack_loop<T>(
       v.n,
@@ -200,36 +252,36 @@ __global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, con
         acc[1] += (double)z * (double)z;
       });
   block_sum<2>(acc, partial);
-}
-
-__global__ void cg_beta_final(CGState* st, const double* partial) {
-  if (st->done) return;
-  double s[2];
-  final_sum<2>(partial, s);
-  if (threadIdx.x == 0) {
-    st->its += 1;
-    st->zz = s[1];
-    const double dp = sqrt(s[1]);
-    if (!(dp == dp)) {
-      st->done = 1;
-      st->reason = CG_DIVERGED_NAN;
-    } else if (dp <= st->ttol) {
-      st->done = 1;
-      st->reason = CG_CONVERGED_RTOL;
-    } else if (dp >= st->dtol * st->rnorm0) {
-      st->done = 1;
-      st->reason = CG_DIVERGED_DTOL;
-    } else if (st->its >= st->maxit) {
-      st->done = 1;
-      st->reason = CG_DIVERGED_ITS;
-    } else {
-      st->beta = s[0] / st->rz;
-      st->rz = s[0];
-      if (s[0] == 0.) {
-        st->done = 1;
-        st->reason = CG_CONVERGED_ATOL;
-      }
+  __shared__ bool last;
+  __threadfence();  // this block's partials are visible before it is counted
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(&st->arrive, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  double sum[2] = {0., 0.};
+  {
+    __shared__ double red[2][RED_THREADS];
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += RED_THREADS) {
+      sum[0] += __ldcg(partial + 2 * b);
+      sum[1] += __ldcg(partial + 2 * b + 1);
     }
+    red[0][threadIdx.x] = sum[0];
+    red[1][threadIdx.x] = sum[1];
+    __syncthreads();
+    for (int s2 = RED_THREADS / 2; s2 > 0; s2 >>= 1) {
+      if (threadIdx.x < s2) {
+        red[0][threadIdx.x] += red[0][threadIdx.x + s2];
+        red[1][threadIdx.x] += red[1][threadIdx.x + s2];
+      }
+      __syncthreads();
+    }
+    sum[0] = red[0][0];
+    sum[1] = red[1][0];
+  }
+  if (threadIdx.x == 0) {
+    st->arrive = 0;
+    cg_finish_iteration(st, sum[0], sum[1]);
   }
 }
 
@@ -433,10 +485,16 @@ template <typename T> static bool aligned16(const CGVecs<T>& v) {
 template <typename T>
 cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s) {
   if (!aligned16(v)) return cudaErrorMisalignedAddress;  // caught on the host, nothing launched
-  cg_pw_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);
-  cg_alpha_final<<<1, RED_THREADS, 0, s>>>(st, partial);
-  cg_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);
-  cg_beta_final<<<1, RED_THREADS, 0, s>>>(st, partial);
+  if (!v.dotp) {  // the apply did not accumulate p.w: a separate pass into partial[2R, 3R)
+    cg_pw_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial + 2 * RED_BLOCKS);
+    CGVecs<T> u = v;
+    u.dotp = partial + 2 * RED_BLOCKS;
+    u.ndot = RED_BLOCKS;
+    cg_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(u, st, partial);
+  } else {
+    if (v.ndot <= 0) return cudaErrorInvalidValue;
+    cg_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);
+  }
   cg_p_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st);
   return cudaGetLastError();
 }

@@ -183,7 +183,7 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
   auto body = [&](int nb) {
     cudaError_t eb = cudaSuccess;
     for (int b = 0; b < nb && eb == cudaSuccess; b++) {
-      eb = apply(v.p, v.w, &c->d_cg->done);
+      eb = apply(v.p, v.w, &c->d_cg->done, const_cast<double*>(v.dotp));
       if (eb == cudaSuccess) eb = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream);
     }
     return eb;
@@ -207,15 +207,33 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
 }
 
 // ---------------------------------------------------------------------------- U
-static cudaError_t u_apply64(vfgpu_ctx* c, const double* x, double* y, const int* skip) {
+// dot: if non-null the apply also writes the block partials of x.y there (the CG's p.w)
+static cudaError_t u_apply64(vfgpu_ctx* c, const double* x, double* y, const int* skip,
+                             double* dot = nullptr) {
   UApplyArgs<double> A = u_args<double>(c, x, c->f[VFGPU_FIELD_V], y, c->seam64, c->plan64);
   A.skip = skip;
+  A.dot = dot;
   return launch_u_apply<double>(A, c->plan64, c->layers, c->stream);
 }
-static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* skip) {
+static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* skip,
+                             double* dot = nullptr) {
   UApplyArgs<float> A = u_args<float>(c, x, c->V32, y, c->seam32, c->plan32);
   A.skip = skip;
+  A.dot = dot;
   return launch_u_apply<float>(A, c->plan32, c->layers, c->stream);
+}
+static int dots_of(const vfgpu_ctx* c, const TilePlan& p) { return tile_dot_count(p, c->nx, c->ny, c->nz); }
+
+// Which CG call sites let the operator apply accumulate p.w (bit k-1 for call site k:
+// 1 U FP64, 2 U FP32, 3 V FP64, 4 V FP32); the others use a separate p.w pass.  The
+// FP64 sites only: in the FP32 U kernel the accumulator costs a register spill, and
+// the 129^3 AM step measured U FP32 0.064 s fused-off against 0.066 s fused-on
+// (FP64 U: 0.0957 s fused, 0.0972 s separate).
+#ifndef VFGPU_FUSE_DOT_MASK
+#define VFGPU_FUSE_DOT_MASK 5
+#endif
+static double* dot_buf(vfgpu_ctx* c, int kind) {
+  return ((VFGPU_FUSE_DOT_MASK >> (kind - 1)) & 1) ? c->d_dot : nullptr;
 }
 
 // F = K(V) U - f, Dirichlet rows U - ubc (VF_UResidual, VFMech.c:1456-1887).
@@ -283,13 +301,17 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   const double ttol = o.snes_rtol * fnorm;
   int reason = 0;
   if (fnorm < o.snes_atol) reason = 2;  // SNES_CONVERGED_FNORM_ABS
-  auto apply64 = [&](const double* x, double* y, const int* skip) { return u_apply64(c, x, y, skip); };
-  auto apply32 = [&](const float* x, float* y, const int* skip) { return u_apply32(c, x, y, skip); };
+  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot) {
+    return u_apply64(c, x, y, skip, dot);
+  };
+  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot) {
+    return u_apply32(c, x, y, skip, dot);
+  };
   for (int it = 0; !reason && it < o.snes_maxit; it++) {
     int kits = 0, kreason = 0;
     bool tmo = false;
     if (!mixed) {
-      CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3};
+      CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), dots_of(c, c->plan64)};
       rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
@@ -309,7 +331,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         float* b32 = reinterpret_cast<float*>(P);  // FP32 right-hand side staged in P
         e = dev_to_f32(R, b32, n3, c->stream);
         if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
-        CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3};
+        CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3, dot_buf(c, 2), dots_of(c, c->plan32)};
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
         rc = run_cg<float>(c, 2, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
@@ -388,15 +410,17 @@ namespace vfgpu {
 
 // ---------------------------------------------------------------------------- V
 static cudaError_t v_apply64(vfgpu_ctx* c, const double* x, double* y, const uint8_t* mask,
-                             const int* skip) {
+                             const int* skip, double* dot = nullptr) {
   VApplyArgs<double> A = v_args<double>(c, x, y, mask, c->coef64, c->seam64, c->vplan64);
   A.skip = skip;
+  A.dot = dot;
   return launch_v_apply<double>(A, c->vplan64, c->layers, c->stream);
 }
 static cudaError_t v_apply32(vfgpu_ctx* c, const float* x, float* y, const uint8_t* mask,
-                             const int* skip) {
+                             const int* skip, double* dot = nullptr) {
   VApplyArgs<float> A = v_args<float>(c, x, y, mask, c->coef32, c->seam32, c->vplan32);
   A.skip = skip;
+  A.dot = dot;
   return launch_v_apply<float>(A, c->vplan32, c->layers, c->stream);
 }
 
@@ -458,8 +482,12 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   const double ttol = o.snes_rtol * fnorm;
   int reason = 0;
   if (fnorm < o.snes_atol) reason = 2;
-  auto apply64 = [&](const double* x, double* y, const int* skip) { return v_apply64(c, x, y, mask, skip); };
-  auto apply32 = [&](const float* x, float* y, const int* skip) { return v_apply32(c, x, y, mask, skip); };
+  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot) {
+    return v_apply64(c, x, y, mask, skip, dot);
+  };
+  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot) {
+    return v_apply32(c, x, y, mask, skip, dot);
+  };
   for (int it = 0; !reason && it < o.snes_maxit; it++) {
     e = dev_v_mask(F, V, lb, ub, c->f[VFGPU_FIELD_VIRREV], c->bcV_kind, c->vf.irrevtol, at2, mask, N,
                    c->stream);
@@ -467,7 +495,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     int kits = 0, kreason = 0;
     bool tmo = false;
     if (!mixed) {
-      CGVecs<double> v{Y, R, P, Wv, dinv, F, mask, N};
+      CGVecs<double> v{Y, R, P, Wv, dinv, F, mask, N, dot_buf(c, 3), dots_of(c, c->vplan64)};
       rc = run_cg<double>(c, 3, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
@@ -485,7 +513,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
       for (int k = 0; k < o.max_refine && zr > target; k++) {
         e = dev_to_f32(R, b32, N, c->stream);
         if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
-        CGVecs<float> v{x32, r32, pp32, w32, dinv32, b32, mask, N};
+        CGVecs<float> v{x32, r32, pp32, w32, dinv32, b32, mask, N, dot_buf(c, 4), dots_of(c, c->vplan32)};
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
         rc = run_cg<float>(c, 4, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,

@@ -21,10 +21,13 @@
 //   element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]) (EPT = 1) or
 //   element_multi(A, L, ex, ey[EPT], ez, ok[EPT], in[EPT][8][NIN], out[EPT][8][NC])
 //   (EPT > 1; out[e] must be 0 where ok[e] is false),
-//   finish_node(A, n, val[NC]) (writes y, applying Dirichlet rows / masks), and an
+//   finish_node<DOT>(A, n, val[NC]) (writes y, applying Dirichlet rows / masks; with
+//   DOT returns the node's x.y), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
 //   so that a queued batch of iterations costs nothing once it is done).
 #pragma once
+
+#include <algorithm>
 
 #include "common.cuh"
 
@@ -61,7 +64,9 @@ __device__ __forceinline__ void cp_async_val(T* smem, const T* gmem, bool valid)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-template <class Op, int TY, int MINB>
+// DOT: also write this block's share of x.y to A.dot (the CG's p.w); a separate
+// instantiation, so that plain applies carry none of its registers.
+template <class Op, int TY, int MINB, bool DOT>
 __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     tile_apply_kernel(const typename Op::Args A, const LayerTable L) {
   using T = typename Op::T;
@@ -76,7 +81,11 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   const int X0 = bx * 32, Y0 = by * TY;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
   const int z0 = bz * A.zc;
-  if (z0 >= nz) return;
+  const int blin = (bz * gridDim.y + by) * gridDim.x + bx;
+  if (z0 >= nz) {
+    if (DOT && tid == 0) A.dot[blin] = 0.;
+    return;
+  }
   if (A.skip && *A.skip) return;  // converged solve: uniform early exit, before any barrier
   const int z1 = min(z0 + A.zc, nz);
   const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
@@ -97,11 +106,12 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     cp_async_commit();
   };
 
+  double dacc = 0.;  // this thread's share of x.y over the nodes it finishes (A.dot)
   auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC]) {
     const bool left = (l == 0 && bx > 0), right = (l == 32 && bx < A.ntx - 1);
     const bool bot = (w == 0 && by > 0), top = (w == TY && by < A.nty - 1);
     if (!(left || right || bot || top)) {
-      Op::finish_node(A, node_index(X, Y, z, nx, ny), val);
+      dacc += Op::template finish_node<DOT>(A, node_index(X, Y, z, nx, ny), val);
     } else if (left || right) {
       const int i = left ? bx : bx + 1;
       const int slot = (bot ? 2 : 0) + (left ? 1 : 0);
@@ -247,18 +257,26 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       emit(l, w, X, Y, nz - 1, carry[si]);
     }
   }
+  if constexpr (DOT) {
+    __syncthreads();  // the shared-memory buffers are no longer read
+    const double bs = block_sum_dbl(dacc, reinterpret_cast<double*>(smem_raw));
+    if (tid == 0) A.dot[blin] = bs;
+  }
 #undef SXA
 #undef SCA
 }
 
 // Sums the 2 (or 4 where an x-seam crosses a y-seam) tile partials of every
-// seam node in a fixed order and finishes the node (Op::finish_node).
-template <class Op>
-__global__ void seam_fixup_kernel(const typename Op::Args A, int TY) {
+// seam node in a fixed order and finishes the node (Op::finish_node); with A.dot,
+// block b's share of x.y goes to A.dot[dot_base + b].
+template <class Op, bool DOT>
+__global__ void __launch_bounds__(256) seam_fixup_kernel(const typename Op::Args A, int TY, int dot_base) {
   using T = typename Op::T;
   constexpr int NC = Op::NC;
+  __shared__ double red[32];
   const int nx = A.nx, ny = A.ny, nz = A.nz;
   if (A.skip && *A.skip) return;
+  double dacc = 0.;
   const int64_t nxs = (int64_t)(A.ntx - 1) * nz * ny;
   const int64_t nys = (int64_t)(A.nty - 1) * nz * nx;
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nxs + nys;
@@ -286,9 +304,14 @@ __global__ void seam_fixup_kernel(const typename Op::Args A, int TY) {
       for (int c = 0; c < NC; c++) val[c] = p[c] + p[NC + c];
       n = node_index(X, TY * j, z, nx, ny);
     }
-    Op::finish_node(A, n, val);
+    dacc += Op::template finish_node<DOT>(A, n, val);
+  }
+  if constexpr (DOT) {
+    const double bs = block_sum_dbl(dacc, red);
+    if (threadIdx.x == 0) A.dot[dot_base + blockIdx.x] = bs;
   }
 }
+
 
 // Launch plan: xy tiles of 32 x ty elements, z-chunks of zc planes (chosen to fill
 // the SMs in whole waves), and the seam buffer sizes in elements of T.
@@ -320,6 +343,17 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
   return p;
 }
 
+// Launch shape of the seam fix-up (0 blocks: no seams) and the number of x.y block
+// partials one operator launch writes when it accumulates the CG dot.
+inline int seam_blocks(const TilePlan& p, int nx, int ny, int nz) {
+  const int64_t nseam = (int64_t)(p.ntx - 1) * nz * ny + (int64_t)(p.nty - 1) * nz * nx;
+  if (nseam <= 0) return 0;
+  return (int)std::min<int64_t>((nseam + 255) / 256, 148 * 8);
+}
+inline int tile_dot_count(const TilePlan& p, int nx, int ny, int nz) {
+  return p.ntx * p.nty * p.nzc + seam_blocks(p, nx, ny, nz);
+}
+
 // Opt-in to the dynamic shared memory the kernel needs; done once per device (and
 // up front, from vfgpu_create, so that no attribute call happens inside a capture).
 // Callers serialise (apply_kernel_attributes holds a mutex).
@@ -330,8 +364,12 @@ template <class Op, int TY, int MINB> cudaError_t set_tile_attributes() {
   if (e != cudaSuccess) return e;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
   if (g_tile_attr_set<Op, TY, MINB> & bit) return cudaSuccess;
-  e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)tile_smem_bytes<Op, TY>());
+  const int smem = (int)tile_smem_bytes<Op, TY>();
+  e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB> |= bit;
   return e;
 }
@@ -346,13 +384,13 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
   cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
   if (ea != cudaSuccess) return ea;
   dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY / Op::EPT);
-  tile_apply_kernel<Op, TY, MINB><<<grid, block, smem, s>>>(A, L);
-  const int64_t nseam = (int64_t)(p.ntx - 1) * A.nz * A.ny + (int64_t)(p.nty - 1) * A.nz * A.nx;
-  if (nseam > 0) {
-    const int threads = 256;
-    const int blocks = (int)((nseam + threads - 1) / threads < 148 * 8 ? (nseam + threads - 1) / threads
-                                                                       : 148 * 8);
-    seam_fixup_kernel<Op><<<blocks, threads, 0, s>>>(A, TY);
+  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = p.ntx * p.nty * p.nzc;
+  if (A.dot) {
+    tile_apply_kernel<Op, TY, MINB, true><<<grid, block, smem, s>>>(A, L);
+    if (sblocks > 0) seam_fixup_kernel<Op, true><<<sblocks, 256, 0, s>>>(A, TY, base);
+  } else {
+    tile_apply_kernel<Op, TY, MINB, false><<<grid, block, smem, s>>>(A, L);
+    if (sblocks > 0) seam_fixup_kernel<Op, false><<<sblocks, 256, 0, s>>>(A, TY, base);
   }
   return cudaGetLastError();
 }

@@ -40,6 +40,7 @@ template <typename T> struct UApplyArgs {
   T* __restrict__ seamY;              // y-seam partials [(nty-1)][nz][nx][2][3]
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   const DevParams* __restrict__ P;    // material and eta; null => the by-value LayerTable and eta
+  double* __restrict__ dot;           // if non-null: per-block partials of x.y (see tile_engine.cuh)
   int nx, ny, nz;
   int ntx, nty, zc;                   // tiles in x, y; owned node planes per z-chunk
   T ihx, ihy, ihz, vol, eta;

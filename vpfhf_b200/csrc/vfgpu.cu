@@ -158,7 +158,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   c->graphs.clear();
   free_solver(c);
   for (auto& p : c->f) cudaFree(p);
-  void* bufs[] = {c->d_params, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -220,6 +220,12 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   ALLOC(c->V32, c->N * sizeof(float));
   ALLOC(c->d_elayer, std::max(1, c->nz - 1));
   ALLOC(c->d_params, sizeof(DevParams));
+  {
+    int nd = 1;
+    for (const TilePlan* p : {&c->plan64, &c->plan32, &c->vplan64, &c->vplan32})
+      nd = std::max(nd, tile_dot_count(*p, c->nx, c->ny, c->nz));
+    ALLOC(c->d_dot, (size_t)nd * sizeof(double));
+  }
   ALLOC(c->bcU_kind, 3 * c->N);
   ALLOC(c->bcU_bits, c->N);
   ALLOC(c->bcV_kind, c->N);
