@@ -129,6 +129,17 @@ int vfgpu_set_vfprop(vfgpu_ctx* ctx, const vfgpu_vfprop* vf);
 /* ctx->bcU[3], ctx->bcV[1] (VFBCSetFromOptions, VFCartFE.c:1506-1574). */
 int vfgpu_set_bc(vfgpu_ctx* ctx, const vfgpu_bc bcU[3], const vfgpu_bc* bcV);
 
+/* In-situ stresses (-insitumin / -insitumax, VFCommon.c:132-149): Voigt
+ * (s11, s22, s33, s23, s13, s12) at z = 0 and z = lz, linear in z between;
+ * insitumax NULL = insitumin; insitumin NULL switches them off (hasInsitu).
+ * Their tractions sigma.n load every boundary face component without a Dirichlet
+ * BC (VF_UResidual, VFMech.c:1630-1848) and their work is the in-situ term of
+ * vfgpu_u_energy (VFMech.c:1238-1407, with the reference's choice of the node
+ * layer one inside the box for the X1/Y1/Z1 faces).  Where a component has a
+ * Dirichlet BC on a face, no traction is used for it there; the reference's work
+ * sum reuses the value another face wrote at a shared edge node instead. */
+int vfgpu_set_insitu(vfgpu_ctx* ctx, const double insitumin[6], const double insitumax[6]);
+
 int vfgpu_set_field(vfgpu_ctx* ctx, int field, const double* data);
 int vfgpu_get_field(vfgpu_ctx* ctx, int field, double* data);
 
@@ -150,7 +161,7 @@ void vfgpu_default_solve_opts(vfgpu_solve_opts* opts);
 
 /* VF_StepU (VFMech.c:1436-1452): SNESSolve(snesU) on the resident U with the
  * resident V, theta, thetaRef, pressure; Newton + L2 line search, PCG(Jacobi),
- * the residual of VF_UResidual (VFMech.c:1456-1887, no in-situ tractions).
+ * the residual of VF_UResidual (VFMech.c:1456-1887).
  * Returns VFGPU_OK when converged, VFGPU_NOT_CONVERGED (iteration cap or
  * watchdog) or VFGPU_DIVERGED; the reference's VF_StepU returns 0 in all three
  * cases and only prints (VFMech.c:1445-1450).  opts may be NULL (defaults). */
@@ -171,8 +182,8 @@ int vfgpu_time_step_prepare(vfgpu_ctx* ctx);
 int vfgpu_am_step(vfgpu_ctx* ctx, const vfgpu_solve_opts* opts, double* errV,
                   vfgpu_solve_stats* statsU, vfgpu_solve_stats* statsV);
 
-/* VF_UEnergy3D (VFMech.c:1111-1427): elastic energy and pressure work (the in-situ
- * work is 0: in-situ tractions are not on this path). */
+/* VF_UEnergy3D (VFMech.c:1111-1427): elastic energy, in-situ work (0 unless
+ * vfgpu_set_insitu) and pressure work. */
 int vfgpu_u_energy(vfgpu_ctx* ctx, double* elastic, double* insitu, double* pressurework);
 /* VF_VEnergy3D (VFMech.c:2474-2526): AT1/AT2 surface energy. */
 int vfgpu_v_energy(vfgpu_ctx* ctx, double* surface);

@@ -258,6 +258,148 @@ static void gather_cell(const vfo_problem *P, int ei, int ej, int ek, const doub
 /* VF_UResidual (VFMech.c:1456-1887) without in-situ tractions: element loop in
  * the reference's order, F += K_e u_e then F -= (thermo-poro + crack pressure),
  * then ResidualApplyDirichletBC (F = u - ubc on BC rows). */
+/* ------------------------------------------------------------------------ */
+/* In-situ tractions.  Face order and the stress component / sign of each face
+ * component (VFMech.c:1630-1848): t_c = dir * s_comp(z) with s linear in z
+ * between insitumin (z = BBmin = 0) and insitumax (z = BBmax = lz). */
+static const int insitu_comp[6][3] = {{0, 5, 4}, {0, 5, 4}, {5, 1, 3},
+                                      {5, 1, 3}, {4, 3, 2}, {4, 3, 2}};
+static const double insitu_dir[6] = {-1., 1., -1., 1., -1., 1.};
+enum { F_X0 = 0, F_X1, F_Y0, F_Y1, F_Z0, F_Z1 };
+
+static double insitu_traction(const vfo_problem *P, int face, int c, double z) {
+  const int s = insitu_comp[face][c];
+  return insitu_dir[face] *
+         (P->insitumin[s] + (z - 0.) / (P->lz - 0.) * (P->insitumax[s] - P->insitumin[s]));
+}
+
+/* Local node (i,j,k) of a cell projected onto the face's node layer: the face
+ * layer index replaces the normal-direction index (VFMech.c:610-700). */
+static void face_project(int face, int i, int j, int k, int *pi, int *pj, int *pk) {
+  *pi = i;
+  *pj = j;
+  *pk = k;
+  if (face == F_X0) *pi = 0;
+  if (face == F_X1) *pi = 1;
+  if (face == F_Y0) *pj = 0;
+  if (face == F_Y1) *pj = 1;
+  if (face == F_Z0) *pk = 0;
+  if (face == F_Z1) *pk = 1;
+}
+
+/* VF_GradientUInSituStresses3D_local for one boundary cell and face, added to the
+ * face nodes as the reference does (every local row lands on the face layer).
+ * Components with a Dirichlet BC on the face get no traction (their rows are
+ * replaced by the BC; the reference leaves stale values there). */
+static void insitu_load_cell(const vfo_problem *P, int ei, int ej, int ek, int face, double sgn,
+                             double *f) {
+  double hx, hy, hz;
+  etab e;
+  cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+  etab_init(&e, hx, hy, hz);
+  const double hn = face <= F_X1 ? hx : (face <= F_Y1 ? hy : hz);
+  double t[8][3], felem[3][27], rl[8][3];
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        int pi, pj, pk;
+        face_project(face, i, j, k, &pi, &pj, &pk);
+        const double z = coord(ek + pk, P->lz, P->nz);
+        for (int c = 0; c < 3; c++)
+          t[i + 2 * j + 4 * k][c] = P->insitu_free[face][c] ? insitu_traction(P, face, c, z) : 0.;
+      }
+  for (int c = 0; c < 3; c++)
+    for (int g = 0; g < 27; g++) felem[c][g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++)
+      for (int g = 0; g < 27; g++) felem[c][g] += e.phi[a][g] * t[a][c] / hn;
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) {
+      rl[a][c] = 0.;
+      for (int g = 0; g < 27; g++) rl[a][c] += e.w[g] * e.phi[a][g] * felem[c][g];
+    }
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        int pi, pj, pk;
+        face_project(face, i, j, k, &pi, &pj, &pk);
+        const int64_t q = NODE(P, ei + pi, ej + pj, ek + pk);
+        for (int c = 0; c < 3; c++) f[3 * q + c] += sgn * rl[i + 2 * j + 4 * k][c];
+      }
+}
+
+/* The in-situ part of one cell's residual contribution, faces in the reference's
+ * order (VFMech.c:1630-1848); sgn = +1 adds the load to f, -1 subtracts it from F. */
+static void insitu_cell(const vfo_problem *P, int ei, int ej, int ek, double sgn, double *f) {
+  const int ncx = P->nx - 1, ncy = P->ny - 1, ncz = P->nz - 1;
+  if (ek == 0) insitu_load_cell(P, ei, ej, ek, F_Z0, sgn, f);
+  if (ek == ncz - 1) insitu_load_cell(P, ei, ej, ek, F_Z1, sgn, f);
+  if (ej == 0) insitu_load_cell(P, ei, ej, ek, F_Y0, sgn, f);
+  if (ej == ncy - 1) insitu_load_cell(P, ei, ej, ek, F_Y1, sgn, f);
+  if (ei == 0) insitu_load_cell(P, ei, ej, ek, F_X0, sgn, f);
+  if (ei == ncx - 1) insitu_load_cell(P, ei, ej, ek, F_X1, sgn, f);
+}
+
+static void insitu_load(const vfo_problem *P, double *f) {
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) insitu_cell(P, ei, ej, ek, 1., f);
+}
+
+/* VF_InSituStressWork3D_local over the faces as VF_UEnergy3D visits them
+ * (VFMech.c:1238-1400): X0/Y0/Z0 at the first cell layer; X1/Y1/Z1 at cell layer
+ * ncells-2 (the reference compares the cell index with the cell count minus 2), so
+ * u and the traction are taken at the node layer one inside the box. */
+static double insitu_work_cell(const vfo_problem *P, const double *u, int ei, int ej, int ek,
+                               int face) {
+  double hx, hy, hz;
+  etab e;
+  cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+  etab_init(&e, hx, hy, hz);
+  const double hn = face <= F_X1 ? hx : (face <= F_Y1 ? hy : hz);
+  double ue[3][27], fe[3][27];
+  for (int c = 0; c < 3; c++)
+    for (int g = 0; g < 27; g++) ue[c][g] = fe[c][g] = 0.;
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        int pi, pj, pk;
+        face_project(face, i, j, k, &pi, &pj, &pk);
+        const int64_t q = NODE(P, ei + pi, ej + pj, ek + pk);
+        const double z = coord(ek + pk, P->lz, P->nz);
+        const int a = i + 2 * j + 4 * k;
+        for (int c = 0; c < 3; c++) {
+          const double t = P->insitu_free[face][c] ? insitu_traction(P, face, c, z) : 0.;
+          for (int g = 0; g < 27; g++) {
+            ue[c][g] += e.phi[a][g] * u[3 * q + c] / hn;
+            fe[c][g] += e.phi[a][g] * t;
+          }
+        }
+      }
+  double w = 0.;
+  for (int c = 0; c < 3; c++)
+    for (int g = 0; g < 27; g++) w += e.w[g] * ue[c][g] * fe[c][g];
+  return w;
+}
+
+int vfo_insitu_work(const vfo_problem *P, const double *u, double *work) {
+  const int ncx = P->nx - 1, ncy = P->ny - 1, ncz = P->nz - 1;
+  double w = 0.;
+  if (P->hasInsitu)
+    for (int ek = 0; ek < ncz; ek++)
+      for (int ej = 0; ej < ncy; ej++)
+        for (int ei = 0; ei < ncx; ei++) {
+          if (ek == 0) w += insitu_work_cell(P, u, ei, ej, ek, F_Z0);
+          if (ek == ncz - 2) w += insitu_work_cell(P, u, ei, ej, ek, F_Z1);
+          if (ej == 0) w += insitu_work_cell(P, u, ei, ej, ek, F_Y0);
+          if (ej == ncy - 2) w += insitu_work_cell(P, u, ei, ej, ek, F_Y1);
+          if (ei == 0) w += insitu_work_cell(P, u, ei, ej, ek, F_X0);
+          if (ei == ncx - 2) w += insitu_work_cell(P, u, ei, ej, ek, F_X1);
+        }
+  *work = w;
+  return 0;
+}
+
 int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
                        const double *theta, const double *thetaRef, const double *p,
                        const uint8_t *bcmask, const double *bcval, double *F) {
@@ -285,6 +427,7 @@ int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
         if (P->hasCrackPressure) u_rhs_crackpressure(&e, p8, v8, rl);
         for (int a = 0, l2 = 0; a < 8; a++)
           for (int c = 0; c < 3; c++, l2++) F[3 * n[a] + c] -= rl[l2];
+        if (P->hasInsitu) insitu_cell(P, ei, ej, ek, -1., F);
       }
   if (bcmask)
     for (int64_t q = 0; q < 3 * N; q++)
@@ -406,6 +549,7 @@ int vfo_u_rhs(const vfo_problem *P, const double *v, const double *theta,
         for (int a = 0, l = 0; a < 8; a++)
           for (int c = 0; c < 3; c++, l++) f[3 * n[a] + c] += rl[l];
       }
+  if (P->hasInsitu) insitu_load(P, f);
   return 0;
 }
 

@@ -51,6 +51,12 @@ typedef struct {
   int    atnum;                 /* 1 = AT1, 2 = AT2                                   */
   int    hasCrackPressure;
   int    nthreads;              /* OpenMP threads for the fast variants (0 = default) */
+  /* in-situ stresses (VFCommon.c:132-149): Voigt s11 s22 s33 s23 s13 s12 at z = 0
+   * (min) and z = lz (max), linear in z between; insitu_free[face][c] = 1 where
+   * bcU[c].face[face] == NONE (faces X0 X1 Y0 Y1 Z0 Z1) */
+  int    hasInsitu;
+  double insitumin[6], insitumax[6];
+  int    insitu_free[6][3];
 } vfo_problem;
 
 typedef struct {
@@ -120,6 +126,11 @@ int vfo_u_energy(const vfo_problem *P, const double *u, const double *v,
 int vfo_v_energy(const vfo_problem *P, const double *v, double *surface);
 int vfo_cov(const vfo_problem *P, const double *u, const double *v, double *cov,
             double *cellcov /* (nx-1)(ny-1)(nz-1) or NULL */);
+
+/* ---- in-situ boundary tractions (VFMech.c:598-715, 983-1102, 1196-1407, 1630-1848) ----
+ * Work of the tractions on U, with the reference's layer choice for the X1/Y1/Z1
+ * faces (the cell layer before the last, so the node layer one inside the box). */
+int vfo_insitu_work(const vfo_problem *P, const double *u, double *work);
 
 /* ---- penny crack initial V (VFCracks.c:101-227) ---- */
 int vfo_penny_crack_v(const vfo_problem *P, const double center[3], double r,

@@ -51,6 +51,8 @@ class Problem(C.Structure):
         ("cellE", C.POINTER(C.c_double)),
         ("epsilon", C.c_double), ("eta", C.c_double), ("irrevtol", C.c_double),
         ("atnum", C.c_int), ("hasCrackPressure", C.c_int), ("nthreads", C.c_int),
+        ("hasInsitu", C.c_int), ("insitumin", C.c_double * 6), ("insitumax", C.c_double * 6),
+        ("insitu_free", (C.c_int * 3) * 6),
     ]
 
 
@@ -115,6 +117,7 @@ def _declare(L):
         "vfo_penny_crack_v": [_P, _dp, C.c_double, C.c_double, C.c_double, C.c_double, _dp],
         "vfo_rect_crack_v": [_P, _dp, C.c_double, _dp],
         "vfo_cracks_v": [_P, C.c_int, odp, C.c_int, odp, _dp],
+        "vfo_insitu_work": [_P, _dp, C.POINTER(C.c_double)],
         "vfo_step_u": [_P, _dp, _dp, odp, odp, odp, ou8, odp, C.POINTER(SolverOpts),
                        C.POINTER(Stats)],
         "vfo_step_v": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
@@ -271,6 +274,27 @@ class Oracle:
         self.L.vfo_penny_crack_v(C.byref(self.P), np.asarray(center, np.float64), float(r),
                                  float(theta), float(phi), float(thickness), v)
         return v
+
+    def set_insitu(self, smin, smax=None, face_bc=None):
+        """In-situ stresses (Voigt s11 s22 s33 s23 s13 s12) at z = 0 and z = lz; face_bc:
+        [3][6] U BC types per component and face (X0 X1 Y0 Y1 Z0 Z1), traction only
+        where the type is NONE.  smin=None switches them off."""
+        P = self.P
+        P.hasInsitu = int(smin is not None)
+        if smin is None:
+            return
+        smax = smin if smax is None else smax
+        for i in range(6):
+            P.insitumin[i], P.insitumax[i] = float(smin[i]), float(smax[i])
+        fb = np.zeros((3, 6), int) if face_bc is None else np.asarray(face_bc).reshape(3, 6)
+        for f in range(6):
+            for c in range(3):
+                P.insitu_free[f][c] = int(fb[c, f] == NONE)
+
+    def insitu_work(self, u):
+        w = C.c_double()
+        self.L.vfo_insitu_work(C.byref(self.P), u, C.byref(w))
+        return w.value
 
     def rect_v(self, corners, thickness=0.0):
         v = np.zeros(self.N)

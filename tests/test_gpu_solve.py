@@ -243,3 +243,47 @@ def test_sneddon_penny_crack_opening(cuda):
         assert 4.0 < (r - 1) * a / h < 8.0
     extrap = (ratios[2] * hs[1] - ratios[1] * hs[2]) / (hs[1] - hs[2])
     assert abs(extrap - 1) < 0.1
+
+
+def test_insitu_tractions_match_oracle(cuda, oracle_mod):
+    """In-situ stresses varying in z (all six components) on a box with mixed BCs:
+    residual (load), StepU solution, elastic energy and in-situ work against the oracle."""
+    import vpfhf_b200 as vg
+    n, L = (17, 13, 11), (2.0, 1.5, 1.2)
+    smin = [-2e6, -1.5e6, -3e6, 0.2e6, -0.1e6, 0.3e6]
+    smax = [-3e6, -2.5e6, -4e6, 0.1e6, 0.2e6, -0.2e6]
+    o = oracle_mod.Oracle(n, L, E=1e10, nu=0.25, Gc=100.0, epsilon=0.3, eta=1e-8, atnum=1,
+                          pressurize=False)
+    ctx = vg.VFContext(n, L, dict(E=1e10, nu=0.25, Gc=100.0), epsilon=0.3, eta=1e-8, atnum=1)
+    # X0 clamped (all components), Z0 rollers, the rest free
+    bc = [vg.BCSpec(X0=vg.BC_ZERO), vg.BCSpec(X0=vg.BC_ZERO), vg.BCSpec(X0=vg.BC_ZERO, Z0=vg.BC_ZERO)]
+    ctx.set_bc(bc)
+    ctx.set_insitu(smin, smax)
+    face = np.zeros((3, 6), np.int32)
+    face[:, 0] = oracle_mod.ZERO
+    face[2, 4] = oracle_mod.ZERO
+    o.set_insitu(smin, smax, face)
+    mask, val = o.bc(face)
+    v = o.penny_v((1.0, 0.75, 0.6), 0.4)
+    ctx.set_field("V", v)
+    rng = np.random.default_rng(4)
+    u = rng.standard_normal(3 * o.N) * 1e-4
+    u[mask == 1] = 0.0
+    ctx.set_field("U", u)
+    F = ctx.u_residual()
+    Fr = o.u_residual_ref(u, v, None, None, None, mask, val)
+    assert np.abs(F - Fr).max() <= 1e-11 * np.abs(Fr).max()
+    el, iw, pw = ctx.u_energy()
+    assert iw == pytest.approx(o.insitu_work(u), rel=1e-12)
+    ctx.set_field("U", np.zeros(3 * o.N))
+    rc, st = ctx.step_u()
+    assert rc == 0, st
+    uo = np.zeros(3 * o.N)
+    o.step_u(uo, v, mask=mask, value=val)
+    ug = ctx.get_field("U")
+    assert np.linalg.norm(ug - uo) <= 1e-6 * np.linalg.norm(uo)
+    el, iw, pw = ctx.u_energy()
+    el_o, _ = o.u_energy(uo, v)
+    assert el == pytest.approx(el_o, rel=1e-7)
+    assert iw == pytest.approx(o.insitu_work(uo), rel=1e-7)
+    ctx.close()

@@ -108,3 +108,42 @@ def test_penny_surface_energy_converges_to_gc_area(oracle_mod):
         assert abs(s / (Gc * np.pi * r * r) - 1) < 1.8 * eps / r
     assert 0.7 < excess[0] < 0.95 and 0.7 < excess[1] < 0.95
     assert abs(excess[0] - excess[1]) < 0.05
+
+
+def _uniform_insitu_case(oracle_mod, n=(7, 6, 5), L=(1.2, 1.0, 0.8), s=(-1.0, -0.7, -0.4)):
+    E, nu = 2.0, 0.3
+    o = oracle_mod.Oracle(n, L, E=E, nu=nu, Gc=1.0, eta=0.0, pressurize=False)
+    face = np.zeros((3, 6), np.int32)
+    face[0, 0] = face[1, 2] = face[2, 4] = oracle_mod.ZERO  # rollers on X0, Y0, Z0 only
+    stress = list(s) + [0.0, 0.0, 0.0]
+    o.set_insitu(stress, stress, face)
+    lam, mu = E * nu / (1 + nu) / (1 - 2 * nu), E / 2 / (1 + nu)
+    C = np.array([[lam + 2 * mu, lam, lam], [lam, lam + 2 * mu, lam], [lam, lam, lam + 2 * mu]])
+    eps = np.linalg.solve(C, np.array(s))
+    xs = [np.arange(k) * (l / (k - 1)) for k, l in zip(n, L)]
+    Z, Y, X = np.meshgrid(xs[2], xs[1], xs[0], indexing="ij")
+    uex = np.stack([eps[0] * X, eps[1] * Y, eps[2] * Z], -1).reshape(-1)
+    return o, face, stress, eps, uex
+
+
+def test_insitu_uniform_stress_known_answer(oracle_mod):
+    """Uniform in-situ stress on the free faces of a box on rollers (X0, Y0, Z0): the
+    exact solution is the uniform strain C^-1 s (reproduced by Q1 elements), the elastic
+    energy is s:eps V / 2, and the in-situ work follows VF_UEnergy3D's face layers --
+    X1/Y1/Z1 taken one node layer inside the box, so W = V sum_d s_d eps_d (n_d-2)/(n_d-1)."""
+    o, face, stress, eps, uex = _uniform_insitu_case(oracle_mod)
+    mask, val = o.bc(face)
+    v = np.ones(o.N)
+    F = o.u_residual_ref(uex, v, mask=mask, value=val)
+    assert np.abs(F).max() <= 1e-13
+    u = np.zeros(3 * o.N)
+    opts = oracle_mod.default_opts()
+    opts.rtol, opts.atol, opts.snes_rtol, opts.snes_atol = 1e-12, 1e-14, 1e-12, 1e-14
+    o.step_u(u, v, mask=mask, value=val, opts=opts)
+    assert np.abs(u - uex).max() <= 1e-12
+    V = 1.2 * 1.0 * 0.8
+    el, _ = o.u_energy(u, v)
+    assert el == pytest.approx(0.5 * V * np.dot(stress[:3], eps), rel=1e-12)
+    n = (7, 6, 5)
+    w = sum(stress[d] * eps[d] * (n[d] - 2) / (n[d] - 1) for d in range(3)) * V
+    assert o.insitu_work(u) == pytest.approx(w, rel=1e-12)

@@ -111,6 +111,13 @@ class VFContext:
                          int(bool(pressurize)))
         _abi.check(self.L.vfgpu_set_vfprop(self.h, C.byref(vf)), "vfgpu_set_vfprop")
 
+    def set_insitu(self, smin, smax=None):
+        """In-situ stresses (Voigt s11 s22 s33 s23 s13 s12) at z = 0 and z = lz
+        (-insitumin / -insitumax); None switches them off."""
+        a = None if smin is None else np.ascontiguousarray(smin, dtype=np.float64)
+        b = None if smax is None else np.ascontiguousarray(smax, dtype=np.float64)
+        _abi.check(self.L.vfgpu_set_insitu(self.h, _abi.ptr(a), _abi.ptr(b)), "vfgpu_set_insitu")
+
     def set_bc(self, bcU, bcV=None):
         u = (_abi.BC * 3)(*[b.to_c() for b in bcU])
         v = (bcV or BCSpec()).to_c()

@@ -26,6 +26,10 @@ struct vfgpu_ctx {
   bool have_mat = false;
   vfgpu_vfprop vf{0.2, 1e-5, 5e-2, 2, 0};  // VFPropGet defaults (VFCommon.c:468-480)
 
+  // in-situ stresses (VFCtx.hasInsitu, insitumin, insitumax)
+  bool has_insitu = false;
+  double insitu_min[6]{}, insitu_max[6]{};
+
   // BCs
   vfgpu_bc bcU[3]{}, bcV{};
   uint8_t* bcU_kind = nullptr;  // 3N: VFGPU_BC_* per dof

@@ -48,4 +48,18 @@ cudaError_t launch_energies(const ElemArgs& E, const double* u, const double* v,
                             const double* theta, const double* thetaRef, const double* p,
                             double* partial, double* out, double* cellcov, cudaStream_t s);
 
+// In-situ boundary tractions (VFMech.c:598-715, 983-1102, 1196-1407, 1630-1848).
+struct InsituArgs {
+  int nx, ny, nz;
+  double hx, hy, hz, lz;
+  double smin[6], smax[6];  // Voigt s11 s22 s33 s23 s13 s12 at z = 0 and z = lz
+  int freec[6][3];          // face X0 X1 Y0 Y1 Z0 Z1 x component: 1 = no Dirichlet BC there
+};
+// f += the consistent face load of the tractions (faces in the order X0..Z1).
+cudaError_t launch_insitu_load(const InsituArgs& A, double* f, cudaStream_t s);
+// out[0] = work of the tractions on u, with the reference's layers (X1/Y1/Z1 one node
+// layer inside the box); partial: >= 6 * 64 doubles of device memory.
+cudaError_t launch_insitu_work(const InsituArgs& A, const double* u, double* partial, double* out,
+                               cudaStream_t s);
+
 }  // namespace vfgpu

@@ -86,6 +86,32 @@ static ElemArgs elem_args(vfgpu_ctx* c) {
   return E;
 }
 
+static InsituArgs insitu_args(const vfgpu_ctx* c) {
+  InsituArgs A{};
+  A.nx = c->nx;
+  A.ny = c->ny;
+  A.nz = c->nz;
+  A.hx = c->hx;
+  A.hy = c->hy;
+  A.hz = c->hz;
+  A.lz = c->lz;
+  for (int i = 0; i < 6; i++) {
+    A.smin[i] = c->insitu_min[i];
+    A.smax[i] = c->insitu_max[i];
+  }
+  for (int f = 0; f < 6; f++)
+    for (int comp = 0; comp < 3; comp++) A.freec[f][comp] = c->bcU[comp].face[f] == VFGPU_BC_NONE;
+  return A;
+}
+
+// f (3N) = the U load of VF_UResidual: thermo-poro, crack pressure and in-situ tractions.
+static cudaError_t u_load(vfgpu_ctx* c, const ElemArgs& E, double* f) {
+  cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
+                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+  if (e == cudaSuccess && c->has_insitu) e = launch_insitu_load(insitu_args(c), f, c->stream);
+  return e;
+}
+
 template <typename T>
 static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask, const T* coef,
                             T* seam, const TilePlan& p) {
@@ -285,8 +311,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   double* U = c->f[VFGPU_FIELD_U];
   const bool mixed = o.precision == VFGPU_MIXED;
   ElemArgs E = elem_args(c);
-  cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
-                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+  cudaError_t e = u_load(c, E, f);
   if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream);
   if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
   if (mixed && e == cudaSuccess) {
@@ -639,9 +664,14 @@ static int energies(vfgpu_ctx* c, double* cellcov) {
   cudaError_t e = launch_energies(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
                                   c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE],
                                   c->d_red + RED_BLOCKS * 4, c->d_out, cc, c->stream);
+  // d_out[4] = in-situ work (partials in the CG part of d_red, idle outside solves)
+  if (e == cudaSuccess && c->has_insitu)
+    e = launch_insitu_work(insitu_args(c), c->f[VFGPU_FIELD_U], c->d_red, c->d_out + 4, c->stream);
+  else if (e == cudaSuccess)
+    e = cudaMemsetAsync(c->d_out + 4, 0, sizeof(double), c->stream);
   if (e == cudaSuccess && stage)
     e = cudaMemcpyAsync(cellcov, cc, c->NC * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = fetch(c, 4);
+  if (e == cudaSuccess) e = fetch(c, 5);
   if (e != cudaSuccess) return cuda_fail(e, "energies");
   return VFGPU_OK;
 }
@@ -650,7 +680,7 @@ int vfgpu_u_energy(vfgpu_ctx* c, double* elastic, double* insitu, double* pressu
   int rc = energies(c, nullptr);
   if (rc) return rc;
   if (elastic) *elastic = c->h_out[0];
-  if (insitu) *insitu = 0.0;  // in-situ tractions are not part of this path (hasInsitu = false)
+  if (insitu) *insitu = c->h_out[4];
   if (pressurework) *pressurework = c->h_out[1];
   return VFGPU_OK;
 }
@@ -696,8 +726,7 @@ int vfgpu_u_residual(vfgpu_ctx* c, double* F) {
   if (rc) return rc;
   ElemArgs E = elem_args(c);
   double *f = c->p64[0], *tmp = c->p64[1], *Fd = c->p64[2];
-  cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
-                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+  cudaError_t e = u_load(c, E, f);
   if (e == cudaSuccess) e = u_residual(c, c->f[VFGPU_FIELD_U], f, tmp, Fd);
   if (e == cudaSuccess) e = copy_out(c, F, Fd, 3 * c->N);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

@@ -336,6 +336,18 @@ int vfgpu_set_vfprop(vfgpu_ctx* c, const vfgpu_vfprop* vf) {
   return upload_params(c);
 }
 
+int vfgpu_set_insitu(vfgpu_ctx* c, const double* smin, const double* smax) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_set_insitu: null ctx");
+  c->has_insitu = smin != nullptr;
+  for (int i = 0; i < 6; i++) {
+    c->insitu_min[i] = smin ? smin[i] : 0.;
+    c->insitu_max[i] = smin ? (smax ? smax[i] : smin[i]) : 0.;
+    if (!(c->insitu_min[i] == c->insitu_min[i]) || !(c->insitu_max[i] == c->insitu_max[i]))
+      return fail(VFGPU_ERR_INVALID, "vfgpu_set_insitu: NaN stress component %d", i);
+  }
+  return VFGPU_OK;
+}
+
 int vfgpu_set_bc(vfgpu_ctx* c, const vfgpu_bc bcU[3], const vfgpu_bc* bcV) {
   if (!c || !bcU || !bcV) return fail(VFGPU_ERR_INVALID, "vfgpu_set_bc: null argument");
   for (int k = 0; k < 4; k++) {

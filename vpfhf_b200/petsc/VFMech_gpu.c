@@ -55,7 +55,6 @@ static PetscErrorCode vfgpu_setup(VFCtx *ctx) {
   PetscFunctionBegin;
   ierr = MPI_Comm_size(PETSC_COMM_WORLD, &size);CHKERRQ(ierr);
   if (size != 1) SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: one rank per problem");
-  if (ctx->hasInsitu) SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: in-situ tractions not supported");
   if (ctx->unilateral != UNILATERAL_NONE)
     SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: only -unilateral none is supported");
   if (ctx->nlayer > 16) SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: at most 16 layers");
@@ -89,6 +88,14 @@ static PetscErrorCode vfgpu_setup(VFCtx *ctx) {
   for (l = 0; l < 3; l++) to_vfgpu_bc(&ctx->bcU[l], &bu[l]);
   to_vfgpu_bc(&ctx->bcV[0], &bv);
   VFGPU_CHK(vfgpu_set_bc(gpu_ctx, bu, &bv));
+  {
+    double smin[6], smax[6];
+    for (l = 0; l < 6; l++) {
+      smin[l] = ctx->insitumin[l];
+      smax[l] = ctx->insitumax[l];
+    }
+    VFGPU_CHK(vfgpu_set_insitu(gpu_ctx, ctx->hasInsitu ? smin : NULL, smax));
+  }
   PetscFunctionReturn(0);
 }
 
