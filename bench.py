@@ -45,6 +45,17 @@ def _rank():
         int(os.environ.get("LOCAL_RANK", "0"))
 
 
+def max_over_ranks(vals, dist=None, device="cpu"):
+    """Element-wise maximum of a list of times over the ranks (the slowest rank sets
+    every timed number); identity without a process group."""
+    if dist is None:
+        return [float(v) for v in vals]
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
 def _peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -179,10 +190,7 @@ def run_gpu(args):
     t32 = timed_applies(vg.MIXED, x32, y32, args.steps, args.warmup)
     ms64 = float(np.mean(t64))
     ms32 = float(np.mean(t32))
-    if dist:
-        m = torch.tensor([ms64, ms32], dtype=torch.float64, device="cuda")
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms64, ms32 = m.tolist()
+    ms64, ms32 = max_over_ranks([ms64, ms32], dist, "cuda")
 
     if args.only_am:
         out = {}
@@ -235,10 +243,7 @@ def run_gpu(args):
         ctx.u_apply(xpn, vg.FP64, out=ypn)
     barrier()
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    if dist:
-        m = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        e2e_ms = m.item()
+    (e2e_ms,) = max_over_ranks([e2e_ms], dist, "cuda")
 
     # AM steps (StepU + StepV to tolerance) from the penny-crack start, FP64 and mixed
     am, vfin = {}, {}

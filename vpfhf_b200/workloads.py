@@ -61,13 +61,13 @@ def random_pennies(rng, l, count, rmin=0.05, rmax=0.2):
 def c3_problem(seed=1003, n=(257, 257, 129), l=(4.0, 4.0, 2.0)):
     """Heterogeneous poroelastic set-up: lognormal E (mean 10 GPa, log-sigma 0.5, 8h
     smoothing), nu 0.25, Biot 0.7, pore pressure 10 -> 12 MPa in x plus a 0.1 MPa smooth
-    perturbation (also the crack pressure: one field, as in the reference), 16 random
-    penny cracks, AT1, eps = 2h, eta = 1e-8, Gc = 100."""
+    perturbation acting through the Biot term (no separate crack-pressure term), 16
+    random penny cracks, AT1, eps = 2h, eta = 1e-8, Gc = 100."""
     rng = np.random.default_rng(seed)
     h = l[0] / (n[0] - 1)
     return dict(n=n, l=l, cellE=heterogeneous_modulus(n, seed), nu=0.25, beta=0.7, Gc=100.0,
                 pressure=pore_pressure(n, l, seed), pennies=random_pennies(rng, l, 16),
-                epsilon=2 * h, eta=1e-8, atnum=1)
+                epsilon=2 * h, eta=1e-8, atnum=1, pressurize=False)
 
 
 def c5_problem(seed=1005, n=(321, 321, 321), l=(4.0, 4.0, 4.0), p=1e6):
@@ -77,7 +77,7 @@ def c5_problem(seed=1005, n=(321, 321, 321), l=(4.0, 4.0, 4.0), p=1e6):
     h = l[0] / (n[0] - 1)
     return dict(n=n, l=l, cellE=heterogeneous_modulus(n, seed), nu=0.25, beta=0.0, Gc=100.0,
                 pressure=np.full(n[0] * n[1] * n[2], p), pennies=random_pennies(rng, l, 8),
-                epsilon=2 * h, eta=1e-8, atnum=1)
+                epsilon=2 * h, eta=1e-8, atnum=1, pressurize=True)
 
 
 def make_context(vg, prob):
@@ -85,7 +85,7 @@ def make_context(vg, prob):
     n, l = prob["n"], prob["l"]
     ctx = vg.VFContext(n, l, dict(E=1.0, nu=prob["nu"], beta=prob["beta"], Gc=prob["Gc"]),
                        epsilon=prob["epsilon"], eta=prob["eta"], atnum=prob["atnum"],
-                       pressurize=True)
+                       pressurize=prob["pressurize"])
     ctx.set_cell_modulus(prob["cellE"])
     ctx.set_bc(vg.rollers())
     ctx.set_field("pressure", prob["pressure"])
