@@ -400,11 +400,11 @@ def run_large(args):
     rank, world, local = _rank()
     torch.cuda.set_device(local)
     t0 = time.perf_counter()
-    prob = wl.c5_problem() if args.config == "c5" else wl.c3_problem()
-    if args.grid != N_EDGE:  # smaller instance of the same set-up (tests, probes)
-        scale = args.grid / prob["n"][0]
-        n = tuple(max(9, int(round((k - 1) * scale)) + 1) for k in prob["n"])
-        prob = (wl.c5_problem(n=n) if args.config == "c5" else wl.c3_problem(n=n))
+    make = wl.c5_problem if args.config == "c5" else wl.c3_problem
+    full = (321, 321, 321) if args.config == "c5" else (257, 257, 129)
+    # --scale < 1: a smaller instance of the same set-up (probes); cells scale linearly
+    n = tuple(max(9, int(round((k - 1) * args.scale)) + 1) for k in full)
+    prob = make(n=n)
     gen_s = time.perf_counter() - t0
     ctx = wl.make_context(vg, prob)
     n = prob["n"]
@@ -503,6 +503,8 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c2", "c3", "c5"],
                     help="c2: the headline line; c3 / c5: the large set-ups (one JSON line)")
     ap.add_argument("--load-steps", type=int, default=20, help="c3 quasi-static steps")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="c3 / c5: cells per axis scaled by this factor (1 = the full set-up)")
     ap.add_argument("--max-am", type=int, default=25, help="c3 AM cap per load step")
     ap.add_argument("--only-am", action="store_true",
                     help="run the AM steps only, with a per-solve breakdown; the last step of "
