@@ -243,6 +243,104 @@ static void u_rhs_crackpressure(const etab *e, const double p8[8], const double 
       for (int g = 0; g < 27; g++) rl[l] += e->w[g] * pe[g] * gv[c][g] * e->phi[a][g];
 }
 
+/* VF_BilinearFormUNoCompression3D_local (VFMech.c:299-376): at the Gauss points
+ * where tr(eps(u0)) < 0 (UNILATERAL_THRES = 0, VFMech.c:6) the spherical part keeps
+ * kappa (1 + eta) instead of kappa s; the deviatoric part is always degraded. */
+static void u_element_matrix_nc(const etab *e, const cellmat *m, double eta, const double v8[8],
+                                const double u8[8][3], double K[576]) {
+  const double kappa = m->lambda + 2. * m->mu / 3.;
+  double s[27], tr[27];
+  for (int g = 0; g < 27; g++) s[g] = tr[g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      s[g] += v8[a] * e->phi[a][g];
+      tr[g] += e->dphi[a][0][g] * u8[a][0] + e->dphi[a][1][g] * u8[a][1] +
+               e->dphi[a][2][g] * u8[a][2];
+    }
+  for (int g = 0; g < 27; g++) s[g] = s[g] * s[g] + eta;
+  for (int l = 0; l < 576; l++) K[l] = 0;
+  int l = 0;
+  for (int a = 0; a < 8; a++)
+    for (int c1 = 0; c1 < 3; c1++)
+      for (int b = 0; b < 8; b++)
+        for (int c2 = 0; c2 < 3; c2++, l++)
+          for (int g = 0; g < 27; g++) {
+            double mg = (tr[g] < 0. ? kappa * (1. + eta) : kappa * s[g]) * e->dphi[a][c1][g] *
+                        e->dphi[b][c2][g];
+            mg -= 2. * m->mu * s[g] * e->dphi[a][c1][g] * e->dphi[b][c2][g] / 3.;
+            mg += m->mu * s[g] * e->dphi[a][c2][g] * e->dphi[b][c1][g];
+            if (c1 == c2)
+              mg += m->mu * s[g] *
+                    (e->dphi[a][0][g] * e->dphi[b][0][g] + e->dphi[a][1][g] * e->dphi[b][1][g] +
+                     e->dphi[a][2][g] * e->dphi[b][2][g]);
+            K[l] += e->w[g] * mg;
+          }
+}
+
+/* VF_GradientUThermoPoroNoCompression3D_local (VFMech.c:456-524): where
+ * tr(eps(u0)) < 0 the thermal term is not degraded and the pore pressure is not
+ * multiplied by v. */
+static void u_rhs_thermoporo_nc(const etab *e, const cellmat *m, double eta, const double th8[8],
+                                const double p8[8], const double v8[8], const double u8[8][3],
+                                double rl[24]) {
+  double coefalpha = (3. * m->lambda + 2. * m->mu) * m->alpha, beta = m->beta;
+  double te[27], pe[27], ve[27], tr[27];
+  for (int g = 0; g < 27; g++) te[g] = pe[g] = ve[g] = tr[g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      te[g] += e->phi[a][g] * th8[a];
+      pe[g] += e->phi[a][g] * p8[a];
+      ve[g] += e->phi[a][g] * v8[a];
+      tr[g] += e->dphi[a][0][g] * u8[a][0] + e->dphi[a][1][g] * u8[a][1] +
+               e->dphi[a][2][g] * u8[a][2];
+    }
+  for (int g = 0; g < 27; g++)
+    for (int a = 0, l = 0; a < 8; a++)
+      for (int c = 0; c < 3; c++, l++) {
+        if (tr[g] < 0.)
+          rl[l] += e->w[g] * e->dphi[a][c][g] * (coefalpha * te[g] * (1. + eta) + beta * pe[g]);
+        else
+          rl[l] += e->w[g] * e->dphi[a][c][g] *
+                   (coefalpha * te[g] * (ve[g] * ve[g] + eta) + beta * pe[g] * ve[g]);
+      }
+}
+
+/* u at the 8 nodes of a cell, zeros for u = NULL */
+static void gather_u8z(const vfo_problem *P, int ei, int ej, int ek, const double *u,
+                       double u8[8][3]) {
+  int64_t n[8];
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) n[i + 2 * j + 4 * k] = NODE(P, ei + i, ej + j, ek + k);
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) u8[a][c] = u ? u[3 * n[a] + c] : 0.;
+}
+
+/* The U element matrix of the problem's unilateral model at u0. */
+static void u_element_matrix_any(const vfo_problem *P, int ei, int ej, int ek, const etab *e,
+                                 const cellmat *m, const double v8[8], const double *u0,
+                                 double K[576]) {
+  if (P->unilateral) {
+    double u8[8][3];
+    gather_u8z(P, ei, ej, ek, u0, u8);
+    u_element_matrix_nc(e, m, P->eta, v8, u8, K);
+  } else {
+    u_element_matrix(e, m, P->eta, v8, K);
+  }
+}
+
+static void u_rhs_thermoporo_any(const vfo_problem *P, int ei, int ej, int ek, const etab *e,
+                                 const cellmat *m, const double th8[8], const double p8[8],
+                                 const double v8[8], const double *u0, double rl[24]) {
+  if (P->unilateral) {
+    double u8[8][3];
+    gather_u8z(P, ei, ej, ek, u0, u8);
+    u_rhs_thermoporo_nc(e, m, P->eta, th8, p8, v8, u8, rl);
+  } else {
+    u_rhs_thermoporo(e, m, P->eta, th8, p8, v8, rl);
+  }
+}
+
 static void gather_cell(const vfo_problem *P, int ei, int ej, int ek, const double *v,
                         const double *theta, const double *thetaRef, const double *p,
                         double v8[8], double th8[8], double p8[8]) {
@@ -416,14 +514,14 @@ int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
         cellmat m = cell_material(P, ei, ej, ek);
         cell_nodes(P, ei, ej, ek, n);
         gather_cell(P, ei, ej, ek, v, theta, thetaRef, p, v8, th8, p8);
-        u_element_matrix(&e, &m, P->eta, v8, K);
+        u_element_matrix_any(P, ei, ej, ek, &e, &m, v8, u, K);
         int l = 0;
         for (int a = 0; a < 8; a++)
           for (int c1 = 0; c1 < 3; c1++)
             for (int b = 0; b < 8; b++)
               for (int c2 = 0; c2 < 3; c2++, l++) F[3 * n[a] + c1] += K[l] * u[3 * n[b] + c2];
         for (l = 0; l < 24; l++) rl[l] = 0.;
-        u_rhs_thermoporo(&e, &m, P->eta, th8, p8, v8, rl);
+        u_rhs_thermoporo_any(P, ei, ej, ek, &e, &m, th8, p8, v8, u, rl);
         if (P->hasCrackPressure) u_rhs_crackpressure(&e, p8, v8, rl);
         for (int a = 0, l2 = 0; a < 8; a++)
           for (int c = 0; c < 3; c++, l2++) F[3 * n[a] + c] -= rl[l2];
@@ -439,15 +537,25 @@ int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
  * BC rows are identity, BC columns are kept (MatZeroRowsStencil, VFCartFE.c:1293). */
 int vfo_u_apply_ref(const vfo_problem *P, const double *v, const double *x,
                     const uint8_t *bcmask, double *y) {
+  return vfo_u_apply_ref_u(P, NULL, v, x, bcmask, y);
+}
+
+int vfo_u_apply_ref_u(const vfo_problem *P, const double *u0, const double *v, const double *x,
+                      const uint8_t *bcmask, double *y) {
   int64_t N = (int64_t)P->nx * P->ny * P->nz;
   for (int64_t q = 0; q < 3 * N; q++) y[q] = 0.;
-  double K[576];
+  double K[576], hx, hy, hz, v8[8];
   int64_t n[8];
+  etab e;
   for (int ek = 0; ek < P->nz - 1; ek++)
     for (int ej = 0; ej < P->ny - 1; ej++)
       for (int ei = 0; ei < P->nx - 1; ei++) {
-        vfo_u_element_matrix(P, ei, ej, ek, v, K);
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
         cell_nodes(P, ei, ej, ek, n);
+        for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
+        u_element_matrix_any(P, ei, ej, ek, &e, &m, v8, u0, K);
         int l = 0;
         for (int a = 0; a < 8; a++)
           for (int c1 = 0; c1 < 3; c1++)
@@ -467,6 +575,13 @@ int vfo_u_apply_ref(const vfo_problem *P, const double *v, const double *x,
  * and the result is independent of the thread count. */
 int vfo_u_apply_mf(const vfo_problem *P, const double *v, const double *x,
                    const uint8_t *bcmask, double *y) {
+  return vfo_u_apply_mf_u(P, NULL, v, x, bcmask, y);
+}
+
+/* NOCOMPRESSION: sigma = w [lambda' tr(G) I + s mu (G + G^T)] with
+ * lambda' = kappa (1 + eta) - 2 mu s / 3 where tr(eps(u0)) < 0, else lambda s. */
+int vfo_u_apply_mf_u(const vfo_problem *P, const double *u0, const double *v, const double *x,
+                     const uint8_t *bcmask, double *y) {
   int64_t N = (int64_t)P->nx * P->ny * P->nz;
   for (int64_t q = 0; q < 3 * N; q++) y[q] = 0.;
   int nex = P->nx - 1, ney = P->ny - 1, nez = P->nz - 1;
@@ -491,26 +606,34 @@ int vfo_u_apply_mf(const vfo_problem *P, const double *v, const double *x,
       cellmat m = cell_material(P, ei, ej, ek);
       int64_t n[8];
       cell_nodes(P, ei, ej, ek, n);
-      double ue[8][3], v8[8], ye[8][3];
+      double ue[8][3], v8[8], ye[8][3], u08[8][3];
       for (int a = 0; a < 8; a++) {
         v8[a] = v[n[a]];
         for (int c = 0; c < 3; c++) {
           ue[a][c] = x[3 * n[a] + c];
+          u08[a][c] = u0 ? u0[3 * n[a] + c] : 0.;
           ye[a][c] = 0.;
         }
       }
+      const double kappa = m.lambda + 2. * m.mu / 3.;
       for (int g = 0; g < 27; g++) {
-        double s = 0., G[3][3] = {{0}};
+        double s = 0., tr0 = 0., G[3][3] = {{0}};
         for (int a = 0; a < 8; a++) {
           s += v8[a] * e.phi[a][g];
-          for (int c = 0; c < 3; c++)
+          for (int c = 0; c < 3; c++) {
+            tr0 += e.dphi[a][c][g] * u08[a][c];
             for (int d = 0; d < 3; d++) G[c][d] += e.dphi[a][d][g] * ue[a][c];
+          }
         }
-        double ws = e.w[g] * (s * s + P->eta);
+        const double sv = s * s + P->eta;
+        double ws = e.w[g] * sv;
         double tr = G[0][0] + G[1][1] + G[2][2], sg[3][3];
+        const double lam_tr = (P->unilateral && tr0 < 0.)
+                                  ? e.w[g] * (kappa * (1. + P->eta) - 2. * m.mu * sv / 3.) * tr
+                                  : ws * m.lambda * tr;
         for (int c = 0; c < 3; c++)
           for (int d = 0; d < 3; d++)
-            sg[c][d] = ws * ((c == d ? m.lambda * tr : 0.) + m.mu * (G[c][d] + G[d][c]));
+            sg[c][d] = (c == d ? lam_tr : 0.) + ws * m.mu * (G[c][d] + G[d][c]);
         for (int a = 0; a < 8; a++)
           for (int c = 0; c < 3; c++)
             ye[a][c] += e.dphi[a][0][g] * sg[c][0] + e.dphi[a][1][g] * sg[c][1] +
@@ -530,6 +653,11 @@ int vfo_u_apply_mf(const vfo_problem *P, const double *v, const double *x,
  * VF_UResidual (VFMech.c:1600-1626), summed in element order. */
 int vfo_u_rhs(const vfo_problem *P, const double *v, const double *theta,
               const double *thetaRef, const double *p, double *f) {
+  return vfo_u_rhs_u(P, NULL, v, theta, thetaRef, p, f);
+}
+
+int vfo_u_rhs_u(const vfo_problem *P, const double *u0, const double *v, const double *theta,
+                const double *thetaRef, const double *p, double *f) {
   int64_t N = (int64_t)P->nx * P->ny * P->nz;
   for (int64_t q = 0; q < 3 * N; q++) f[q] = 0.;
   double rl[24], v8[8], th8[8], p8[8], hx, hy, hz;
@@ -544,7 +672,7 @@ int vfo_u_rhs(const vfo_problem *P, const double *v, const double *theta,
         cell_nodes(P, ei, ej, ek, n);
         gather_cell(P, ei, ej, ek, v, theta, thetaRef, p, v8, th8, p8);
         for (int l = 0; l < 24; l++) rl[l] = 0.;
-        u_rhs_thermoporo(&e, &m, P->eta, th8, p8, v8, rl);
+        u_rhs_thermoporo_any(P, ei, ej, ek, &e, &m, th8, p8, v8, u0, rl);
         if (P->hasCrackPressure) u_rhs_crackpressure(&e, p8, v8, rl);
         for (int a = 0, l = 0; a < 8; a++)
           for (int c = 0; c < 3; c++, l++) f[3 * n[a] + c] += rl[l];
@@ -556,15 +684,25 @@ int vfo_u_rhs(const vfo_problem *P, const double *v, const double *theta,
 /* Diagonal of K(v) (the Jacobi preconditioner of KSPCG with -U_pc_type jacobi),
  * BC rows 1 as after MatZeroRowsStencil. */
 int vfo_u_diag(const vfo_problem *P, const double *v, const uint8_t *bcmask, double *d) {
+  return vfo_u_diag_u(P, NULL, v, bcmask, d);
+}
+
+int vfo_u_diag_u(const vfo_problem *P, const double *u0, const double *v, const uint8_t *bcmask,
+                 double *d) {
   int64_t N = (int64_t)P->nx * P->ny * P->nz;
   for (int64_t q = 0; q < 3 * N; q++) d[q] = 0.;
-  double K[576];
+  double K[576], hx, hy, hz, v8[8];
   int64_t n[8];
+  etab e;
   for (int ek = 0; ek < P->nz - 1; ek++)
     for (int ej = 0; ej < P->ny - 1; ej++)
       for (int ei = 0; ei < P->nx - 1; ei++) {
-        vfo_u_element_matrix(P, ei, ej, ek, v, K);
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        cellmat m = cell_material(P, ei, ej, ek);
         cell_nodes(P, ei, ej, ek, n);
+        for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
+        u_element_matrix_any(P, ei, ej, ek, &e, &m, v8, u0, K);
         for (int a = 0; a < 8; a++)
           for (int c = 0; c < 3; c++) d[3 * n[a] + c] += K[(3 * a + c) * 24 + 3 * a + c];
       }
@@ -696,8 +834,46 @@ static void elastic_energy_density(const etab *e, const cellmat *m, const double
   }
 }
 
+/* ElasticEnergyDensitySphericalDeviatoricNoCompression3D_local (VFMech.c:115-218):
+ * W = sigma(eps - e0) : eps (the strain itself, not eps - e0, on the right), and the
+ * coupling uses S + D = W - (kappa/2) tr^2 where tr < 0, W elsewhere
+ * (kappa = lambda + 2 mu / 3). */
+static void elastic_energy_density_nc(const etab *e, const cellmat *m, const double u8[8][3],
+                                      const double th8[8], double W[27]) {
+  double e11[27], e22[27], e33[27], e12[27], e23[27], e13[27], e0[27];
+  double lambda = m->lambda, mu = m->mu, alpha = m->alpha, kappa = lambda + 2. * mu / 3.;
+  for (int g = 0; g < 27; g++)
+    e11[g] = e22[g] = e33[g] = e12[g] = e23[g] = e13[g] = e0[g] = W[g] = 0.;
+  for (int a = 0; a < 8; a++)
+    for (int g = 0; g < 27; g++) {
+      e11[g] += e->dphi[a][0][g] * u8[a][0];
+      e22[g] += e->dphi[a][1][g] * u8[a][1];
+      e33[g] += e->dphi[a][2][g] * u8[a][2];
+      e12[g] += (e->dphi[a][0][g] * u8[a][1] + e->dphi[a][1][g] * u8[a][0]) * .5;
+      e23[g] += (e->dphi[a][1][g] * u8[a][2] + e->dphi[a][2][g] * u8[a][1]) * .5;
+      e13[g] += (e->dphi[a][0][g] * u8[a][2] + e->dphi[a][2][g] * u8[a][0]) * .5;
+      e0[g] += alpha * e->phi[a][g] * th8[a];
+    }
+  for (int g = 0; g < 27; g++) {
+    double s11 = (lambda + 2. * mu) * (e11[g] - e0[g]) + lambda * (e22[g] - e0[g]) +
+                 lambda * (e33[g] - e0[g]);
+    double s22 = lambda * (e11[g] - e0[g]) + (lambda + 2. * mu) * (e22[g] - e0[g]) +
+                 lambda * (e33[g] - e0[g]);
+    double s33 = lambda * (e11[g] - e0[g]) + lambda * (e22[g] - e0[g]) +
+                 (lambda + 2. * mu) * (e33[g] - e0[g]);
+    double s12 = 2. * mu * e12[g], s23 = 2. * mu * e23[g], s13 = 2. * mu * e13[g];
+    double Wf = (s11 * e11[g] + s22 * e22[g] + s33 * e33[g]) * .5 + s12 * e12[g] +
+                s23 * e23[g] + s13 * e13[g];
+    double tr = e11[g] + e22[g] + e33[g];
+    double S = tr < 0. ? 0. : kappa * tr * tr * .5;
+    double D = Wf - kappa * tr * tr * .5;
+    W[g] = S + D;
+  }
+}
+
 /* VF_BilinearFormVAT1/AT23D_local + VF_BilinearFormVCoupling3D_local
- * (VFMech.c:2040-2115), accumulated in the order VF_VResidual uses. */
+ * (VFMech.c:2040-2115; NOCOMPRESSION: VF_BilinearFormVCouplingNoCompression3D_local,
+ * VFMech.c:2125-2153), accumulated in the order VF_VResidual uses. */
 static void v_element_matrix(const vfo_problem *P, const etab *e, const cellmat *m,
                              const double u8[8][3], const double th8[8], double K[64]) {
   double coef = m->Gc / atCv(P) * .5, eps = P->epsilon, W[27];
@@ -712,7 +888,10 @@ static void v_element_matrix(const vfo_problem *P, const etab *e, const cellmat 
         else
           K[l] += coef * e->w[g] * (e->phi[a][g] * e->phi[b][g] / eps + dd * eps);
       }
-  elastic_energy_density(e, m, u8, th8, W);
+  if (P->unilateral)
+    elastic_energy_density_nc(e, m, u8, th8, W);
+  else
+    elastic_energy_density(e, m, u8, th8, W);
   for (int a = 0, l = 0; a < 8; a++)
     for (int b = 0; b < 8; b++, l++)
       for (int g = 0; g < 27; g++) K[l] += e->w[g] * e->phi[a][g] * e->phi[b][g] * W[g] * 2.;
@@ -931,7 +1110,10 @@ int vfo_u_energy(const vfo_problem *P, const double *u, const double *v,
           El += (D11[g] * D11[g] + D22[g] * D22[g] + D33[g] * D33[g] +
                  (D12[g] * D12[g] + D23[g] * D23[g] + D13[g] * D13[g]) * 2.) *
                 ve[g] * ve[g] * (1. + P->eta) * m.mu * e.w[g];
-          double WD = (tr / 3. - m.alpha * te[g]) * ve[g] - coefbeta * pe[g];
+          /* NOCOMPRESSION (VF_ElasticEnergyNoCompression3D_local, VFMech.c:819-908): the
+           * spherical factor is 1 instead of v where tr(eps) < 0 */
+          const double sph = (P->unilateral && tr < 0.) ? 1. : ve[g];
+          double WD = (tr / 3. - m.alpha * te[g]) * sph - coefbeta * pe[g];
           El += 3. * threekappa / 2. * WD * WD * e.w[g];
           El += threekappa / 6. * tr * tr * P->eta * e.w[g];
         }

@@ -57,6 +57,10 @@ typedef struct {
   int    hasInsitu;
   double insitumin[6], insitumax[6];
   int    insitu_free[6][3];
+  /* VFCtx.unilateral (VFCommon.c:176-177): 0 = UNILATERAL_NONE, 1 = NOCOMPRESSION --
+   * the spherical part of the energy is not degraded where tr(eps(u)) < 0
+   * (UNILATERAL_THRES = 0, VFMech.c:6), which makes the U residual depend on U */
+  int    unilateral;
 } vfo_problem;
 
 typedef struct {
@@ -96,6 +100,19 @@ int vfo_u_residual_ref(const vfo_problem *P, const double *u, const double *v,
                        const double *theta, const double *thetaRef, const double *p,
                        const uint8_t *bcmask, const double *bcval, double *F);
 int vfo_u_diag(const vfo_problem *P, const double *v, const uint8_t *bcmask, double *d);
+/* NOCOMPRESSION forms need the displacement u0 that fixes the sign of tr(eps) at each
+ * Gauss point (VF_BilinearFormUNoCompression3D_local, VFMech.c:299-376, and
+ * VF_GradientUThermoPoroNoCompression3D_local, VFMech.c:456-524); with
+ * unilateral = 0, or u0 = NULL (tr = 0: the tensile branch), they equal the
+ * functions above. */
+int vfo_u_apply_mf_u(const vfo_problem *P, const double *u0, const double *v, const double *x,
+                     const uint8_t *bcmask, double *y);
+int vfo_u_apply_ref_u(const vfo_problem *P, const double *u0, const double *v, const double *x,
+                      const uint8_t *bcmask, double *y);
+int vfo_u_rhs_u(const vfo_problem *P, const double *u0, const double *v, const double *theta,
+                const double *thetaRef, const double *p, double *f);
+int vfo_u_diag_u(const vfo_problem *P, const double *u0, const double *v, const uint8_t *bcmask,
+                 double *d);
 /* CSR assembly of K(v) with BC rows -> identity (VF_UIJacobian, VFMech.c:1897-2029). */
 int64_t vfo_u_csr_nnz(const vfo_problem *P);
 int vfo_u_assemble_csr(const vfo_problem *P, const double *v, const uint8_t *bcmask,

@@ -92,27 +92,38 @@ static int pcg(int64_t n, apply_fn A, void *ctx, const double *dinv, const doubl
 /* ------------------------------------------------------------------------ */
 typedef struct {
   const vfo_problem *P;
-  const double *v;
+  const double *u0, *v;
   const uint8_t *bcmask;
 } uctx;
 
 static void u_apply_cb(void *c, const double *x, double *y) {
   uctx *u = (uctx *)c;
-  vfo_u_apply_mf(u->P, u->v, x, u->bcmask, y);
+  vfo_u_apply_mf_u(u->P, u->u0, u->v, x, u->bcmask, y);
 }
 
-/* F(u) = K(v) u - f, BC rows u - ubc (VF_UResidual semantics). */
-static void u_func(const vfo_problem *P, const double *v, const double *f, const uint8_t *bc,
-                   const double *bcval, const double *u, double *F) {
+typedef struct {
+  const vfo_problem *P;
+  const double *v, *theta, *thetaRef, *p;
+  double *f;  /* work space for the load */
+} uload;
+
+/* F(u) = K(v; u) u - f(u), BC rows u - ubc (VF_UResidual semantics); the load and,
+ * for NOCOMPRESSION, the operator depend on u through the sign of tr(eps(u)). */
+static void u_func(const uload *L, const uint8_t *bc, const double *bcval, const double *u,
+                   double *F) {
+  const vfo_problem *P = L->P;
   int64_t n = 3 * (int64_t)P->nx * P->ny * P->nz;
-  vfo_u_apply_mf(P, v, u, NULL, F);
-  for (int64_t i = 0; i < n; i++) F[i] = bc[i] ? u[i] - bcval[i] : F[i] - f[i];
+  vfo_u_rhs_u(P, u, L->v, L->theta, L->thetaRef, L->p, L->f);
+  vfo_u_apply_mf_u(P, u, L->v, u, NULL, F);
+  for (int64_t i = 0; i < n; i++) F[i] = bc[i] ? u[i] - bcval[i] : F[i] - L->f[i];
 }
 
-/* VF_StepU = SNESSolve(snesU): SNESNEWTONLS + SNESLINESEARCHL2.  For the
- * affine U residual ||F(x - lambda y)||^2 is exactly quadratic in lambda, so
- * the L2 line search's secant step on the derivative (fitted from lambda = 0,
- * 1/2, 1) lands on the quadratic's minimiser; that minimiser is used here. */
+/* VF_StepU = SNESSolve(snesU): SNESNEWTONLS + SNESLINESEARCHL2 (one secant step on
+ * the derivative of ||F(x - lambda Y)||^2 fitted from lambda = 0, 1/2, 1).  For the
+ * affine U residual that lands on the exact minimiser; for NOCOMPRESSION the
+ * residual is piecewise affine, the Jacobian K(v; u) is re-formed at every Newton
+ * iterate (VF_UIJacobian, VFMech.c:1942-1980) and so are the Jacobi diagonal and
+ * the load. */
 int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *theta,
                const double *thetaRef, const double *p, const uint8_t *bcmask,
                const double *bcval, const vfo_solver_opts *o, vfo_stats *st) {
@@ -120,19 +131,25 @@ int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *t
   double *f = malloc(n * sizeof(double)), *F = malloc(n * sizeof(double));
   double *Y = malloc(n * sizeof(double)), *W = malloc(n * sizeof(double));
   double *Fw = malloc(n * sizeof(double)), *dinv = malloc(n * sizeof(double));
-  vfo_u_rhs(P, v, theta, thetaRef, p, f);
-  vfo_u_diag(P, v, bcmask, dinv);
+  uload L = {P, v, theta, thetaRef, p, f};
+  vfo_u_diag_u(P, u, v, bcmask, dinv);
   for (int64_t i = 0; i < n; i++) dinv[i] = 1. / dinv[i];
-  u_func(P, v, f, bcmask, bcval, u, F);
+  u_func(&L, bcmask, bcval, u, F);
   double fnorm = sqrt(dot(n, F, F));
   memset(st, 0, sizeof *st);
   st->fnorm0 = fnorm;
   double ttol = o->snes_rtol * fnorm;
   int reason = 0;
   if (fnorm < o->snes_atol) reason = 2;
-  uctx c = {P, v, bcmask};
+  double *u0 = malloc(n * sizeof(double));
+  uctx c = {P, u0, v, bcmask};
   for (int it = 0; !reason && it < o->snes_maxit; it++) {
     int kits = 0;
+    memcpy(u0, u, n * sizeof(double));  /* the Jacobian's linearisation point */
+    if (P->unilateral && it > 0) {
+      vfo_u_diag_u(P, u, v, bcmask, dinv);
+      for (int64_t i = 0; i < n; i++) dinv[i] = 1. / dinv[i];
+    }
     int kr = pcg(n, u_apply_cb, &c, dinv, F, Y, NULL, o, &kits);
     st->ksp_its += kits;
     if (kr < 0) {
@@ -142,10 +159,10 @@ int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *t
     /* L2 line search: samples at lambda = 0, 1/2, 1. */
     double q0 = fnorm * fnorm, qm, q1;
     for (int64_t i = 0; i < n; i++) W[i] = u[i] - 0.5 * Y[i];
-    u_func(P, v, f, bcmask, bcval, W, Fw);
+    u_func(&L, bcmask, bcval, W, Fw);
     qm = dot(n, Fw, Fw);
     for (int64_t i = 0; i < n; i++) W[i] = u[i] - Y[i];
-    u_func(P, v, f, bcmask, bcval, W, Fw);
+    u_func(&L, bcmask, bcval, W, Fw);
     q1 = dot(n, Fw, Fw);
     double dE = 3. * q1 - 4. * qm + q0, dE_old = -3. * q0 + 4. * qm - q1;
     double lambda = 1.;
@@ -154,7 +171,7 @@ int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *t
       if (lu == lu && lu > 1e-12) lambda = lu;
     }
     for (int64_t i = 0; i < n; i++) u[i] -= lambda * Y[i];
-    u_func(P, v, f, bcmask, bcval, u, F);
+    u_func(&L, bcmask, bcval, u, F);
     fnorm = sqrt(dot(n, F, F));
     double ynorm = lambda * sqrt(dot(n, Y, Y)), xnorm = sqrt(dot(n, u, u));
     st->newton_its = it + 1;
@@ -176,6 +193,7 @@ int vfo_step_u(const vfo_problem *P, double *u, const double *v, const double *t
   free(W);
   free(Fw);
   free(dinv);
+  free(u0);
   return 0;
 }
 

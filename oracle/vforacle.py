@@ -52,7 +52,7 @@ class Problem(C.Structure):
         ("epsilon", C.c_double), ("eta", C.c_double), ("irrevtol", C.c_double),
         ("atnum", C.c_int), ("hasCrackPressure", C.c_int), ("nthreads", C.c_int),
         ("hasInsitu", C.c_int), ("insitumin", C.c_double * 6), ("insitumax", C.c_double * 6),
-        ("insitu_free", (C.c_int * 3) * 6),
+        ("insitu_free", (C.c_int * 3) * 6), ("unilateral", C.c_int),
     ]
 
 
@@ -118,6 +118,10 @@ def _declare(L):
         "vfo_rect_crack_v": [_P, _dp, C.c_double, _dp],
         "vfo_cracks_v": [_P, C.c_int, odp, C.c_int, odp, _dp],
         "vfo_insitu_work": [_P, _dp, C.POINTER(C.c_double)],
+        "vfo_u_apply_mf_u": [_P, odp, _dp, _dp, ou8, _dp],
+        "vfo_u_apply_ref_u": [_P, odp, _dp, _dp, ou8, _dp],
+        "vfo_u_rhs_u": [_P, odp, _dp, odp, odp, odp, _dp],
+        "vfo_u_diag_u": [_P, odp, _dp, ou8, _dp],
         "vfo_step_u": [_P, _dp, _dp, odp, odp, odp, ou8, odp, C.POINTER(SolverOpts),
                        C.POINTER(Stats)],
         "vfo_step_v": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
@@ -138,7 +142,7 @@ class Oracle:
 
     def __init__(self, n, l, E=1.0, nu=0.0, Gc=1.0, alpha=0.0, beta=0.0, epsilon=0.2,
                  eta=1e-8, atnum=1, irrevtol=5e-2, pressurize=True, cellE=None, layer=None,
-                 nthreads=0):
+                 nthreads=0, unilateral=0):
         L = lib()
         self.L = L
         nx, ny, nz = (int(x) for x in n)
@@ -163,6 +167,7 @@ class Oracle:
                    else None)
         P.epsilon, P.eta, P.irrevtol = float(epsilon), float(eta), float(irrevtol)
         P.atnum, P.hasCrackPressure, P.nthreads = int(atnum), int(bool(pressurize)), int(nthreads)
+        P.unilateral = int(unilateral)
         self.P = P
 
     # -- helpers ---------------------------------------------------------
@@ -295,6 +300,23 @@ class Oracle:
         w = C.c_double()
         self.L.vfo_insitu_work(C.byref(self.P), u, C.byref(w))
         return w.value
+
+    def u_apply_u(self, u0, v, x, mask=None, ref=False):
+        """K(v; u0) x: the operator linearised at u0 (NOCOMPRESSION sign pattern)."""
+        y = np.zeros(3 * self.N)
+        f = self.L.vfo_u_apply_ref_u if ref else self.L.vfo_u_apply_mf_u
+        f(C.byref(self.P), u0, v, x, mask, y)
+        return y
+
+    def u_rhs_u(self, u0, v, theta=None, thetaRef=None, p=None):
+        f = np.zeros(3 * self.N)
+        self.L.vfo_u_rhs_u(C.byref(self.P), u0, v, theta, thetaRef, p, f)
+        return f
+
+    def u_diag_u(self, u0, v, mask=None):
+        d = np.zeros(3 * self.N)
+        self.L.vfo_u_diag_u(C.byref(self.P), u0, v, mask, d)
+        return d
 
     def rect_v(self, corners, thickness=0.0):
         v = np.zeros(self.N)
