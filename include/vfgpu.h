@@ -129,6 +129,17 @@ int vfgpu_set_vfprop(vfgpu_ctx* ctx, const vfgpu_vfprop* vf);
 /* ctx->bcU[3], ctx->bcV[1] (VFBCSetFromOptions, VFCartFE.c:1506-1574). */
 int vfgpu_set_bc(vfgpu_ctx* ctx, const vfgpu_bc bcU[3], const vfgpu_bc* bcV);
 
+/* Unilateral model (-unilateral, VFCommon.c:176-177; VFUnilateralType).  With
+ * NOCOMPRESSION the spherical part of the elastic energy is not degraded at Gauss
+ * points where tr(eps(U)) < 0 (UNILATERAL_THRES = 0, VFMech.c:6): the U operator
+ * (VFMech.c:299-376), thermo-poro load (456-524), elastic energy (819-908) and the
+ * V coupling (2125-2153) switch per Gauss point, and StepU's Newton iterations
+ * re-form operator, load and Jacobi diagonal at every iterate.  vfgpu_u_apply then
+ * applies K(V; U) linearised at the resident U. */
+#define VFGPU_UNILATERAL_NONE 0
+#define VFGPU_UNILATERAL_NOCOMPRESSION 1
+int vfgpu_set_unilateral(vfgpu_ctx* ctx, int type);
+
 /* In-situ stresses (-insitumin / -insitumax, VFCommon.c:132-149): Voigt
  * (s11, s22, s33, s23, s13, s12) at z = 0 and z = lz, linear in z between;
  * insitumax NULL = insitumin; insitumin NULL switches them off (hasInsitu).

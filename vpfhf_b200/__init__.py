@@ -111,6 +111,12 @@ class VFContext:
                          int(bool(pressurize)))
         _abi.check(self.L.vfgpu_set_vfprop(self.h, C.byref(vf)), "vfgpu_set_vfprop")
 
+    def set_unilateral(self, kind):
+        """-unilateral: 0 / "none" or 1 / "nocompression"."""
+        if isinstance(kind, str):
+            kind = {"none": 0, "nocompression": 1}[kind.lower()]
+        _abi.check(self.L.vfgpu_set_unilateral(self.h, int(kind)), "vfgpu_set_unilateral")
+
     def set_insitu(self, smin, smax=None):
         """In-situ stresses (Voigt s11 s22 s33 s23 s13 s12) at z = 0 and z = lz
         (-insitumin / -insitumax); None switches them off."""

@@ -16,6 +16,7 @@ LIBPATH = os.path.join(HERE, "libvfgpu.so")
 OK, NOT_CONVERGED, DIVERGED = 0, 1, 2
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_STATE = -1, -2, -3, -4
 FP64, MIXED = 0, 1
+UNILATERAL_NONE, UNILATERAL_NOCOMPRESSION = 0, 1
 BC_NONE, BC_ZERO, BC_ONE, BC_FIXED = 0, 1, 2, 3
 FIELD_U, FIELD_V, FIELD_VIRREV, FIELD_BCU, FIELD_THETA, FIELD_THETAREF, FIELD_PRESSURE = range(7)
 FIELD_NAMES = {"U": FIELD_U, "V": FIELD_V, "VIrrev": FIELD_VIRREV, "BCU": FIELD_BCU,
@@ -123,6 +124,7 @@ _SIGS = {
     "vfgpu_set_vfprop": [C.c_void_p, C.POINTER(VFProp)],
     "vfgpu_set_bc": [C.c_void_p, C.POINTER(BC), C.POINTER(BC)],
     "vfgpu_set_insitu": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "vfgpu_set_unilateral": [C.c_void_p, C.c_int],
     "vfgpu_set_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_get_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_u_apply": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],

@@ -12,6 +12,8 @@ cudaError_t copy_out(vfgpu_ctx* c, double* dst, const double* src, int64_t n);
 int ensure_v32(vfgpu_ctx* c);
 void free_solver(vfgpu_ctx* c);
 int upload_params(vfgpu_ctx* c);
+// NOCOMPRESSION: recompute the per-cell compression bits from displacement u (device).
+cudaError_t nc_flags(vfgpu_ctx* c, const double* u);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
 }  // namespace vfgpu

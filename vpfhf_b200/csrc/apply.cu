@@ -29,6 +29,8 @@ cudaError_t apply_kernel_attributes() {
   std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U_TY, 1>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpNC<float>, U_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, 3>();
   return e;
@@ -45,11 +47,15 @@ TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
 template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
+  if (A.cflag) return launch_tile_apply<UOpNC<double>, U_TY, 1>(A, p, L, s);
   return launch_tile_apply<UOp<double>, U_TY, 1>(A, p, L, s);
 }
 template <>
 cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
                                   const LayerTable& L, cudaStream_t s) {
+  // NOCOMPRESSION needs the scalar layout: its plan is the FP32 plan only with the
+  // scalar tile (the packed build option keeps the plain operator packed)
+  if (A.cflag) return launch_tile_apply<UOpNC<float>, U_TY, 2>(A, p, L, s);
   return launch_tile_apply<U32Op, U32_TY, U32_MINB>(A, p, L, s);
 }
 template <>

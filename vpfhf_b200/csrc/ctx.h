@@ -26,6 +26,11 @@ struct vfgpu_ctx {
   bool have_mat = false;
   vfgpu_vfprop vf{0.2, 1e-5, 5e-2, 2, 0};  // VFPropGet defaults (VFCommon.c:468-480)
 
+  // unilateral model (VFCtx.unilateral): 1 = NOCOMPRESSION, with the per-cell
+  // compression bits of the current linearisation point
+  int unilateral = 0;
+  uint32_t* d_cflag = nullptr;  // NC
+
   // in-situ stresses (VFCtx.hasInsitu, insitumin, insitumax)
   bool has_insitu = false;
   double insitu_min[6]{}, insitu_max[6]{};

@@ -87,9 +87,24 @@ __device__ __forceinline__ bool colour_cell(const ElemArgs& E, int color, int64_
   return true;
 }
 
+// tr(eps(u)) at Gauss point g from the 8 nodal displacements, in the reference's order
+__device__ __forceinline__ double trace_at(const ETab& e, const double (&u8)[8][3], int g) {
+  double tr = 0.;
+  for (int a = 0; a < 8; a++)
+    tr += e.dphi[a][0][g] * u8[a][0] + e.dphi[a][1][g] * u8[a][1] + e.dphi[a][2][g] * u8[a][2];
+  return tr;
+}
+
+__device__ __forceinline__ void gather_u8(const int64_t (&n)[8], const double* __restrict__ u,
+                                          double (&u8)[8][3]) {
+  for (int a = 0; a < 8; a++)
+    for (int c = 0; c < 3; c++) u8[a][c] = u ? u[3 * n[a] + c] : 0.;
+}
+
 __global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restrict__ v,
                              const double* __restrict__ theta, const double* __restrict__ thetaRef,
-                             const double* __restrict__ p, double* __restrict__ f) {
+                             const double* __restrict__ p, double* __restrict__ f,
+                             const double* __restrict__ u0) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
   const ETab& e = *E.tab;
@@ -104,8 +119,11 @@ __global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restri
   }
   for (int l = 0; l < 24; l++) rl[l] = 0.;
   const CellMat m = cell_mat(E, ei, ej, ek);
-  // VF_GradientUThermoPoro3D_local (VFMech.c:386-447)
+  // VF_GradientUThermoPoro3D_local (VFMech.c:386-447); NOCOMPRESSION
+  // (VFMech.c:456-524): undegraded thermal term and p instead of p v where tr < 0
   const double coefalpha = (3. * m.lambda + 2. * m.mu) * m.alpha, beta = m.beta;
+  double u8[8][3];
+  if (E.unilateral) gather_u8(n, u0, u8);
   for (int g = 0; g < 27; g++) {
     double te = 0., pe = 0., ve = 0.;
     for (int a = 0; a < 8; a++) {
@@ -113,7 +131,9 @@ __global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restri
       pe += e.phi[a][g] * p8[a];
       ve += e.phi[a][g] * v8[a];
     }
-    const double s = coefalpha * te * (ve * ve + E.eta) + beta * pe * ve;
+    const bool comp = E.unilateral && trace_at(e, u8, g) < 0.;
+    const double s = comp ? coefalpha * te * (1. + E.eta) + beta * pe
+                          : coefalpha * te * (ve * ve + E.eta) + beta * pe * ve;
     for (int a = 0; a < 8; a++)
       for (int c = 0; c < 3; c++) rl[3 * a + c] += e.w[g] * e.dphi[a][c][g] * s;
   }
@@ -134,7 +154,7 @@ __global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restri
 }
 
 __global__ void u_diag_kernel(const ElemArgs E, int color, const double* __restrict__ v,
-                              double* __restrict__ d) {
+                              double* __restrict__ d, const double* __restrict__ u0) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
   const ETab& e = *E.tab;
@@ -145,20 +165,44 @@ __global__ void u_diag_kernel(const ElemArgs E, int color, const double* __restr
   for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
   for (int l = 0; l < 24; l++) dg[l] = 0.;
   const CellMat m = cell_mat(E, ei, ej, ek);
+  double u8[8][3];
+  if (E.unilateral) gather_u8(n, u0, u8);
+  const double kappa = m.lambda + 2. * m.mu / 3.;
   for (int g = 0; g < 27; g++) {
     double s = 0.;
     for (int a = 0; a < 8; a++) s += v8[a] * e.phi[a][g];
-    const double ws = e.w[g] * (s * s + E.eta);
+    const double sv = s * s + E.eta, ws = e.w[g] * sv;
+    // spherical coefficient: lambda s, or kappa (1 + eta) - 2 mu s / 3 in compression
+    const bool comp = E.unilateral && trace_at(e, u8, g) < 0.;
+    const double lw = comp ? e.w[g] * (kappa * (1. + E.eta) - 2. * m.mu * sv / 3.) : ws * m.lambda;
     for (int a = 0; a < 8; a++) {
       const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
       const double g2 = d0 * d0 + d1 * d1 + d2 * d2;
-      dg[3 * a + 0] += ws * ((m.lambda + m.mu) * d0 * d0 + m.mu * g2);
-      dg[3 * a + 1] += ws * ((m.lambda + m.mu) * d1 * d1 + m.mu * g2);
-      dg[3 * a + 2] += ws * ((m.lambda + m.mu) * d2 * d2 + m.mu * g2);
+      dg[3 * a + 0] += (lw + ws * m.mu) * d0 * d0 + ws * m.mu * g2;
+      dg[3 * a + 1] += (lw + ws * m.mu) * d1 * d1 + ws * m.mu * g2;
+      dg[3 * a + 2] += (lw + ws * m.mu) * d2 * d2 + ws * m.mu * g2;
     }
   }
   for (int a = 0; a < 8; a++)
     for (int c = 0; c < 3; c++) d[3 * n[a] + c] += dg[3 * a + c];
+}
+
+__global__ void nc_flags_kernel(const ElemArgs E, const double* __restrict__ u,
+                                uint32_t* __restrict__ flags) {
+  const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (cell >= NCELL) return;
+  const int ei = (int)(cell % (E.nx - 1));
+  const int ej = (int)((cell / (E.nx - 1)) % (E.ny - 1));
+  const int ek = (int)(cell / ((int64_t)(E.nx - 1) * (E.ny - 1)));
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double u8[8][3];
+  gather_u8(n, u, u8);
+  uint32_t bits = 0u;
+  for (int g = 0; g < 27; g++)
+    if (trace_at(*E.tab, u8, g) < 0.) bits |= 1u << g;
+  flags[cell] = bits;
 }
 
 __global__ void bc_diag_kernel(const uint8_t* __restrict__ bcbits, double* __restrict__ d, int64_t N) {
@@ -192,6 +236,33 @@ __global__ void v_coef_kernel(const ElemArgs E, const double* __restrict__ u,
   const CellMat m = cell_mat(E, ei, ej, ek);
   const double mass = E.atnum == 2 ? m.Gc / E.atcv * .5 / E.epsilon : 0.;
   for (int g = 0; g < 27; g++) {
+    if (E.unilateral) {
+      // ElasticEnergyDensitySphericalDeviatoricNoCompression3D_local (VFMech.c:115-218):
+      // W = sigma(eps - e0) : eps, less (kappa/2) tr^2 where tr < 0
+      double f11 = 0, f22 = 0, f33 = 0, f12 = 0, f23 = 0, f13 = 0, e0 = 0;
+      for (int a = 0; a < 8; a++) {
+        const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
+        f11 += d0 * u8[a][0];
+        f22 += d1 * u8[a][1];
+        f33 += d2 * u8[a][2];
+        f12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
+        f23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
+        f13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
+        e0 += m.alpha * e.phi[a][g] * th8[a];
+      }
+      const double l = m.lambda, mu = m.mu, kappa = l + 2. * mu / 3.;
+      const double s11 = (l + 2. * mu) * (f11 - e0) + l * (f22 - e0) + l * (f33 - e0);
+      const double s22 = l * (f11 - e0) + (l + 2. * mu) * (f22 - e0) + l * (f33 - e0);
+      const double s33 = l * (f11 - e0) + l * (f22 - e0) + (l + 2. * mu) * (f33 - e0);
+      const double Wf = (s11 * f11 + s22 * f22 + s33 * f33) * .5 +
+                        2. * mu * (f12 * f12 + f23 * f23 + f13 * f13);
+      const double tr = f11 + f22 + f33;
+      const double S = tr < 0. ? 0. : kappa * tr * tr * .5, D = Wf - kappa * tr * tr * .5;
+      const double cgv = e.w[g] * (2. * (S + D) + mass);
+      coef[27 * cell + g] = cgv;
+      if (coef32) coef32[27 * cell + g] = (float)cgv;
+      continue;
+    }
     double e11 = 0, e22 = 0, e33 = 0, e12 = 0, e23 = 0, e13 = 0;
     for (int a = 0; a < 8; a++) {
       const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
@@ -337,7 +408,10 @@ __global__ void __launch_bounds__(EN_THREADS) energy_kernel(
       D33 -= tr / 3.;
       el += (D11 * D11 + D22 * D22 + D33 * D33 + (D12 * D12 + D23 * D23 + D13 * D13) * 2.) * ve * ve *
             (1. + E.eta) * m.mu * e.w[g];
-      const double WD = (tr / 3. - m.alpha * te) * ve - coefbeta * pe;
+      // NOCOMPRESSION (VF_ElasticEnergyNoCompression3D_local, VFMech.c:819-908): the
+      // spherical factor is 1 instead of v where tr < 0
+      const double sph = (E.unilateral && tr < 0.) ? 1. : ve;
+      const double WD = (tr / 3. - m.alpha * te) * sph - coefbeta * pe;
       el += 3. * threekappa / 2. * WD * WD * e.w[g];
       el += threekappa / 6. * tr * tr * E.eta * e.w[g];
       const double udv = ue[0] * gv[0] + ue[1] * gv[1] + ue[2] * gv[2];
@@ -393,18 +467,25 @@ cudaError_t colours(const ElemArgs& E, K kernel, cudaStream_t s, Args... args) {
 }  // namespace
 
 cudaError_t launch_u_rhs(const ElemArgs& E, const double* v, const double* theta,
-                         const double* thetaRef, const double* p, double* f, cudaStream_t s) {
+                         const double* thetaRef, const double* p, double* f, cudaStream_t s,
+                         const double* u0) {
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(f, 0, 3 * N * sizeof(double), s);
   if (e != cudaSuccess) return e;
-  return colours(E, u_rhs_kernel, s, v, theta, thetaRef, p, f);
+  return colours(E, u_rhs_kernel, s, v, theta, thetaRef, p, f, u0);
+}
+
+cudaError_t launch_nc_flags(const ElemArgs& E, const double* u, uint32_t* flags, cudaStream_t s) {
+  const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  nc_flags_kernel<<<(int)((NCELL + 127) / 128), 128, 0, s>>>(E, u, flags);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcbits, double* d,
-                          cudaStream_t s) {
+                          cudaStream_t s, const double* u0) {
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(d, 0, 3 * N * sizeof(double), s);
-  if (e == cudaSuccess) e = colours(E, u_diag_kernel, s, v, d);
+  if (e == cudaSuccess) e = colours(E, u_diag_kernel, s, v, d, u0);
   if (e == cudaSuccess && bcbits) {
     bc_diag_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 2368), 256, 0, s>>>(bcbits, d, N);
     e = cudaGetLastError();

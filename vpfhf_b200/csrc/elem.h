@@ -22,15 +22,21 @@ struct ElemArgs {
   LayerTable L;
   double eta, epsilon, atcv;
   int atnum, hasCrackPressure;
+  int unilateral;  // 1 = NOCOMPRESSION (VFCtx.unilateral)
 };
 
 // f (3N) = thermo-poro + crack-pressure load (VFMech.c:386-447, 533-589), so that
 // F_U = K u - f.  Overwrites f.
+// With E.unilateral the thermo-poro load depends on u0 through the sign of tr(eps(u0))
+// (VF_GradientUThermoPoroNoCompression3D_local, VFMech.c:456-524); u0 = null reads as 0.
 cudaError_t launch_u_rhs(const ElemArgs& E, const double* v, const double* theta,
-                         const double* thetaRef, const double* p, double* f, cudaStream_t s);
-// d (3N) = diag K(v), Dirichlet rows 1.  Overwrites d.
+                         const double* thetaRef, const double* p, double* f, cudaStream_t s,
+                         const double* u0 = nullptr);
+// d (3N) = diag K(v) (with E.unilateral: of K(v; u0)), Dirichlet rows 1.  Overwrites d.
 cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcbits, double* d,
-                          cudaStream_t s);
+                          cudaStream_t s, const double* u0 = nullptr);
+// NOCOMPRESSION sign pattern: flags[cell] bit g = (tr(eps(u)) < 0 at Gauss point g).
+cudaError_t launch_nc_flags(const ElemArgs& E, const double* u, uint32_t* flags, cudaStream_t s);
 // coef (27 per cell) = w_g (2 W_g(u,theta) [+ Gc/(2c_w)/eps for AT2]) in FP64 and,
 // if coef32 is not null, FP32.
 cudaError_t launch_v_coef(const ElemArgs& E, const double* u, const double* theta,

@@ -69,6 +69,47 @@ template <typename T_> struct UOp {
   }
 };
 
+// The NOCOMPRESSION U operator: UOp with the per-point element u_element_nc and the
+// per-cell compression bits A.cflag.
+template <typename T_> struct UOpNC {
+  using T = T_;
+  using Args = UApplyArgs<T>;
+  static constexpr int NC = 3, NIN = 4, EPT = 1;
+  __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
+    UOp<T>::node_src(A, n, src);
+  }
+  __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
+                                                 int ey, int ez, const T (&in)[8][NIN],
+                                                 T (&out)[8][NC]) {
+    T xn[8][3], vn[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      xn[a][0] = in[a][0];
+      xn[a][1] = in[a][1];
+      xn[a][2] = in[a][2];
+      vn[a] = in[a][3];
+    }
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    const LayerTable& LT = A.P ? A.P->L : L;
+    const T eta = A.P ? T(A.P->eta) : A.eta;
+    const int64_t cell = ((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex;
+    T lam, mu;
+    if (A.cellE) {
+      const T E = T(A.cellE[cell]);
+      lam = E * T(LT.lamfac[layer]);
+      mu = E * T(LT.mufac[layer]);
+    } else {
+      lam = T(LT.lambda[layer]);
+      mu = T(LT.mu[layer]);
+    }
+    u_element_nc<T>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, A.cflag[cell], out);
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    return UOp<T>::template finish_node<DOT>(A, n, val);
+  }
+};
+
 // The FP32 U operator on two y-adjacent elements per thread, one per lane of the
 // packed FP32 instructions (f2): the same arithmetic as UOp<float> with half the
 // instructions.

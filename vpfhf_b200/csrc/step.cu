@@ -83,7 +83,14 @@ static ElemArgs elem_args(vfgpu_ctx* c) {
   E.atcv = c->vf.atnum == 1 ? 2. / 3. : .5;  // VFCommon.c:482-492
   E.atnum = c->vf.atnum;
   E.hasCrackPressure = c->vf.hasCrackPressure;
+  E.unilateral = c->unilateral;
   return E;
+}
+
+cudaError_t nc_flags(vfgpu_ctx* c, const double* u) {
+  if (!c->unilateral) return cudaSuccess;
+  if (solve_buffers(c) != VFGPU_OK) return cudaErrorMemoryAllocation;
+  return launch_nc_flags(elem_args(c), u, c->d_cflag, c->stream);
 }
 
 static InsituArgs insitu_args(const vfgpu_ctx* c) {
@@ -104,10 +111,12 @@ static InsituArgs insitu_args(const vfgpu_ctx* c) {
   return A;
 }
 
-// f (3N) = the U load of VF_UResidual: thermo-poro, crack pressure and in-situ tractions.
-static cudaError_t u_load(vfgpu_ctx* c, const ElemArgs& E, double* f) {
+// f (3N) = the U load of VF_UResidual: thermo-poro, crack pressure and in-situ tractions;
+// u0: the displacement that fixes the NOCOMPRESSION sign pattern of the thermo-poro term.
+static cudaError_t u_load(vfgpu_ctx* c, const ElemArgs& E, double* f, const double* u0) {
   cudaError_t e = launch_u_rhs(E, c->f[VFGPU_FIELD_V], c->f[VFGPU_FIELD_THETA],
-                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream);
+                               c->f[VFGPU_FIELD_THETAREF], c->f[VFGPU_FIELD_PRESSURE], f, c->stream,
+                               u0);
   if (e == cudaSuccess && c->has_insitu) e = launch_insitu_load(insitu_args(c), f, c->stream);
   return e;
 }
@@ -311,8 +320,10 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   double* U = c->f[VFGPU_FIELD_U];
   const bool mixed = o.precision == VFGPU_MIXED;
   ElemArgs E = elem_args(c);
-  cudaError_t e = u_load(c, E, f);
-  if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream);
+  const bool nc = c->unilateral != 0;
+  cudaError_t e = nc_flags(c, U);
+  if (e == cudaSuccess) e = u_load(c, E, f, U);
+  if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream, U);
   if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
   if (mixed && e == cudaSuccess) {
     rc = ensure_v32(c);
@@ -332,9 +343,22 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   auto apply32 = [&](const float* x, float* y, const int* skip, double* dot) {
     return u_apply32(c, x, y, skip, dot);
   };
+  // NOCOMPRESSION: F(X) = K(V; X) X - f(X) with the sign pattern of X (flags left at X)
+  auto nc_residual = [&](const double* X, double* Fout) {
+    cudaError_t ee = nc_flags(c, X);
+    if (ee == cudaSuccess) ee = u_load(c, E, f, X);
+    if (ee == cudaSuccess) ee = u_residual(c, X, f, JY, Fout);
+    return ee;
+  };
   for (int it = 0; !reason && it < o.snes_maxit; it++) {
     int kits = 0, kreason = 0;
     bool tmo = false;
+    if (nc && it > 0) {  // the Jacobian K(V; U) and its diagonal at the new iterate
+      e = nc_flags(c, U);
+      if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream, U);
+      if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+    }
     if (!mixed) {
       CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), dots_of(c, c->plan64)};
       rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
@@ -388,23 +412,45 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
       reason = -3;  // SNES_DIVERGED_LINEAR_SOLVE
       break;
     }
-    // L2 line search.  F is affine in U, so ||F(U - l Y)||^2 is an exact quadratic in l
-    // whose minimiser (what SNESLINESEARCHL2's secant step lands on) is
-    // l* = (F . JY) / (JY . JY).
-    e = u_apply64(c, Y, JY, nullptr);
-    const double* pa[3] = {F, JY, Y};
-    const double* pb[3] = {JY, JY, Y};
-    if (e == cudaSuccess) e = dev_dots(pa, pb, 3, n3, c->d_red, c->d_out, c->stream);
-    if (e == cudaSuccess) e = fetch(c, 3);
-    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
-    double lambda = 1.0;
-    if (c->h_out[1] > 0) {
-      const double l = c->h_out[0] / c->h_out[1];
-      if (l == l && l > 1e-12) lambda = l;
+    double lambda = 1.0, ynorm = 0.;
+    if (!nc) {
+      // L2 line search.  F is affine in U, so ||F(U - l Y)||^2 is an exact quadratic in l
+      // whose minimiser (what SNESLINESEARCHL2's secant step lands on) is
+      // l* = (F . JY) / (JY . JY).
+      e = u_apply64(c, Y, JY, nullptr);
+      const double* pa[3] = {F, JY, Y};
+      const double* pb[3] = {JY, JY, Y};
+      if (e == cudaSuccess) e = dev_dots(pa, pb, 3, n3, c->d_red, c->d_out, c->stream);
+      if (e == cudaSuccess) e = fetch(c, 3);
+      if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+      if (c->h_out[1] > 0) {
+        const double l = c->h_out[0] / c->h_out[1];
+        if (l == l && l > 1e-12) lambda = l;
+      }
+      ynorm = lambda * sqrt(c->h_out[2]);
+      e = dev_axpy(U, -lambda, Y, n3, c->stream);
+      if (e == cudaSuccess) e = u_residual(c, U, f, JY, F);
+    } else {
+      // L2 line search on the piecewise-affine NOCOMPRESSION residual: one secant step
+      // on the derivative of ||F(U - l Y)||^2 fitted through l = 0, 1/2, 1.
+      double q[2];
+      for (int sidx = 0; sidx < 2; sidx++) {
+        e = cudaMemcpyAsync(W, U, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = dev_axpy(W, sidx == 0 ? -0.5 : -1.0, Y, n3, c->stream);
+        if (e == cudaSuccess) e = nc_residual(W, R);
+        q[sidx] = dot_host(c, R, R, n3, e);
+        if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
+      }
+      const double q0 = fnorm * fnorm, qm = q[0], q1 = q[1];
+      const double dE = 3. * q1 - 4. * qm + q0, dE_old = -3. * q0 + 4. * qm - q1;
+      if (dE - dE_old != 0.) {
+        const double lu = 1. - dE / (dE - dE_old);
+        if (lu == lu && lu > 1e-12) lambda = lu;
+      }
+      ynorm = lambda * sqrt(dot_host(c, Y, Y, n3, e));
+      if (e == cudaSuccess) e = dev_axpy(U, -lambda, Y, n3, c->stream);
+      if (e == cudaSuccess) e = nc_residual(U, F);
     }
-    const double ynorm = lambda * sqrt(c->h_out[2]);
-    e = dev_axpy(U, -lambda, Y, n3, c->stream);
-    if (e == cudaSuccess) e = u_residual(c, U, f, JY, F);
     const double* qa[2] = {F, U};
     const double* qb[2] = {F, U};
     if (e == cudaSuccess) e = dev_dots(qa, qb, 2, n3, c->d_red, c->d_out, c->stream);
@@ -726,7 +772,8 @@ int vfgpu_u_residual(vfgpu_ctx* c, double* F) {
   if (rc) return rc;
   ElemArgs E = elem_args(c);
   double *f = c->p64[0], *tmp = c->p64[1], *Fd = c->p64[2];
-  cudaError_t e = u_load(c, E, f);
+  cudaError_t e = nc_flags(c, c->f[VFGPU_FIELD_U]);
+  if (e == cudaSuccess) e = u_load(c, E, f, c->f[VFGPU_FIELD_U]);
   if (e == cudaSuccess) e = u_residual(c, c->f[VFGPU_FIELD_U], f, tmp, Fd);
   if (e == cudaSuccess) e = copy_out(c, F, Fd, 3 * c->N);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);

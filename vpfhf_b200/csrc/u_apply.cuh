@@ -41,6 +41,8 @@ template <typename T> struct UApplyArgs {
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   const DevParams* __restrict__ P;    // material and eta; null => the by-value LayerTable and eta
   double* __restrict__ dot;           // if non-null: per-block partials of x.y (see tile_engine.cuh)
+  const uint32_t* __restrict__ cflag; // NOCOMPRESSION: per cell, bit g = tr(eps(u0)) < 0 at Gauss
+                                      // point g (u_element_nc); null = the plain operator
   int nx, ny, nz;
   int ntx, nty, zc;                   // tiles in x, y; owned node planes per z-chunk
   T ihx, ihy, ihz, vol, eta;
@@ -244,6 +246,117 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
 
   // Inverse butterfly: direction-d part of node (i,j,k) is
   //   s_d/h_d * (Q0/4 + s_1 Q1/2 + s_2 Q2/2 + s_1 s_2 Q3), s = -1 (node 0) or +1 (node 1).
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    T A[3][2][2];
+    inv_butterfly(QX[c], ihx, A[0]);
+    inv_butterfly(QY[c], ihy, A[1]);
+    inv_butterfly(QZ[c], ihz, A[2]);
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+#pragma unroll
+      for (int j = 0; j < 2; j++)
+#pragma unroll
+        for (int i = 0; i < 2; i++)
+          y[i + 2 * j + 4 * k][c] = signed_sum3(A[0][j][k], A[1][i][k], A[2][i][j], i, j, k);
+  }
+}
+
+// The NOCOMPRESSION operator K(v; u0) (VF_BilinearFormUNoCompression3D_local,
+// VFMech.c:299-376) for one element: at Gauss point g, if bit g of `flags` is set
+// (tr(eps(u0)) < 0 there) the spherical part keeps kappa (1 + eta), so the stress is
+//   w [lambda' tr(G) I + s mu (G + G^T)],  lambda' = kappa (1 + eta) - 2 mu s / 3,
+// and otherwise the plain w s (lambda tr(G) I + mu (G + G^T)).  The coefficient is
+// no longer one polynomial along a row, so this variant sums point by point (same
+// modal gradients and moments as u_element); the z moments are accumulated at every
+// point to keep the register count down.
+template <typename T>
+__device__ __forceinline__ void u_element_nc(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
+                                             T eta, T ihx, T ihy, T ihz, T vol, uint32_t flags,
+                                             T (&y)[8][3]) {
+  T m[3][8], mv[8];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    T f[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) f[a] = xn[a][c];
+    modal8(f, m[c]);
+  }
+  modal8(vn, mv);
+  T QX[3][4], QY[3][4], QZ[3][4];
+#pragma unroll
+  for (int c = 0; c < 3; c++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) QX[c][q] = QY[c][q] = QZ[c][q] = T(0);
+  const T mu2 = T(2) * mu, kap1 = (lam + T(2.0 / 3.0) * mu) * (T(1) + eta), mu23 = T(2.0 / 3.0) * mu;
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++) {
+    const T volw = vol * gw<T>(gz);
+    T ax[3], bx[3], ay[3], by[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const T t37 = lin(gz, m[c][3], m[c][7]);
+      ax[c] = lin(gz, m[c][1], m[c][5]) * ihx;
+      bx[c] = t37 * ihx;
+      ay[c] = lin(gz, m[c][2], m[c][6]) * ihy;
+      by[c] = t37 * ihy;
+    }
+    const T p0 = lin(gz, mv[0], mv[4]), p1 = lin(gz, mv[1], mv[5]);
+    const T p2 = lin(gz, mv[2], mv[6]), p3 = lin(gz, mv[3], mv[7]);
+    T SY[3][3];
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++) {
+      T Gx[3], al[3], be[3];
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        Gx[c] = lin(gy, ax[c], bx[c]);
+        al[c] = lin(gy, m[c][4], m[c][6]) * ihz;
+        be[c] = lin(gy, m[c][5], m[c][7]) * ihz;
+      }
+      const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
+      T SX[3];
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        T Gy[3], Gz[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+          Gy[c] = lin(gx, ay[c], by[c]);
+          Gz[c] = lin(gx, al[c], be[c]);
+        }
+        const T vg = lin(gx, q0, q1);
+        const T sv = fma(vg, vg, eta);
+        const T wq = volw * T(gwd(gx) * gwd(gy));
+        const T ws = wq * sv;
+        const T tr = Gx[0] + Gy[1] + Gz[2];
+        const bool comp = (flags >> (gx + 3 * gy + 9 * gz)) & 1u;
+        const T L = comp ? (wq * (kap1 - mu23 * sv)) * tr : (ws * lam) * tr;
+        const T m2 = ws * mu2, m1 = ws * mu;
+        const T s00 = fma(m2, Gx[0], L), s11 = fma(m2, Gy[1], L), s22 = fma(m2, Gz[2], L);
+        const T s01 = m1 * (Gy[0] + Gx[1]);
+        const T s02 = m1 * (Gz[0] + Gx[2]);
+        const T s12 = m1 * (Gz[1] + Gy[2]);
+        if (gx == 0) {
+          SX[0] = s00; SX[1] = s01; SX[2] = s02;
+        } else {
+          SX[0] += s00; SX[1] += s01; SX[2] += s02;
+        }
+        if (gy == 0) {
+          SY[0][gx] = s01; SY[1][gx] = s11; SY[2][gx] = s12;
+        } else {
+          SY[0][gx] += s01; SY[1][gx] += s11; SY[2][gx] += s12;
+        }
+        moment4(QZ[0], gx, gy, s02);
+        moment4(QZ[1], gx, gy, s12);
+        moment4(QZ[2], gx, gy, s22);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) moment4(QX[c], gy, gz, SX[c]);
+    }
+#pragma unroll
+    for (int gx = 0; gx < 3; gx++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) moment4(QY[c], gx, gz, SY[c][gx]);
+  }
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     T A[3][2][2];

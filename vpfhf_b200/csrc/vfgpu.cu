@@ -135,6 +135,7 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   A.vol = T(c->hx * c->hy * c->hz);
   A.eta = T(c->vf.eta);
   A.P = c->d_params;
+  A.cflag = c->unilateral ? c->d_cflag : nullptr;
   return A;
 }
 template UApplyArgs<double> u_args<double>(vfgpu_ctx*, const double*, const double*, double*,
@@ -158,7 +159,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   c->graphs.clear();
   free_solver(c);
   for (auto& p : c->f) cudaFree(p);
-  void* bufs[] = {c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -336,6 +337,26 @@ int vfgpu_set_vfprop(vfgpu_ctx* c, const vfgpu_vfprop* vf) {
   return upload_params(c);
 }
 
+int vfgpu_set_unilateral(vfgpu_ctx* c, int type) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_set_unilateral: null ctx");
+  if (type != VFGPU_UNILATERAL_NONE && type != VFGPU_UNILATERAL_NOCOMPRESSION)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_set_unilateral: unknown type %d", type);
+  cudaSetDevice(c->dev);
+  if (type == VFGPU_UNILATERAL_NOCOMPRESSION && !c->d_cflag) {
+    cudaError_t e = cudaMalloc((void**)&c->d_cflag, std::max<int64_t>(1, c->NC) * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cflag, 0, std::max<int64_t>(1, c->NC) * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+      cudaFree(c->d_cflag);
+      c->d_cflag = nullptr;
+      return cuda_fail(e, "vfgpu_set_unilateral");
+    }
+  }
+  if (type != c->unilateral) c->gen++;  // captured CG graphs launch the other operator kernel
+  c->unilateral = type;
+  return VFGPU_OK;
+}
+
 int vfgpu_set_insitu(vfgpu_ctx* c, const double* smin, const double* smax) {
   if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_set_insitu: null ctx");
   c->has_insitu = smin != nullptr;
@@ -414,6 +435,7 @@ int vfgpu_u_apply(vfgpu_ctx* c, int precision, const double* x, double* y) {
     xd = c->t64a;
   }
   double* yd = ydev ? y : c->t64b;
+  if (e == cudaSuccess && c->unilateral) e = nc_flags(c, c->f[VFGPU_FIELD_U]);
   if (e == cudaSuccess) {
     if (precision == VFGPU_FP64) {
       e = launch_u_apply<double>(u_args<double>(c, xd, c->f[VFGPU_FIELD_V], yd, c->seam64, c->plan64),
@@ -442,7 +464,8 @@ int vfgpu_u_apply_dev(vfgpu_ctx* c, int precision, const void* x, void* y) {
   if (!is_device_ptr(x) || !is_device_ptr(y))
     return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_dev: x and y must be device pointers");
   cudaSetDevice(c->dev);
-  cudaError_t e;
+  cudaError_t e = c->unilateral ? nc_flags(c, c->f[VFGPU_FIELD_U]) : cudaSuccess;
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_dev");
   if (precision == VFGPU_FP64) {
     e = launch_u_apply<double>(u_args<double>(c, (const double*)x, c->f[VFGPU_FIELD_V], (double*)y,
                                               c->seam64, c->plan64),

@@ -55,8 +55,6 @@ static PetscErrorCode vfgpu_setup(VFCtx *ctx) {
   PetscFunctionBegin;
   ierr = MPI_Comm_size(PETSC_COMM_WORLD, &size);CHKERRQ(ierr);
   if (size != 1) SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: one rank per problem");
-  if (ctx->unilateral != UNILATERAL_NONE)
-    SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: only -unilateral none is supported");
   if (ctx->nlayer > 16) SETERRQ(PETSC_COMM_WORLD, PETSC_ERR_SUP, "vfgpu: at most 16 layers");
   ierr = DMDAGetInfo(ctx->daVect, NULL, &nx, &ny, &nz, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
                      NULL, NULL);CHKERRQ(ierr);
@@ -96,6 +94,9 @@ static PetscErrorCode vfgpu_setup(VFCtx *ctx) {
     }
     VFGPU_CHK(vfgpu_set_insitu(gpu_ctx, ctx->hasInsitu ? smin : NULL, smax));
   }
+  VFGPU_CHK(vfgpu_set_unilateral(gpu_ctx, ctx->unilateral == UNILATERAL_NOCOMPRESSION
+                                              ? VFGPU_UNILATERAL_NOCOMPRESSION
+                                              : VFGPU_UNILATERAL_NONE));
   PetscFunctionReturn(0);
 }
 
