@@ -93,7 +93,12 @@ typedef struct {
   double inner_rtol;      /* VFGPU_MIXED: relative tolerance of each FP32 inner solve   */
   int max_refine;         /* VFGPU_MIXED: cap on FP64 refinement steps per Newton step  */
   double time_limit;      /* wall-clock watchdog in seconds (0 = none)                  */
+  int pc;                 /* StepU preconditioner: VFGPU_PC_JACOBI (the reference's) or  */
+                          /* VFGPU_PC_MG (geometric multigrid V-cycle; FP64)             */
 } vfgpu_solve_opts;
+
+#define VFGPU_PC_JACOBI 0
+#define VFGPU_PC_MG 1
 
 typedef struct {
   int newton_its;         /* SNES iterations                                            */

@@ -17,6 +17,7 @@ OK, NOT_CONVERGED, DIVERGED = 0, 1, 2
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_STATE = -1, -2, -3, -4
 FP64, MIXED = 0, 1
 UNILATERAL_NONE, UNILATERAL_NOCOMPRESSION = 0, 1
+PC_JACOBI, PC_MG = 0, 1
 BC_NONE, BC_ZERO, BC_ONE, BC_FIXED = 0, 1, 2, 3
 FIELD_U, FIELD_V, FIELD_VIRREV, FIELD_BCU, FIELD_THETA, FIELD_THETAREF, FIELD_PRESSURE = range(7)
 FIELD_NAMES = {"U": FIELD_U, "V": FIELD_V, "VIrrev": FIELD_VIRREV, "BCU": FIELD_BCU,
@@ -47,7 +48,8 @@ class SolveOpts(C.Structure):
     _fields_ = [("precision", C.c_int), ("ksp_rtol", C.c_double), ("ksp_atol", C.c_double),
                 ("ksp_dtol", C.c_double), ("ksp_maxit", C.c_int), ("snes_rtol", C.c_double),
                 ("snes_atol", C.c_double), ("snes_stol", C.c_double), ("snes_maxit", C.c_int),
-                ("inner_rtol", C.c_double), ("max_refine", C.c_int), ("time_limit", C.c_double)]
+                ("inner_rtol", C.c_double), ("max_refine", C.c_int), ("time_limit", C.c_double),
+                ("pc", C.c_int)]
 
 
 class SolveStats(C.Structure):

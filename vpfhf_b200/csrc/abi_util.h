@@ -14,6 +14,12 @@ void free_solver(vfgpu_ctx* c);
 int upload_params(vfgpu_ctx* c);
 // NOCOMPRESSION: recompute the per-cell compression bits from displacement u (device).
 cudaError_t nc_flags(vfgpu_ctx* c, const double* u);
+// Geometric multigrid preconditioned CG of the U Jacobian (mg.cu): x = K^-1 b with the
+// stopping test of the Jacobi PCG; levels = size of the hierarchy.
+int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double* w,
+             const double* dinv0, double rtol, double atol, double dtol, int maxit, int* its,
+             int* reason, int* levels);
+void free_mg(vfgpu_ctx* c);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
 }  // namespace vfgpu

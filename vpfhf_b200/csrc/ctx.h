@@ -70,6 +70,24 @@ struct vfgpu_ctx {
   double* h_out = nullptr;        // pinned host mirror of d_out
   bool have_solver = false;
 
+  // Geometric multigrid hierarchy of the U operator (VFGPU_PC_MG), built at the first
+  // MG solve: level 0 is the ctx's own grid, levels 1.. halve the cells per axis.
+  struct MGLevel {
+    int nx = 0, ny = 0, nz = 0;
+    int64_t N = 0, NC = 0;
+    double hx = 0, hy = 0, hz = 0;
+    vfgpu::TilePlan plan{};
+    double* seam = nullptr;
+    double *v = nullptr, *dinv = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr,
+           *t = nullptr;
+    uint8_t *bc = nullptr, *elayer = nullptr;
+    float* cellE = nullptr;
+    vfgpu::ETab* tab = nullptr;
+    double lmax = 0;
+  };
+  std::vector<MGLevel> mg;      // mg[0] holds the fine level's extra work vectors only
+  double* mg_z = nullptr;       // fine preconditioned residual
+
   // Captured CUDA graphs of CG iteration batches, keyed by (call site, batch size).
   // Kernels read the material table, eta and the AT gradient weights through
   // d_params, so new material / vfprop values leave the graphs valid; a set-up call

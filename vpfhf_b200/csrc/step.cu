@@ -299,6 +299,7 @@ void vfgpu_default_solve_opts(vfgpu_solve_opts* o) {
   o->inner_rtol = 1e-4;
   o->max_refine = 12;
   o->time_limit = 0.;
+  o->pc = VFGPU_PC_JACOBI;
 }
 
 int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st) {
@@ -308,6 +309,10 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   if (o_) o = *o_; else vfgpu_default_solve_opts(&o);
   if (o.precision != VFGPU_FP64 && o.precision != VFGPU_MIXED)
     return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad precision");
+  if (o.pc != VFGPU_PC_JACOBI && o.pc != VFGPU_PC_MG)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad preconditioner");
+  if (o.pc == VFGPU_PC_MG && o.precision != VFGPU_FP64)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: the multigrid preconditioner runs in FP64");
   vfgpu_solve_stats S{};
   cudaSetDevice(c->dev);
   int rc = solve_buffers(c);
@@ -359,7 +364,14 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
       if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
       if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
     }
-    if (!mixed) {
+    if (o.pc == VFGPU_PC_MG) {
+      int levels = 0;
+      rc = run_mgcg(c, F, Y, R, P, W, dinv, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, &kits,
+                    &kreason, &levels);
+      if (rc) return rc;
+      S.ksp_its += kits;
+      tmo = w.expired();
+    } else if (!mixed) {
       CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), dots_of(c, c->plan64)};
       rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
