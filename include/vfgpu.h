@@ -94,7 +94,9 @@ typedef struct {
   int max_refine;         /* VFGPU_MIXED: cap on FP64 refinement steps per Newton step  */
   double time_limit;      /* wall-clock watchdog in seconds (0 = none)                  */
   int pc;                 /* StepU preconditioner: VFGPU_PC_JACOBI (the reference's) or  */
-                          /* VFGPU_PC_MG (geometric multigrid V-cycle; FP64)             */
+                          /* VFGPU_PC_MG (geometric multigrid V-cycle, FP32 under       */
+                          /* VFGPU_MIXED, FP64 otherwise; FP64 CG with the Jacobi       */
+                          /* solve's stopping test; needs an even cell count per axis)  */
 } vfgpu_solve_opts;
 
 #define VFGPU_PC_JACOBI 0

@@ -25,8 +25,10 @@ def _penny_ctx(n, L=4.0, cellE=None):
     return ctx
 
 
-def test_mg_matches_oracle_step_u(cuda, oracle_mod):
-    """17^3 penny (levels 17, 9, 5): U and energies against the oracle's Jacobi StepU."""
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mg_matches_oracle_step_u(cuda, oracle_mod, precision):
+    """17^3 penny (levels 17, 9, 5), V-cycle in FP64 or FP32: U and energies against the
+    oracle's Jacobi StepU."""
     import vpfhf_b200 as vg
     n, L = 17, 4.0
     h = L / (n - 1)
@@ -43,7 +45,7 @@ def test_mg_matches_oracle_step_u(cuda, oracle_mod):
     ctx.set_field("V", v)
     ctx.set_field("VIrrev", v)
     ctx.set_field("pressure", p)
-    rc, st = ctx.step_u(dict(pc="mg"))
+    rc, st = ctx.step_u(dict(pc="mg", precision=precision))
     assert rc == 0 and st["reason"] > 0, st
     ug = ctx.get_field("U")
     assert np.linalg.norm(ug - u) <= 1e-6 * np.linalg.norm(u)
@@ -53,10 +55,11 @@ def test_mg_matches_oracle_step_u(cuda, oracle_mod):
     ctx.close()
 
 
-@pytest.mark.parametrize("hetero", [False, True])
-def test_mg_matches_jacobi_65(cuda, hetero):
-    """65^3 inclined penny, uniform or log-normal per-cell modulus: the multigrid and the
-    Jacobi StepU reach the same U, the multigrid in a tenth of the Krylov iterations."""
+@pytest.mark.parametrize("hetero,precision", [(False, "fp64"), (True, "fp64"), (True, "mixed")])
+def test_mg_matches_jacobi_65(cuda, hetero, precision):
+    """65^3 inclined penny, uniform or log-normal per-cell modulus: the multigrid (FP64 or
+    FP32 V-cycle) and the FP64 Jacobi StepU reach the same U, the multigrid in a tenth of
+    the Krylov iterations."""
     n = 65
     cellE = None
     if hetero:
@@ -65,7 +68,7 @@ def test_mg_matches_jacobi_65(cuda, hetero):
     res = {}
     for pc in ("jacobi", "mg"):
         ctx = _penny_ctx(n, cellE=cellE)
-        rc, st = ctx.step_u(dict(pc=pc))
+        rc, st = ctx.step_u(dict(pc=pc, precision=precision if pc == "mg" else "fp64"))
         assert rc == 0 and st["reason"] > 0, (pc, st)
         res[pc] = (ctx.get_field("U"), st, ctx.u_energy())
         ctx.close()
@@ -76,7 +79,8 @@ def test_mg_matches_jacobi_65(cuda, hetero):
     assert sm["ksp_its"] * 10 <= sj["ksp_its"], (sm, sj)
 
 
-def test_mg_nocompression_newton(cuda, oracle_mod):
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mg_nocompression_newton(cuda, oracle_mod, precision):
     """The squeezed NOCOMPRESSION crack (13^3: levels 13, 7): the multigrid preconditions
     the re-formed Jacobian of every Newton step and lands on the oracle's solution."""
     import vpfhf_b200 as vg
@@ -102,7 +106,7 @@ def test_mg_nocompression_newton(cuda, oracle_mod):
     ctx.set_bc(bc)
     ctx.set_field("BCU", bcu)
     ctx.time_step_prepare()
-    rc, s = ctx.step_u(dict(pc="mg"))
+    rc, s = ctx.step_u(dict(pc="mg", precision=precision))
     assert rc == 0 and s["reason"] > 0 and s["newton_its"] >= 2, s
     ug = ctx.get_field("U")
     assert np.linalg.norm(ug - uo) <= 1e-6 * np.linalg.norm(uo)
@@ -110,15 +114,39 @@ def test_mg_nocompression_newton(cuda, oracle_mod):
 
 
 def test_mg_rejected_cases(cuda):
-    """An odd cell count (no coarse grid) and the mixed-precision solve are refused with
-    VFGPU_ERR_INVALID; the context stays usable for a Jacobi solve."""
+    """An odd cell count (no coarse grid) is refused with VFGPU_ERR_INVALID in both
+    precisions; the context stays usable for a Jacobi solve."""
     import vpfhf_b200 as vg
     ctx = _penny_ctx(16)  # 15 cells per axis
     with pytest.raises(vg.VFGPUError) as ei:
         ctx.step_u(dict(pc="mg"))
     assert ei.value.code == -1 and "multigrid" in str(ei.value)
-    with pytest.raises(vg.VFGPUError):
+    with pytest.raises(vg.VFGPUError) as ei:
         ctx.step_u(dict(pc="mg", precision="mixed"))
+    assert ei.value.code == -1
     rc, st = ctx.step_u()
     assert rc == 0 and st["reason"] > 0, st
     ctx.close()
+
+
+def test_mg_precision_switch_and_am_loop(cuda):
+    """One context alternating FP64 and FP32 V-cycles (the hierarchy is rebuilt on each
+    switch) through AM steps: each result is bit-identical to a fresh context's."""
+    n = 33
+
+    def run(ctx, precisions):
+        out = []
+        for prec in precisions:
+            rc, err, su, sv = ctx.am_step(dict(pc="mg", precision=prec))
+            assert rc == 0, (su, sv)
+            out.append((ctx.get_field("U"), ctx.get_field("V")))
+        return out
+
+    a = _penny_ctx(n)
+    got = run(a, ["fp64", "mixed", "fp64"])
+    a.close()
+    for k, prec in enumerate(["fp64", "mixed", "fp64"]):
+        b = _penny_ctx(n)
+        ref = run(b, ["fp64", "mixed", "fp64"][:k + 1])[-1]
+        b.close()
+        assert np.array_equal(got[k][0], ref[0]) and np.array_equal(got[k][1], ref[1]), prec

@@ -1,6 +1,8 @@
 // abi_util.h -- helpers shared by the C-ABI translation units.
 #pragma once
 
+#include <functional>
+
 #include "ctx.h"
 
 namespace vfgpu {
@@ -14,11 +16,17 @@ void free_solver(vfgpu_ctx* c);
 int upload_params(vfgpu_ctx* c);
 // NOCOMPRESSION: recompute the per-cell compression bits from displacement u (device).
 cudaError_t nc_flags(vfgpu_ctx* c, const double* u);
-// Geometric multigrid preconditioned CG of the U Jacobian (mg.cu): x = K^-1 b with the
-// stopping test of the Jacobi PCG; levels = size of the hierarchy.
-int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double* w,
-             const double* dinv0, double rtol, double atol, double dtol, int maxit, int* its,
-             int* reason, int* levels);
+// Geometric multigrid preconditioned CG of the U Jacobian (mg.cu): x = K^-1 b, FP64
+// Krylov vectors, V-cycle in FP32 (fp32) or FP64, with the stopping test of the
+// Jacobi PCG (dinv0 = FP64 inverse diagonal; dinv0_32 its FP32 copy for fp32).
+// reuse: the operator is unchanged since the last call (keeps the level set-up).
+int run_mgcg(vfgpu_ctx* c, bool fp32, const double* b, double* x, double* r, double* p, double* w,
+             const double* dinv0, const float* dinv0_32, bool reuse, double rtol, double atol,
+             double dtol, int maxit, int* its, int* reason, int* levels);
+// Graph of one call site's launch sequence, captured on first use and re-captured when
+// ctx->gen moves on (null: capture failed, run the body directly).
+cudaGraphExec_t ctx_graph(vfgpu_ctx* c, int kind, int batch,
+                          const std::function<cudaError_t()>& body);
 void free_mg(vfgpu_ctx* c);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);

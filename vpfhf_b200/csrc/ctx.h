@@ -71,22 +71,28 @@ struct vfgpu_ctx {
   bool have_solver = false;
 
   // Geometric multigrid hierarchy of the U operator (VFGPU_PC_MG), built at the first
-  // MG solve: level 0 is the ctx's own grid, levels 1.. halve the cells per axis.
+  // MG solve in the V-cycle's precision (mg_bytes: 8 FP64, 4 FP32): level 0 is the
+  // ctx's own grid (work vectors only), levels 1.. halve the cells per axis.
   struct MGLevel {
     int nx = 0, ny = 0, nz = 0;
     int64_t N = 0, NC = 0;
     double hx = 0, hy = 0, hz = 0;
     vfgpu::TilePlan plan{};
-    double* seam = nullptr;
-    double *v = nullptr, *dinv = nullptr, *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr,
-           *t = nullptr;
+    void* seam = nullptr;                      // V-cycle precision
+    void *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;  // 3N each
+    void *v = nullptr, *dinv = nullptr;        // coarse phase field (N), inverse diagonal (3N)
+    double* v64 = nullptr;                     // coarse phase field in FP64 (the diagonal's input)
     uint8_t *bc = nullptr, *elayer = nullptr;
     float* cellE = nullptr;
     vfgpu::ETab* tab = nullptr;
-    double lmax = 0;
+    double* coef = nullptr;  // device, 64: lmax, 1/theta, Chebyshev (c1, c2) pairs, scratch
   };
-  std::vector<MGLevel> mg;      // mg[0] holds the fine level's extra work vectors only
-  double* mg_z = nullptr;       // fine preconditioned residual
+  std::vector<MGLevel> mg;
+  int mg_bytes = 0;
+  bool mg_ready = false;          // coarse fields, diagonals and eigenvalue bounds are current
+  double* mg_coef = nullptr;      // 64 doubles per level (MGLevel::coef points into it)
+  double* mg_z = nullptr;         // FP32 V-cycle: the preconditioned residual in FP64 (3N)
+  const void* mg_dinv0 = nullptr; // fine inverse diagonal in the V-cycle's precision
 
   // Captured CUDA graphs of CG iteration batches, keyed by (call site, batch size).
   // Kernels read the material table, eta and the AT gradient weights through

@@ -1,22 +1,28 @@
 // mg.cu -- geometric multigrid V-cycle as the preconditioner of the U solve's CG
 // (solve option VFGPU_PC_MG).  No counterpart in the reference, whose snesU uses
 // KSPCG with Jacobi (or hypre when PETSc has it, VFCommon.c:1044-1047); the solve it
-// feeds keeps the reference's semantics (same residual, same SNES tests), only the
-// Krylov iterations get fewer.
+// feeds keeps the reference's semantics (same residual, same SNES tests, the CG
+// stopping test of the Jacobi solve), only the Krylov iterations get fewer.
 //
 // Levels halve the cells per axis while every axis has an even cell count and the
 // coarse grid keeps >= 5 nodes per axis.  Each coarse level rediscretises the same
 // operator (the tile engine's U apply) on its grid with the phase field injected
 // from the level above (v_c(I) = v_f(2I)), the Dirichlet bits injected the same
-// way, the element layer of the lower child layer and, for a per-cell modulus, the
+// way, the element layer of the lowest child layer and, for a per-cell modulus, the
 // mean of the 8 children.  Transfers: trilinear prolongation and its transpose
-// (full weighting), Dirichlet dofs zeroed after each.  Smoother: Chebyshev
-// iteration of D^-1 K of degree 3 on [lmax/10, lmax] (lmax from 12 power
-// iterations per level and solve), pre and post; the coarsest level runs degree 30
-// on [lmax/100, lmax].  Everything is a fixed sequence of deterministic kernels, so
-// the V-cycle is a fixed symmetric linear operator and plain PCG applies.
+// (full weighting), Dirichlet dofs excluded on both sides.  Smoother: Chebyshev
+// iteration of D^-1 K of degree 3 on [lmax/10, lmax] (lmax = 1.1 x the estimate of
+// 12 power iterations, per level and operator), pre and post; the coarsest level
+// runs degree 30 on [lmax/100, lmax].  Every step is a fixed sequence of
+// deterministic kernels reading its Chebyshev coefficients from device memory, so
+// the V-cycle is a fixed symmetric linear operator (plain PCG applies) and is
+// replayed as one CUDA graph.
+//
+// Precision: the V-cycle runs in FP64 (solve precision FP64) or FP32 (MIXED); the
+// outer CG, its residual and its stopping test stay FP64 in both.
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "abi_util.h"
@@ -27,7 +33,10 @@ namespace vfgpu {
 namespace {
 
 constexpr int kSmoothDeg = 3, kCoarseDeg = 30, kPowerIts = 12;
-constexpr double kSmoothLo = 0.1, kCoarseLo = 0.01;
+constexpr double kSmoothLo = 0.1, kCoarseLo = 0.01, kLmaxSafety = 1.1;
+constexpr int kCoefPerLevel = 64;  // [0] lmax [1] 1/theta [2..59] (c1, c2) [62..63] scratch
+constexpr int kPowBlocks = 296, kPowThreads = 256;
+constexpr int kGraphMG64 = 5, kGraphMG32 = 6;  // vfgpu_ctx::Graph kinds
 
 inline int blocks_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256, 148 * 16); }
 
@@ -35,61 +44,63 @@ inline int blocks_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n);              \
        i += (int64_t)gridDim.x * blockDim.x)
 
-// Full weighting: coarse node I gathers the fine nodes 2I + o, o in {-1,0,1}^3, with
-// weight prod_d (1 - |o_d| / 2), skipping fine Dirichlet dofs; Dirichlet dofs of the
-// coarse level are zeroed.  This is the transpose of prolong_add_kernel.
-__global__ void restrict_kernel(const double* __restrict__ rf, const uint8_t* __restrict__ bc_f,
-                                int fx, int fy, int fz, double* __restrict__ rc, int cx, int cy,
-                                int cz, const uint8_t* __restrict__ bc_c) {
+// Full weighting of the residual b - t: coarse node I gathers the fine nodes 2I + o,
+// o in {-1,0,1}^3, with weight prod_d (1 - |o_d| / 2), skipping fine Dirichlet dofs;
+// coarse Dirichlet dofs are zeroed.  The transpose of prolong_add_kernel.
+template <typename T>
+__global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ tf,
+                                const uint8_t* __restrict__ bc_f, int fx, int fy, int fz,
+                                T* __restrict__ rc, int cx, int cy, int cz,
+                                const uint8_t* __restrict__ bc_c) {
   const int64_t Nc = (int64_t)cx * cy * cz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % cx), J = (int)((q / cx) % cy), K = (int)(q / ((int64_t)cx * cy));
-    double acc[3] = {0., 0., 0.};
+    T acc[3] = {T(0), T(0), T(0)};
     for (int oz = -1; oz <= 1; oz++) {
       const int k = 2 * K + oz;
       if (k < 0 || k >= fz) continue;
-      const double wz = oz ? 0.5 : 1.0;
+      const T wz = oz ? T(0.5) : T(1);
       for (int oy = -1; oy <= 1; oy++) {
         const int j = 2 * J + oy;
         if (j < 0 || j >= fy) continue;
-        const double wy = oy ? 0.5 : 1.0;
+        const T wy = oy ? T(0.5) : T(1);
         for (int ox = -1; ox <= 1; ox++) {
           const int i = 2 * I + ox;
           if (i < 0 || i >= fx) continue;
-          const double w = wz * wy * (ox ? 0.5 : 1.0);
+          const T w = wz * wy * (ox ? T(0.5) : T(1));
           const int64_t n = node_index(i, j, k, fx, fy);
-          const unsigned bf = bc_f[n];
+          const unsigned bf_bits = bc_f[n];
           for (int c = 0; c < 3; c++)
-            if (!((bf >> c) & 1u)) acc[c] += w * rf[3 * n + c];
+            if (!((bf_bits >> c) & 1u)) acc[c] += w * (bf[3 * n + c] - tf[3 * n + c]);
         }
       }
     }
     const unsigned b = bc_c[q];
-    for (int c = 0; c < 3; c++) rc[3 * q + c] = ((b >> c) & 1u) ? 0. : acc[c];
+    for (int c = 0; c < 3; c++) rc[3 * q + c] = ((b >> c) & 1u) ? T(0) : acc[c];
   }
 }
 
-// x_f += trilinear interpolation of e_c (fine Dirichlet dofs untouched: they stay 0).
-__global__ void prolong_add_kernel(const double* __restrict__ ec, int cx, int cy,
-                                   double* __restrict__ xf, int fx, int fy, int fz,
+// x_f += trilinear interpolation of e_c; fine Dirichlet dofs untouched.
+template <typename T>
+__global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy,
+                                   T* __restrict__ xf, int fx, int fy, int fz,
                                    const uint8_t* __restrict__ bc_f) {
   const int64_t Nf = (int64_t)fx * fy * fz;
   GRID_STRIDE(q, Nf) {
     const int i = (int)(q % fx), j = (int)((q / fx) % fy), k = (int)(q / ((int64_t)fx * fy));
     const int i0 = i >> 1, j0 = j >> 1, k0 = k >> 1;
     const int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
-    const double wi = (i & 1) ? 0.5 : 1.0, wj = (j & 1) ? 0.5 : 1.0, wk = (k & 1) ? 0.5 : 1.0;
-    double acc[3] = {0., 0., 0.};
+    const T w = ((i & 1) ? T(0.5) : T(1)) * ((j & 1) ? T(0.5) : T(1)) * ((k & 1) ? T(0.5) : T(1));
+    T acc[3] = {T(0), T(0), T(0)};
     for (int dk = 0; dk < nk; dk++)
       for (int dj = 0; dj < nj; dj++)
         for (int di = 0; di < ni; di++) {
           const int64_t n = node_index(i0 + di, j0 + dj, k0 + dk, cx, cy);
-          const double w = wi * wj * wk;
-          for (int c = 0; c < 3; c++) acc[c] += w * ec[3 * n + c];
+          for (int c = 0; c < 3; c++) acc[c] += ec[3 * n + c];
         }
     const unsigned b = bc_f[q];
     for (int c = 0; c < 3; c++)
-      if (!((b >> c) & 1u)) xf[3 * q + c] += acc[c];
+      if (!((b >> c) & 1u)) xf[3 * q + c] += w * acc[c];
   }
 }
 
@@ -122,79 +133,197 @@ __global__ void cell_mean_kernel(const float* __restrict__ ef, int fcx, int fcy,
 }
 
 // r = dinv * (b - t), or dinv * b when t is null (x = 0); d = r / theta.
-__global__ void cheb_init_kernel(const double* __restrict__ b, const double* __restrict__ t,
-                                 const double* __restrict__ dinv, double* __restrict__ r,
-                                 double* __restrict__ d, double inv_theta, int64_t n) {
+template <typename T>
+__global__ void cheb_init_kernel(const T* __restrict__ b, const T* __restrict__ t,
+                                 const T* __restrict__ dinv, T* __restrict__ r, T* __restrict__ d,
+                                 const double* __restrict__ coef, int64_t n) {
+  const T inv_theta = T(coef[1]);
   GRID_STRIDE(i, n) {
-    const double ri = dinv[i] * (t ? b[i] - t[i] : b[i]);
+    const T ri = dinv[i] * (t ? b[i] - t[i] : b[i]);
     r[i] = ri;
     d[i] = ri * inv_theta;
   }
 }
 
-// x += d; and unless last: r -= dinv * t (t = A d); d = c1 d + c2 r.
-__global__ void cheb_step_kernel(double* __restrict__ x, double* __restrict__ d,
-                                 double* __restrict__ r, const double* __restrict__ t,
-                                 const double* __restrict__ dinv, double c1, double c2, int last,
-                                 int64_t n) {
+// x += d; and unless last: r -= dinv * t (t = K d); d = c1 d + c2 r, (c1, c2) = cf[0..1].
+template <typename T>
+__global__ void cheb_step_kernel(T* __restrict__ x, T* __restrict__ d, T* __restrict__ r,
+                                 const T* __restrict__ t, const T* __restrict__ dinv,
+                                 const double* __restrict__ cf, int last, int64_t n) {
+  const T c1 = last ? T(0) : T(cf[0]), c2 = last ? T(0) : T(cf[1]);
   GRID_STRIDE(i, n) {
-    const double di = d[i];
+    const T di = d[i];
     x[i] += di;
     if (!last) {
-      const double ri = r[i] - dinv[i] * t[i];
+      const T ri = r[i] - dinv[i] * t[i];
       r[i] = ri;
       d[i] = c1 * di + c2 * ri;
     }
   }
 }
 
-// Deterministic start vector of the power iteration (0 on Dirichlet dofs).
-__global__ void seed_kernel(double* __restrict__ x, const uint8_t* __restrict__ bc, int64_t N) {
+// Deterministic start vector of the power iteration in (-1/2, 1/2), 0 on Dirichlet dofs.
+template <typename T>
+__global__ void seed_kernel(T* __restrict__ x, const uint8_t* __restrict__ bc, int64_t N) {
   GRID_STRIDE(q, N) {
     const unsigned b = bc[q];
     for (int c = 0; c < 3; c++) {
       const uint64_t h = (uint64_t)(3 * q + c) * 0x9E3779B97F4A7C15ull;
-      x[3 * q + c] = ((b >> c) & 1u) ? 0. : (double)((h >> 11) & 0xFFFFF) / 1048576.0 - 0.5;
+      x[3 * q + c] = ((b >> c) & 1u) ? T(0) : T((double)((h >> 11) & 0xFFFFF) / 1048576.0 - 0.5);
     }
   }
 }
 
-// y = dinv * t
-__global__ void scale_kernel(const double* __restrict__ t, const double* __restrict__ dinv,
-                             double* __restrict__ y, int64_t n) {
-  GRID_STRIDE(i, n) y[i] = dinv[i] * t[i];
+// y = dinv * t; block partials of y.y and x.x (FP64) in partial[b], partial[nb + b].
+template <typename T>
+__global__ void __launch_bounds__(kPowThreads)
+    power_dots_kernel(const T* __restrict__ t, const T* __restrict__ dinv, T* __restrict__ y,
+                      const T* __restrict__ x, int64_t n, double* __restrict__ partial) {
+  __shared__ double scratch[32];
+  double yy = 0., xx = 0.;
+  GRID_STRIDE(i, n) {
+    const T yi = dinv[i] * t[i];
+    y[i] = yi;
+    yy += (double)yi * (double)yi;
+    xx += (double)x[i] * (double)x[i];
+  }
+  const double syy = block_sum_dbl(yy, scratch);
+  __syncthreads();
+  const double sxx = block_sum_dbl(xx, scratch);
+  if (threadIdx.x == 0) {
+    partial[blockIdx.x] = syy;
+    partial[gridDim.x + blockIdx.x] = sxx;
+  }
 }
 
-}  // namespace
+// slot[0] = sqrt(y.y / x.x) (the eigenvalue estimate), slot[1] = 1 / |y| (0 if y = 0).
+__global__ void __launch_bounds__(kPowThreads) power_final_kernel(const double* __restrict__ partial,
+                                                                  int nb, double* __restrict__ slot) {
+  __shared__ double scratch[32];
+  double yy = 0., xx = 0.;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+    yy += partial[b];
+    xx += partial[nb + b];
+  }
+  const double syy = block_sum_dbl(yy, scratch);
+  __syncthreads();
+  const double sxx = block_sum_dbl(xx, scratch);
+  if (threadIdx.x == 0) {
+    slot[0] = sxx > 0. ? sqrt(syy / sxx) : 0.;
+    slot[1] = syy > 0. ? 1. / sqrt(syy) : 0.;
+  }
+}
+
+// x = y * slot[1]
+template <typename T>
+__global__ void power_norm_kernel(const T* __restrict__ y, T* __restrict__ x,
+                                  const double* __restrict__ slot, int64_t n) {
+  const T s = T(slot[1]);
+  GRID_STRIDE(i, n) x[i] = y[i] * s;
+}
+
+// Chebyshev coefficients on [lo lmax, lmax], lmax = safety x estimate (Saad,
+// Iterative Methods for Sparse Linear Systems, 2nd ed., Alg. 12.1):
+// theta = (lmax + lmin) / 2, delta = (lmax - lmin) / 2, sigma = theta / delta,
+// rho_0 = 1 / sigma, rho_{k+1} = 1 / (2 sigma - rho_k), c1 = rho_{k+1} rho_k,
+// c2 = 2 rho_{k+1} / delta.  An estimate that is not positive leaves lmax = 0.
+__global__ void cheb_coef_kernel(double* __restrict__ coef, int deg, double lo, double safety) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const double est = coef[kCoefPerLevel - 2];
+  const double lmax = est > 0. ? safety * est : 0.;
+  coef[0] = lmax;
+  const double lmin = lo * lmax, theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
+  if (!(lmax > 0.)) {
+    for (int k = 1; k < kCoefPerLevel - 2; k++) coef[k] = 0.;
+    return;
+  }
+  const double sigma = theta / delta;
+  double rho = 1. / sigma;
+  coef[1] = 1. / theta;
+  for (int k = 0; k + 1 < deg; k++) {
+    const double rho_new = 1. / (2. * sigma - rho);
+    coef[2 + 2 * k] = rho_new * rho;
+    coef[3 + 2 * k] = 2. * rho_new / delta;
+    rho = rho_new;
+  }
+}
 
 // ---------------------------------------------------------------------------------
-// The level's view as a U operator: apply, the element arguments for its diagonal.
-struct LevelView {
+// A level seen as a U operator in precision T.
+template <typename T> struct LevelT {
   int nx, ny, nz;
   double hx, hy, hz;
   const TilePlan* plan;
-  double* seam;
-  const double* v;
+  T* seam;
+  const T* v;
   const uint8_t* bc;
   const uint8_t* elayer;
   const float* cellE;
-  const ETab* tab;
-  const double* dinv;
+  const T* dinv;
   const uint32_t* cflag;  // fine level under NOCOMPRESSION: the Jacobian's bits
+  T *x, *b, *r, *d, *t;
+  double* coef;
+  int64_t n3;
 };
 
-static LevelView view(vfgpu_ctx* c, int l, const double* dinv0) {
-  if (l == 0)
-    return {c->nx, c->ny, c->nz, c->hx, c->hy, c->hz, &c->plan64, c->seam64,
-            c->f[VFGPU_FIELD_V], c->bcU_bits, c->d_elayer, c->d_cellE, c->d_tab, dinv0,
-            c->unilateral ? c->d_cflag : nullptr};
-  const auto& L = c->mg[l];
-  return {L.nx, L.ny, L.nz, L.hx, L.hy, L.hz, &L.plan, L.seam, L.v, L.bc, L.elayer, L.cellE,
-          L.tab, L.dinv, nullptr};
+template <typename T> const TilePlan* fine_plan(vfgpu_ctx* c);
+template <> const TilePlan* fine_plan<double>(vfgpu_ctx* c) { return &c->plan64; }
+template <> const TilePlan* fine_plan<float>(vfgpu_ctx* c) { return &c->plan32; }
+template <typename T> T* fine_seam(vfgpu_ctx* c);
+template <> double* fine_seam<double>(vfgpu_ctx* c) { return c->seam64; }
+template <> float* fine_seam<float>(vfgpu_ctx* c) { return c->seam32; }
+template <typename T> const T* fine_v(vfgpu_ctx* c);
+template <> const double* fine_v<double>(vfgpu_ctx* c) { return c->f[VFGPU_FIELD_V]; }
+template <> const float* fine_v<float>(vfgpu_ctx* c) { return c->V32; }
+
+template <typename T> LevelT<T> view(vfgpu_ctx* c, int l) {
+  auto& L = c->mg[l];
+  LevelT<T> V;
+  V.x = (T*)L.x;
+  V.b = (T*)L.b;
+  V.r = (T*)L.r;
+  V.d = (T*)L.d;
+  V.t = (T*)L.t;
+  V.coef = L.coef;
+  if (l == 0) {
+    V.nx = c->nx;
+    V.ny = c->ny;
+    V.nz = c->nz;
+    V.hx = c->hx;
+    V.hy = c->hy;
+    V.hz = c->hz;
+    V.plan = fine_plan<T>(c);
+    V.seam = fine_seam<T>(c);
+    V.v = fine_v<T>(c);
+    V.bc = c->bcU_bits;
+    V.elayer = c->d_elayer;
+    V.cellE = c->d_cellE;
+    V.dinv = (const T*)c->mg_dinv0;
+    V.cflag = c->unilateral ? c->d_cflag : nullptr;
+    V.n3 = 3 * c->N;
+  } else {
+    V.nx = L.nx;
+    V.ny = L.ny;
+    V.nz = L.nz;
+    V.hx = L.hx;
+    V.hy = L.hy;
+    V.hz = L.hz;
+    V.plan = &L.plan;
+    V.seam = (T*)L.seam;
+    V.v = (const T*)L.v;
+    V.bc = L.bc;
+    V.elayer = L.elayer;
+    V.cellE = L.cellE;
+    V.dinv = (const T*)L.dinv;
+    V.cflag = nullptr;
+    V.n3 = 3 * L.N;
+  }
+  return V;
 }
 
-static cudaError_t level_apply(vfgpu_ctx* c, const LevelView& V, const double* x, double* y) {
-  UApplyArgs<double> A{};
+template <typename T>
+cudaError_t level_apply(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
+  UApplyArgs<T> A{};
   A.x = x;
   A.v = V.v;
   A.y = y;
@@ -206,48 +335,119 @@ static cudaError_t level_apply(vfgpu_ctx* c, const LevelView& V, const double* x
   A.nx = V.nx;
   A.ny = V.ny;
   A.nz = V.nz;
-  A.ihx = 1.0 / V.hx;
-  A.ihy = 1.0 / V.hy;
-  A.ihz = 1.0 / V.hz;
-  A.vol = V.hx * V.hy * V.hz;
-  A.eta = c->vf.eta;
+  A.ihx = T(1.0 / V.hx);
+  A.ihy = T(1.0 / V.hy);
+  A.ihz = T(1.0 / V.hz);
+  A.vol = T(V.hx * V.hy * V.hz);
+  A.eta = T(c->vf.eta);
   A.P = c->d_params;
   A.cflag = V.cflag;
-  return launch_u_apply<double>(A, *V.plan, c->layers, c->stream);
+  return launch_u_apply<T>(A, *V.plan, c->layers, c->stream);
 }
 
-static int64_t level_n3(vfgpu_ctx* c, int l) { return 3 * (l == 0 ? c->N : c->mg[l].N); }
-
-void free_mg(vfgpu_ctx* c) {
-  for (auto& L : c->mg) {
-    void* bufs[] = {L.seam, L.v, L.dinv, L.x, L.b, L.r, L.d, L.t, L.bc, L.elayer, L.cellE, L.tab};
-    for (void* p : bufs) cudaFree(p);
+// Chebyshev iteration on D^-1 K x = D^-1 b with the level's coefficients; x updated in
+// place (zero_start: x = 0 on entry and no initial residual apply).
+template <typename T>
+cudaError_t chebyshev(vfgpu_ctx* c, const LevelT<T>& V, const T* b, T* x, int deg, bool zero_start) {
+  const int64_t n3 = V.n3;
+  cudaError_t e = zero_start ? cudaMemsetAsync(x, 0, n3 * sizeof(T), c->stream)
+                             : level_apply<T>(c, V, x, V.t);
+  if (e == cudaSuccess) {
+    cheb_init_kernel<T><<<blocks_for(n3), 256, 0, c->stream>>>(b, zero_start ? nullptr : V.t, V.dinv,
+                                                              V.r, V.d, V.coef, n3);
+    e = cudaGetLastError();
   }
-  c->mg.clear();
-  cudaFree(c->mg_z);
-  c->mg_z = nullptr;
+  for (int k = 0; k < deg && e == cudaSuccess; k++) {
+    const bool last = k == deg - 1;
+    if (!last) e = level_apply<T>(c, V, V.d, V.t);
+    if (e == cudaSuccess) {
+      cheb_step_kernel<T><<<blocks_for(n3), 256, 0, c->stream>>>(x, V.d, V.r, V.t, V.dinv,
+                                                                V.coef + 2 + 2 * k, last ? 1 : 0, n3);
+      e = cudaGetLastError();
+    }
+  }
+  return e;
 }
 
-// Allocates the hierarchy (once per ctx).
-static int mg_build(vfgpu_ctx* c) {
-  if (!c->mg.empty()) return VFGPU_OK;
-  c->mg.emplace_back();  // level 0: fine work vectors
+// z = V-cycle(b) from level l down.
+template <typename T> cudaError_t vcycle(vfgpu_ctx* c, int l, const T* b, T* z) {
+  const LevelT<T> V = view<T>(c, l);
+  if (l == (int)c->mg.size() - 1) return chebyshev<T>(c, V, b, z, kCoarseDeg, true);
+  const LevelT<T> C = view<T>(c, l + 1);
+  cudaError_t e = chebyshev<T>(c, V, b, z, kSmoothDeg, true);
+  if (e == cudaSuccess) e = level_apply<T>(c, V, z, V.t);
+  if (e == cudaSuccess) {
+    restrict_kernel<T><<<blocks_for(C.n3 / 3), 256, 0, c->stream>>>(b, V.t, V.bc, V.nx, V.ny, V.nz,
+                                                                    C.b, C.nx, C.ny, C.nz, C.bc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = vcycle<T>(c, l + 1, C.b, C.x);
+  if (e == cudaSuccess) {
+    prolong_add_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(C.x, C.nx, C.ny, z, V.nx,
+                                                                      V.ny, V.nz, V.bc);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = chebyshev<T>(c, V, b, z, kSmoothDeg, false);
+  return e;
+}
+
+template <typename T> void* dalloc(int64_t n, cudaError_t& e) {
+  void* p = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&p, std::max<int64_t>(1, n) * sizeof(T));
+  return p;
+}
+
+// Allocates the hierarchy in precision T (rebuilt when the precision changes).
+template <typename T> int mg_build(vfgpu_ctx* c) {
+  if (!c->mg.empty() && c->mg_bytes == (int)sizeof(T)) return VFGPU_OK;
+  free_mg(c);
+  int nlev = 1;
+  {
+    int nx = c->nx, ny = c->ny, nz = c->nz;
+    while ((nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 && (nx - 1) / 2 + 1 >= 5 &&
+           (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
+      nx = (nx - 1) / 2 + 1;
+      ny = (ny - 1) / 2 + 1;
+      nz = (nz - 1) / 2 + 1;
+      nlev++;
+    }
+  }
+  if (nlev < 2)
+    return fail(VFGPU_ERR_INVALID,
+                "multigrid needs an even cell count on every axis and >= 9 nodes per axis");
   cudaError_t e = cudaSuccess;
-  auto& L0 = c->mg[0];
-  const size_t n3 = 3 * (size_t)c->N * sizeof(double);
-  for (double** p : {&L0.x, &L0.r, &L0.d, &L0.t, &c->mg_z})
-    if (e == cudaSuccess) e = cudaMalloc((void**)p, n3);
+  c->mg_coef = (double*)dalloc<double>((int64_t)kCoefPerLevel * nlev, e);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->mg_coef, 0, sizeof(double) * kCoefPerLevel * nlev, c->stream);
+  const bool f32 = sizeof(T) == 4;
+  c->mg.resize(nlev);
+  {
+    auto& L0 = c->mg[0];
+    const int64_t n3 = 3 * c->N;
+    L0.nx = c->nx;
+    L0.ny = c->ny;
+    L0.nz = c->nz;
+    L0.N = c->N;
+    L0.NC = c->NC;
+    L0.x = dalloc<T>(n3, e);
+    L0.r = dalloc<T>(n3, e);
+    L0.d = dalloc<T>(n3, e);
+    L0.t = dalloc<T>(n3, e);
+    if (f32) {
+      L0.b = dalloc<T>(n3, e);
+      c->mg_z = (double*)dalloc<double>(n3, e);
+    }
+    L0.coef = c->mg_coef;
+  }
   int nx = c->nx, ny = c->ny, nz = c->nz;
   double hx = c->hx, hy = c->hy, hz = c->hz;
-  while (e == cudaSuccess && (nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 &&
-         (nx - 1) / 2 + 1 >= 5 && (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
+  for (int l = 1; l < nlev && e == cudaSuccess; l++) {
     nx = (nx - 1) / 2 + 1;
     ny = (ny - 1) / 2 + 1;
     nz = (nz - 1) / 2 + 1;
     hx *= 2;
     hy *= 2;
     hz *= 2;
-    vfgpu_ctx::MGLevel L;
+    auto& L = c->mg[l];
     L.nx = nx;
     L.ny = ny;
     L.nz = nz;
@@ -256,62 +456,70 @@ static int mg_build(vfgpu_ctx* c) {
     L.hx = hx;
     L.hy = hy;
     L.hz = hz;
-    L.plan = u_plan(nx, ny, nz, 8, c->nsm);
-    const size_t b3 = 3 * (size_t)L.N * sizeof(double);
-    if (e == cudaSuccess)
-      e = cudaMalloc((void**)&L.seam, std::max<size_t>(1, L.plan.seamX + L.plan.seamY) * sizeof(double));
-    for (double** p : {&L.dinv, &L.x, &L.b, &L.r, &L.d, &L.t})
-      if (e == cudaSuccess) e = cudaMalloc((void**)p, b3);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&L.v, L.N * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&L.bc, L.N);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&L.elayer, nz - 1);
-    if (e == cudaSuccess && c->d_cellE) e = cudaMalloc((void**)&L.cellE, L.NC * sizeof(float));
-    if (e == cudaSuccess) e = cudaMalloc((void**)&L.tab, sizeof(ETab));
+    L.plan = u_plan(nx, ny, nz, (int)sizeof(T), c->nsm);
+    L.seam = dalloc<T>((int64_t)(L.plan.seamX + L.plan.seamY), e);
+    for (void** p : {&L.x, &L.b, &L.r, &L.d, &L.t, &L.dinv}) *p = dalloc<T>(3 * L.N, e);
+    L.v64 = (double*)dalloc<double>(L.N, e);
+    L.v = f32 ? dalloc<float>(L.N, e) : (void*)L.v64;
+    L.bc = (uint8_t*)dalloc<uint8_t>(L.N, e);
+    L.elayer = (uint8_t*)dalloc<uint8_t>(nz - 1, e);
+    if (c->d_cellE) L.cellE = (float*)dalloc<float>(L.NC, e);
+    L.tab = (ETab*)dalloc<ETab>(1, e);
+    L.coef = c->mg_coef + (int64_t)kCoefPerLevel * l;
     if (e == cudaSuccess) {
       ETab t;
       etab_host(hx, hy, hz, &t);
       e = cudaMemcpyAsync(L.tab, &t, sizeof t, cudaMemcpyHostToDevice, c->stream);
       if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     }
-    c->mg.push_back(L);
   }
-  if (e != cudaSuccess || c->mg.size() < 2) {
+  c->mg_bytes = (int)sizeof(T);
+  c->mg_ready = false;
+  if (e != cudaSuccess) {
     free_mg(c);
-    if (e != cudaSuccess) return cuda_fail(e, "multigrid hierarchy");
-    return fail(VFGPU_ERR_INVALID,
-                "multigrid needs an even cell count on every axis and >= 9 nodes per axis");
+    return cuda_fail(e, "multigrid hierarchy");
   }
   return VFGPU_OK;
 }
 
-// Per solve: coarse fields from the fine ones, diagonals, lmax per level.
-static int mg_setup(vfgpu_ctx* c, const double* dinv0) {
+// Per operator: coarse fields from the fine ones, diagonals, eigenvalue bounds and
+// Chebyshev coefficients.
+template <typename T> int mg_setup(vfgpu_ctx* c) {
   cudaError_t e = cudaSuccess;
-  // coarse modulus buffers follow the ctx (set_cell_modulus may have added one)
-  for (size_t l = 1; l < c->mg.size() && e == cudaSuccess; l++) {
+  const bool f32 = sizeof(T) == 4;
+  const int nlev = (int)c->mg.size();
+  for (int l = 1; l < nlev && e == cudaSuccess; l++) {  // set_cell_modulus after the build
     auto& L = c->mg[l];
     if (c->d_cellE && !L.cellE) e = cudaMalloc((void**)&L.cellE, L.NC * sizeof(float));
   }
   std::vector<uint8_t> el(std::max(1, c->nz - 1));
   if (e == cudaSuccess) e = cudaMemcpyAsync(el.data(), c->d_elayer, el.size(), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  for (size_t l = 1; l < c->mg.size() && e == cudaSuccess; l++) {
+  for (int l = 1; l < nlev && e == cudaSuccess; l++) {
     auto& L = c->mg[l];
-    const LevelView F = view(c, (int)l - 1, dinv0);
-    inject_kernel<<<blocks_for(L.N), 256, 0, c->stream>>>(F.v, F.bc, F.nx, F.ny, L.v, L.bc, L.nx,
-                                                          L.ny, L.nz);
+    auto& F = c->mg[l - 1];
+    const double* vf = l == 1 ? c->f[VFGPU_FIELD_V] : F.v64;
+    const uint8_t* bcf = l == 1 ? c->bcU_bits : F.bc;
+    const float* cellEf = l == 1 ? c->d_cellE : F.cellE;
+    const int fx = l == 1 ? c->nx : F.nx, fy = l == 1 ? c->ny : F.ny;
+    inject_kernel<<<blocks_for(L.N), 256, 0, c->stream>>>(vf, bcf, fx, fy, L.v64, L.bc, L.nx, L.ny,
+                                                          L.nz);
     e = cudaGetLastError();
+    if (e == cudaSuccess && f32) e = convert_f64_f32(L.v64, (float*)L.v, L.N, c->stream);
     std::vector<uint8_t> lc(L.nz - 1);
-    for (int k = 0; k < L.nz - 1; k++) lc[k] = el[(size_t)k << l];  // lower child layer
+    for (int k = 0; k < L.nz - 1; k++) lc[k] = el[(size_t)k << l];  // lowest child layer
     if (e == cudaSuccess) e = cudaMemcpyAsync(L.elayer, lc.data(), lc.size(), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // lc leaves scope
     if (e == cudaSuccess && c->d_cellE) {
-      cell_mean_kernel<<<blocks_for(L.NC), 256, 0, c->stream>>>(F.cellE, F.nx - 1, F.ny - 1, L.cellE,
+      cell_mean_kernel<<<blocks_for(L.NC), 256, 0, c->stream>>>(cellEf, fx - 1, fy - 1, L.cellE,
                                                                L.nx - 1, L.ny - 1, L.nz - 1);
       e = cudaGetLastError();
     }
-    // diagonal of the level operator (t as scratch)
     if (e == cudaSuccess) {
+      // FP64 diagonal; FP32 hierarchy: computed in the fine level's FP32 work vectors,
+      // which hold 12 N_0 >= 24 N_l bytes each
+      double* diag = f32 ? (double*)c->mg[0].r : (double*)L.t;
+      double* dinv64 = f32 ? (double*)c->mg[0].d : (double*)L.dinv;
       ElemArgs E{};
       E.tab = L.tab;
       E.nx = L.nx;
@@ -321,142 +529,93 @@ static int mg_setup(vfgpu_ctx* c, const double* dinv0) {
       E.cellE = c->d_cellE ? L.cellE : nullptr;
       E.L = c->layers;
       E.eta = c->vf.eta;
-      e = launch_u_diag(E, L.v, L.bc, L.t, c->stream);
-      if (e == cudaSuccess) e = dev_inv(L.t, L.dinv, nullptr, 3 * L.N, c->stream);
+      e = launch_u_diag(E, L.v64, L.bc, diag, c->stream);
+      if (e == cudaSuccess) e = dev_inv(diag, dinv64, f32 ? (float*)L.dinv : nullptr, 3 * L.N, c->stream);
     }
   }
   if (e != cudaSuccess) return cuda_fail(e, "multigrid set-up");
-  // largest eigenvalue of D^-1 K per level by power iteration
-  for (size_t l = 0; l < c->mg.size(); l++) {
-    const LevelView V = view(c, (int)l, dinv0);
-    const int64_t n3 = level_n3(c, (int)l);
-    double* x = c->mg[l].x;
-    double* t = c->mg[l].t;
-    double* y = c->mg[l].d;
-    seed_kernel<<<blocks_for(n3 / 3), 256, 0, c->stream>>>(x, V.bc, n3 / 3);
+  // largest eigenvalue of D^-1 K per level by power iteration, then the coefficients
+  for (int l = 0; l < nlev && e == cudaSuccess; l++) {
+    const LevelT<T> V = view<T>(c, l);
+    double* slot = V.coef + kCoefPerLevel - 2;
+    seed_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(V.x, V.bc, V.n3 / 3);
     e = cudaGetLastError();
-    double lam = 0.;
     for (int it = 0; it < kPowerIts && e == cudaSuccess; it++) {
-      e = level_apply(c, V, x, t);
+      e = level_apply<T>(c, V, V.x, V.t);
       if (e == cudaSuccess) {
-        scale_kernel<<<blocks_for(n3), 256, 0, c->stream>>>(t, V.dinv, y, n3);
+        power_dots_kernel<T><<<kPowBlocks, kPowThreads, 0, c->stream>>>(V.t, V.dinv, V.d, V.x, V.n3,
+                                                                       c->d_red);
+        power_final_kernel<<<1, kPowThreads, 0, c->stream>>>(c->d_red, kPowBlocks, slot);
+        power_norm_kernel<T><<<blocks_for(V.n3), 256, 0, c->stream>>>(V.d, V.x, slot, V.n3);
         e = cudaGetLastError();
       }
-      const double* pa[2] = {y, x};
-      const double* pb[2] = {y, x};
-      if (e == cudaSuccess) e = dev_dots(pa, pb, 2, n3, c->d_red, c->d_out, c->stream);
-      double h[2] = {0., 0.};
-      if (e == cudaSuccess) e = cudaMemcpyAsync(h, c->d_out, sizeof h, cudaMemcpyDeviceToHost, c->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-      if (e != cudaSuccess || !(h[0] > 0.) || !(h[1] > 0.)) break;
-      lam = sqrt(h[0] / h[1]);
-      // x = y / |y|
-      e = cudaMemsetAsync(x, 0, n3 * sizeof(double), c->stream);
-      if (e == cudaSuccess) e = dev_axpy(x, 1.0 / sqrt(h[0]), y, n3, c->stream);
-    }
-    if (e != cudaSuccess) return cuda_fail(e, "multigrid eigenvalue estimate");
-    if (!(lam > 0.)) return fail(VFGPU_ERR_STATE, "multigrid: no positive eigenvalue estimate of a level operator");
-    c->mg[l].lmax = 1.1 * lam;
-  }
-  return VFGPU_OK;
-}
-
-// Chebyshev iteration on D^-1 K x = D^-1 b of degree deg on [lo lmax, lmax]; x is
-// updated in place (zero_start: x = 0 on entry, so no initial residual apply).
-static cudaError_t chebyshev(vfgpu_ctx* c, const LevelView& V, int l, const double* b, double* x,
-                             int deg, double lo, bool zero_start) {
-  auto& L = c->mg[l];
-  const int64_t n3 = level_n3(c, l);
-  const double lmax = L.lmax, lmin = lo * lmax;
-  const double theta = 0.5 * (lmax + lmin), delta = 0.5 * (lmax - lmin);
-  const double sigma = theta / delta;
-  double rho = 1.0 / sigma;
-  cudaError_t e = cudaSuccess;
-  if (zero_start) {
-    e = cudaMemsetAsync(x, 0, n3 * sizeof(double), c->stream);
-  } else {
-    e = level_apply(c, V, x, L.t);
-  }
-  if (e == cudaSuccess) {
-    cheb_init_kernel<<<blocks_for(n3), 256, 0, c->stream>>>(b, zero_start ? nullptr : L.t, V.dinv,
-                                                           L.r, L.d, 1.0 / theta, n3);
-    e = cudaGetLastError();
-  }
-  for (int k = 0; k < deg && e == cudaSuccess; k++) {
-    const bool last = k == deg - 1;
-    double c1 = 0., c2 = 0.;
-    if (!last) {
-      e = level_apply(c, V, L.d, L.t);
-      const double rho_new = 1.0 / (2.0 * sigma - rho);
-      c1 = rho_new * rho;
-      c2 = 2.0 * rho_new / delta;
-      rho = rho_new;
     }
     if (e == cudaSuccess) {
-      cheb_step_kernel<<<blocks_for(n3), 256, 0, c->stream>>>(x, L.d, L.r, L.t, V.dinv, c1, c2,
-                                                             last ? 1 : 0, n3);
+      const bool last = l == nlev - 1;
+      cheb_coef_kernel<<<1, 32, 0, c->stream>>>(V.coef, last ? kCoarseDeg : kSmoothDeg,
+                                                last ? kCoarseLo : kSmoothLo, kLmaxSafety);
       e = cudaGetLastError();
     }
   }
-  return e;
+  std::vector<double> coef((size_t)kCoefPerLevel * nlev);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(coef.data(), c->mg_coef, coef.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "multigrid eigenvalue estimate");
+  for (int l = 0; l < nlev; l++)
+    if (!(coef[(size_t)kCoefPerLevel * l] > 0.) || !std::isfinite(coef[(size_t)kCoefPerLevel * l]))
+      return fail(VFGPU_ERR_STATE, "multigrid: no positive eigenvalue estimate on level %d", l);
+  c->mg_ready = true;
+  return VFGPU_OK;
 }
 
-// z = V-cycle(b) at level l (z and b are the level's own vectors, or the fine ones).
-static cudaError_t vcycle(vfgpu_ctx* c, int l, const double* dinv0, const double* b, double* z) {
-  const LevelView V = view(c, l, dinv0);
-  const int last = (int)c->mg.size() - 1;
-  if (l == last) return chebyshev(c, V, l, b, z, kCoarseDeg, kCoarseLo, true);
-  cudaError_t e = chebyshev(c, V, l, b, z, kSmoothDeg, kSmoothLo, true);
-  auto& L = c->mg[l];
-  auto& C = c->mg[l + 1];
-  const int64_t n3 = level_n3(c, l);
-  // residual b - K z into L.r (t = K z)
-  if (e == cudaSuccess) e = level_apply(c, V, z, L.t);
-  if (e == cudaSuccess) e = dev_axpby(L.r, b, -1.0, L.t, n3, c->stream);
-  if (e == cudaSuccess) {
-    restrict_kernel<<<blocks_for(C.N), 256, 0, c->stream>>>(L.r, V.bc, V.nx, V.ny, V.nz, C.b, C.nx,
-                                                           C.ny, C.nz, C.bc);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) e = vcycle(c, l + 1, dinv0, C.b, C.x);
-  if (e == cudaSuccess) {
-    prolong_add_kernel<<<blocks_for(n3 / 3), 256, 0, c->stream>>>(C.x, C.nx, C.ny, z, V.nx, V.ny,
-                                                                 V.nz, V.bc);
-    e = cudaGetLastError();
-  }
-  if (e == cudaSuccess) e = chebyshev(c, V, l, b, z, kSmoothDeg, kSmoothLo, false);
-  return e;
+// One preconditioner application z = M^-1 r (FP64 in and out), as a graph replay.
+template <typename T> cudaError_t precondition(vfgpu_ctx* c, const double* r, double* z);
+template <> cudaError_t precondition<double>(vfgpu_ctx* c, const double* r, double* z) {
+  auto body = [c, r, z]() { return vcycle<double>(c, 0, r, z); };
+  cudaGraphExec_t g = c->use_graphs ? ctx_graph(c, kGraphMG64, 0, body) : nullptr;
+  return g ? cudaGraphLaunch(g, c->stream) : body();
+}
+template <> cudaError_t precondition<float>(vfgpu_ctx* c, const double* r, double* z) {
+  auto body = [c, r, z]() {
+    const LevelT<float> V = view<float>(c, 0);
+    cudaError_t e = convert_f64_f32(r, V.b, V.n3, c->stream);
+    if (e == cudaSuccess) e = vcycle<float>(c, 0, V.b, V.x);
+    if (e == cudaSuccess) e = convert_f32_f64(V.x, z, V.n3, c->stream);
+    return e;
+  };
+  cudaGraphExec_t g = c->use_graphs ? ctx_graph(c, kGraphMG32, 0, body) : nullptr;
+  return g ? cudaGraphLaunch(g, c->stream) : body();
 }
 
-// PCG with the V-cycle as preconditioner.  Stopping test of the Jacobi-preconditioned
-// solve it replaces (KSPCG's preconditioned norm with B = D^-1): ||D^-1 r|| <=
-// max(rtol ||D^-1 b||, atol), diverged on ||D^-1 r|| >= dtol ||D^-1 b||, NaN, an
-// indefinite p.Kp or maxit, so that both preconditioners stop at the same residual.
-// Scalars are read back on the host once per iteration.
-int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double* w,
-             const double* dinv0, double rtol, double atol, double dtol, int maxit, int* its,
-             int* reason, int* levels) {
-  int rc = mg_build(c);
+template <typename T>
+int mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double* w,
+         const double* dinv0, bool reuse, double rtol, double atol, double dtol, int maxit,
+         int* its, int* reason, int* levels) {
+  int rc = mg_build<T>(c);
   if (rc) return rc;
-  rc = mg_setup(c, dinv0);
-  if (rc) return rc;
+  if (!reuse || !c->mg_ready) {
+    rc = mg_setup<T>(c);
+    if (rc) return rc;
+  }
   *levels = (int)c->mg.size();
   const int64_t n3 = 3 * c->N;
-  double* z = c->mg_z;
+  // the preconditioned residual: the V-cycle's own output vector in FP64
+  double* z = sizeof(T) == 8 ? (double*)c->mg[0].x : c->mg_z;
   cudaError_t e = cudaMemsetAsync(x, 0, n3 * sizeof(double), c->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(r, b, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-  // out[0] = a0.b0, out[1] = a1.b1 (a1 null: skipped), out[2] = ||D^-1 r||^2
+  // h[0] = r.z, h[2] = ||D^-1 r||^2
   double h[3] = {0., 0., 0.};
-  auto scalars = [&](const double* a0, const double* b0, const double* a1, const double* b1) {
-    const double* pa[2] = {a0, a1};
-    const double* pb[2] = {b0, b1};
-    if (e == cudaSuccess) e = dev_dots(pa, pb, a1 ? 2 : 1, n3, c->d_red, c->d_out, c->stream);
+  auto scalars = [&]() {
+    const double* pa[1] = {r};
+    const double* pb[1] = {z};
+    if (e == cudaSuccess) e = dev_dots(pa, pb, 1, n3, c->d_red, c->d_out, c->stream);
     if (e == cudaSuccess) e = dev_znorm2(r, dinv0, n3, c->d_red, c->d_out + 2, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, c->d_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   };
-  if (e == cudaSuccess) e = vcycle(c, 0, dinv0, r, z);
-  scalars(r, z, nullptr, nullptr);
+  if (e == cudaSuccess) e = precondition<T>(c, r, z);
+  scalars();
   if (e != cudaSuccess) return cuda_fail(e, "multigrid PCG");
   double rz = h[0];
   const double rnorm0 = sqrt(h[2]), ttol = std::max(rtol * rnorm0, atol);
@@ -466,8 +625,22 @@ int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, dou
   else if (rnorm0 <= ttol) *reason = rnorm0 <= atol ? CG_CONVERGED_ATOL : CG_CONVERGED_RTOL;
   else if (!(rz > 0.)) *reason = rz == 0. ? CG_CONVERGED_ATOL : CG_DIVERGED_INDEFINITE;
   if (!*reason) e = cudaMemcpyAsync(p, z, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+  LevelT<double> outer{};  // the FP64 Jacobian whatever the V-cycle's precision
+  outer.nx = c->nx;
+  outer.ny = c->ny;
+  outer.nz = c->nz;
+  outer.hx = c->hx;
+  outer.hy = c->hy;
+  outer.hz = c->hz;
+  outer.plan = &c->plan64;
+  outer.seam = c->seam64;
+  outer.v = c->f[VFGPU_FIELD_V];
+  outer.bc = c->bcU_bits;
+  outer.elayer = c->d_elayer;
+  outer.cellE = c->d_cellE;
+  outer.cflag = c->unilateral ? c->d_cflag : nullptr;
   while (!*reason && e == cudaSuccess) {
-    e = level_apply(c, view(c, 0, dinv0), p, w);
+    e = level_apply<double>(c, outer, p, w);
     const double* pa[1] = {p};
     const double* pb[1] = {w};
     if (e == cudaSuccess) e = dev_dots(pa, pb, 1, n3, c->d_red, c->d_out, c->stream);
@@ -482,8 +655,8 @@ int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, dou
     const double alpha = rz / pw;
     e = dev_axpy(x, alpha, p, n3, c->stream);
     if (e == cudaSuccess) e = dev_axpy(r, -alpha, w, n3, c->stream);
-    if (e == cudaSuccess) e = vcycle(c, 0, dinv0, r, z);
-    scalars(r, z, nullptr, nullptr);
+    if (e == cudaSuccess) e = precondition<T>(c, r, z);
+    scalars();
     if (e != cudaSuccess) break;
     *its += 1;
     const double dp = sqrt(h[2]);
@@ -500,6 +673,42 @@ int run_mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, dou
   }
   if (e != cudaSuccess) return cuda_fail(e, "multigrid PCG");
   return VFGPU_OK;
+}
+
+}  // namespace
+
+void free_mg(vfgpu_ctx* c) {
+  for (size_t k = 0; k < c->graphs.size();) {  // the V-cycle graphs hold the old pointers
+    auto& g = c->graphs[k];
+    if (g.kind == kGraphMG64 || g.kind == kGraphMG32) {
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+      c->graphs.erase(c->graphs.begin() + k);
+    } else {
+      k++;
+    }
+  }
+  for (auto& L : c->mg) {
+    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.bc, L.elayer, L.cellE, L.tab};
+    for (void* p : bufs) cudaFree(p);
+    if (L.v != (void*)L.v64) cudaFree(L.v);
+    cudaFree(L.v64);
+  }
+  c->mg.clear();
+  cudaFree(c->mg_coef);
+  cudaFree(c->mg_z);
+  c->mg_coef = nullptr;
+  c->mg_z = nullptr;
+  c->mg_bytes = 0;
+  c->mg_ready = false;
+}
+
+int run_mgcg(vfgpu_ctx* c, bool fp32, const double* b, double* x, double* r, double* p, double* w,
+             const double* dinv0, const float* dinv0_32, bool reuse, double rtol, double atol,
+             double dtol, int maxit, int* its, int* reason, int* levels) {
+  c->mg_dinv0 = fp32 ? (const void*)dinv0_32 : (const void*)dinv0;
+  if (fp32)
+    return mgcg<float>(c, b, x, r, p, w, dinv0, reuse, rtol, atol, dtol, maxit, its, reason, levels);
+  return mgcg<double>(c, b, x, r, p, w, dinv0, reuse, rtol, atol, dtol, maxit, its, reason, levels);
 }
 
 }  // namespace vfgpu

@@ -208,6 +208,11 @@ static cudaGraphExec_t cg_graph(vfgpu_ctx* c, int kind, int batch, Body body) {
   return exec;
 }
 
+cudaGraphExec_t ctx_graph(vfgpu_ctx* c, int kind, int batch,
+                          const std::function<cudaError_t()>& body) {
+  return cg_graph(c, kind, batch, body);
+}
+
 template <typename T, class Apply>
 static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, double rtol,
                   double atol, double dtol, int maxit, const Watch& w, int* its, int* reason,
@@ -311,8 +316,6 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad precision");
   if (o.pc != VFGPU_PC_JACOBI && o.pc != VFGPU_PC_MG)
     return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad preconditioner");
-  if (o.pc == VFGPU_PC_MG && o.precision != VFGPU_FP64)
-    return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: the multigrid preconditioner runs in FP64");
   vfgpu_solve_stats S{};
   cudaSetDevice(c->dev);
   int rc = solve_buffers(c);
@@ -366,8 +369,10 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     }
     if (o.pc == VFGPU_PC_MG) {
       int levels = 0;
-      rc = run_mgcg(c, F, Y, R, P, W, dinv, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, &kits,
-                    &kreason, &levels);
+      // FP64 Krylov vectors with a V-cycle in the solve's precision; the set-up is
+      // kept across Newton steps unless NOCOMPRESSION re-formed the Jacobian
+      rc = run_mgcg(c, mixed, F, Y, R, P, W, dinv, c->p32[4], it > 0 && !nc, o.ksp_rtol, o.ksp_atol,
+                    o.ksp_dtol, o.ksp_maxit, &kits, &kreason, &levels);
       if (rc) return rc;
       S.ksp_its += kits;
       tmo = w.expired();
