@@ -8,7 +8,8 @@ A "step" is one application of the degraded elasticity operator K(v) to a
 is flushed between timed steps.  `e2e` times the same step through the C ABI
 (vfgpu_u_apply) from pinned host memory, copies included.  The AM-step rate
 (StepU + StepV to tolerance, FP64 and mixed, 10 iterations from the penny-crack
-start) is reported beside it with the mixed-vs-FP64 differences of the energies,
+start; U solve with the reference's Jacobi PCG and with the multigrid PCG) is
+reported beside it with the mixed-vs-FP64 differences of the energies,
 the crack opening and V, and so is the serving stream (p50 / p99 latency and
 throughput of independent problems through the library's request loop).
 
@@ -37,6 +38,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_EDGE, L_BOX = 129, 4.0
+# AM-step variants: (key, precision, U preconditioner)
+AM_VARIANTS = (("fp64", "fp64", "jacobi"), ("mixed", "mixed", "jacobi"),
+               ("mg_fp64", "fp64", "mg"), ("mg_mixed", "mixed", "mg"))
 WORKLOAD = "penny crack 129^3 (6.44M U dofs), E=1e10 nu=0.25 Gc=100 AT1 eps=2h eta=1e-8 p=1e6"
 
 
@@ -205,7 +209,7 @@ def run_gpu(args):
                 if last and prec == args.profile_precision:
                     torch.cuda.profiler.start()
                 t0 = time.perf_counter()
-                rc, err, su, sv = ctx.am_step(dict(precision=prec))
+                rc, err, su, sv = ctx.am_step(dict(precision=prec, pc=args.am_pc))
                 barrier()
                 dt = time.perf_counter() - t0
                 if last and prec == args.profile_precision:
@@ -216,7 +220,7 @@ def run_gpu(args):
                                   v_ksp=sv["ksp_its"], v_refine=sv["refine_its"], err=err))
             out[prec] = steps
         if rank == 0:
-            print(json.dumps({"grid": n, "am": out}))
+            print(json.dumps({"grid": n, "pc": args.am_pc, "am": out}))
         ctx.close()
         if dist:
             dist.destroy_process_group()
@@ -245,9 +249,10 @@ def run_gpu(args):
     e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
     (e2e_ms,) = max_over_ranks([e2e_ms], dist, "cuda")
 
-    # AM steps (StepU + StepV to tolerance) from the penny-crack start, FP64 and mixed
+    # AM steps (StepU + StepV to tolerance) from the penny-crack start: FP64 and mixed,
+    # with the reference's Jacobi-preconditioned U solve and with the multigrid one
     am, vfin = {}, {}
-    for prec in ("fp64", "mixed"):
+    for key, prec, pc in AM_VARIANTS:
         ctx.set_field("U", np.zeros(N3))
         ctx.set_field("V", v0)
         ctx.time_step_prepare()
@@ -255,20 +260,23 @@ def run_gpu(args):
         for it in range(args.am_steps):
             barrier()
             t0 = time.perf_counter()
-            rc, err, su, sv = ctx.am_step(dict(precision=prec))
+            rc, err, su, sv = ctx.am_step(dict(precision=prec, pc=pc))
             barrier()
             times.append(time.perf_counter() - t0)
             el, _, pw = ctx.u_energy()
             energies.append((el, pw, ctx.v_energy(), ctx.crack_opening()))
-        am[prec] = dict(s_per_step=float(np.mean(times[1:] if len(times) > 1 else times)),
-                        energies=energies, last_kspU=su["ksp_its"], last_kspV=sv["ksp_its"])
-        vfin[prec] = ctx.get_field("V")
-    rel = max(abs(a - b) / abs(b) for ea, eb in zip(am["mixed"]["energies"], am["fp64"]["energies"])
-              for a, b in zip(ea, eb))
+        am[key] = dict(s_per_step=float(np.mean(times[1:] if len(times) > 1 else times)),
+                       energies=energies, last_kspU=su["ksp_its"], last_kspV=sv["ksp_its"])
+        vfin[key] = ctx.get_field("V")
     names = ("elastic", "pressure_work", "surface", "cov")
-    rel_last = {k: abs(a - b) / abs(b) for k, a, b in
-                zip(names, am["mixed"]["energies"][-1], am["fp64"]["energies"][-1])}
-    v_linf = float(np.abs(vfin["mixed"] - vfin["fp64"]).max())
+
+    def versus_fp64(key):  # against the FP64 Jacobi run (the reference's solve)
+        rel = max(abs(a - b) / abs(b) for ea, eb in zip(am[key]["energies"], am["fp64"]["energies"])
+                  for a, b in zip(ea, eb))
+        rel_last = {k: abs(a - b) / abs(b) for k, a, b in
+                    zip(names, am[key]["energies"][-1], am["fp64"]["energies"][-1])}
+        return rel, rel_last, float(np.abs(vfin[key] - vfin["fp64"]).max())
+    rel, rel_last, v_linf = versus_fp64("mixed")
 
     serving = run_serving(args) if args.serve_problems > 0 else None
 
@@ -319,11 +327,15 @@ def run_gpu(args):
             "per_gauss_point_equiv_tflops": round(cells * 8856 / (ms64 * 1e-3) / 1e12, 2)},
         "mixed": {"value": round(N3 * world / (ms32 * 1e-3) / 1e9, 3), "unit": "GDOF/s",
                   "ms_per_step": round(ms32, 4), "dtype": "f32"},
-        "am_steps_per_s": {"fp64": round(1.0 / am["fp64"]["s_per_step"], 3),
-                           "mixed": round(1.0 / am["mixed"]["s_per_step"], 3),
+        "am_steps_per_s": {**{k: round(1.0 / am[k]["s_per_step"], 3) for k in am},
                            "mixed_vs_fp64_max_rel_energy_diff": rel,
                            "mixed_vs_fp64_rel_at_last_step": rel_last,
                            "mixed_vs_fp64_v_linf": v_linf,
+                           "vs_fp64_jacobi_max_rel_energy_diff": {
+                               k: versus_fp64(k)[0] for k in am if k != "fp64"},
+                           "vs_fp64_jacobi_v_linf": {k: versus_fp64(k)[2] for k in am if k != "fp64"},
+                           "note": "fp64 / mixed: Jacobi-preconditioned U solve (the reference's); "
+                                   "mg_*: multigrid-preconditioned U solve, same stopping test",
                            "steps": args.am_steps,
                            "kspU_last": {k: am[k]["last_kspU"] for k in am}},
         "clocks": clocks,
@@ -365,7 +377,7 @@ def run_serving(args):
     return out
 
 
-def _am_run(ctx, prob, prec, its, altmintol=0.0, reset=True):
+def _am_run(ctx, prob, prec, its, altmintol=0.0, reset=True, pc="jacobi"):
     """AM iterations on `ctx`: exactly `its` (altmintol 0) or until ||V - Vold||_inf <
     altmintol; returns per-iteration records."""
     import torch
@@ -377,7 +389,7 @@ def _am_run(ctx, prob, prec, its, altmintol=0.0, reset=True):
     for it in range(its):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        rc, err, su, sv = ctx.am_step(dict(precision=prec))
+        rc, err, su, sv = ctx.am_step(dict(precision=prec, pc=pc))
         dt = time.perf_counter() - t0
         recs.append(dict(s=dt, err=err, rc=rc, kspU=su["ksp_its"], kspV=sv["ksp_its"]))
         if altmintol > 0 and err < altmintol:
@@ -412,32 +424,40 @@ def run_large(args):
            "cracks": len(prob["pennies"])}
     if args.config == "c5":
         res, fields = {}, {}
-        for prec in ("fp64", "mixed"):
-            recs = _am_run(ctx, prob, prec, args.am_steps)
-            res[prec] = dict(s_per_step=float(np.mean([r["s"] for r in recs[1:]])),
-                             kspU=[r["kspU"] for r in recs], kspV=[r["kspV"] for r in recs],
-                             **_energies(ctx))
-            fields[prec] = ctx.get_field("V")
+        variants = [v for v in AM_VARIANTS if args.pc == "both" or v[2] == args.pc]
+        if variants[0][0] != "fp64":  # the FP64 Jacobi run is the reference for the diffs
+            variants.insert(0, AM_VARIANTS[0])
+        for key, prec, pc in variants:
+            recs = _am_run(ctx, prob, prec, args.am_steps, pc=pc)
+            res[key] = dict(s_per_step=float(np.mean([r["s"] for r in recs[1:]])),
+                            kspU=[r["kspU"] for r in recs], kspV=[r["kspV"] for r in recs],
+                            **_energies(ctx))
+            fields[key] = ctx.get_field("V")
+        ekeys = ("elastic", "pressure_work", "surface", "cov")
         out.update({
             "am_its": args.am_steps,
             "am_steps_per_s": {k: round(1.0 / res[k]["s_per_step"], 4) for k in res},
-            "mixed_over_fp64": round(res["fp64"]["s_per_step"] / res["mixed"]["s_per_step"], 3),
-            "mixed_vs_fp64_rel": {k: abs(res["mixed"][k] - res["fp64"][k]) / abs(res["fp64"][k])
-                                  for k in ("elastic", "pressure_work", "surface", "cov")},
-            "mixed_vs_fp64_v_linf": float(np.abs(fields["mixed"] - fields["fp64"]).max()),
-            "fp64": res["fp64"], "mixed": res["mixed"]})
+            "over_fp64": {k: round(res["fp64"]["s_per_step"] / res[k]["s_per_step"], 3)
+                          for k in res if k != "fp64"},
+            "vs_fp64_rel": {k: {e: abs(res[k][e] - res["fp64"][e]) / abs(res["fp64"][e])
+                                for e in ekeys} for k in res if k != "fp64"},
+            "vs_fp64_v_linf": {k: float(np.abs(fields[k] - fields["fp64"]).max())
+                               for k in res if k != "fp64"},
+            **res})
     else:
         pfull = prob["pressure"]
         steps, am_total, t_total = [], 0, 0.0
         for k in range(1, args.load_steps + 1):
             ctx.set_field("pressure", pfull * (k / args.load_steps))
             ctx.time_step_prepare()
-            recs = _am_run(ctx, prob, "mixed", args.max_am, altmintol=1e-3, reset=False)
+            recs = _am_run(ctx, prob, "mixed", args.max_am, altmintol=1e-3, reset=False,
+                           pc="jacobi" if args.pc == "both" else args.pc)
             am_total += len(recs)
             t_total += sum(r["s"] for r in recs)
             steps.append(dict(step=k, am_its=len(recs), last_err=recs[-1]["err"],
                               s=round(sum(r["s"] for r in recs), 3), **_energies(ctx)))
-        out.update({"precision": "mixed", "load_steps": args.load_steps, "altmintol": 1e-3,
+        out.update({"precision": "mixed", "pc": "jacobi" if args.pc == "both" else args.pc,
+                    "load_steps": args.load_steps, "altmintol": 1e-3,
                     "max_am_per_step": args.max_am, "am_steps": am_total,
                     "am_steps_per_s": round(am_total / t_total, 4), "solve_s": round(t_total, 2),
                     "steps": steps})
@@ -506,10 +526,14 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="c3 / c5: cells per axis scaled by this factor (1 = the full set-up)")
     ap.add_argument("--max-am", type=int, default=25, help="c3 AM cap per load step")
+    ap.add_argument("--pc", default="both", choices=["jacobi", "mg", "both"],
+                    help="U preconditioner of the c3 / c5 runs (c3: both = jacobi)")
     ap.add_argument("--only-am", action="store_true",
                     help="run the AM steps only, with a per-solve breakdown; the last step of "
                          "--profile-precision is bracketed by cudaProfilerStart/Stop")
     ap.add_argument("--profile-precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--am-pc", default="jacobi", choices=["jacobi", "mg"],
+                    help="U preconditioner of the --only-am runs")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

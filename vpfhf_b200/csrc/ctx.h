@@ -62,7 +62,7 @@ struct vfgpu_ctx {
   double* coef64 = nullptr;       // 27 per cell: V coupling coefficient
   float* coef32 = nullptr;
   uint8_t* vmask = nullptr;       // N
-  vfgpu::ETab* d_tab = nullptr;   // element tables of the uniform element
+  vfgpu::ETab h_tab{};            // element tables of the uniform element (kernel parameter)
   vfgpu::CGState* d_cg = nullptr; // device CG scalars
   vfgpu::CGState* h_cg = nullptr; // pinned host mirror
   double* d_red = nullptr;        // reduction partials (RED_BLOCKS * 4 + energy blocks * 4)
@@ -84,7 +84,7 @@ struct vfgpu_ctx {
     double* v64 = nullptr;                     // coarse phase field in FP64 (the diagonal's input)
     uint8_t *bc = nullptr, *elayer = nullptr;
     float* cellE = nullptr;
-    vfgpu::ETab* tab = nullptr;
+    vfgpu::ETab tab{};
     double* coef = nullptr;  // device, 64: lmax, 1/theta, Chebyshev (c1, c2) pairs, scratch
   };
   std::vector<MGLevel> mg;

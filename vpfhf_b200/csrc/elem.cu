@@ -1,7 +1,9 @@
 // elem.cu -- once-per-solve element kernels, written per Gauss point after the
-// reference's element routines (they run once per StepU / StepV, so clarity wins
-// over speed here).  Scatter to nodes is done in 8 parity colours of elements so
-// that no two threads of a launch touch the same node: deterministic, no atomics.
+// reference's element routines.  Scatter to nodes is done in 8 parity colours of
+// elements so that no two threads of a launch touch the same node: deterministic, no
+// atomics.  The element tables travel by value in the kernel parameters
+// (__grid_constant__): every thread of a warp reads the same entry, which the
+// constant bank broadcasts.
 #include <cmath>
 
 #include "elem.h"
@@ -101,13 +103,13 @@ __device__ __forceinline__ void gather_u8(const int64_t (&n)[8], const double* _
     for (int c = 0; c < 3; c++) u8[a][c] = u ? u[3 * n[a] + c] : 0.;
 }
 
-__global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restrict__ v,
+__global__ void u_rhs_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ v,
                              const double* __restrict__ theta, const double* __restrict__ thetaRef,
                              const double* __restrict__ p, double* __restrict__ f,
                              const double* __restrict__ u0) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   double v8[8], th8[8], p8[8], rl[24];
@@ -153,11 +155,11 @@ __global__ void u_rhs_kernel(const ElemArgs E, int color, const double* __restri
     for (int c = 0; c < 3; c++) f[3 * n[a] + c] += rl[3 * a + c];
 }
 
-__global__ void u_diag_kernel(const ElemArgs E, int color, const double* __restrict__ v,
+__global__ void u_diag_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ v,
                               double* __restrict__ d, const double* __restrict__ u0) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   double v8[8], dg[24];
@@ -187,7 +189,7 @@ __global__ void u_diag_kernel(const ElemArgs E, int color, const double* __restr
     for (int c = 0; c < 3; c++) d[3 * n[a] + c] += dg[3 * a + c];
 }
 
-__global__ void nc_flags_kernel(const ElemArgs E, const double* __restrict__ u,
+__global__ void nc_flags_kernel(const __grid_constant__ ElemArgs E, const double* __restrict__ u,
                                 uint32_t* __restrict__ flags) {
   const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
   const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -201,7 +203,7 @@ __global__ void nc_flags_kernel(const ElemArgs E, const double* __restrict__ u,
   gather_u8(n, u, u8);
   uint32_t bits = 0u;
   for (int g = 0; g < 27; g++)
-    if (trace_at(*E.tab, u8, g) < 0.) bits |= 1u << g;
+    if (trace_at(E.tab, u8, g) < 0.) bits |= 1u << g;
   flags[cell] = bits;
 }
 
@@ -216,7 +218,7 @@ __global__ void bc_diag_kernel(const uint8_t* __restrict__ bcbits, double* __res
 
 // ElasticEnergyDensity3D_local (VFMech.c:32-106) at every Gauss point, times 2 and
 // the Gauss weight, plus the AT2 mass coefficient (VFMech.c:2040-2058).
-__global__ void v_coef_kernel(const ElemArgs E, const double* __restrict__ u,
+__global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* __restrict__ u,
                               const double* __restrict__ theta, const double* __restrict__ thetaRef,
                               double* __restrict__ coef, float* __restrict__ coef32) {
   const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
@@ -225,7 +227,7 @@ __global__ void v_coef_kernel(const ElemArgs E, const double* __restrict__ u,
   const int ei = (int)(cell % (E.nx - 1));
   const int ej = (int)((cell / (E.nx - 1)) % (E.ny - 1));
   const int ek = (int)(cell / ((int64_t)(E.nx - 1) * (E.ny - 1)));
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   double u8[8][3], th8[8];
@@ -285,11 +287,11 @@ __global__ void v_coef_kernel(const ElemArgs E, const double* __restrict__ u,
   }
 }
 
-__global__ void v_rhs_kernel(const ElemArgs E, int color, const double* __restrict__ u,
+__global__ void v_rhs_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ u,
                              const double* __restrict__ p, double* __restrict__ b) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   const CellMat m = cell_mat(E, ei, ej, ek);
@@ -320,11 +322,11 @@ __global__ void v_rhs_kernel(const ElemArgs E, int color, const double* __restri
   for (int a = 0; a < 8; a++) b[n[a]] += rl[a];
 }
 
-__global__ void v_diag_kernel(const ElemArgs E, int color, const double* __restrict__ coef,
+__global__ void v_diag_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ coef,
                               double* __restrict__ d) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   const CellMat m = cell_mat(E, ei, ej, ek);
@@ -356,11 +358,11 @@ constexpr int EN_THREADS = 256, EN_BLOCKS = 592;
 // One thread per element (grid-stride, fixed assignment), per-thread compensated
 // sums, pairwise tree in shared memory, per-block partials: deterministic.
 __global__ void __launch_bounds__(EN_THREADS) energy_kernel(
-    const ElemArgs E, const double* __restrict__ u, const double* __restrict__ v,
+    const __grid_constant__ ElemArgs E, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ theta, const double* __restrict__ thetaRef,
     const double* __restrict__ p, double* __restrict__ partial, double* __restrict__ cellcov) {
   __shared__ double red[4][EN_THREADS];
-  const ETab& e = *E.tab;
+  const ETab& e = E.tab;
   const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
   KSum acc[4];
   for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < NCELL;

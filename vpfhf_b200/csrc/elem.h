@@ -15,7 +15,7 @@ struct ETab {
 void etab_host(double hx, double hy, double hz, ETab* e);
 
 struct ElemArgs {
-  const ETab* __restrict__ tab;
+  ETab tab;  // by value: the kernels read the tables from the parameter (constant) bank
   int nx, ny, nz;
   const uint8_t* __restrict__ elayer;
   const float* __restrict__ cellE;

@@ -464,14 +464,8 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     L.bc = (uint8_t*)dalloc<uint8_t>(L.N, e);
     L.elayer = (uint8_t*)dalloc<uint8_t>(nz - 1, e);
     if (c->d_cellE) L.cellE = (float*)dalloc<float>(L.NC, e);
-    L.tab = (ETab*)dalloc<ETab>(1, e);
+    etab_host(hx, hy, hz, &L.tab);
     L.coef = c->mg_coef + (int64_t)kCoefPerLevel * l;
-    if (e == cudaSuccess) {
-      ETab t;
-      etab_host(hx, hy, hz, &t);
-      e = cudaMemcpyAsync(L.tab, &t, sizeof t, cudaMemcpyHostToDevice, c->stream);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    }
   }
   c->mg_bytes = (int)sizeof(T);
   c->mg_ready = false;
@@ -688,7 +682,7 @@ void free_mg(vfgpu_ctx* c) {
     }
   }
   for (auto& L : c->mg) {
-    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.bc, L.elayer, L.cellE, L.tab};
+    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.bc, L.elayer, L.cellE};
     for (void* p : bufs) cudaFree(p);
     if (L.v != (void*)L.v64) cudaFree(L.v);
     cudaFree(L.v64);

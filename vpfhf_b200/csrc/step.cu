@@ -18,7 +18,6 @@ void free_solver(vfgpu_ctx* c) {
   cudaFree(c->coef64);
   cudaFree(c->coef32);
   cudaFree(c->vmask);
-  cudaFree(c->d_tab);
   cudaFree(c->d_cg);
   cudaFree(c->d_red);
   cudaFree(c->d_out);
@@ -27,7 +26,6 @@ void free_solver(vfgpu_ctx* c) {
   c->coef64 = nullptr;
   c->coef32 = nullptr;
   c->vmask = nullptr;
-  c->d_tab = nullptr;
   c->d_cg = nullptr;
   c->d_red = nullptr;
   c->d_out = nullptr;
@@ -48,19 +46,13 @@ static int solve_buffers(vfgpu_ctx* c) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef64, 27 * (size_t)c->NC * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef32, 27 * (size_t)c->NC * sizeof(float));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->vmask, (size_t)c->N);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_tab, sizeof(ETab));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cg, sizeof(CGState));
   if (e == cudaSuccess)
     e = cudaMalloc((void**)&c->d_red, (size_t)(RED_BLOCKS + energy_blocks()) * 4 * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_out, 16 * sizeof(double));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_cg, sizeof(CGState));
   if (e == cudaSuccess) e = cudaMallocHost((void**)&c->h_out, 16 * sizeof(double));
-  if (e == cudaSuccess) {
-    ETab t;
-    etab_host(c->hx, c->hy, c->hz, &t);
-    e = cudaMemcpyAsync(c->d_tab, &t, sizeof t, cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  }
+  etab_host(c->hx, c->hy, c->hz, &c->h_tab);
   if (e != cudaSuccess) {
     free_solver(c);
     return cuda_fail(e, "solver work space");
@@ -71,7 +63,7 @@ static int solve_buffers(vfgpu_ctx* c) {
 
 static ElemArgs elem_args(vfgpu_ctx* c) {
   ElemArgs E{};
-  E.tab = c->d_tab;
+  E.tab = c->h_tab;
   E.nx = c->nx;
   E.ny = c->ny;
   E.nz = c->nz;
