@@ -159,6 +159,51 @@ def test_results_same_alone_and_in_the_mix(cuda):
             assert np.array_equal(vs[p.tag], va), (p.tag, budget)
 
 
+def test_multigrid_problems_in_the_mix(cuda):
+    """Multigrid-preconditioned problems (FP64 and FP32 V-cycles) served among Jacobi ones
+    on 3 workers: each result has the bits it has alone, and matches the Jacobi solve of
+    the same problem to the solver tolerance."""
+    import dataclasses
+    from vpfhf_b200.serve import Server, serving_stream
+    base = serving_stream(count=9, seed=77, edges=(17, 33, 65), am_its=3)
+    probs = []
+    for i, p in enumerate(base):
+        pc, prec = (("mg", "fp64"), ("mg", "mixed"), ("jacobi", "fp64"))[i % 3]
+        probs.append(dataclasses.replace(p, pc=pc, precision=prec, tag=i))
+    alone = {}
+    for p in probs[:6]:
+        with Server(workers=1) as srv:
+            srv.submit(p)
+            r = srv.next(300.0)
+        assert r["status"] >= 0, r
+        alone[p.tag] = r
+    with Server(workers=3) as srv:
+        for p in probs:
+            srv.submit(p)
+        got = {}
+        for _ in probs:
+            r = srv.next(600.0)
+            assert r is not None and r["status"] >= 0, r
+            got[r["tag"]] = r
+    for tag, ra in alone.items():
+        for k in ("elastic", "pressure_work", "surface", "cov", "am_err", "ksp_its_u"):
+            assert got[tag][k] == ra[k], (tag, k)
+    # against the Jacobi solve of the same problems
+    with Server(workers=2) as srv:
+        for p in probs[:6]:
+            srv.submit(dataclasses.replace(p, pc="jacobi", precision="fp64"))
+        jac = {}
+        for _ in range(6):
+            r = srv.next(600.0)
+            jac[r["tag"]] = r
+    for tag, ra in alone.items():
+        if probs[tag].pc != "mg":
+            continue
+        for k in ("elastic", "pressure_work", "surface", "cov"):
+            assert ra[k] == pytest.approx(jac[tag][k], rel=1e-6), (tag, k)
+        assert ra["ksp_its_u"] * 5 < jac[tag]["ksp_its_u"], tag
+
+
 def test_server_errors(cuda):
     from vpfhf_b200 import VFGPUError
     from vpfhf_b200.serve import Problem, Server

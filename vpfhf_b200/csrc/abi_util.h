@@ -28,6 +28,9 @@ int run_mgcg(vfgpu_ctx* c, bool fp32, const double* b, double* x, double* r, dou
 cudaGraphExec_t ctx_graph(vfgpu_ctx* c, int kind, int batch,
                           const std::function<cudaError_t()>& body);
 void free_mg(vfgpu_ctx* c);
+// Device bytes of the multigrid hierarchy of a grid in V-cycle precision `bytes` (4 or 8),
+// a per-cell modulus included; 0 when the grid has no coarse level.
+long long mg_memory_bytes(int nx, int ny, int nz, int bytes);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
 }  // namespace vfgpu

@@ -696,6 +696,25 @@ void free_mg(vfgpu_ctx* c) {
   c->mg_ready = false;
 }
 
+long long mg_memory_bytes(int nx, int ny, int nz, int bytes) {
+  const long long N = (long long)nx * ny * nz;
+  long long b = 4 * 3 * N * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine work vectors
+  int nlev = 1;
+  while ((nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 && (nx - 1) / 2 + 1 >= 5 &&
+         (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
+    nx = (nx - 1) / 2 + 1;
+    ny = (ny - 1) / 2 + 1;
+    nz = (nz - 1) / 2 + 1;
+    nlev++;
+    const long long Nl = (long long)nx * ny * nz, NCl = (long long)(nx - 1) * (ny - 1) * (nz - 1);
+    const TilePlan p = u_plan(nx, ny, nz, bytes, 148);
+    b += (long long)(p.seamX + p.seamY) * bytes + 6 * 3 * Nl * bytes + Nl * 8 +
+         (bytes == 4 ? Nl * 4 : 0) + Nl + (nz - 1) + NCl * 4;
+  }
+  if (nlev < 2) return 0;
+  return b + (long long)kCoefPerLevel * nlev * 8;
+}
+
 int run_mgcg(vfgpu_ctx* c, bool fp32, const double* b, double* x, double* r, double* p, double* w,
              const double* dinv0, const float* dinv0_32, bool reuse, double rtol, double atol,
              double dtol, int maxit, int* its, int* reason, int* levels) {

@@ -26,11 +26,16 @@ using clk = std::chrono::steady_clock;
 
 namespace {
 
+// A pooled ctx serves problems of one grid and one multigrid mode (mg: 0 = Jacobi U
+// solve, else the V-cycle's bytes per value), so that its reservation covers the
+// hierarchy it holds.
 struct GridKey {
   int nx, ny, nz;
   double lx, ly, lz;
+  int mg;
   bool operator==(const GridKey& o) const {
-    return nx == o.nx && ny == o.ny && nz == o.nz && lx == o.lx && ly == o.ly && lz == o.lz;
+    return nx == o.nx && ny == o.ny && nz == o.nz && lx == o.lx && ly == o.ly && lz == o.lz &&
+           mg == o.mg;
   }
 };
 
@@ -72,7 +77,11 @@ struct vfgpu_server {
 
 namespace {
 
-GridKey key_of(const vfgpu_grid& g) { return {g.nx, g.ny, g.nz, g.lx, g.ly, g.lz}; }
+GridKey key_of(const vfgpu_request& q) {
+  const vfgpu_grid& g = q.grid;
+  const int mg = q.opts.pc == VFGPU_PC_MG ? (q.opts.precision == VFGPU_MIXED ? 4 : 8) : 0;
+  return {g.nx, g.ny, g.nz, g.lx, g.ly, g.lz, mg};
+}
 
 // Takes an idle ctx of the job's grid or makes room for a new one.  Called with the
 // lock held; may release it while destroying or creating contexts.  Returns the pool
@@ -88,6 +97,7 @@ int acquire(vfgpu_server* s, std::unique_lock<std::mutex>& lk, const GridKey& ke
     *err = vfgpu_last_error();
     return -1;
   }
+  if (key.mg) need += mg_memory_bytes(key.nx, key.ny, key.nz, key.mg);
   auto oom = [&] {
     *rc = VFGPU_ERR_OOM;
     char b[160];
@@ -204,7 +214,7 @@ void worker_main(vfgpu_server* s, int wid) {
     bool reused = false;
     std::string err;
     int rc = VFGPU_OK;
-    const int slot = acquire(s, lk, key_of(job.req.grid), &reused, &rc, &err);
+    const int slot = acquire(s, lk, key_of(job.req), &reused, &rc, &err);
     if (slot >= 0) {
       vfgpu_ctx* c = s->pool[slot].ctx;
       lk.unlock();

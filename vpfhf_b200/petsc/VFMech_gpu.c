@@ -136,11 +136,15 @@ static PetscErrorCode push_inputs(VFFields *fields) {
 
 static void solve_opts(vfgpu_solve_opts *o) {
   PetscBool flg;
-  PetscInt prec = 0;
+  PetscInt prec = 0, pc = VFGPU_PC_JACOBI;
   vfgpu_default_solve_opts(o);
   /* -vfgpu_precision 0 (FP64, default) | 1 (FP32 inner solves + FP64 refinement) */
   PetscOptionsGetInt(NULL, NULL, "-vfgpu_precision", &prec, &flg);
   o->precision = (int)prec;
+  /* -vfgpu_pc 0 (Jacobi, the reference's KSPCG+Jacobi, default) | 1 (multigrid V-cycle;
+     same stopping test; needs an even cell count per axis) */
+  PetscOptionsGetInt(NULL, NULL, "-vfgpu_pc", &pc, &flg);
+  o->pc = (int)pc;
 }
 
 PetscErrorCode VF_StepU(VFFields *fields, VFCtx *ctx) {

@@ -44,6 +44,7 @@ class Problem:
     altmintol: float = 0.0
     max_am_its: int = 0
     precision: str = "fp64"
+    pc: str = "jacobi"  # StepU preconditioner: "jacobi" (the reference's) or "mg"
     bcU: list | None = None  # three BCSpec (default rollers)
     bcV: BCSpec | None = None
     tag: int = 0
@@ -75,7 +76,7 @@ def make_request(p: Problem, out_u=None, out_v=None, out_cellcov=None) -> _abi.R
     for i in range(len(ra)):
         q.rect[i] = ra[i]
     q.am_its, q.altmintol, q.max_am_its = p.am_its, p.altmintol, p.max_am_its
-    q.opts = solve_opts(precision=p.precision)
+    q.opts = solve_opts(precision=p.precision, pc=p.pc)
     q.out_u = _abi.ptr(out_u)
     q.out_v = _abi.ptr(out_v)
     q.out_cellcov = _abi.ptr(out_cellcov)
@@ -157,7 +158,7 @@ def random_penny(rng, L):
 
 
 def serving_stream(count=512, seed=1004, edges=(17, 33, 65, 97), L=4.0, am_its=5,
-                   precision="fp64"):
+                   precision="fp64", pc="jacobi"):
     """`count` independent problems: grid edge uniform over `edges`, 1-4 random penny
     cracks, E ~ U[5, 30] GPa, nu ~ U[0.15, 0.35], AT1 or AT2 with probability 1/2,
     epsilon = 2h, eta = 1e-8, Gc = 100, 1 MPa crack pressure on rollers."""
@@ -170,7 +171,8 @@ def serving_stream(count=512, seed=1004, edges=(17, 33, 65, 97), L=4.0, am_its=5
         pennies = [random_penny(rng, box) for _ in range(ncr)]
         out.append(Problem(n=(e, e, e), l=box, E=rng.uniform(5e9, 30e9),
                            nu=rng.uniform(0.15, 0.35), atnum=1 if rng.uniform() < 0.5 else 2,
-                           pennies=pennies, am_its=am_its, precision=precision, tag=i))
+                           pennies=pennies, am_its=am_its, precision=precision, pc=pc,
+                           tag=i))
     return out
 
 
