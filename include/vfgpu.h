@@ -209,6 +209,27 @@ int vfgpu_v_energy(vfgpu_ctx* ctx, double* surface);
  * NULL, the per-cell average ((nx-1)(ny-1)(nz-1)). */
 int vfgpu_crack_opening(vfgpu_ctx* ctx, double* cov, double* cellcov);
 
+/* ---- flow-coupling boundary (what VPFHF.c:91-101 calls between VF_StepP and VF_StepU's
+ * consumers; the flow solvers themselves stay with the host) ---- */
+typedef struct {
+  double int_length;      /* VFCtx.WidthIntLenght; <= 0: 3 res + 4 epsilon (VFCommon.c:897-914) */
+  double width_tol;       /* VFCtx.width_tol (-widthremoval_tol, VFCommon.c:111; default 0.1)  */
+  int remove_tip_effect;  /* VFCtx.removeTipEffect (-removetipeffect, VFCommon.c:108; 0)       */
+} vfgpu_width_opts;
+void vfgpu_default_width_opts(vfgpu_width_opts* opts);
+/* UpdateFractureWidth (VFPermfield.c:267-562) at the resident U and V: fields->widthc
+ * (cells), fields->width (nodes, CellToNodeInterpolation VFPermfield.c:1156-1330) and
+ * fields->pmult (cells: 0 where the integrated grad V exceeds width_tol, else 1).
+ * Each output is host or device memory, or NULL (the results stay resident either
+ * way).  nstalled (may be NULL): band cells whose march cannot advance because grad V
+ * vanishes at their centre (the reference's loop does not end there); they get width 0. */
+int vfgpu_update_fracture_width(vfgpu_ctx* ctx, const vfgpu_width_opts* opts, double* widthc,
+                                double* width, double* pmult, int* nstalled);
+/* VolumetricFractureWellRate (VFPermfield.c:1552-1604): sum over cells of the nodal
+ * rate field regrate (ctx->RegFracWellFlowRate; N, host or device) times |grad V|,
+ * integrated with the 27-point rule. */
+int vfgpu_fracture_well_rate(vfgpu_ctx* ctx, const double* regrate, double* rate);
+
 /* The SNES residuals at the resident fields: VF_UResidual (3N) and VF_VResidual (N). */
 int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);
 int vfgpu_v_residual(vfgpu_ctx* ctx, double* F);

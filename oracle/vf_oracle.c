@@ -1211,6 +1211,262 @@ int vfo_cov(const vfo_problem *P, const double *u, const double *v, double *cov,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Flow-coupling boundary: the fracture width UpdateFractureWidth
+ * (VFPermfield.c:267-562) with CellToNodeInterpolation (VFPermfield.c:1156-1330), the
+ * width integration length (VFCommon.c:897-914) and VolumetricFractureWellRate
+ * (VFPermfield.c:1513-1604), restated serially in the reference's loop order. */
+
+/* WidthIntLenght = 3 res + 4 epsilon, res the grid spacing picked by the reference's
+ * comparison chain (VFCommon.c:897-914; for bx == by < bz it picks bz). */
+double vfo_width_int_length(const vfo_problem *P) {
+  const double bx = P->lx / (P->nx - 1), by = P->ly / (P->ny - 1), bz = P->lz / (P->nz - 1);
+  double res;
+  if (P->nx == 2) res = by < bz ? by : bz;
+  else if (P->ny == 2) res = bx < bz ? bx : bz;
+  else if (P->nz == 2) res = bx < by ? bx : by;
+  else if (bx < by && bx < bz) res = bx;
+  else if (by < bx && by < bz) res = by;
+  else res = bz;
+  return 3 * res + 4 * P->epsilon;
+}
+
+/* CartFEElement1DInit (VFCartFE.c:1773-1785): the linear basis at x in a segment of
+ * length l, through the reference's map var = (x - l/2)/l/2 (so var stays in
+ * [-1/4, 1/4] across the segment). */
+static void pt_basis1d(double x, double l, double phi[2], double dphi[2]) {
+  const double var = (x - l / 2.) / l / 2.;
+  phi[0] = (1. - var) * .5;
+  phi[1] = (1. + var) * .5;
+  dphi[0] = -1. / l;
+  dphi[1] = 1. / l;
+}
+
+typedef struct {
+  double phi[8], dphi[8][3];
+} ptelem;
+
+/* CartFEElement3DInit (VFCartFE.c:1837-1866) at the point (x, y, z) of a cell. */
+static void pt_elem(double x, double y, double z, double lx, double ly, double lz, ptelem *s) {
+  double px[2], py[2], pz[2], dx[2], dy[2], dz[2];
+  pt_basis1d(x, lx, px, dx);
+  pt_basis1d(y, ly, py, dy);
+  pt_basis1d(z, lz, pz, dz);
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        const int a = i + 2 * j + 4 * k;
+        s->phi[a] = pz[k] * py[j] * px[i];
+        s->dphi[a][0] = pz[k] * py[j] * dx[i];
+        s->dphi[a][1] = pz[k] * dy[j] * px[i];
+        s->dphi[a][2] = dz[k] * py[j] * px[i];
+      }
+}
+
+/* ComputeAveVGradVandNormal_local (VFPermfield.c:2124-2156): V, grad V, the unit
+ * normal grad V / |grad V| (0 when not finite) and U at the point of cell (ei,ej,ek). */
+static void pt_fields(const vfo_problem *P, const double *u, const double *v, int ei, int ej,
+                      int ek, const ptelem *s, double *vave, double g[3], double n[3],
+                      double uc[3]) {
+  *vave = 0.;
+  for (int c = 0; c < 3; c++) g[c] = n[c] = uc[c] = 0.;
+  for (int k = 0; k < 2; k++)
+    for (int j = 0; j < 2; j++)
+      for (int i = 0; i < 2; i++) {
+        const int a = i + 2 * j + 4 * k;
+        const int64_t q = NODE(P, ei + i, ej + j, ek + k);
+        for (int c = 0; c < 3; c++) {
+          g[c] += v[q] * s->dphi[a][c];
+          uc[c] += u[3 * q + c] * s->phi[a];
+        }
+        *vave += v[q] * s->phi[a];
+      }
+  const double mag = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+  for (int c = 0; c < 3; c++) n[c] = g[c] / mag;
+  if (!isfinite(n[0]) || !isfinite(n[1]) || !isfinite(n[2])) n[0] = n[1] = n[2] = 0.;
+}
+
+/* IntegrateUcdotGradVlocal (VFPermfield.c:589-610) on the segment element of
+ * VFCartFEElement1DInit(len): acc += sum_g (f0 phi_0 + f1 phi_1)(g) w_g / 2. */
+static void seg_integrate(double *acc, double f0, double f1, const double w[3],
+                          const double phi[2][3]) {
+  double fe[3] = {0., 0., 0.};
+  for (int i = 0; i < 2; i++)
+    for (int g = 0; g < 3; g++) fe[g] += (i ? f1 : f0) * phi[i][g];
+  for (int g = 0; g < 3; g++) *acc += fe[g] * w[g] / 2.;
+}
+
+/* The cell whose closed box holds coordinate c along one axis, the last one in the
+ * reference's ascending scan (VFPermfield.c:370-384); -1 if none. */
+static int axis_cell(double c, double l, int n) {
+  for (int i = n - 2; i >= 0; i--)
+    if (coord(i + 1, l, n) >= c && coord(i, l, n) <= c) return i;
+  return -1;
+}
+
+/* One march of UpdateFractureWidth from the centre of cell (ei,ej,ek) along +n
+ * (dir = 1, VFPermfield.c:356-440) or -n (dir = -1, :441-527); cur holds the cell
+ * the previous point was found in (the reference keeps it when a point lies in no
+ * cell).  Returns 0, or 1 if the march hit max_steps. */
+static int width_march(const vfo_problem *P, const double *u, const double *v, int ei, int ej,
+                       int ek, int dir, double len, double L, int cur[3], double *w,
+                       double val[3], long max_steps) {
+  double hx, hy, hz, vave, g[3], n[3], uc[3], ref[3], g0[3], ca[3], cc[3];
+  ptelem s;
+  cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+  pt_elem(hx / 2., hy / 2., hz / 2., hx, hy, hz, &s);
+  pt_fields(P, u, v, ei, ej, ek, &s, &vave, g, n, uc);
+  for (int c = 0; c < 3; c++) ref[c] = n[c];
+  for (int c = 0; c < 3; c++) g0[c] = g[c];
+  double cod0 = g[0] * uc[0] + g[1] * uc[1] + g[2] * uc[2];
+  ca[0] = (coord(ei + 1, P->lx, P->nx) + coord(ei, P->lx, P->nx)) / 2.;
+  ca[1] = (coord(ej + 1, P->ly, P->ny) + coord(ej, P->ly, P->ny)) / 2.;
+  ca[2] = (coord(ek + 1, P->lz, P->nz) + coord(ek, P->lz, P->nz)) / 2.;
+  for (int c = 0; c < 3; c++) cc[c] = dir > 0 ? ca[c] + n[c] * len : ca[c] - n[c] * len;
+  double lc = len, sw[3], sphi[2][3], sdphi[2][3];
+  tables1d(len, sw, sphi, sdphi); /* VFCartFEElement1DInit(len), VFCartFE.c:90-116 */
+  long steps = 0;
+  do {
+    const int fi = axis_cell(cc[0], P->lx, P->nx), fj = axis_cell(cc[1], P->ly, P->ny),
+              fk = axis_cell(cc[2], P->lz, P->nz);
+    if (fi >= 0 && fj >= 0 && fk >= 0) {
+      cur[0] = fi;
+      cur[1] = fj;
+      cur[2] = fk;
+    }
+    cell_h(P, cur[0], cur[1], cur[2], &hx, &hy, &hz);
+    const double hwx = cc[0] - coord(cur[0], P->lx, P->nx);
+    const double hwy = cc[1] - coord(cur[1], P->ly, P->ny);
+    const double hwz = cc[2] - coord(cur[2], P->lz, P->nz);
+    const double nold[3] = {n[0], n[1], n[2]};
+    pt_elem(hwx, hwy, hwz, hx, hy, hz, &s);
+    pt_fields(P, u, v, cur[0], cur[1], cur[2], &s, &vave, g, n, uc);
+    const double cod1 = g[0] * uc[0] + g[1] * uc[1] + g[2] * uc[2];
+    seg_integrate(w, cod0, cod1, sw, sphi);
+    for (int c = 0; c < 3; c++) seg_integrate(&val[c], g0[c], g[c], sw, sphi);
+    if (n[0] == 0 && n[1] == 0 && n[2] == 0)
+      for (int c = 0; c < 3; c++) n[c] = nold[c];
+    double c1[3], c2[3];
+    for (int c = 0; c < 3; c++) {
+      c1[c] = cc[c] + n[c] * len;
+      c2[c] = cc[c] - n[c] * len;
+    }
+    const double t1 = sqrt((c1[0] - ca[0]) * (c1[0] - ca[0]) + (c1[1] - ca[1]) * (c1[1] - ca[1]) +
+                           (c1[2] - ca[2]) * (c1[2] - ca[2]));
+    const double t2 = sqrt((c2[0] - ca[0]) * (c2[0] - ca[0]) + (c2[1] - ca[1]) * (c2[1] - ca[1]) +
+                           (c2[2] - ca[2]) * (c2[2] - ca[2]));
+    if (t1 > t2) {
+      for (int c = 0; c < 3; c++) cc[c] = c1[c];
+    } else {
+      for (int c = 0; c < 3; c++) {
+        cc[c] = c2[c];
+        n[c] = -1 * n[c];
+      }
+    }
+    lc += len;
+    cod0 = cod1;
+    for (int c = 0; c < 3; c++) g0[c] = g[c];
+    if (++steps >= max_steps) return 1;
+  } while (lc < L - len && vave < 1.0 &&
+           (dir > 0 ? ref[0] * n[0] + ref[1] * n[1] + ref[2] * n[2] >= 0.
+                    : -ref[0] * n[0] - ref[1] * n[1] - ref[2] * n[2] >= 0.));
+  return 0;
+}
+
+int vfo_fracture_width(const vfo_problem *P, const double *u, const double *v, double L,
+                       double width_tol, int remove_tip, double *widthc, double *pmult,
+                       int *nstall) {
+  const long max_steps = 1000000;
+  int cur[3] = {0, 0, 0}, stall = 0;
+  double value = 0.; /* kept from cell to cell like the reference's */
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        const int64_t cell = ((int64_t)ek * (P->ny - 1) + ej) * (P->nx - 1) + ei;
+        double hx, hy, hz, vave, g[3], n[3], uc[3], w = 0., val[3] = {0., 0., 0.};
+        ptelem s;
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        pt_elem(hx / 2., hy / 2., hz / 2., hx, hy, hz, &s);
+        pt_fields(P, u, v, ei, ej, ek, &s, &vave, g, n, uc);
+        const double len =
+            sqrt((n[0] * hx) * (n[0] * hx) + (n[1] * hy) * (n[1] * hy) + (n[2] * hz) * (n[2] * hz)) / 20;
+        pmult[cell] = 1.;
+        if (vave < 1.0 && vave > 0.0) {
+          if (!(len > 0.)) {
+            /* the reference's march does not advance here (and does not end) */
+            stall++;
+          } else {
+            stall += width_march(P, u, v, ei, ej, ek, 1, len, L, cur, &w, val, max_steps);
+            stall += width_march(P, u, v, ei, ej, ek, -1, len, L, cur, &w, val, max_steps);
+            value = sqrt(val[0] * val[0] + val[1] * val[1] + val[2] * val[2]);
+            if (value > width_tol) pmult[cell] = 0.;
+          }
+        }
+        if (w < 0.0) w = 0;
+        if (remove_tip && value > width_tol) w = 0;
+        widthc[cell] = w;
+      }
+  if (nstall) *nstall = stall;
+  return 0;
+}
+
+int vfo_cell_to_node(const vfo_problem *P, const double *cellv, double *nodev) {
+  const int64_t N = (int64_t)P->nx * P->ny * P->nz;
+  double *vol = (double *)calloc((size_t)N, sizeof(double));
+  if (!vol) return -1;
+  for (int64_t q = 0; q < N; q++) nodev[q] = 0.;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        const double c = cellv[((int64_t)ek * (P->ny - 1) + ej) * (P->nx - 1) + ei];
+        double hx, hy, hz;
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        for (int k = 0; k < 2; k++)
+          for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+              const int64_t q = NODE(P, ei + i, ej + j, ek + k);
+              vol[q] += hz * hy * hx;
+              nodev[q] += c * hx * hy * hz;
+            }
+      }
+  for (int64_t q = 0; q < N; q++) nodev[q] = nodev[q] / vol[q];
+  free(vol);
+  return 0;
+}
+
+int vfo_fracture_well_rate(const vfo_problem *P, const double *v, const double *regrate,
+                           double *rate) {
+  double total = 0., hx, hy, hz;
+  etab e;
+  for (int ek = 0; ek < P->nz - 1; ek++)
+    for (int ej = 0; ej < P->ny - 1; ej++)
+      for (int ei = 0; ei < P->nx - 1; ei++) {
+        cell_h(P, ei, ej, ek, &hx, &hy, &hz);
+        etab_init(&e, hx, hy, hz);
+        double dv[3][27], rg[27];
+        for (int g = 0; g < 27; g++) {
+          dv[0][g] = dv[1][g] = dv[2][g] = 0.;
+          rg[g] = 0.;
+        }
+        for (int k = 0; k < 2; k++)
+          for (int j = 0; j < 2; j++)
+            for (int i = 0; i < 2; i++) {
+              const int a = i + 2 * j + 4 * k;
+              const int64_t q = NODE(P, ei + i, ej + j, ek + k);
+              for (int g = 0; g < 27; g++) {
+                for (int c = 0; c < 3; c++) dv[c][g] += v[q] * e.dphi[a][c][g];
+                rg[g] += regrate[q] * e.phi[a][g];
+              }
+            }
+        double loc = 0.;
+        for (int g = 0; g < 27; g++)
+          loc += rg[g] * sqrt(dv[0][g] * dv[0][g] + dv[1][g] * dv[1][g] + dv[2][g] * dv[2][g]) * e.w[g];
+        total += loc;
+      }
+  *rate = total;
+  return 0;
+}
+
+/* ------------------------------------------------------------------------ */
 /* VFDistanceToPennyCrack (VFCracks.c:101-126) and VFPennyCrackBuildVAT1/2
  * (VFCracks.c:136-227). */
 static double penny_distance(const double x[3], const double ctr[3], double r, double th,

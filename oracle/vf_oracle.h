@@ -149,6 +149,20 @@ int vfo_cov(const vfo_problem *P, const double *u, const double *v, double *cov,
  * faces (the cell layer before the last, so the node layer one inside the box). */
 int vfo_insitu_work(const vfo_problem *P, const double *u, double *work);
 
+/* ---- flow-coupling boundary (VFPermfield.c, VFCommon.c:897-914) ----
+ * vfo_width_int_length: VFCtx.WidthIntLenght.  vfo_fracture_width: UpdateFractureWidth
+ * (VFPermfield.c:267-562) -- widthc and pmult per cell; nstall counts band cells whose
+ * march cannot advance (zero grad V at the centre: the reference loops there forever).
+ * vfo_cell_to_node: CellToNodeInterpolation (VFPermfield.c:1156-1330), volume-weighted.
+ * vfo_fracture_well_rate: VolumetricFractureWellRate (VFPermfield.c:1513-1604). */
+double vfo_width_int_length(const vfo_problem *P);
+int vfo_fracture_width(const vfo_problem *P, const double *u, const double *v, double L,
+                       double width_tol, int remove_tip, double *widthc, double *pmult,
+                       int *nstall);
+int vfo_cell_to_node(const vfo_problem *P, const double *cellv, double *nodev);
+int vfo_fracture_well_rate(const vfo_problem *P, const double *v, const double *regrate,
+                           double *rate);
+
 /* ---- penny crack initial V (VFCracks.c:101-227) ---- */
 int vfo_penny_crack_v(const vfo_problem *P, const double center[3], double r,
                       double theta_deg, double phi_deg, double thickness, double *v);

@@ -122,6 +122,10 @@ def _declare(L):
         "vfo_u_apply_ref_u": [_P, odp, _dp, _dp, ou8, _dp],
         "vfo_u_rhs_u": [_P, odp, _dp, odp, odp, odp, _dp],
         "vfo_u_diag_u": [_P, odp, _dp, ou8, _dp],
+        "vfo_fracture_width": [_P, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp,
+                               C.POINTER(C.c_int)],
+        "vfo_cell_to_node": [_P, _dp, _dp],
+        "vfo_fracture_well_rate": [_P, _dp, _dp, C.POINTER(C.c_double)],
         "vfo_step_u": [_P, _dp, _dp, odp, odp, odp, ou8, odp, C.POINTER(SolverOpts),
                        C.POINTER(Stats)],
         "vfo_step_v": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
@@ -133,6 +137,8 @@ def _declare(L):
         f.restype = C.c_int
     L.vfo_rect_distance.argtypes = [_dp, _dp]
     L.vfo_rect_distance.restype = C.c_double
+    L.vfo_width_int_length.argtypes = [_P]
+    L.vfo_width_int_length.restype = C.c_double
     L.vfo_u_csr_nnz.argtypes = [_P]
     L.vfo_u_csr_nnz.restype = C.c_int64
 
@@ -273,6 +279,33 @@ class Oracle:
         cc = np.zeros((self.n[0] - 1) * (self.n[1] - 1) * (self.n[2] - 1)) if cell else None
         self.L.vfo_cov(C.byref(self.P), u, v, C.byref(c), cc)
         return (c.value, cc) if cell else c.value
+
+    def width_int_length(self):
+        """VFCtx.WidthIntLenght = 3 res + 4 epsilon (VFCommon.c:897-914)."""
+        return self.L.vfo_width_int_length(C.byref(self.P))
+
+    def fracture_width(self, u, v, int_length=None, width_tol=0.1, remove_tip=False):
+        """UpdateFractureWidth (VFPermfield.c:267-562) + CellToNodeInterpolation:
+        returns (widthc per cell, width per node, pmult per cell, stalled band cells)."""
+        nc = (self.n[0] - 1) * (self.n[1] - 1) * (self.n[2] - 1)
+        wc, pm, st = np.zeros(nc), np.zeros(nc), C.c_int()
+        L = self.width_int_length() if int_length is None else float(int_length)
+        self.L.vfo_fracture_width(C.byref(self.P), np.ascontiguousarray(u, np.float64),
+                                  np.ascontiguousarray(v, np.float64), L, float(width_tol),
+                                  int(bool(remove_tip)), wc, pm, C.byref(st))
+        return wc, self.cell_to_node(wc), pm, st.value
+
+    def cell_to_node(self, cellv):
+        out = np.zeros(self.N)
+        self.L.vfo_cell_to_node(C.byref(self.P), np.ascontiguousarray(cellv, np.float64), out)
+        return out
+
+    def fracture_well_rate(self, v, regrate):
+        """VolumetricFractureWellRate (VFPermfield.c:1513-1604)."""
+        r = C.c_double()
+        self.L.vfo_fracture_well_rate(C.byref(self.P), np.ascontiguousarray(v, np.float64),
+                                      np.ascontiguousarray(regrate, np.float64), C.byref(r))
+        return r.value
 
     def penny_v(self, center, r, theta=0.0, phi=0.0, thickness=0.0):
         v = np.zeros(self.N)

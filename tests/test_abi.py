@@ -35,7 +35,7 @@ def test_struct_layouts_match_header(tmp_path):
                "vfgpu_solve_opts": _abi.SolveOpts, "vfgpu_solve_stats": _abi.SolveStats,
                "vfgpu_penny": _abi.Penny, "vfgpu_rect": _abi.Rect,
                "vfgpu_request": _abi.Request, "vfgpu_result": _abi.Result,
-               "vfgpu_server_info": _abi.ServerInfo}
+               "vfgpu_server_info": _abi.ServerInfo, "vfgpu_width_opts": _abi.WidthOpts}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "vfgpu.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')

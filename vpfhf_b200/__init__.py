@@ -223,6 +223,27 @@ class VFContext:
         _abi.check(self.L.vfgpu_v_energy(self.h, C.byref(s)), "vfgpu_v_energy")
         return s.value
 
+    def update_fracture_width(self, int_length=0.0, width_tol=0.1, remove_tip_effect=False):
+        """UpdateFractureWidth (VFPermfield.c:267-562) at the resident U and V: returns
+        (widthc per cell, width per node, pmult per cell, stalled band cells).
+        int_length <= 0 takes WidthIntLenght = 3 res + 4 epsilon (VFCommon.c:897-914)."""
+        o = _abi.WidthOpts(float(int_length), float(width_tol), int(bool(remove_tip_effect)))
+        n = self.n
+        nc = (n[0] - 1) * (n[1] - 1) * (n[2] - 1)
+        wc, wn, pm, st = np.empty(nc), np.empty(self.N), np.empty(nc), C.c_int()
+        _abi.check(self.L.vfgpu_update_fracture_width(self.h, C.byref(o), _abi.ptr(wc),
+                                                      _abi.ptr(wn), _abi.ptr(pm), C.byref(st)),
+                   "vfgpu_update_fracture_width")
+        return wc, wn, pm, st.value
+
+    def fracture_well_rate(self, regrate):
+        """VolumetricFractureWellRate (VFPermfield.c:1552-1604) of a nodal rate field."""
+        r = C.c_double()
+        reg = np.ascontiguousarray(regrate, np.float64)
+        _abi.check(self.L.vfgpu_fracture_well_rate(self.h, _abi.ptr(reg), C.byref(r)),
+                   "vfgpu_fracture_well_rate")
+        return r.value
+
     def crack_opening(self, cell=False):
         cov = C.c_double()
         n = self.n

@@ -52,6 +52,11 @@ class SolveOpts(C.Structure):
                 ("pc", C.c_int)]
 
 
+class WidthOpts(C.Structure):
+    _fields_ = [("int_length", C.c_double), ("width_tol", C.c_double),
+                ("remove_tip_effect", C.c_int)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("newton_its", C.c_int), ("ksp_its", C.c_int), ("refine_its", C.c_int),
                 ("reason", C.c_int), ("fnorm0", C.c_double), ("fnorm", C.c_double),
@@ -144,6 +149,9 @@ _SIGS = {
     "vfgpu_u_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_v_residual": [C.c_void_p, C.c_void_p],
     "vfgpu_init_cracks": [C.c_void_p, C.c_int, C.POINTER(Penny), C.c_int, C.POINTER(Rect)],
+    "vfgpu_update_fracture_width": [C.c_void_p, C.POINTER(WidthOpts), C.c_void_p, C.c_void_p,
+                                    C.c_void_p, C.POINTER(C.c_int)],
+    "vfgpu_fracture_well_rate": [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)],
     "vfgpu_server_create": [C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_void_p)],
     "vfgpu_server_submit": [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_ulonglong)],
     "vfgpu_server_next": [C.c_void_p, C.c_double, C.POINTER(Result)],
@@ -153,7 +161,8 @@ _SIGS = {
     "vfgpu_u_apply_noalloc": [C.POINTER(Grid), C.POINTER(MatProp), C.c_double, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],
 }
-_VOID_SIGS = {"vfgpu_default_solve_opts": [C.POINTER(SolveOpts)]}
+_VOID_SIGS = {"vfgpu_default_solve_opts": [C.POINTER(SolveOpts)],
+              "vfgpu_default_width_opts": [C.POINTER(WidthOpts)]}
 
 
 def lib():

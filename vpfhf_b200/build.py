@@ -21,8 +21,9 @@ LIB = os.path.join(HERE, "libvfgpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
-# Per-file extra flags: the crack initialisers round like the reference's C code.
-FILE_FLAGS = {"cracks.cu": ["-fmad=false"]}
+# Per-file extra flags: the crack initialisers and the fracture width round like the
+# reference's C code.
+FILE_FLAGS = {"cracks.cu": ["-fmad=false"], "width.cu": ["-fmad=false"]}
 
 
 def _flags(debug: bool) -> list[str]:

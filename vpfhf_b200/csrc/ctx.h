@@ -94,6 +94,11 @@ struct vfgpu_ctx {
   double* mg_z = nullptr;         // FP32 V-cycle: the preconditioned residual in FP64 (3N)
   const void* mg_dinv0 = nullptr; // fine inverse diagonal in the V-cycle's precision
 
+  // Flow-coupling boundary (width.cu): cell width, permeability multiplier, node width,
+  // stalled-march count, well-rate scratch; allocated at the first width call.
+  double *d_widthc = nullptr, *d_pmult = nullptr, *d_width = nullptr, *d_wpart = nullptr;
+  unsigned* d_wstall = nullptr;
+
   // Captured CUDA graphs of CG iteration batches, keyed by (call site, batch size).
   // Kernels read the material table, eta and the AT gradient weights through
   // d_params, so new material / vfprop values leave the graphs valid; a set-up call

@@ -160,7 +160,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   free_solver(c);
   free_mg(c);
   for (auto& p : c->f) cudaFree(p);
-  void* bufs[] = {c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
