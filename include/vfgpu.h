@@ -229,6 +229,10 @@ int vfgpu_update_fracture_width(vfgpu_ctx* ctx, const vfgpu_width_opts* opts, do
  * rate field regrate (ctx->RegFracWellFlowRate; N, host or device) times |grad V|,
  * integrated with the 27-point rule. */
 int vfgpu_fracture_well_rate(vfgpu_ctx* ctx, const double* regrate, double* rate);
+/* CellToNodeInterpolation (VFPermfield.c:1156-1330) of a scalar cell field: each node
+ * takes the volume-weighted mean of its cells (cellv: (nx-1)(ny-1)(nz-1), nodev: N; host
+ * or device memory). */
+int vfgpu_cell_to_node(vfgpu_ctx* ctx, const double* cellv, double* nodev);
 
 /* The SNES residuals at the resident fields: VF_UResidual (3N) and VF_VResidual (N). */
 int vfgpu_u_residual(vfgpu_ctx* ctx, double* F);

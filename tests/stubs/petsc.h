@@ -44,5 +44,7 @@ PetscErrorCode VecRestoreArray(Vec, PetscScalar **);
 PetscErrorCode VecMin(Vec, PetscInt *, PetscReal *);
 PetscErrorCode VecMax(Vec, PetscInt *, PetscReal *);
 PetscErrorCode PetscPrintf(MPI_Comm, const char[], ...);
+PetscErrorCode PetscMalloc(size_t, void *);
+PetscErrorCode PetscFree(void *);
 PetscErrorCode PetscOptionsGetInt(PetscOptions, const char[], const char[], PetscInt *, PetscBool *);
 #endif

@@ -78,3 +78,25 @@ def test_well_rate_matches_oracle(cuda, oracle_mod):
     r = ctx.fracture_well_rate(reg)
     assert r == pytest.approx(o.fracture_well_rate(v, reg), rel=1e-12)
     ctx.close()
+
+
+def test_cell_to_node_and_cov_nodes_match_oracle(cuda, oracle_mod):
+    """CellToNodeInterpolation on the device (gather over each node's cells in the
+    reference's scatter order) is the oracle's to the bit; with the per-cell crack
+    opening it gives VolumetricCrackOpening's fields->VolCrackOpening."""
+    import vpfhf_b200 as vg
+    n, L = (21, 17, 13), (2.0, 1.6, 1.2)
+    o = oracle_mod.Oracle(n, L, E=1e10, nu=0.25, Gc=100.0, epsilon=0.2, eta=1e-8, atnum=1)
+    ctx = _ctx(vg, n, L, 0.2)
+    rng = np.random.default_rng(12)
+    cell = rng.standard_normal(20 * 16 * 12)
+    assert np.array_equal(ctx.cell_to_node(cell), o.cell_to_node(cell))
+    v = o.penny_v((1.0, 0.8, 0.6), 0.5, theta=10.0, phi=30.0)
+    u = rng.standard_normal(3 * o.N) * 1e-3
+    ctx.set_field("V", v)
+    ctx.set_field("U", u)
+    cov, cellcov = ctx.crack_opening(cell=True)
+    cov_o, cellcov_o = o.cov(u, v, cell=True)
+    assert cov == pytest.approx(cov_o, rel=1e-12)
+    assert np.allclose(ctx.cell_to_node(cellcov), o.cell_to_node(cellcov_o), rtol=1e-10, atol=1e-18)
+    ctx.close()

@@ -236,6 +236,14 @@ class VFContext:
                    "vfgpu_update_fracture_width")
         return wc, wn, pm, st.value
 
+    def cell_to_node(self, cellv):
+        """CellToNodeInterpolation (VFPermfield.c:1156-1330) of a scalar cell field."""
+        cv = np.ascontiguousarray(cellv, np.float64)
+        out = np.empty(self.N)
+        _abi.check(self.L.vfgpu_cell_to_node(self.h, _abi.ptr(cv), _abi.ptr(out)),
+                   "vfgpu_cell_to_node")
+        return out
+
     def fracture_well_rate(self, regrate):
         """VolumetricFractureWellRate (VFPermfield.c:1552-1604) of a nodal rate field."""
         r = C.c_double()

@@ -152,6 +152,7 @@ _SIGS = {
     "vfgpu_update_fracture_width": [C.c_void_p, C.POINTER(WidthOpts), C.c_void_p, C.c_void_p,
                                     C.c_void_p, C.POINTER(C.c_int)],
     "vfgpu_fracture_well_rate": [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)],
+    "vfgpu_cell_to_node": [C.c_void_p, C.c_void_p, C.c_void_p],
     "vfgpu_server_create": [C.c_int, C.c_int, C.c_longlong, C.POINTER(C.c_void_p)],
     "vfgpu_server_submit": [C.c_void_p, C.POINTER(Request), C.POINTER(C.c_ulonglong)],
     "vfgpu_server_next": [C.c_void_p, C.c_double, C.POINTER(Result)],

@@ -322,7 +322,8 @@ int width_buffers(vfgpu_ctx* c) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_pmult, std::max<int64_t>(1, c->NC) * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_width, c->N * sizeof(double));
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_wstall, sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_wpart, (c->N + kRateBlocks + 1) * sizeof(double));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void**)&c->d_wpart, (c->N + c->NC + kRateBlocks + 1) * sizeof(double));
   if (e != cudaSuccess) {
     for (void* p : {(void*)c->d_widthc, (void*)c->d_pmult, (void*)c->d_width, (void*)c->d_wstall,
                     (void*)c->d_wpart})
@@ -396,14 +397,34 @@ int vfgpu_update_fracture_width(vfgpu_ctx* c, const vfgpu_width_opts* o_, double
   return VFGPU_OK;
 }
 
+int vfgpu_cell_to_node(vfgpu_ctx* c, const double* cellv, double* nodev) {
+  if (!c || !cellv || !nodev) return fail(VFGPU_ERR_INVALID, "vfgpu_cell_to_node: null argument");
+  cudaSetDevice(c->dev);
+  int rc = width_buffers(c);
+  if (rc) return rc;
+  // d_wpart: the node values (N), then the cell values (NC)
+  double* nd = c->d_wpart;
+  double* cd = c->d_wpart + c->N;
+  cudaError_t e = copy_in(c, cd, cellv, c->NC);
+  if (e == cudaSuccess) {
+    cell_to_node_kernel<<<(int)std::min<int64_t>((c->N + 255) / 256, (int64_t)c->nsm * 16), 256, 0,
+                          c->stream>>>(cd, nd, c->nx, c->ny, c->nz, c->lx, c->ly, c->lz);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = copy_out(c, nodev, nd, c->N);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_cell_to_node");
+  return VFGPU_OK;
+}
+
 int vfgpu_fracture_well_rate(vfgpu_ctx* c, const double* regrate, double* rate) {
   if (!c || !regrate || !rate) return fail(VFGPU_ERR_INVALID, "vfgpu_fracture_well_rate: null argument");
   cudaSetDevice(c->dev);
   int rc = width_buffers(c);
   if (rc) return rc;
-  // d_wpart: the nodal rate (N), the block partials, the sum
+  // d_wpart: the nodal rate (N), (NC unused), the block partials, the sum
   double* r = c->d_wpart;
-  double* partial = c->d_wpart + c->N;
+  double* partial = c->d_wpart + c->N + c->NC;
   double* out = partial + kRateBlocks;
   cudaError_t e = copy_in(c, r, regrate, c->N);
   if (e == cudaSuccess) {

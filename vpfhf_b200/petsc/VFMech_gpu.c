@@ -1,19 +1,20 @@
 /*
  * VFMech_gpu.c -- drop-in replacements of the mechanics entry points of VPFHF
- * (VFMech.h:21-24: VF_StepU, VF_StepV, VF_UEnergy3D, VF_VEnergy3D) that run on a
- * B200 through the vfgpu C ABI (include/vfgpu.h).
+ * (VFMech.h:21-24: VF_StepU, VF_StepV, VF_UEnergy3D, VF_VEnergy3D) and of the
+ * flow-coupling boundary (VFPermfield.h: VolumetricCrackOpening, VolumetricFractureWellRate,
+ * UpdateFractureWidth) that run on a B200 through the vfgpu C ABI (include/vfgpu.h).
  *
  * Build it into VPFHF instead of VFMech.c's versions of these four functions
  * (see INTEGRATION.md): the callers (VPFHF.c, VFCommon.c:1166-1231 and the
  * ValidationTests drivers) link unchanged.  One MPI rank per GPU problem: the
- * DMDA must not be distributed (comm size 1).  Paths the GPU build does not
- * cover (in-situ tractions, UNILATERAL_NOCOMPRESSION) are refused with
- * PETSC_ERR_SUP instead of being silently skipped.
+ * DMDA must not be distributed (comm size 1); in-situ tractions and
+ * UNILATERAL_NOCOMPRESSION are passed on to the device problem.
  */
 #include "petsc.h"
 #include "VFCartFE.h"
 #include "VFCommon.h"
 #include "VFMech.h"
+#include "VFPermfield.h"
 #include "vfgpu.h"
 
 /* one device problem per VFCtx (VFCtx is the application's singleton in practice) */
@@ -216,5 +217,75 @@ PetscErrorCode VF_VEnergy3D(PetscReal *SurfaceEnergy, VFFields *fields, VFCtx *c
   ierr = push(fields->V, VFGPU_FIELD_V);CHKERRQ(ierr);
   VFGPU_CHK(vfgpu_v_energy(gpu_ctx, &s));
   *SurfaceEnergy = s;
+  PetscFunctionReturn(0);
+}
+
+/* ---- flow-coupling boundary: drop-in replacements of VFPermfield.h:32 and :36 (build
+ * them instead of VFPermfield.c's versions).  fields->widthc and fields->pmult are cell
+ * vectors (daScalCell), fields->width a node vector (daScal), as UpdateFractureWidth
+ * fills them (VFPermfield.c:267-562). ---- */
+PetscErrorCode UpdateFractureWidth(VFCtx *ctx, VFFields *fields) {
+  PetscErrorCode ierr;
+  PetscScalar *wc, *wn, *pm;
+  vfgpu_width_opts o;
+  int nstall = 0;
+  PetscFunctionBegin;
+  ierr = vfgpu_setup(ctx);CHKERRQ(ierr);
+  ierr = push(fields->U, VFGPU_FIELD_U);CHKERRQ(ierr);
+  ierr = push(fields->V, VFGPU_FIELD_V);CHKERRQ(ierr);
+  vfgpu_default_width_opts(&o);
+  o.int_length = ctx->WidthIntLenght;
+  o.width_tol = ctx->width_tol;
+  o.remove_tip_effect = ctx->removeTipEffect ? 1 : 0;
+  ierr = VecGetArray(fields->widthc, &wc);CHKERRQ(ierr);
+  ierr = VecGetArray(fields->width, &wn);CHKERRQ(ierr);
+  ierr = VecGetArray(fields->pmult, &pm);CHKERRQ(ierr);
+  VFGPU_CHK(vfgpu_update_fracture_width(gpu_ctx, &o, (double *)wc, (double *)wn, (double *)pm,
+                                        &nstall));
+  ierr = VecRestoreArray(fields->pmult, &pm);CHKERRQ(ierr);
+  ierr = VecRestoreArray(fields->width, &wn);CHKERRQ(ierr);
+  ierr = VecRestoreArray(fields->widthc, &wc);CHKERRQ(ierr);
+  if (nstall) {
+    ierr = PetscPrintf(PETSC_COMM_WORLD,
+                       "      vfgpu: %d band cells with zero grad V at the centre kept width 0\n",
+                       nstall);CHKERRQ(ierr);
+  }
+  PetscFunctionReturn(0);
+}
+
+/* VolumetricCrackOpening (VFPermfield.c:75-152): the total and fields->VolCrackOpening,
+ * the node average of the per-cell opening. */
+PetscErrorCode VolumetricCrackOpening(PetscReal *CrackVolume, VFCtx *ctx, VFFields *fields) {
+  PetscErrorCode ierr;
+  PetscInt nx, ny, nz;
+  PetscScalar *nodev;
+  double cov = 0., *cellv = NULL;
+  PetscFunctionBegin;
+  ierr = vfgpu_setup(ctx);CHKERRQ(ierr);
+  ierr = push(fields->U, VFGPU_FIELD_U);CHKERRQ(ierr);
+  ierr = push(fields->V, VFGPU_FIELD_V);CHKERRQ(ierr);
+  ierr = DMDAGetInfo(ctx->daVect, NULL, &nx, &ny, &nz, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
+                     NULL, NULL);CHKERRQ(ierr);
+  ierr = PetscMalloc((size_t)(nx - 1) * (ny - 1) * (nz - 1) * sizeof(double), &cellv);CHKERRQ(ierr);
+  VFGPU_CHK(vfgpu_crack_opening(gpu_ctx, &cov, cellv));
+  ierr = VecGetArray(fields->VolCrackOpening, &nodev);CHKERRQ(ierr);
+  VFGPU_CHK(vfgpu_cell_to_node(gpu_ctx, cellv, (double *)nodev));
+  ierr = VecRestoreArray(fields->VolCrackOpening, &nodev);CHKERRQ(ierr);
+  ierr = PetscFree(cellv);CHKERRQ(ierr);
+  *CrackVolume = cov;
+  PetscFunctionReturn(0);
+}
+
+PetscErrorCode VolumetricFractureWellRate(PetscReal *InjectedVolume, VFCtx *ctx, VFFields *fields) {
+  PetscErrorCode ierr;
+  const PetscScalar *r;
+  double rate = 0.;
+  PetscFunctionBegin;
+  ierr = vfgpu_setup(ctx);CHKERRQ(ierr);
+  ierr = push(fields->V, VFGPU_FIELD_V);CHKERRQ(ierr);
+  ierr = VecGetArrayRead(ctx->RegFracWellFlowRate, &r);CHKERRQ(ierr);
+  VFGPU_CHK(vfgpu_fracture_well_rate(gpu_ctx, (const double *)r, &rate));
+  ierr = VecRestoreArrayRead(ctx->RegFracWellFlowRate, &r);CHKERRQ(ierr);
+  *InjectedVolume = rate;
   PetscFunctionReturn(0);
 }
