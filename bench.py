@@ -291,7 +291,12 @@ def run_gpu(args):
     nodes, cells = ctx.N, (n - 1) ** 3
     # algorithmic traffic per apply: read u (24 B) + v (8 B), write y (24 B) per node
     alg_bytes = 56.0 * nodes
-    ops_el = 1400  # arithmetic operations per element of the modal apply (u_apply.cuh)
+    # FP64 instructions per element of the modal apply, counted by ncu on this workload
+    # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells:
+    # profiles/u_apply_fp64_129_instructions.md); an FMA is 2 flops
+    dfma_el, dadd_el, dmul_el = 412.2, 344.1, 325.5
+    instr_el = dfma_el + dadd_el + dmul_el
+    flops_el = 2 * dfma_el + dadd_el + dmul_el
     f64_peak = fp_peak_tflops(torch, "f64")
     value = N3 * world / (ms64 * 1e-3) / 1e9
     line = {
@@ -315,16 +320,22 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (ms64 * 1e-3) / 1e9, 1),
                      "peak": hbm, "unit": "GB/s",
                      "frac": round(alg_bytes / (ms64 * 1e-3) / 1e9 / hbm, 4),
-                     "traffic": None,
-                     "note": "compute-bound operator; see compute_roofline"},
+                     "traffic": 93.3e6 if n == N_EDGE else None,
+                     "note": "FP64-pipe-bound operator (see compute_roofline); traffic: ncu "
+                             "dram read+write per launch at 129^3 (74.1 + 19.2 MB; part of the "
+                             "51.5 MB output is still in the 126 MB L2 when the launch ends)"},
         "compute_roofline": {
             "pipe": "fp64 CUDA cores",
-            "ops_per_element": ops_el,
-            "achieved_tops": round(cells * ops_el / (ms64 * 1e-3) / 1e12, 3),
-            "peak_tops_measured": f64_peak,
-            "frac": (round(cells * ops_el / (ms64 * 1e-3) / 1e12 / f64_peak, 3)
-                     if f64_peak else None),
-            "per_gauss_point_equiv_tflops": round(cells * 8856 / (ms64 * 1e-3) / 1e12, 2)},
+            "fp64_instructions_per_element": {"dfma": dfma_el, "dadd": dadd_el, "dmul": dmul_el},
+            "flops_per_element": round(flops_el, 1),
+            "achieved_tflops": round(cells * flops_el / (ms64 * 1e-3) / 1e12, 3),
+            "peak_tflops_measured": f64_peak,
+            "frac_flops": (round(cells * flops_el / (ms64 * 1e-3) / 1e12 / f64_peak, 3)
+                           if f64_peak else None),
+            "fp64_pipe_issue_frac": (round(cells * instr_el / (ms64 * 1e-3) / 1e12 / (f64_peak / 2), 3)
+                                     if f64_peak else None),
+            "note": "frac_flops counts DADD/DMUL as 1 flop; fp64_pipe_issue_frac = FP64 "
+                    "instructions issued / (measured DFMA rate), the pipe's occupancy"},
         "mixed": {"value": round(N3 * world / (ms32 * 1e-3) / 1e9, 3), "unit": "GDOF/s",
                   "ms_per_step": round(ms32, 4), "dtype": "f32"},
         "am_steps_per_s": {**{k: round(1.0 / am[k]["s_per_step"], 3) for k in am},
