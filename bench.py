@@ -294,7 +294,7 @@ def run_gpu(args):
     # FP64 instructions per element of the modal apply, counted by ncu on this workload
     # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells:
     # profiles/u_apply_fp64_129_instructions.md); an FMA is 2 flops
-    dfma_el, dadd_el, dmul_el = 412.2, 344.1, 325.5
+    dfma_el, dadd_el, dmul_el = 310.4, 405.6, 208.9
     instr_el = dfma_el + dadd_el + dmul_el
     flops_el = 2 * dfma_el + dadd_el + dmul_el
     f64_peak = fp_peak_tflops(torch, "f64")
@@ -320,9 +320,9 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (ms64 * 1e-3) / 1e9, 1),
                      "peak": hbm, "unit": "GB/s",
                      "frac": round(alg_bytes / (ms64 * 1e-3) / 1e9 / hbm, 4),
-                     "traffic": 93.3e6 if n == N_EDGE else None,
+                     "traffic": 95.3e6 if n == N_EDGE else None,
                      "note": "FP64-pipe-bound operator (see compute_roofline); traffic: ncu "
-                             "dram read+write per launch at 129^3 (74.1 + 19.2 MB; part of the "
+                             "dram read+write per launch at 129^3 (74.0 + 21.3 MB; part of the "
                              "51.5 MB output is still in the 126 MB L2 when the launch ends)"},
         "compute_roofline": {
             "pipe": "fp64 CUDA cores",

@@ -174,6 +174,101 @@ def u_element(xn, vn, lam, mu, eta, h):
     return y
 
 
+def modal8s(f):
+    """modal8 without the halvings: m'[p] = 2^(3 - popcount p) m[p]."""
+    a = np.empty(8)
+    b = np.empty(8)
+    m = np.empty(8)
+    for p in range(4):
+        a[2 * p] = f[2 * p] + f[2 * p + 1]
+        a[2 * p + 1] = f[2 * p + 1] - f[2 * p]
+    for k in range(2):
+        for al in range(2):
+            lo, hi = a[al + 4 * k], a[al + 2 + 4 * k]
+            b[al + 4 * k] = lo + hi
+            b[al + 2 + 4 * k] = hi - lo
+    for q in range(4):
+        lo, hi = b[q], b[q + 4]
+        m[q] = lo + hi
+        m[q + 4] = hi - lo
+    return m
+
+
+def u_element_sums(xn, vn, lam, mu, eta, h, cubic=False):
+    """The arithmetic of u_element<T, CUBIC> in u_apply.cuh: the row closed form of
+    u_element on the modal sums in the doubled coordinate 2t (gradient column d =
+    G'/(4 h_d), v = v'/8, moments against 2t), with W = Wr/64 and, on cubic cells,
+    every 1/(4h) folded into W."""
+    ihx, ihy, ihz = 1 / h[0], 1 / h[1], 1 / h[2]
+    vol = h[0] * h[1] * h[2]
+    assert not cubic or (ihx == ihy == ihz)
+    m = [modal8s(xn[:, c]) for c in range(3)]
+    mv = modal8s(vn)
+    T2 = [2 * t for t in GT]
+    sx, sy, sz = (1.0, 1.0, 1.0) if cubic else (ihx / 4, ihy / 4, ihz / 4)
+    wsc = vol * ihx * ihx / 1024 if cubic else vol / 64
+    QX = np.zeros((3, 4))
+    QY = np.zeros((3, 4))
+    QZ = np.zeros((3, 4))
+    SZ0 = np.zeros((3, 3))
+    SZ1 = np.zeros((3, 3))
+
+    def D(G):
+        tr = G[0, 0] + G[1, 1] + G[2, 2]
+        return lam * tr * np.eye(3) + mu * (G + G.T)
+
+    for gz in range(3):
+        tz = T2[gz]
+        SY0 = np.zeros(3)
+        SY1 = np.zeros(3)
+        for gy in range(3):
+            ty = T2[gy]
+            G0 = np.zeros((3, 3))
+            G1 = np.zeros((3, 3))
+            for c in range(3):
+                ax = (m[c][1] + m[c][5] * tz) * sx
+                bx = (m[c][3] + m[c][7] * tz) * sx
+                G0[c, 0] = ax + bx * ty
+                G0[c, 1] = (m[c][2] + m[c][6] * tz) * sy
+                G1[c, 1] = (m[c][3] + m[c][7] * tz) * sy
+                G0[c, 2] = (m[c][4] + m[c][6] * ty) * sz
+                G1[c, 2] = (m[c][5] + m[c][7] * ty) * sz
+            p0, p1 = mv[0] + mv[4] * tz, mv[1] + mv[5] * tz
+            p2, p3 = mv[2] + mv[6] * tz, mv[3] + mv[7] * tz
+            q0, q1 = p0 + p2 * ty, p1 + p3 * ty
+            A0, A2, H1 = q0 * q0 + 64 * eta, q1 * q1, q0 * q1
+            W = wsc * GW[gz] * GW[gy]
+            C0, C1, E1 = W * (A0 + A2 / 3), W * 2 * H1 / 3, W * (A0 + 0.6 * A2) / 3
+            d, e = D(G0), D(G1)
+            n = C0 * d + C1 * e
+            o = C1 * d + E1 * e
+            for c in range(3):
+                QX[c] += n[c, 0] * np.array([1, ty, tz, ty * tz])
+            SY0 += n[:, 1]
+            SY1 += o[:, 1]
+            SZ0[:, gy] += n[:, 2]
+            SZ1[:, gy] += o[:, 2]
+        for c in range(3):
+            QY[c] += np.array([SY0[c], SY1[c], tz * SY0[c], tz * SY1[c]])
+    for gy in range(3):
+        for c in range(3):
+            QZ[c] += np.array([SZ0[c, gy], SZ1[c, gy], T2[gy] * SZ0[c, gy], T2[gy] * SZ1[c, gy]])
+
+    # monomial coefficients in (s_i, s_j, s_k), then the signed 8-point butterfly
+    y = np.zeros((8, 3))
+    for c in range(3):
+        w = np.zeros(8)
+        w[1], w[2], w[4] = QX[c][0] * sx, QY[c][0] * sy, QZ[c][0] * sz
+        w[3] = QX[c][1] * sx + QY[c][1] * sy
+        w[5] = QX[c][2] * sx + QZ[c][1] * sz
+        w[6] = QY[c][2] * sy + QZ[c][2] * sz
+        w[7] = QX[c][3] * sx + QY[c][3] * sy + QZ[c][3] * sz
+        for a in range(8):
+            s = [1 if (a >> b) & 1 else -1 for b in range(3)]
+            y[a, c] = sum(w[p] * np.prod([s[b] for b in range(3) if (p >> b) & 1]) for p in range(1, 8))
+    return y
+
+
 def plan(nx, ny, nz, TY, zc):
     ntx = -(-(nx - 1) // 32)
     nty = -(-(ny - 1) // TY)

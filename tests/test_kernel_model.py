@@ -13,9 +13,23 @@ def test_modal_element_matches_element_matrix(oracle_mod):
     for _ in range(4):
         v, x = rng.uniform(0, 1, 8), rng.standard_normal(24)
         yref = o.u_element_matrix(0, 0, 0, v) @ x
-        for f in (km.u_element, km.u_element_points):
+        for f in (km.u_element, km.u_element_points, km.u_element_sums):
             y = f(x.reshape(8, 3), v, lam, mu, 1e-3, (0.3, 0.5, 0.7)).reshape(24)
             assert np.abs(y - yref).max() <= 1e-14 * np.abs(yref).max()
+
+
+def test_modal_sum_element_cubic(oracle_mod):
+    """The cubic-cell variant of the sum-mode element (every 1/h in the row weight)."""
+    rng = np.random.default_rng(4)
+    h = 0.25
+    o = oracle_mod.Oracle((2, 2, 2), (h, h, h), E=2.0, nu=0.3, eta=1e-3)
+    lam, mu = 2.0 * 0.3 / 1.3 / 0.4, 2.0 / 1.3 * 0.5
+    for _ in range(4):
+        v, x = rng.uniform(0, 1, 8), rng.standard_normal(24)
+        yref = o.u_element_matrix(0, 0, 0, v) @ x
+        for cubic in (False, True):
+            y = km.u_element_sums(x.reshape(8, 3), v, lam, mu, 1e-3, (h, h, h), cubic=cubic)
+            assert np.abs(y.reshape(24) - yref).max() <= 1e-14 * np.abs(yref).max()
 
 
 @pytest.mark.parametrize("n,TY,zc", [((37, 21, 13), 8, 5), ((34, 10, 7), 4, 3), ((3, 2, 4), 8, 2)])

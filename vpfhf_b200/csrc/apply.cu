@@ -23,12 +23,18 @@ constexpr bool kU32Packed = VFGPU_U32_PACKED != 0;
 constexpr int U32_TY = kU32Packed ? VFGPU_U32_PACKED_TY : U_TY;
 constexpr int U32_MINB = kU32Packed ? (VFGPU_U32_PACKED_TY == 16 ? 1 : 2) : 2;
 using U32Op = std::conditional_t<kU32Packed, UOpF2, UOp<float>>;
+using U32OpC = std::conditional_t<kU32Packed, UOpF2, UOp<float, true>>;
+
+// Cubic cells take the U element with every 1/h folded into the row weight.
+template <typename T> bool cubic(const UApplyArgs<T>& A) { return A.ihx == A.ihy && A.ihy == A.ihz; }
 
 cudaError_t apply_kernel_attributes() {
   static std::mutex m;  // contexts may be created from several threads
   std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<float>, U_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();
@@ -48,6 +54,7 @@ template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
   if (A.cflag) return launch_tile_apply<UOpNC<double>, U_TY, 1>(A, p, L, s);
+  if (cubic(A)) return launch_tile_apply<UOp<double, true>, U_TY, 1>(A, p, L, s);
   return launch_tile_apply<UOp<double>, U_TY, 1>(A, p, L, s);
 }
 template <>
@@ -56,6 +63,7 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
   // NOCOMPRESSION needs the scalar layout: its plan is the FP32 plan only with the
   // scalar tile (the packed build option keeps the plain operator packed)
   if (A.cflag) return launch_tile_apply<UOpNC<float>, U_TY, 2>(A, p, L, s);
+  if (cubic(A)) return launch_tile_apply<U32OpC, U32_TY, U32_MINB>(A, p, L, s);
   return launch_tile_apply<U32Op, U32_TY, U32_MINB>(A, p, L, s);
 }
 template <>

@@ -18,7 +18,8 @@
 
 namespace vfgpu {
 
-template <typename T_> struct UOp {
+// CUBIC: hx = hy = hz, every 1/h factor folds into the row weight (u_element).
+template <typename T_, bool CUBIC = false> struct UOp {
   using T = T_;
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4, EPT = 1;
@@ -51,7 +52,7 @@ template <typename T_> struct UOp {
       lam = T(LT.lambda[layer]);
       mu = T(LT.mu[layer]);
     }
-    u_element<T>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+    u_element<T, CUBIC>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   // Writes y of node n (Dirichlet rows: y = x); with DOT, returns x.y over its dofs
   // (the launch accumulates the CG dot into A.dot).

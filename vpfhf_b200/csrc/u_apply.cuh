@@ -117,6 +117,46 @@ __device__ __forceinline__ T signed_sum3(T a0, T a1, T a2, int i, int j, int k) 
   return k ? a2 - (a0 + a1) : -((a0 + a1) + a2);
 }
 
+// Modal sums: modal8 without the halvings, m'[p] = 2^(3 - popcount p) m[p] exactly
+// (every intermediate is the mean form scaled by a power of two).
+template <typename T>
+__device__ __forceinline__ void modal8s(const T (&f)[8], T (&m)[8]) {
+  T a[8], b[8];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    a[2 * p] = f[2 * p] + f[2 * p + 1];
+    a[2 * p + 1] = f[2 * p + 1] - f[2 * p];
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int al = 0; al < 2; al++) {
+      T lo = a[al + 4 * k], hi = a[al + 2 + 4 * k];
+      b[al + 4 * k] = lo + hi;
+      b[al + 2 + 4 * k] = hi - lo;
+    }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    T lo = b[q], hi = b[q + 4];
+    m[q] = lo + hi;
+    m[q + 4] = hi - lo;
+  }
+}
+
+// a + b (2 t_g): the polynomials of the modal sums in the doubled coordinate 2t.
+template <typename T> __device__ __forceinline__ T lin2(int g, T a, T b) {
+  return g == 1 ? a : (g == 0 ? fma(b, T(-2 * VF_TAU), a) : fma(b, T(2 * VF_TAU), a));
+}
+
+// q[0..3] += s * {1, 2t1, 2t2, 4 t1 t2} for Gauss indices (g1, g2).
+template <typename T>
+__device__ __forceinline__ void moment4s(T (&q)[4], int g1, int g2, T s) {
+  q[0] += s;
+  if (g1 != 1) q[1] = fma(T(2 * gtd(g1)), s, q[1]);
+  if (g2 != 1) q[2] = fma(T(2 * gtd(g2)), s, q[2]);
+  if (g1 != 1 && g2 != 1) q[3] = fma(T(4 * gtd(g1) * gtd(g2)), s, q[3]);
+}
+
 // y[a][c] = (K_e(v) x_e)[a][c] for one element.
 //
 // Along a Gauss row (fixed gy, gz) the gradient is G(t) = G0 + t G1 in t = tx, with
@@ -128,7 +168,18 @@ __device__ __forceinline__ T signed_sum3(T a0, T a1, T a2, int i, int j, int k) 
 // follow from sum w_x = 1, sum w_x t^2 = 1/12, sum w_x t^4 = 1/80 (the odd sums
 // vanish): the same 3-point Gauss sum as point by point, in about 2/3 of the
 // operations.  Wr = vol w_y w_z.
-template <typename T>
+//
+// Scaling.  The element works on the modal sums (modal8s) in the doubled coordinate
+// 2t, where the gradient column d is exactly G'/(4 h_d) and v is v'/8; the moments
+// are taken against 2t as well (Q1' = 2 Q1, Q3' = 4 Q3), so the inverse butterfly
+// needs no halvings either and node values are (Q0 +- Q1' +- Q2' +- Q3')/(4 h_d).
+// With A0 = q0'^2 + 64 eta, A2 = q1'^2, H1 = q0' q1' (q0' + 2t q1' = 8 v along the
+// row) the row scalars are C0 = W (A0 + A2/3), C1 = W 2 H1/3, E1 = W (A0 + 0.6 A2)/3
+// with W = Wr/64, and M0, 2 M1 = C0 D0' + C1 D1', C1 D0' + E1 D1' (D1' = D(G1)/2).
+// On cubic cells (CUBIC) every 1/(4h) factor is the same, so they all fold into W
+// (W = Wr/(1024 h^2)); otherwise the gradient columns and the node values carry
+// their own ih_d/4.  All the dropped halvings are powers of two: exact.
+template <typename T, bool CUBIC = false>
 __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
                                           T eta, T ihx, T ihy, T ihz, T vol, T (&y)[8][3]) {
   T m[3][8], mv[8];
@@ -137,38 +188,43 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
     T f[8];
 #pragma unroll
     for (int a = 0; a < 8; a++) f[a] = xn[a][c];
-    modal8(f, m[c]);
+    modal8s(f, m[c]);
   }
-  modal8(vn, mv);
-  // Gradients from the 7 difference modes of each component (m[c][0] is unused):
-  //   d/dx u_c = (m1 + m3 ty + m5 tz + m7 ty tz)/hx, d/dy u_c = (m2 + m3 tx + m6 tz + m7 tx tz)/hy,
-  //   d/dz u_c = (m4 + m5 tx + m6 ty + m7 tx ty)/hz; the 1/h scaling is applied per plane/row
-  //   so only 21 coefficients stay live.
+  modal8s(vn, mv);
   // QX, QY, QZ: the 4 bilinear moments per component of the x, y, z stress columns.
-  // SY0/SY1: M0/M1 of the y column summed over the rows of a plane; SZ0/SZ1[c][gy]:
-  // M0/M1 of the z column summed over the planes, per row index.
+  // SY0/SY1: M0/2M1 of the y column summed over the rows of a plane; SZ0/SZ1[c][gy]:
+  // M0/2M1 of the z column summed over the planes, per row index.
   T QX[3][4], QY[3][4], QZ[3][4], SZ0[3][3], SZ1[3][3];
 #pragma unroll
   for (int c = 0; c < 3; c++)
 #pragma unroll
     for (int q = 0; q < 4; q++) QX[c][q] = QY[c][q] = QZ[c][q] = T(0);
-  const T mu2 = T(2) * mu;
+  const T mu2 = T(2) * mu, eta64 = T(64) * eta;
+  const T sx = T(0.25) * ihx, sy = T(0.25) * ihy, sz = T(0.25) * ihz;
+  const T wsc = CUBIC ? vol * (ihx * ihx) * T(1.0 / 1024.0) : vol * T(1.0 / 64.0);
 
 #pragma unroll
   for (int gz = 0; gz < 3; gz++) {
-    const T volw = vol * gw<T>(gz);
+    const T volw = wsc * gw<T>(gz);
     T ax[3], bx[3], ay[3], by[3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const T t37 = lin(gz, m[c][3], m[c][7]);
-      ax[c] = lin(gz, m[c][1], m[c][5]) * ihx;
-      bx[c] = t37 * ihx;
-      ay[c] = lin(gz, m[c][2], m[c][6]) * ihy;
-      by[c] = t37 * ihy;
+      const T t37 = lin2(gz, m[c][3], m[c][7]);
+      if (CUBIC) {
+        ax[c] = lin2(gz, m[c][1], m[c][5]);
+        bx[c] = t37;
+        ay[c] = lin2(gz, m[c][2], m[c][6]);
+        by[c] = t37;
+      } else {
+        ax[c] = lin2(gz, m[c][1], m[c][5]) * sx;
+        bx[c] = t37 * sx;
+        ay[c] = lin2(gz, m[c][2], m[c][6]) * sy;
+        by[c] = t37 * sy;
+      }
     }
-    const T p0 = lin(gz, mv[0], mv[4]), p1 = lin(gz, mv[1], mv[5]);
-    const T p2 = lin(gz, mv[2], mv[6]), p3 = lin(gz, mv[3], mv[7]);
-    // D1 = D(G1), G1 = [0 | by | be]: the y part is constant over the plane
+    const T p0 = lin2(gz, mv[0], mv[4]), p1 = lin2(gz, mv[1], mv[5]);
+    const T p2 = lin2(gz, mv[2], mv[6]), p3 = lin2(gz, mv[3], mv[7]);
+    // D1' = D(G1') with G1' = [0 | by | be]: the y part is constant over the plane
     const T e01y = mu * by[0];
     T SY0[3], SY1[3];
 #pragma unroll
@@ -176,35 +232,37 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
       T Gx[3], al[3], be[3];
 #pragma unroll
       for (int c = 0; c < 3; c++) {
-        Gx[c] = lin(gy, ax[c], bx[c]);
-        al[c] = lin(gy, m[c][4], m[c][6]) * ihz;
-        be[c] = lin(gy, m[c][5], m[c][7]) * ihz;
+        Gx[c] = lin2(gy, ax[c], bx[c]);
+        al[c] = lin2(gy, m[c][4], m[c][6]);
+        be[c] = lin2(gy, m[c][5], m[c][7]);
+        if (!CUBIC) {
+          al[c] = al[c] * sz;
+          be[c] = be[c] * sz;
+        }
       }
-      const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
-      // v^2 + eta = a0 + 2 h1 t + a2 t^2 along the row; row weights
-      const T Wr = volw * gw<T>(gy);
-      const T a0 = fma(q0, q0, eta), a2 = q1 * q1, h1 = q0 * q1;
-      const T C0 = Wr * fma(a2, T(1.0 / 12.0), a0);
-      const T C1 = Wr * (h1 * T(1.0 / 6.0));
-      const T E1 = Wr * (fma(a2, T(0.15), a0) * T(1.0 / 12.0));
-      // D0 = D(G0), G0 = [Gx | ay | al]
+      const T q0 = lin2(gy, p0, p2), q1 = lin2(gy, p1, p3);
+      const T A0 = fma(q0, q0, eta64), A2 = q1 * q1, H1 = q0 * q1;
+      const T C0 = (volw * T(gwd(gy))) * fma(A2, T(1.0 / 3.0), A0);
+      const T C1 = (volw * T(gwd(gy) * (2.0 / 3.0))) * H1;
+      const T E1 = (volw * T(gwd(gy) * (1.0 / 3.0))) * fma(A2, T(0.6), A0);
+      // D0' = D(G0'), G0' = [Gx | ay | al]
       const T L0 = lam * ((Gx[0] + ay[1]) + al[2]);
       const T d00 = fma(mu2, Gx[0], L0), d11 = fma(mu2, ay[1], L0), d22 = fma(mu2, al[2], L0);
       const T d01 = mu * (ay[0] + Gx[1]), d02 = mu * (al[0] + Gx[2]), d12 = mu * (al[1] + ay[2]);
-      // D1 = D(G1)
+      // D1'
       const T L1 = lam * (by[1] + be[2]);
       const T e11 = fma(mu2, by[1], L1), e22 = fma(mu2, be[2], L1);
       const T e02 = mu * be[0], e12 = mu * (be[1] + by[2]);
-      // M0 of the 6 stress components, M1 of the 5 the y and z columns need
+      // M0 of the 6 stress components, 2 M1 of the 5 the y and z columns need
       const T n00 = fma(C0, d00, C1 * L1), n01 = fma(C0, d01, C1 * e01y);
       const T n02 = fma(C0, d02, C1 * e02), n11 = fma(C0, d11, C1 * e11);
       const T n12 = fma(C0, d12, C1 * e12), n22 = fma(C0, d22, C1 * e22);
       const T o01 = fma(C1, d01, E1 * e01y), o02 = fma(C1, d02, E1 * e02);
       const T o11 = fma(C1, d11, E1 * e11), o12 = fma(C1, d12, E1 * e12);
       const T o22 = fma(C1, d22, E1 * e22);
-      moment4(QX[0], gy, gz, n00);
-      moment4(QX[1], gy, gz, n01);
-      moment4(QX[2], gy, gz, n02);
+      moment4s(QX[0], gy, gz, n00);
+      moment4s(QX[1], gy, gz, n01);
+      moment4s(QX[2], gy, gz, n02);
       if (gy == 0) {
         SY0[0] = n01; SY0[1] = n11; SY0[2] = n12;
         SY1[0] = o01; SY1[1] = o11; SY1[2] = o12;
@@ -220,18 +278,18 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
         SZ1[0][gy] += o02; SZ1[1][gy] += o12; SZ1[2][gy] += o22;
       }
     }
-    // QY moments {1, tx, tz, tx tz}: the tx moment is M1
+    // QY moments {1, 2tx, 2tz, 4 tx tz}: the 2tx moment is 2 M1
 #pragma unroll
     for (int c = 0; c < 3; c++) {
       QY[c][0] += SY0[c];
       QY[c][1] += SY1[c];
       if (gz != 1) {
-        QY[c][2] = fma(gt<T>(gz), SY0[c], QY[c][2]);
-        QY[c][3] = fma(gt<T>(gz), SY1[c], QY[c][3]);
+        QY[c][2] = fma(T(2 * gtd(gz)), SY0[c], QY[c][2]);
+        QY[c][3] = fma(T(2 * gtd(gz)), SY1[c], QY[c][3]);
       }
     }
   }
-  // QZ moments {1, tx, ty, tx ty}
+  // QZ moments {1, 2tx, 2ty, 4 tx ty}
 #pragma unroll
   for (int gy = 0; gy < 3; gy++)
 #pragma unroll
@@ -239,26 +297,62 @@ __device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8],
       QZ[c][0] += SZ0[c][gy];
       QZ[c][1] += SZ1[c][gy];
       if (gy != 1) {
-        QZ[c][2] = fma(gt<T>(gy), SZ0[c][gy], QZ[c][2]);
-        QZ[c][3] = fma(gt<T>(gy), SZ1[c][gy], QZ[c][3]);
+        QZ[c][2] = fma(T(2 * gtd(gy)), SZ0[c][gy], QZ[c][2]);
+        QZ[c][3] = fma(T(2 * gtd(gy)), SZ1[c][gy], QZ[c][3]);
       }
     }
 
-  // Inverse butterfly: direction-d part of node (i,j,k) is
-  //   s_d/h_d * (Q0/4 + s_1 Q1/2 + s_2 Q2/2 + s_1 s_2 Q3), s = -1 (node 0) or +1 (node 1).
+  // Back to the nodes.  The direction-d part of node (i,j,k) is
+  //   s_d (Q0 + s_1 Q1' + s_2 Q2' + s_1 s_2 Q3') / (4 h_d), s = -1 (node 0) or +1 (node 1),
+  // so y_ijk is a polynomial in (s_i, s_j, s_k) with the monomial coefficients
+  //   s_i: QX0, s_j: QY0, s_k: QZ0, s_i s_j: QX1 + QY1, s_i s_k: QX2 + QZ1,
+  //   s_j s_k: QY2 + QZ2, s_i s_j s_k: QX3 + QY3 + QZ3 (each Q times its ih_d/4),
+  // evaluated at the 8 sign patterns by a 3-stage signed butterfly.
 #pragma unroll
   for (int c = 0; c < 3; c++) {
-    T A[3][2][2];
-    inv_butterfly(QX[c], ihx, A[0]);
-    inv_butterfly(QY[c], ihy, A[1]);
-    inv_butterfly(QZ[c], ihz, A[2]);
+    T w[8];
+    if (CUBIC) {
+      w[1] = QX[c][0];
+      w[2] = QY[c][0];
+      w[3] = QX[c][1] + QY[c][1];
+      w[4] = QZ[c][0];
+      w[5] = QX[c][2] + QZ[c][1];
+      w[6] = QY[c][2] + QZ[c][2];
+      w[7] = (QX[c][3] + QY[c][3]) + QZ[c][3];
+    } else {
+      w[1] = QX[c][0] * sx;
+      w[2] = QY[c][0] * sy;
+      w[3] = fma(QX[c][1], sx, QY[c][1] * sy);
+      w[4] = QZ[c][0] * sz;
+      w[5] = fma(QX[c][2], sx, QZ[c][1] * sz);
+      w[6] = fma(QY[c][2], sy, QZ[c][2] * sz);
+      w[7] = fma(QX[c][3], sx, fma(QY[c][3], sy, QZ[c][3] * sz));
+    }
+    // k: b[p][k] = w[p] -+ w[p + 4] (w[0] = 0)
+    T b[4][2], d[2][2][2];
+    b[0][0] = -w[4];
+    b[0][1] = w[4];
+#pragma unroll
+    for (int p = 1; p < 4; p++) {
+      b[p][0] = w[p] - w[p + 4];
+      b[p][1] = w[p] + w[p + 4];
+    }
+    // j: d[p][j][k] = b[p][k] -+ b[p + 2][k]
 #pragma unroll
     for (int k = 0; k < 2; k++)
 #pragma unroll
-      for (int j = 0; j < 2; j++)
+      for (int p = 0; p < 2; p++) {
+        d[p][0][k] = b[p][k] - b[p + 2][k];
+        d[p][1][k] = b[p][k] + b[p + 2][k];
+      }
+    // i
 #pragma unroll
-        for (int i = 0; i < 2; i++)
-          y[i + 2 * j + 4 * k][c] = signed_sum3(A[0][j][k], A[1][i][k], A[2][i][j], i, j, k);
+    for (int k = 0; k < 2; k++)
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        y[2 * j + 4 * k][c] = d[0][j][k] - d[1][j][k];
+        y[1 + 2 * j + 4 * k][c] = d[0][j][k] + d[1][j][k];
+      }
   }
 }
 
