@@ -80,6 +80,7 @@ struct vfgpu_ctx {
     vfgpu::TilePlan plan{};
     void* seam = nullptr;                      // V-cycle precision
     void *x = nullptr, *b = nullptr, *r = nullptr, *d = nullptr, *t = nullptr;  // 3N each
+    void* ev = nullptr;                        // 3N: the power iteration's vector, kept
     void *v = nullptr, *dinv = nullptr;        // coarse phase field (N), inverse diagonal (3N)
     double* v64 = nullptr;                     // coarse phase field in FP64 (the diagonal's input)
     uint8_t *bc = nullptr, *elayer = nullptr;
@@ -90,6 +91,7 @@ struct vfgpu_ctx {
   std::vector<MGLevel> mg;
   int mg_bytes = 0;
   bool mg_ready = false;          // coarse fields, diagonals and eigenvalue bounds are current
+  bool mg_ev = false;             // the levels' ev vectors hold earlier eigenvector estimates
   double* mg_coef = nullptr;      // 64 doubles per level (MGLevel::coef points into it)
   double* mg_z = nullptr;         // FP32 V-cycle: the preconditioned residual in FP64 (3N)
   const void* mg_dinv0 = nullptr; // fine inverse diagonal in the V-cycle's precision

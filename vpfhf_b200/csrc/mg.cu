@@ -12,7 +12,8 @@
 // mean of the 8 children.  Transfers: trilinear prolongation and its transpose
 // (full weighting), Dirichlet dofs excluded on both sides.  Smoother: Chebyshev
 // iteration of D^-1 K of degree 3 on [lmax/10, lmax] (lmax = 1.1 x the estimate of
-// 12 power iterations, per level and operator), pre and post; the coarsest level
+// 12 power iterations per level, 4 from the previous vector once there is one), pre
+// and post; the coarsest level
 // runs degree 30 on [lmax/100, lmax].  Every step is a fixed sequence of
 // deterministic kernels reading its Chebyshev coefficients from device memory, so
 // the V-cycle is a fixed symmetric linear operator (plain PCG applies) and is
@@ -32,7 +33,10 @@
 namespace vfgpu {
 namespace {
 
-constexpr int kSmoothDeg = 3, kCoarseDeg = 30, kPowerIts = 12;
+// Power iterations per level: from the deterministic seed at the first set-up, then
+// from the previous set-up's vector (the operator of the next StepU differs by the
+// phase field's update only).
+constexpr int kSmoothDeg = 3, kCoarseDeg = 30, kPowerIts = 12, kWarmPowerIts = 4;
 constexpr double kSmoothLo = 0.1, kCoarseLo = 0.01, kLmaxSafety = 1.1;
 constexpr int kCoefPerLevel = 64;  // [0] lmax [1] 1/theta [2..59] (c1, c2) [62..63] scratch
 constexpr int kPowBlocks = 296, kPowThreads = 256;
@@ -321,8 +325,7 @@ template <typename T> LevelT<T> view(vfgpu_ctx* c, int l) {
   return V;
 }
 
-template <typename T>
-cudaError_t level_apply(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
+template <typename T> UApplyArgs<T> level_args(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
   UApplyArgs<T> A{};
   A.x = x;
   A.v = V.v;
@@ -342,16 +345,24 @@ cudaError_t level_apply(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
   A.eta = T(c->vf.eta);
   A.P = c->d_params;
   A.cflag = V.cflag;
-  return launch_u_apply<T>(A, *V.plan, c->layers, c->stream);
+  return A;
+}
+
+template <typename T>
+cudaError_t level_apply(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
+  return launch_u_apply<T>(level_args<T>(c, V, x, y), *V.plan, c->layers, c->stream);
 }
 
 // Chebyshev iteration on D^-1 K x = D^-1 b with the level's coefficients; x updated in
-// place (zero_start: x = 0 on entry and no initial residual apply).
+// place (zero_start: x = 0 on entry and no initial residual apply).  (Carrying the
+// update in the operator's epilogue instead of a separate pass measured slower on B200:
+// StepU 257^3 0.250 s against 0.225 s mixed, 0.378 s against 0.328 s FP64 -- the extra
+// loads stall the compute-bound z-march.)
 template <typename T>
 cudaError_t chebyshev(vfgpu_ctx* c, const LevelT<T>& V, const T* b, T* x, int deg, bool zero_start) {
   const int64_t n3 = V.n3;
-  cudaError_t e = zero_start ? cudaMemsetAsync(x, 0, n3 * sizeof(T), c->stream)
-                             : level_apply<T>(c, V, x, V.t);
+  cudaError_t e =
+      zero_start ? cudaMemsetAsync(x, 0, n3 * sizeof(T), c->stream) : level_apply<T>(c, V, x, V.t);
   if (e == cudaSuccess) {
     cheb_init_kernel<T><<<blocks_for(n3), 256, 0, c->stream>>>(b, zero_start ? nullptr : V.t, V.dinv,
                                                               V.r, V.d, V.coef, n3);
@@ -429,6 +440,7 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     L0.N = c->N;
     L0.NC = c->NC;
     L0.x = dalloc<T>(n3, e);
+    L0.ev = dalloc<T>(n3, e);
     L0.r = dalloc<T>(n3, e);
     L0.d = dalloc<T>(n3, e);
     L0.t = dalloc<T>(n3, e);
@@ -458,7 +470,7 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     L.hz = hz;
     L.plan = u_plan(nx, ny, nz, (int)sizeof(T), c->nsm);
     L.seam = dalloc<T>((int64_t)(L.plan.seamX + L.plan.seamY), e);
-    for (void** p : {&L.x, &L.b, &L.r, &L.d, &L.t, &L.dinv}) *p = dalloc<T>(3 * L.N, e);
+    for (void** p : {&L.x, &L.b, &L.r, &L.d, &L.t, &L.dinv, &L.ev}) *p = dalloc<T>(3 * L.N, e);
     L.v64 = (double*)dalloc<double>(L.N, e);
     L.v = f32 ? dalloc<float>(L.N, e) : (void*)L.v64;
     L.bc = (uint8_t*)dalloc<uint8_t>(L.N, e);
@@ -532,15 +544,19 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
   for (int l = 0; l < nlev && e == cudaSuccess; l++) {
     const LevelT<T> V = view<T>(c, l);
     double* slot = V.coef + kCoefPerLevel - 2;
-    seed_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(V.x, V.bc, V.n3 / 3);
-    e = cudaGetLastError();
-    for (int it = 0; it < kPowerIts && e == cudaSuccess; it++) {
-      e = level_apply<T>(c, V, V.x, V.t);
+    T* ev = (T*)c->mg[l].ev;
+    if (!c->mg_ev) {
+      seed_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(ev, V.bc, V.n3 / 3);
+      e = cudaGetLastError();
+    }
+    const int its = c->mg_ev ? kWarmPowerIts : kPowerIts;
+    for (int it = 0; it < its && e == cudaSuccess; it++) {
+      e = level_apply<T>(c, V, ev, V.t);
       if (e == cudaSuccess) {
-        power_dots_kernel<T><<<kPowBlocks, kPowThreads, 0, c->stream>>>(V.t, V.dinv, V.d, V.x, V.n3,
+        power_dots_kernel<T><<<kPowBlocks, kPowThreads, 0, c->stream>>>(V.t, V.dinv, V.d, ev, V.n3,
                                                                        c->d_red);
         power_final_kernel<<<1, kPowThreads, 0, c->stream>>>(c->d_red, kPowBlocks, slot);
-        power_norm_kernel<T><<<blocks_for(V.n3), 256, 0, c->stream>>>(V.d, V.x, slot, V.n3);
+        power_norm_kernel<T><<<blocks_for(V.n3), 256, 0, c->stream>>>(V.d, ev, slot, V.n3);
         e = cudaGetLastError();
       }
     }
@@ -557,9 +573,12 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "multigrid eigenvalue estimate");
   for (int l = 0; l < nlev; l++)
-    if (!(coef[(size_t)kCoefPerLevel * l] > 0.) || !std::isfinite(coef[(size_t)kCoefPerLevel * l]))
+    if (!(coef[(size_t)kCoefPerLevel * l] > 0.) || !std::isfinite(coef[(size_t)kCoefPerLevel * l])) {
+      c->mg_ev = false;  // reseed next time
       return fail(VFGPU_ERR_STATE, "multigrid: no positive eigenvalue estimate on level %d", l);
+    }
   c->mg_ready = true;
+  c->mg_ev = true;
   return VFGPU_OK;
 }
 
@@ -682,7 +701,7 @@ void free_mg(vfgpu_ctx* c) {
     }
   }
   for (auto& L : c->mg) {
-    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.bc, L.elayer, L.cellE};
+    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.ev, L.bc, L.elayer, L.cellE};
     for (void* p : bufs) cudaFree(p);
     if (L.v != (void*)L.v64) cudaFree(L.v);
     cudaFree(L.v64);
@@ -694,11 +713,12 @@ void free_mg(vfgpu_ctx* c) {
   c->mg_z = nullptr;
   c->mg_bytes = 0;
   c->mg_ready = false;
+  c->mg_ev = false;
 }
 
 long long mg_memory_bytes(int nx, int ny, int nz, int bytes) {
   const long long N = (long long)nx * ny * nz;
-  long long b = 4 * 3 * N * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine work vectors
+  long long b = 5 * 3 * N * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine work vectors
   int nlev = 1;
   while ((nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 && (nx - 1) / 2 + 1 >= 5 &&
          (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
@@ -708,7 +728,7 @@ long long mg_memory_bytes(int nx, int ny, int nz, int bytes) {
     nlev++;
     const long long Nl = (long long)nx * ny * nz, NCl = (long long)(nx - 1) * (ny - 1) * (nz - 1);
     const TilePlan p = u_plan(nx, ny, nz, bytes, 148);
-    b += (long long)(p.seamX + p.seamY) * bytes + 6 * 3 * Nl * bytes + Nl * 8 +
+    b += (long long)(p.seamX + p.seamY) * bytes + 7 * 3 * Nl * bytes + Nl * 8 +
          (bytes == 4 ? Nl * 4 : 0) + Nl + (nz - 1) + NCl * 4;
   }
   if (nlev < 2) return 0;

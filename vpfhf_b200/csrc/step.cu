@@ -673,6 +673,9 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
 int vfgpu_time_step_prepare(vfgpu_ctx* c) {
   if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_time_step_prepare: null ctx");
   cudaSetDevice(c->dev);
+  // the multigrid eigenvalue estimates restart from their seed at each time step, so a
+  // time step's results do not depend on the problems a pooled ctx solved before
+  c->mg_ev = false;
   cudaError_t e = cudaMemcpyAsync(c->f[VFGPU_FIELD_VIRREV], c->f[VFGPU_FIELD_V], c->N * sizeof(double),
                                   cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess) e = dev_apply_bc(c->f[VFGPU_FIELD_U], c->bcU_kind, c->f[VFGPU_FIELD_BCU], 3 * c->N, c->stream);
