@@ -261,8 +261,8 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
       const double tr = f11 + f22 + f33;
       const double S = tr < 0. ? 0. : kappa * tr * tr * .5, D = Wf - kappa * tr * tr * .5;
       const double cgv = e.w[g] * (2. * (S + D) + mass);
-      coef[27 * cell + g] = cgv;
-      if (coef32) coef32[27 * cell + g] = (float)cgv;
+      coef[(int64_t)g * NCELL + cell] = cgv;
+      if (coef32) coef32[(int64_t)g * NCELL + cell] = (float)cgv;
       continue;
     }
     double e11 = 0, e22 = 0, e33 = 0, e12 = 0, e23 = 0, e13 = 0;
@@ -282,8 +282,8 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
     const double s33 = l * e11 + l * e22 + (l + 2. * mu) * e33;
     const double W = (s11 * e11 + s22 * e22 + s33 * e33) * .5 + 2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
     const double cgv = e.w[g] * (2. * W + mass);
-    coef[27 * cell + g] = cgv;
-    if (coef32) coef32[27 * cell + g] = (float)cgv;
+    coef[(int64_t)g * NCELL + cell] = cgv;
+    if (coef32) coef32[(int64_t)g * NCELL + cell] = (float)cgv;
   }
 }
 
@@ -332,11 +332,13 @@ __global__ void v_diag_kernel(const __grid_constant__ ElemArgs E, int color, con
   const CellMat m = cell_mat(E, ei, ej, ek);
   const double aeps = m.Gc / E.atcv * .5 * E.epsilon;
   const int64_t cell = ((int64_t)ek * (E.ny - 1) + ej) * (E.nx - 1) + ei;
+  const int64_t ncell = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
   for (int a = 0; a < 8; a++) {
     double s = 0.;
     for (int g = 0; g < 27; g++) {
       const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
-      s += aeps * e.w[g] * (d0 * d0 + d1 * d1 + d2 * d2) + coef[27 * cell + g] * e.phi[a][g] * e.phi[a][g];
+      s += aeps * e.w[g] * (d0 * d0 + d1 * d1 + d2 * d2) +
+           coef[(int64_t)g * ncell + cell] * e.phi[a][g] * e.phi[a][g];
     }
     d[n[a]] += s;
   }

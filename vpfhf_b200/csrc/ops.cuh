@@ -169,7 +169,7 @@ template <typename T> struct VApplyArgs {
                                       // masked columns drop out
   T* __restrict__ y;                  // N output
   const uint8_t* __restrict__ mask;   // N: nonzero => dof removed (y = 0); or null
-  const T* __restrict__ coef;         // 27 per cell: w_g (2 W_g [+ A/eps]), cell-major
+  const T* __restrict__ coef;         // 27 per cell: w_g (2 W_g [+ A/eps]), coef[g * ncell + cell]
   const uint8_t* __restrict__ elayer; // nz-1 or null
   T* __restrict__ seamX;
   T* __restrict__ seamY;
@@ -182,8 +182,8 @@ template <typename T> struct VApplyArgs {
 
 // y[a] = (K_V,e x_e)[a] for one element (same modal scheme as u_element).
 template <typename T>
-__device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict__ cg, T aeps,
-                                          T ihx, T ihy, T ihz, T vol, T (&y)[8]) {
+__device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict__ cg, int64_t cs,
+                                          T aeps, T ihx, T ihy, T ihz, T vol, T (&y)[8]) {
   T m[8];
   modal8(xn, m);
   const T Ax = m[1] * ihx, Bx = m[3] * ihx, Cx = m[5] * ihx, Dx = m[7] * ihx;
@@ -209,7 +209,7 @@ __device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict_
         const T Gy = lin(gx, ay, by), Gz = lin(gx, al, be), xg = lin(gx, q0, q1);
         const T wa = av * (gw<T>(gx) * gw<T>(gy) * gw<T>(gz));
         const T fx = wa * Gx, fy = wa * Gy, fz = wa * Gz;
-        const T psi = cg[g] * xg;
+        const T psi = cg[g * cs] * xg;
         SX = gx == 0 ? fx : SX + fx;
         SY[gx] = gy == 0 ? fy : SY[gx] + fy;
         SZ[gy][gx] = gz == 0 ? fz : SZ[gy][gx] + fz;
@@ -286,7 +286,8 @@ template <typename T_> struct VOp {
     for (int a = 0; a < 8; a++) xn[a] = in[a][0];
     const int layer = A.elayer ? A.elayer[ez] : 0;
     const int64_t cell = ((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex;
-    v_element<T>(xn, A.coef + 27 * cell, T(A.P->aeps[layer]), A.ihx, A.ihy, A.ihz, A.vol, yn);
+    const int64_t ncell = (int64_t)(A.nx - 1) * (A.ny - 1) * (A.nz - 1);
+    v_element<T>(xn, A.coef + cell, ncell, T(A.P->aeps[layer]), A.ihx, A.ihy, A.ihz, A.vol, yn);
 #pragma unroll
     for (int a = 0; a < 8; a++) out[a][0] = yn[a];
   }
