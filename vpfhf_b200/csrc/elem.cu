@@ -103,6 +103,240 @@ __device__ __forceinline__ void gather_u8(const int64_t (&n)[8], const double* _
     for (int c = 0; c < 3; c++) u8[a][c] = u ? u[3 * n[a] + c] : 0.;
 }
 
+// ---- tensor-product forms (the plain operator).  On the uniform grid the 27-point rule
+// is the tensor product of the 1-D rule, and every table entry is a product of 1-D
+// factors: phi_a(g) = b_k(gz) b_j(gy) b_i(gx), dphi_a,x(g) = b_k(gz) b_j(gy) (-+1/hx),
+// w_g = W_gx W_gy W_gz vol, with b_0(g) = (1 + sqrt(3/5))/2, 1/2, (1 - sqrt(3/5))/2 at
+// the three points, b_1 the mirror, W = 5/18, 8/18, 5/18 (VFCartFEElement1DInit,
+// VFCartFE.c:90-116).  So fields at the points, the integrals against products of
+// basis functions and the scatter back to the nodes are each three 1-D passes.
+constexpr double kB0 = 0.5 * (1.0 + 0.774596669241483377035853079956);  // (1 + sqrt(3/5))/2
+constexpr double kB2 = 0.5 * (1.0 - 0.774596669241483377035853079956);
+__device__ __forceinline__ constexpr double bas(int i, int g) {
+  return g == 1 ? 0.5 : ((g == 0) == (i == 0) ? kB0 : kB2);
+}
+__device__ __forceinline__ constexpr double w1(int g) { return g == 1 ? 8.0 / 18.0 : 5.0 / 18.0; }
+
+// Trilinear field at the 27 points, g = gx + 3 gy + 9 gz.
+__device__ __forceinline__ void interp27(const double (&f)[8], double (&o)[27]) {
+  double fx[4][3], fy[2][3][3];
+#pragma unroll
+  for (int jk = 0; jk < 4; jk++)
+#pragma unroll
+    for (int g = 0; g < 3; g++) fx[jk][g] = bas(0, g) * f[2 * jk] + bas(1, g) * f[2 * jk + 1];
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++)
+        fy[k][gy][gx] = bas(0, gy) * fx[2 * k][gx] + bas(1, gy) * fx[2 * k + 1][gx];
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++)
+        o[gx + 3 * gy + 9 * gz] = bas(0, gz) * fy[0][gy][gx] + bas(1, gz) * fy[1][gy][gx];
+}
+
+// out[i + 2j + 4k] = sum_g q_g b_i(gx) b_j(gy) b_k(gz)
+__device__ __forceinline__ void contract27(const double (&q)[27], double (&out)[8]) {
+  double cx[2][3][3], cy[2][2][3];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+      for (int gy = 0; gy < 3; gy++) {
+        const int b = 3 * gy + 9 * gz;
+        cx[i][gy][gz] = (bas(i, 0) * q[b] + bas(i, 1) * q[b + 1]) + bas(i, 2) * q[b + 2];
+      }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int gz = 0; gz < 3; gz++)
+        cy[i][j][gz] = (bas(j, 0) * cx[i][0][gz] + bas(j, 1) * cx[i][1][gz]) + bas(j, 2) * cx[i][2][gz];
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+        out[i + 2 * j + 4 * k] =
+            (bas(k, 0) * cy[i][j][0] + bas(k, 1) * cy[i][j][1]) + bas(k, 2) * cy[i][j][2];
+}
+
+// Integrals of q against the squared or plain basis products that carry no factor
+// along axis d: F[d][p][q] = sum_g q_g f_p(g_e1) f_q(g_e2) with (e1, e2) the other two
+// axes in increasing order, f = b (SQ = false) or b^2 (SQ = true).
+template <bool SQ>
+__device__ __forceinline__ void face_moments(const double (&q)[27], double (&F)[3][2][2]) {
+  auto f = [](int p, int g) { return SQ ? bas(p, g) * bas(p, g) : bas(p, g); };
+  double R[3][3][3];  // R[d][ga][gb]: q summed along axis d, indexed by the other two
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+#pragma unroll
+    for (int b = 0; b < 3; b++) {
+      R[0][a][b] = (q[0 + 3 * a + 9 * b] + q[1 + 3 * a + 9 * b]) + q[2 + 3 * a + 9 * b];  // (gy, gz)
+      R[1][a][b] = (q[a + 0 + 9 * b] + q[a + 3 + 9 * b]) + q[a + 6 + 9 * b];              // (gx, gz)
+      R[2][a][b] = (q[a + 3 * b] + q[a + 3 * b + 9]) + q[a + 3 * b + 18];                 // (gx, gy)
+    }
+#pragma unroll
+  for (int d = 0; d < 3; d++)
+#pragma unroll
+    for (int pq = 0; pq < 2; pq++) {
+      double t[3];
+#pragma unroll
+      for (int a = 0; a < 3; a++) t[a] = (f(pq, 0) * R[d][a][0] + f(pq, 1) * R[d][a][1]) + f(pq, 2) * R[d][a][2];
+#pragma unroll
+      for (int p = 0; p < 2; p++) F[d][p][pq] = (f(p, 0) * t[0] + f(p, 1) * t[1]) + f(p, 2) * t[2];
+    }
+}
+
+// u_diag_kernel in tensor form (plain operator): diag of node (i,j,k), component x, is
+//   (lambda + 2 mu) Jx[j][k] / hx^2 + mu (Jy[i][k] / hy^2 + Jz[i][j] / hz^2)
+// with J_d the integrals of w (v^2 + eta) against the squared basis functions of the
+// other two axes (and similarly for y, z).
+__global__ void u_diag_tp_kernel(const __grid_constant__ ElemArgs E, int color,
+                                 const double* __restrict__ v, double* __restrict__ d) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double v8[8], v27[27], s27[27];
+#pragma unroll
+  for (int a = 0; a < 8; a++) v8[a] = v[n[a]];
+  interp27(v8, v27);
+  const double vol = E.hx * E.hy * E.hz;
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        const int g = gx + 3 * gy + 9 * gz;
+        s27[g] = (vol * (w1(gx) * w1(gy) * w1(gz))) * fma(v27[g], v27[g], E.eta);
+      }
+  double J[3][2][2];
+  face_moments<true>(s27, J);
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  const double l2m = m.lambda + 2. * m.mu;
+  const double ih2[3] = {1. / (E.hx * E.hx), 1. / (E.hy * E.hy), 1. / (E.hz * E.hz)};
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const double jx = J[0][j][k] * ih2[0], jy = J[1][i][k] * ih2[1], jz = J[2][i][j] * ih2[2];
+        const int64_t q = 3 * n[i + 2 * j + 4 * k];
+        d[q + 0] += fma(l2m, jx, m.mu * (jy + jz));
+        d[q + 1] += fma(l2m, jy, m.mu * (jx + jz));
+        d[q + 2] += fma(l2m, jz, m.mu * (jx + jy));
+      }
+}
+
+// u_rhs_kernel in tensor form (plain operator): the thermo-poro load
+// sum_g w dphi_a,c S_g, S = 3 kappa alpha (theta - thetaRef)(v^2 + eta) + beta p v, as
+// face moments of w S times -+1/h_c, and the crack-pressure load
+// sum_g w p grad_c v phi_a as a full contraction.
+__global__ void u_rhs_tp_kernel(const __grid_constant__ ElemArgs E, int color,
+                                const double* __restrict__ v, const double* __restrict__ theta,
+                                const double* __restrict__ thetaRef, const double* __restrict__ p,
+                                double* __restrict__ f) {
+  int ei, ej, ek;
+  if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  int64_t n[8];
+  cell_nodes(E, ei, ej, ek, n);
+  double v8[8], th8[8], p8[8];
+#pragma unroll
+  for (int a = 0; a < 8; a++) {
+    v8[a] = v[n[a]];
+    th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+    p8[a] = p ? p[n[a]] : 0.;
+  }
+  const CellMat m = cell_mat(E, ei, ej, ek);
+  const double coefalpha = (3. * m.lambda + 2. * m.mu) * m.alpha, beta = m.beta;
+  const double vol = E.hx * E.hy * E.hz;
+  double ve[27], pe[27], ws[27];
+  interp27(v8, ve);
+  interp27(p8, pe);
+  {
+    double te[27];
+    interp27(th8, te);
+#pragma unroll
+    for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+      for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+        for (int gx = 0; gx < 3; gx++) {
+          const int g = gx + 3 * gy + 9 * gz;
+          const double s = coefalpha * te[g] * (ve[g] * ve[g] + E.eta) + beta * pe[g] * ve[g];
+          ws[g] = (vol * (w1(gx) * w1(gy) * w1(gz))) * s;
+        }
+  }
+  double F[3][2][2];
+  face_moments<false>(ws, F);
+  const double ih[3] = {1. / E.hx, 1. / E.hy, 1. / E.hz};
+  double rl[8][3];
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int a = i + 2 * j + 4 * k;
+        rl[a][0] = (i ? ih[0] : -ih[0]) * F[0][j][k];
+        rl[a][1] = (j ? ih[1] : -ih[1]) * F[1][i][k];
+        rl[a][2] = (k ? ih[2] : -ih[2]) * F[2][i][j];
+      }
+  if (E.hasCrackPressure) {
+    // grad v at the points: each component depends on the two other axes only
+    double gv[3][9];  // gv[d][a + 3 b], (a, b) the other axes' point indices
+#pragma unroll
+    for (int a = 0; a < 3; a++)
+#pragma unroll
+      for (int b = 0; b < 3; b++) {
+        double sx = 0., sy = 0., sz = 0.;
+#pragma unroll
+        for (int q = 0; q < 2; q++)
+#pragma unroll
+          for (int r = 0; r < 2; r++) {
+            sx += bas(q, a) * bas(r, b) * (v8[1 + 2 * q + 4 * r] - v8[2 * q + 4 * r]);
+            sy += bas(q, a) * bas(r, b) * (v8[q + 2 + 4 * r] - v8[q + 4 * r]);
+            sz += bas(q, a) * bas(r, b) * (v8[q + 2 * r + 4] - v8[q + 2 * r]);
+          }
+        gv[0][a + 3 * b] = sx * ih[0];
+        gv[1][a + 3 * b] = sy * ih[1];
+        gv[2][a + 3 * b] = sz * ih[2];
+      }
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double qc[27], oc[8];
+#pragma unroll
+      for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+        for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+          for (int gx = 0; gx < 3; gx++) {
+            const int g = gx + 3 * gy + 9 * gz;
+            const double gvc = c == 0 ? gv[0][gy + 3 * gz] : (c == 1 ? gv[1][gx + 3 * gz] : gv[2][gx + 3 * gy]);
+            qc[g] = (vol * (w1(gx) * w1(gy) * w1(gz))) * pe[g] * gvc;
+          }
+      contract27(qc, oc);
+#pragma unroll
+      for (int a = 0; a < 8; a++) rl[a][c] += oc[a];
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 8; a++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) f[3 * n[a] + c] += rl[a][c];
+}
+
 __global__ void u_rhs_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ v,
                              const double* __restrict__ theta, const double* __restrict__ thetaRef,
                              const double* __restrict__ p, double* __restrict__ f,
@@ -476,6 +710,7 @@ cudaError_t launch_u_rhs(const ElemArgs& E, const double* v, const double* theta
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(f, 0, 3 * N * sizeof(double), s);
   if (e != cudaSuccess) return e;
+  if (!E.unilateral) return colours(E, u_rhs_tp_kernel, s, v, theta, thetaRef, p, f);
   return colours(E, u_rhs_kernel, s, v, theta, thetaRef, p, f, u0);
 }
 
@@ -489,7 +724,8 @@ cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcb
                           cudaStream_t s, const double* u0) {
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(d, 0, 3 * N * sizeof(double), s);
-  if (e == cudaSuccess) e = colours(E, u_diag_kernel, s, v, d, u0);
+  if (e == cudaSuccess)
+    e = E.unilateral ? colours(E, u_diag_kernel, s, v, d, u0) : colours(E, u_diag_tp_kernel, s, v, d);
   if (e == cudaSuccess && bcbits) {
     bc_diag_kernel<<<(int)std::min<int64_t>((N + 255) / 256, 2368), 256, 0, s>>>(bcbits, d, N);
     e = cudaGetLastError();

@@ -23,6 +23,7 @@ struct ElemArgs {
   double eta, epsilon, atcv;
   int atnum, hasCrackPressure;
   int unilateral;  // 1 = NOCOMPRESSION (VFCtx.unilateral)
+  double hx, hy, hz;  // cell size (the tensor-product kernels)
 };
 
 // f (3N) = thermo-poro + crack-pressure load (VFMech.c:386-447, 533-589), so that

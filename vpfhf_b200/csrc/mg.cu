@@ -535,6 +535,9 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
       E.cellE = c->d_cellE ? L.cellE : nullptr;
       E.L = c->layers;
       E.eta = c->vf.eta;
+      E.hx = L.hx;
+      E.hy = L.hy;
+      E.hz = L.hz;
       e = launch_u_diag(E, L.v64, L.bc, diag, c->stream);
       if (e == cudaSuccess) e = dev_inv(diag, dinv64, f32 ? (float*)L.dinv : nullptr, 3 * L.N, c->stream);
     }

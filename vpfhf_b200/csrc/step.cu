@@ -76,6 +76,9 @@ static ElemArgs elem_args(vfgpu_ctx* c) {
   E.atnum = c->vf.atnum;
   E.hasCrackPressure = c->vf.hasCrackPressure;
   E.unilateral = c->unilateral;
+  E.hx = c->hx;
+  E.hy = c->hy;
+  E.hz = c->hz;
   return E;
 }
 
