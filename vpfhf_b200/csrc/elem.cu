@@ -169,6 +169,35 @@ __device__ __forceinline__ void contract27(const double (&q)[27], double (&out)[
             (bas(k, 0) * cy[i][j][0] + bas(k, 1) * cy[i][j][1]) + bas(k, 2) * cy[i][j][2];
 }
 
+// out[i + 2j + 4k] = sum_g q_g b_i(gx)^2 b_j(gy)^2 b_k(gz)^2
+__device__ __forceinline__ void contract27sq(const double (&q)[27], double (&out)[8]) {
+  auto f = [](int p, int g) { return bas(p, g) * bas(p, g); };
+  double cx[2][3][3], cy[2][2][3];
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+      for (int gy = 0; gy < 3; gy++) {
+        const int b = 3 * gy + 9 * gz;
+        cx[i][gy][gz] = (f(i, 0) * q[b] + f(i, 1) * q[b + 1]) + f(i, 2) * q[b + 2];
+      }
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int gz = 0; gz < 3; gz++)
+        cy[i][j][gz] = (f(j, 0) * cx[i][0][gz] + f(j, 1) * cx[i][1][gz]) + f(j, 2) * cx[i][2][gz];
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++)
+        out[i + 2 * j + 4 * k] = (f(k, 0) * cy[i][j][0] + f(k, 1) * cy[i][j][1]) + f(k, 2) * cy[i][j][2];
+}
+
 // Integrals of q against the squared or plain basis products that carry no factor
 // along axis d: F[d][p][q] = sum_g q_g f_p(g_e1) f_q(g_e2) with (e1, e2) the other two
 // axes in increasing order, f = b (SQ = false) or b^2 (SQ = true).
@@ -521,61 +550,98 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
   }
 }
 
-__global__ void v_rhs_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ u,
-                             const double* __restrict__ p, double* __restrict__ b) {
+// V load (VF_ResidualVAT1/AT23D_local and VF_ResidualVCrackPressure3D_local,
+// VFMech.c:2294-2384) in tensor form: the AT term coef sum_g w phi_a = coef vol / 8 per
+// node, the crack-pressure term sum_g w p (u . grad phi_a) as face moments of w p u_c.
+__global__ void v_rhs_tp_kernel(const __grid_constant__ ElemArgs E, int color,
+                                const double* __restrict__ u, const double* __restrict__ p,
+                                double* __restrict__ b) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   const CellMat m = cell_mat(E, ei, ej, ek);
-  double rl[8];
-  // VF_ResidualVAT1/AT23D_local (VFMech.c:2350-2384)
+  const double vol = E.hx * E.hy * E.hz;
   const double coef = m.Gc / E.atcv / E.epsilon * (E.atnum == 1 ? .25 : .5);
-  for (int a = 0; a < 8; a++) {
-    rl[a] = 0.;
-    for (int g = 0; g < 27; g++) rl[a] += e.w[g] * e.phi[a][g] * coef;
-  }
-  // VF_ResidualVCrackPressure3D_local (VFMech.c:2294-2341)
+  double rl[8];
+#pragma unroll
+  for (int a = 0; a < 8; a++) rl[a] = coef * vol * 0.125;
   if (E.hasCrackPressure && p) {
-    double u8[8][3], p8[8];
-    for (int a = 0; a < 8; a++) {
-      for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
-      p8[a] = p[n[a]];
-    }
-    for (int g = 0; g < 27; g++) {
-      double pe = 0., ue[3] = {0., 0., 0.};
-      for (int a = 0; a < 8; a++) {
-        pe += e.phi[a][g] * p8[a];
-        for (int c = 0; c < 3; c++) ue[c] += e.phi[a][g] * u8[a][c];
-      }
-      for (int a = 0; a < 8; a++)
-        rl[a] += e.w[g] * pe * (ue[0] * e.dphi[a][0][g] + ue[1] * e.dphi[a][1][g] + ue[2] * e.dphi[a][2][g]);
+    double p8[8], pe[27];
+#pragma unroll
+    for (int a = 0; a < 8; a++) p8[a] = p[n[a]];
+    interp27(p8, pe);
+    const double ih[3] = {1. / E.hx, 1. / E.hy, 1. / E.hz};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      double u8[8], q[27], F[3][2][2];
+#pragma unroll
+      for (int a = 0; a < 8; a++) u8[a] = u[3 * n[a] + c];
+      interp27(u8, q);
+#pragma unroll
+      for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+        for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+          for (int gx = 0; gx < 3; gx++) {
+            const int g = gx + 3 * gy + 9 * gz;
+            q[g] = (vol * (w1(gx) * w1(gy) * w1(gz))) * pe[g] * q[g];
+          }
+      face_moments<false>(q, F);
+#pragma unroll
+      for (int k = 0; k < 2; k++)
+#pragma unroll
+        for (int j = 0; j < 2; j++)
+#pragma unroll
+          for (int i = 0; i < 2; i++) {
+            const int sgn = c == 0 ? i : (c == 1 ? j : k);
+            const double fm = c == 0 ? F[0][j][k] : (c == 1 ? F[1][i][k] : F[2][i][j]);
+            rl[i + 2 * j + 4 * k] += (sgn ? ih[c] : -ih[c]) * fm;
+          }
     }
   }
+#pragma unroll
   for (int a = 0; a < 8; a++) b[n[a]] += rl[a];
 }
 
-__global__ void v_diag_kernel(const __grid_constant__ ElemArgs E, int color, const double* __restrict__ coef,
-                              double* __restrict__ d) {
+// Diagonal of K_V (the AT forms VF_BilinearFormVAT1/AT23D_local, VFMech.c:2040-2090,
+// plus the coupling VF_BilinearFormVCoupling3D_local, :2093-2122) in tensor form:
+// aeps sum_g w |grad phi_a|^2 from the face moments of w, plus sum_g coef_g phi_a^2 as
+// a contraction against the squared basis.
+__global__ void v_diag_tp_kernel(const __grid_constant__ ElemArgs E, int color,
+                                 const double* __restrict__ coef, double* __restrict__ d) {
   int ei, ej, ek;
   if (!colour_cell(E, color, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
   const CellMat m = cell_mat(E, ei, ej, ek);
   const double aeps = m.Gc / E.atcv * .5 * E.epsilon;
+  const double vol = E.hx * E.hy * E.hz;
   const int64_t cell = ((int64_t)ek * (E.ny - 1) + ej) * (E.nx - 1) + ei;
   const int64_t ncell = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
-  for (int a = 0; a < 8; a++) {
-    double s = 0.;
-    for (int g = 0; g < 27; g++) {
-      const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
-      s += aeps * e.w[g] * (d0 * d0 + d1 * d1 + d2 * d2) +
-           coef[(int64_t)g * ncell + cell] * e.phi[a][g] * e.phi[a][g];
-    }
-    d[n[a]] += s;
-  }
+  double w27[27], c27[27], J[3][2][2], M[8];
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        const int g = gx + 3 * gy + 9 * gz;
+        w27[g] = vol * (w1(gx) * w1(gy) * w1(gz));
+        c27[g] = coef[(int64_t)g * ncell + cell];
+      }
+  face_moments<true>(w27, J);
+  contract27sq(c27, M);
+  const double ih2[3] = {1. / (E.hx * E.hx), 1. / (E.hy * E.hy), 1. / (E.hz * E.hz)};
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int j = 0; j < 2; j++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const double lap = (J[0][j][k] * ih2[0] + J[1][i][k] * ih2[1]) + J[2][i][j] * ih2[2];
+        d[n[i + 2 * j + 4 * k]] += fma(aeps, lap, M[i + 2 * j + 4 * k]);
+      }
 }
 
 // Neumaier-compensated accumulation.
@@ -745,14 +811,14 @@ cudaError_t launch_v_rhs(const ElemArgs& E, const double* u, const double* p, do
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(b, 0, N * sizeof(double), s);
   if (e != cudaSuccess) return e;
-  return colours(E, v_rhs_kernel, s, u, p, b);
+  return colours(E, v_rhs_tp_kernel, s, u, p, b);
 }
 
 cudaError_t launch_v_diag(const ElemArgs& E, const double* coef, double* d, cudaStream_t s) {
   const int64_t N = (int64_t)E.nx * E.ny * E.nz;
   cudaError_t e = cudaMemsetAsync(d, 0, N * sizeof(double), s);
   if (e != cudaSuccess) return e;
-  return colours(E, v_diag_kernel, s, coef, d);
+  return colours(E, v_diag_tp_kernel, s, coef, d);
 }
 
 int energy_blocks() { return EN_BLOCKS; }
