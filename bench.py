@@ -6,7 +6,8 @@ pressurized penny crack (the FP64-vs-mixed configuration), one JSON line.
 A "step" is one application of the degraded elasticity operator K(v) to a
 3N-vector (3 x 129^3 = 6,440,067 dofs) with the inputs resident in HBM; the L2
 is flushed between timed steps.  `e2e` times the same step through the C ABI
-(vfgpu_u_apply) from pinned host memory, copies included.  The AM-step rate
+(vfgpu_u_apply) from pinned host memory, copies included (the entry point overlaps the
+copies in both directions with the apply, slab by slab).  The AM-step rate
 (StepU + StepV to tolerance, FP64 and mixed, 10 iterations from the penny-crack
 start; U solve with the reference's Jacobi PCG and with the multigrid PCG) is
 reported beside it with the mixed-vs-FP64 differences of the energies,

@@ -101,6 +101,14 @@ struct vfgpu_ctx {
   double *d_widthc = nullptr, *d_pmult = nullptr, *d_width = nullptr, *d_wpart = nullptr;
   unsigned* d_wstall = nullptr;
 
+  // Host-buffer apply pipeline (vfgpu_u_apply with host x and y): a second output
+  // staging vector, the copy streams and one event per slab, made at the first use.
+  static constexpr int kPipeSlabs = 16;
+  double* t64c = nullptr;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_in[kPipeSlabs] = {}, ev_y[kPipeSlabs] = {},
+              ev_out[kPipeSlabs] = {};
+
   // Captured CUDA graphs of CG iteration batches, keyed by (call site, batch size).
   // Kernels read the material table, eta and the AT gradient weights through
   // d_params, so new material / vfprop values leave the graphs valid; a set-up call

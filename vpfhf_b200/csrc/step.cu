@@ -771,7 +771,7 @@ int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
   b += (2 * 3 * N + 5 * N) * 8;                          // fields U, BCU, V, VIrrev, theta, thetaRef, p
   b += N * 4 + (g->nz - 1) + 3 * N + 3 * N;              // V32, layers, BC kinds and bits
   b += (long long)(p64.seamX + p64.seamY) * 8 + (long long)(p32.seamX + p32.seamY) * 4;
-  b += 2 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
+  b += 3 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
   b += vfgpu_ctx::NP64 * (3 * N + kPoolSlack) * 8 + vfgpu_ctx::NP32 * (3 * N + kPoolSlack) * 4;
   b += 27 * NC * 12 + N;                                 // V coefficient (FP64 + FP32), mask
   b += (RED_BLOCKS + energy_blocks()) * 4 * 8 + 4096;    // reductions, scalars

@@ -160,6 +160,15 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   free_solver(c);
   free_mg(c);
   for (auto& p : c->f) cudaFree(p);
+  if (c->s_in) cudaStreamSynchronize(c->s_in);
+  if (c->s_out) cudaStreamSynchronize(c->s_out);
+  for (int s = 0; s < vfgpu_ctx::kPipeSlabs; s++)
+    for (cudaEvent_t ev : {c->ev_in[s], c->ev_y[s], c->ev_out[s]})
+      if (ev) cudaEventDestroy(ev);
+  if (c->ev_start) cudaEventDestroy(c->ev_start);
+  if (c->s_in) cudaStreamDestroy(c->s_in);
+  if (c->s_out) cudaStreamDestroy(c->s_out);
+  cudaFree(c->t64c);
   void* bufs[] = {c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
@@ -422,6 +431,81 @@ int vfgpu_get_field(vfgpu_ctx* c, int field, double* data) {
   return VFGPU_OK;
 }
 
+namespace {
+
+// Streams, events and the second staging vector of the host-buffer pipeline.
+cudaError_t pipe_resources(vfgpu_ctx* c) {
+  if (c->t64c) return cudaSuccess;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_start, cudaEventDisableTiming);
+  for (int s = 0; s < vfgpu_ctx::kPipeSlabs && e == cudaSuccess; s++)
+    for (cudaEvent_t* ev : {&c->ev_in[s], &c->ev_y[s], &c->ev_out[s]})
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->t64c, 3 * c->N * sizeof(double));
+  return e;
+}
+
+// y = K x with x and y in host memory (FP64), as a pipeline over z-slabs of node planes:
+// slab s's planes go up on s_in, the slab with one halo plane on each side is applied
+// as a sub-grid on the ctx stream (same xy tiles and per-node sum order as the whole-grid
+// apply, so its interior planes carry the same bits; the halo planes' values are
+// discarded), and its interior planes come back on s_out while later slabs are still
+// going up, so that both copy directions and the compute overlap.  Slabs alternate
+// between two output staging vectors, because a slab's apply also writes its halo
+// planes, which belong to its neighbours.
+cudaError_t u_apply_host_pipelined(vfgpu_ctx* c, const double* x, double* y) {
+  cudaError_t e = pipe_resources(c);
+  if (e != cudaSuccess) return e;
+  // slabs of at least 4 planes, at most kPipeSlabs of them
+  const int nz = c->nz, S = std::max(2, std::min(vfgpu_ctx::kPipeSlabs, nz / 4));
+  const int64_t plane = (int64_t)c->nx * c->ny, cplane = (int64_t)(c->nx - 1) * (c->ny - 1);
+  const int P = (nz + S - 1) / S;
+  if (c->unilateral) e = nc_flags(c, c->f[VFGPU_FIELD_U]);
+  if (e == cudaSuccess) e = cudaEventRecord(c->ev_start, c->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_in, c->ev_start, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_start, 0);
+  int up = 0;  // planes [0, up) are on their way up
+  for (int s = 0; s < S && e == cudaSuccess; s++) {
+    const int a = s * P, b = std::min(nz, (s + 1) * P);
+    if (a >= b) break;
+    const int lo = std::max(a - 1, 0), hi = std::min(b + 1, nz);
+    if (hi > up) {
+      e = cudaMemcpyAsync(c->t64a + 3 * up * plane, x + 3 * up * plane,
+                          3 * (hi - up) * plane * sizeof(double), cudaMemcpyHostToDevice, c->s_in);
+      up = hi;
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[s], c->s_in);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_in[s], 0);
+    double* buf = (s & 1) ? c->t64c : c->t64b;
+    if (e == cudaSuccess) {
+      const int nzs = hi - lo;
+      const TilePlan p = u_plan(c->nx, c->ny, nzs, 8, c->nsm);
+      UApplyArgs<double> A = u_args<double>(c, c->t64a + 3 * lo * plane, c->f[VFGPU_FIELD_V] + lo * plane,
+                                            buf + 3 * lo * plane, c->seam64, p);
+      A.nz = nzs;
+      A.bc = c->bcU_bits + lo * plane;
+      A.elayer = c->d_elayer + lo;
+      if (A.cellE) A.cellE += lo * cplane;
+      if (A.cflag) A.cflag += lo * cplane;
+      e = launch_u_apply<double>(A, p, c->layers, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_y[s], c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_y[s], 0);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(y + 3 * a * plane, buf + 3 * a * plane, 3 * (b - a) * plane * sizeof(double),
+                          cudaMemcpyDeviceToHost, c->s_out);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_out[s], c->s_out);
+    // the slab two ahead reuses this buffer's halo planes only: no wait is needed for
+    // correctness; the ctx stream waits for the last copy out before returning
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->s_out);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return e;
+}
+
+}  // namespace
+
 int vfgpu_u_apply(vfgpu_ctx* c, int precision, const double* x, double* y) {
   if (!c || !x || !y) return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply: null argument");
   if (precision != VFGPU_FP64 && precision != VFGPU_MIXED)
@@ -431,6 +515,11 @@ int vfgpu_u_apply(vfgpu_ctx* c, int precision, const double* x, double* y) {
   const int64_t n3 = 3 * c->N;
   const bool xdev = is_device_ptr(x), ydev = is_device_ptr(y);
   cudaError_t e = cudaSuccess;
+  if (precision == VFGPU_FP64 && !xdev && !ydev && c->nz >= 8) {
+    e = u_apply_host_pipelined(c, x, y);
+    if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply");
+    return VFGPU_OK;
+  }
   const double* xd = x;
   if (!xdev) {
     e = copy_in(c, c->t64a, x, n3);
