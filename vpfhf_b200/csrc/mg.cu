@@ -11,10 +11,9 @@
 // way, the element layer of the lowest child layer and, for a per-cell modulus, the
 // mean of the 8 children.  Transfers: trilinear prolongation and its transpose
 // (full weighting), Dirichlet dofs excluded on both sides.  Smoother: Chebyshev
-// iteration of D^-1 K of degree 3 on [lmax/10, lmax] (lmax = 1.1 x the estimate of
-// 12 power iterations per level, 4 from the previous vector once there is one), pre
-// and post; the coarsest level
-// runs degree 30 on [lmax/100, lmax].  Every step is a fixed sequence of
+// iteration of D^-1 K (degree kSmoothDeg) on [lmax/10, lmax] (lmax = 1.1 x the
+// estimate of 12 power iterations per level, 4 from the previous vector once there is
+// one), pre and post; the coarsest level runs degree kCoarseDeg on [lmax/100, lmax].  Every step is a fixed sequence of
 // deterministic kernels reading its Chebyshev coefficients from device memory, so
 // the V-cycle is a fixed symmetric linear operator (plain PCG applies) and is
 // replayed as one CUDA graph.
@@ -36,7 +35,11 @@ namespace {
 // Power iterations per level: from the deterministic seed at the first set-up, then
 // from the previous set-up's vector (the operator of the next StepU differs by the
 // phase field's update only).
-constexpr int kSmoothDeg = 3, kCoarseDeg = 30, kPowerIts = 12, kWarmPowerIts = 4;
+// Degrees: measured on B200 (StepU, 129^3 and 257^3 penny cracks, c5 set-up at 129^3
+// and 193^3), degree 1 pre and post smoothing with a 15-step coarsest solve beat the
+// higher degrees on time although the CG takes more iterations (257^3: 0.163 s mixed
+// with 20 iterations against 0.181 s / 15 for degree 2 and 0.209 s / 13 for degree 3).
+constexpr int kSmoothDeg = 1, kCoarseDeg = 15, kPowerIts = 12, kWarmPowerIts = 4;
 constexpr double kSmoothLo = 0.1, kCoarseLo = 0.01, kLmaxSafety = 1.1;
 constexpr int kCoefPerLevel = 64;  // [0] lmax [1] 1/theta [2..59] (c1, c2) [62..63] scratch
 constexpr int kPowBlocks = 296, kPowThreads = 256;
