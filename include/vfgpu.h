@@ -96,7 +96,7 @@ typedef struct {
   int pc;                 /* StepU preconditioner: VFGPU_PC_JACOBI (the reference's) or  */
                           /* VFGPU_PC_MG (geometric multigrid V-cycle, FP32 under       */
                           /* VFGPU_MIXED, FP64 otherwise; FP64 CG with the Jacobi       */
-                          /* solve's stopping test; needs an even cell count per axis)  */
+                          /* solve's stopping test; needs >= 9 nodes along some axis)   */
 } vfgpu_solve_opts;
 
 #define VFGPU_PC_JACOBI 0

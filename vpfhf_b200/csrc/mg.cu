@@ -4,13 +4,15 @@
 // feeds keeps the reference's semantics (same residual, same SNES tests, the CG
 // stopping test of the Jacobi solve), only the Krylov iterations get fewer.
 //
-// Levels halve the cells per axis while every axis has an even cell count and the
-// coarse grid keeps >= 5 nodes per axis.  Each coarse level rediscretises the same
-// operator (the tile engine's U apply) on its grid with the phase field injected
-// from the level above (v_c(I) = v_f(2I)), the Dirichlet bits injected the same
-// way, the element layer of the lowest child layer and, for a per-cell modulus, the
-// mean of the 8 children.  Transfers: trilinear prolongation and its transpose
-// (full weighting), Dirichlet dofs excluded on both sides.  Smoother: Chebyshev
+// Each coarser level has ceil(cells / 2) uniform cells along every axis that still has
+// >= 9 nodes (the others keep theirs), over the same box: nested where a cell count is
+// even, offset by a fraction of a cell where it is odd.  Each coarse level
+// rediscretises the same operator (the tile engine's U apply) on its grid with the
+// phase field interpolated at its nodes (nested: v_c(I) = v_f(2I)), the Dirichlet
+// bits of the nearest fine node, the element layer of the lowest fine layer it holds
+// and, for a per-cell modulus, the mean of the fine cells whose centres it holds
+// (nested: the 8 children).  Transfers: trilinear prolongation and its exact
+// transpose, Dirichlet dofs excluded on both sides.  Smoother: Chebyshev
 // iteration of D^-1 K (degree kSmoothDeg) on [lmax/10, lmax] (lmax = 1.1 x the
 // estimate of 12 power iterations per level, 4 from the previous vector once there is
 // one), pre and post; the coarsest level runs degree kCoarseDeg on [lmax/100, lmax].  Every step is a fixed sequence of
@@ -51,9 +53,45 @@ inline int blocks_for(int64_t n) { return (int)std::min<int64_t>((n + 255) / 256
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (n);              \
        i += (int64_t)gridDim.x * blockDim.x)
 
-// Full weighting of the residual b - t: coarse node I gathers the fine nodes 2I + o,
-// o in {-1,0,1}^3, with weight prod_d (1 - |o_d| / 2), skipping fine Dirichlet dofs;
-// coarse Dirichlet dofs are zeroed.  The transpose of prolong_add_kernel.
+// Grid transfers between a level and the next coarser one.  Along each axis the coarse
+// grid spans the same interval with nc nodes (nc - 1 = ceil((nf - 1) / 2) cells, or
+// nc = nf on an axis that is not coarsened), so fine node i sits at coarse coordinate
+// i (nc - 1) / (nf - 1): in coarse cell I = floor of it with the linear weights
+// (1 - w, w), w the fractional part, computed exactly from integers.  With an even
+// fine cell count this is the nested case (w = 0 or 1/2 at the fine nodes 2I, 2I + 1).
+struct Lin {
+  int I;
+  double whi;
+};
+__device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
+  const long long num = (long long)i * (nc - 1), den = nf - 1;
+  Lin l;
+  l.I = (int)(num / den);
+  l.whi = (double)(num - (long long)l.I * den) / (double)den;
+  return l;
+}
+
+// The fine nodes of one axis that coarse node I's hat function covers, with its weights
+// (the entries of the prolongation's column I); at most 5 for a ratio of <= 2.
+__device__ __forceinline__ int coarse_support(int I, int nf, int nc, int (&idx)[6], double (&w)[6]) {
+  int n = 0;
+  const int lo = I > 0 ? (int)(((long long)(I - 1) * (nf - 1)) / (nc - 1)) : 0;
+  const int hi = min(nf - 1, (int)(((long long)(I + 1) * (nf - 1) + (nc - 2)) / (nc - 1)));
+  for (int i = lo; i <= hi && n < 6; i++) {
+    const Lin l = fine_in_coarse(i, nf, nc);
+    const double wt = l.I == I ? 1.0 - l.whi : (l.I + 1 == I ? l.whi : 0.0);
+    if (wt != 0.0) {
+      idx[n] = i;
+      w[n] = wt;
+      n++;
+    }
+  }
+  return n;
+}
+
+// Restriction of the residual b - t (the transpose of prolong_add_kernel): coarse node I
+// gathers the fine nodes of its hat function's support with the same weights, skipping
+// fine Dirichlet dofs; coarse Dirichlet dofs are zeroed.
 template <typename T>
 __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ tf,
                                 const uint8_t* __restrict__ bc_f, int fx, int fy, int fz,
@@ -62,26 +100,20 @@ __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ 
   const int64_t Nc = (int64_t)cx * cy * cz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % cx), J = (int)((q / cx) % cy), K = (int)(q / ((int64_t)cx * cy));
+    int ix[6], iy[6], iz[6];
+    double wx[6], wy[6], wz[6];
+    const int nxs = coarse_support(I, fx, cx, ix, wx), nys = coarse_support(J, fy, cy, iy, wy),
+              nzs = coarse_support(K, fz, cz, iz, wz);
     T acc[3] = {T(0), T(0), T(0)};
-    for (int oz = -1; oz <= 1; oz++) {
-      const int k = 2 * K + oz;
-      if (k < 0 || k >= fz) continue;
-      const T wz = oz ? T(0.5) : T(1);
-      for (int oy = -1; oy <= 1; oy++) {
-        const int j = 2 * J + oy;
-        if (j < 0 || j >= fy) continue;
-        const T wy = oy ? T(0.5) : T(1);
-        for (int ox = -1; ox <= 1; ox++) {
-          const int i = 2 * I + ox;
-          if (i < 0 || i >= fx) continue;
-          const T w = wz * wy * (ox ? T(0.5) : T(1));
-          const int64_t n = node_index(i, j, k, fx, fy);
+    for (int c3 = 0; c3 < nzs; c3++)
+      for (int c2 = 0; c2 < nys; c2++)
+        for (int c1 = 0; c1 < nxs; c1++) {
+          const T w = T(wz[c3] * wy[c2] * wx[c1]);
+          const int64_t n = node_index(ix[c1], iy[c2], iz[c3], fx, fy);
           const unsigned bf_bits = bc_f[n];
           for (int c = 0; c < 3; c++)
             if (!((bf_bits >> c) & 1u)) acc[c] += w * (bf[3 * n + c] - tf[3 * n + c]);
         }
-      }
-    }
     const unsigned b = bc_c[q];
     for (int c = 0; c < 3; c++) rc[3 * q + c] = ((b >> c) & 1u) ? T(0) : acc[c];
   }
@@ -89,53 +121,97 @@ __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ 
 
 // x_f += trilinear interpolation of e_c; fine Dirichlet dofs untouched.
 template <typename T>
-__global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy,
+__global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy, int cz,
                                    T* __restrict__ xf, int fx, int fy, int fz,
                                    const uint8_t* __restrict__ bc_f) {
   const int64_t Nf = (int64_t)fx * fy * fz;
   GRID_STRIDE(q, Nf) {
     const int i = (int)(q % fx), j = (int)((q / fx) % fy), k = (int)(q / ((int64_t)fx * fy));
-    const int i0 = i >> 1, j0 = j >> 1, k0 = k >> 1;
-    const int ni = (i & 1) ? 2 : 1, nj = (j & 1) ? 2 : 1, nk = (k & 1) ? 2 : 1;
-    const T w = ((i & 1) ? T(0.5) : T(1)) * ((j & 1) ? T(0.5) : T(1)) * ((k & 1) ? T(0.5) : T(1));
+    const Lin lx = fine_in_coarse(i, fx, cx), ly = fine_in_coarse(j, fy, cy),
+              lz = fine_in_coarse(k, fz, cz);
     T acc[3] = {T(0), T(0), T(0)};
-    for (int dk = 0; dk < nk; dk++)
-      for (int dj = 0; dj < nj; dj++)
-        for (int di = 0; di < ni; di++) {
-          const int64_t n = node_index(i0 + di, j0 + dj, k0 + dk, cx, cy);
-          for (int c = 0; c < 3; c++) acc[c] += ec[3 * n + c];
+    for (int dk = 0; dk < 2; dk++) {
+      const double wzk = dk ? lz.whi : 1.0 - lz.whi;
+      if (wzk == 0.0) continue;
+      for (int dj = 0; dj < 2; dj++) {
+        const double wyj = dj ? ly.whi : 1.0 - ly.whi;
+        if (wyj == 0.0) continue;
+        for (int di = 0; di < 2; di++) {
+          const double wxi = di ? lx.whi : 1.0 - lx.whi;
+          if (wxi == 0.0) continue;
+          const T w = T(wzk * wyj * wxi);
+          const int64_t n = node_index(lx.I + di, ly.I + dj, lz.I + dk, cx, cy);
+          for (int c = 0; c < 3; c++) acc[c] += w * ec[3 * n + c];
         }
+      }
+    }
     const unsigned b = bc_f[q];
     for (int c = 0; c < 3; c++)
-      if (!((b >> c) & 1u)) xf[3 * q + c] += w * acc[c];
+      if (!((b >> c) & 1u)) xf[3 * q + c] += acc[c];
   }
 }
 
-// Coarse node I takes v and the Dirichlet bits of fine node 2I.
+// Coarse node I takes v interpolated at its position (in the nested case: fine node 2I)
+// and the Dirichlet bits of the nearest fine node (box faces map to box faces).
 __global__ void inject_kernel(const double* __restrict__ vf, const uint8_t* __restrict__ bcf,
-                              int fx, int fy, double* __restrict__ vc, uint8_t* __restrict__ bcc,
-                              int cx, int cy, int cz) {
+                              int fx, int fy, int fz, double* __restrict__ vc,
+                              uint8_t* __restrict__ bcc, int cx, int cy, int cz) {
   const int64_t Nc = (int64_t)cx * cy * cz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % cx), J = (int)((q / cx) % cy), K = (int)(q / ((int64_t)cx * cy));
-    const int64_t n = node_index(2 * I, 2 * J, 2 * K, fx, fy);
-    vc[q] = vf[n];
-    bcc[q] = bcf[n];
+    // coarse node in the fine grid's index space: fine_in_coarse with the roles swapped
+    const Lin lx = fine_in_coarse(I, cx, fx), ly = fine_in_coarse(J, cy, fy),
+              lz = fine_in_coarse(K, cz, fz);
+    double v = 0.;
+    for (int dk = 0; dk < 2; dk++) {
+      const double wzk = dk ? lz.whi : 1.0 - lz.whi;
+      if (wzk == 0.0) continue;
+      for (int dj = 0; dj < 2; dj++) {
+        const double wyj = dj ? ly.whi : 1.0 - ly.whi;
+        if (wyj == 0.0) continue;
+        for (int di = 0; di < 2; di++) {
+          const double wxi = di ? lx.whi : 1.0 - lx.whi;
+          if (wxi == 0.0) continue;
+          v += wzk * wyj * wxi * vf[node_index(lx.I + di, ly.I + dj, lz.I + dk, fx, fy)];
+        }
+      }
+    }
+    vc[q] = v;
+    const int ni = lx.I + (lx.whi > 0.5 ? 1 : 0), nj = ly.I + (ly.whi > 0.5 ? 1 : 0),
+              nk = lz.I + (lz.whi > 0.5 ? 1 : 0);
+    bcc[q] = bcf[node_index(ni, nj, nk, fx, fy)];
   }
 }
 
-// Coarse cell modulus = mean of its 8 children.
-__global__ void cell_mean_kernel(const float* __restrict__ ef, int fcx, int fcy,
+// The fine cells (along one axis) whose centres lie in coarse cell k: [first, last).
+__device__ __forceinline__ void fine_cells_of(int k, int ncf, int ncc, int& first, int& last) {
+  // centre of fine cell j at coarse coordinate (j + 1/2) ncc / ncf
+  first = (int)(((long long)2 * k * ncf - ncc + 2 * ncc - 1) / (2 * ncc));  // ceil((2k ncf - ncc) / 2ncc)
+  if (first < 0) first = 0;
+  last = (int)(((long long)2 * (k + 1) * ncf - ncc + 2 * ncc - 1) / (2 * ncc));
+  if (last > ncf) last = ncf;
+}
+
+// Coarse cell modulus = mean of the fine cells whose centres it contains (nested: its 8
+// children).
+__global__ void cell_mean_kernel(const float* __restrict__ ef, int fcx, int fcy, int fcz,
                                  float* __restrict__ ec, int ccx, int ccy, int ccz) {
   const int64_t Nc = (int64_t)ccx * ccy * ccz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % ccx), J = (int)((q / ccx) % ccy), K = (int)(q / ((int64_t)ccx * ccy));
+    int x0, x1, y0, y1, z0, z1;
+    fine_cells_of(I, fcx, ccx, x0, x1);
+    fine_cells_of(J, fcy, ccy, y0, y1);
+    fine_cells_of(K, fcz, ccz, z0, z1);
     float s = 0.f;
-    for (int dk = 0; dk < 2; dk++)
-      for (int dj = 0; dj < 2; dj++)
-        for (int di = 0; di < 2; di++)
-          s += ef[((int64_t)(2 * K + dk) * fcy + (2 * J + dj)) * fcx + (2 * I + di)];
-    ec[q] = 0.125f * s;
+    int cnt = 0;
+    for (int kk = z0; kk < z1; kk++)
+      for (int jj = y0; jj < y1; jj++)
+        for (int ii = x0; ii < x1; ii++) {
+          s += ef[((int64_t)kk * fcy + jj) * fcx + ii];
+          cnt++;
+        }
+    ec[q] = cnt ? s / (float)cnt : 0.f;
   }
 }
 
@@ -397,12 +473,33 @@ template <typename T> cudaError_t vcycle(vfgpu_ctx* c, int l, const T* b, T* z) 
   }
   if (e == cudaSuccess) e = vcycle<T>(c, l + 1, C.b, C.x);
   if (e == cudaSuccess) {
-    prolong_add_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(C.x, C.nx, C.ny, z, V.nx,
-                                                                      V.ny, V.nz, V.bc);
+    prolong_add_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(C.x, C.nx, C.ny, C.nz, z,
+                                                                      V.nx, V.ny, V.nz, V.bc);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = chebyshev<T>(c, V, b, z, kSmoothDeg, false);
   return e;
+}
+
+// Next coarser node count along an axis: ceil(cells / 2) cells while the axis keeps
+// >= 5 nodes, else unchanged.
+inline int coarser(int n) { return n >= 9 ? n / 2 + 1 : n; }
+// Levels of the hierarchy of an nx x ny x nz grid (1: no coarse level).
+inline int mg_levels(int nx, int ny, int nz) {
+  int nlev = 1;
+  while (coarser(nx) != nx || coarser(ny) != ny || coarser(nz) != nz) {
+    nx = coarser(nx);
+    ny = coarser(ny);
+    nz = coarser(nz);
+    nlev++;
+  }
+  return nlev;
+}
+// First fine cell (along one axis) whose centre lies in coarse cell k (host mirror of
+// fine_cells_of).
+inline int first_fine_cell(int k, int ncf, int ncc) {
+  const long long a = 2LL * k * ncf - ncc, b = 2LL * ncc;
+  return a <= 0 ? 0 : (int)((a + b - 1) / b);
 }
 
 template <typename T> void* dalloc(int64_t n, cudaError_t& e) {
@@ -415,20 +512,8 @@ template <typename T> void* dalloc(int64_t n, cudaError_t& e) {
 template <typename T> int mg_build(vfgpu_ctx* c) {
   if (!c->mg.empty() && c->mg_bytes == (int)sizeof(T)) return VFGPU_OK;
   free_mg(c);
-  int nlev = 1;
-  {
-    int nx = c->nx, ny = c->ny, nz = c->nz;
-    while ((nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 && (nx - 1) / 2 + 1 >= 5 &&
-           (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
-      nx = (nx - 1) / 2 + 1;
-      ny = (ny - 1) / 2 + 1;
-      nz = (nz - 1) / 2 + 1;
-      nlev++;
-    }
-  }
-  if (nlev < 2)
-    return fail(VFGPU_ERR_INVALID,
-                "multigrid needs an even cell count on every axis and >= 9 nodes per axis");
+  const int nlev = mg_levels(c->nx, c->ny, c->nz);
+  if (nlev < 2) return fail(VFGPU_ERR_INVALID, "multigrid needs >= 9 nodes along some axis");
   cudaError_t e = cudaSuccess;
   c->mg_coef = (double*)dalloc<double>((int64_t)kCoefPerLevel * nlev, e);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->mg_coef, 0, sizeof(double) * kCoefPerLevel * nlev, c->stream);
@@ -442,10 +527,13 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     L0.nz = c->nz;
     L0.N = c->N;
     L0.NC = c->NC;
+    // FP32: r and d also hold the FP64 diagonal of each coarse level during set-up
+    const int64_t n1 = (int64_t)coarser(c->nx) * coarser(c->ny) * coarser(c->nz);
+    const int64_t nrd = f32 ? std::max<int64_t>(n3, 6 * n1) : n3;
     L0.x = dalloc<T>(n3, e);
     L0.ev = dalloc<T>(n3, e);
-    L0.r = dalloc<T>(n3, e);
-    L0.d = dalloc<T>(n3, e);
+    L0.r = dalloc<T>(nrd, e);
+    L0.d = dalloc<T>(nrd, e);
     L0.t = dalloc<T>(n3, e);
     if (f32) {
       L0.b = dalloc<T>(n3, e);
@@ -454,14 +542,11 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     L0.coef = c->mg_coef;
   }
   int nx = c->nx, ny = c->ny, nz = c->nz;
-  double hx = c->hx, hy = c->hy, hz = c->hz;
   for (int l = 1; l < nlev && e == cudaSuccess; l++) {
-    nx = (nx - 1) / 2 + 1;
-    ny = (ny - 1) / 2 + 1;
-    nz = (nz - 1) / 2 + 1;
-    hx *= 2;
-    hy *= 2;
-    hz *= 2;
+    nx = coarser(nx);
+    ny = coarser(ny);
+    nz = coarser(nz);
+    const double hx = c->lx / (nx - 1), hy = c->ly / (ny - 1), hz = c->lz / (nz - 1);
     auto& L = c->mg[l];
     L.nx = nx;
     L.ny = ny;
@@ -510,23 +595,32 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
     const double* vf = l == 1 ? c->f[VFGPU_FIELD_V] : F.v64;
     const uint8_t* bcf = l == 1 ? c->bcU_bits : F.bc;
     const float* cellEf = l == 1 ? c->d_cellE : F.cellE;
-    const int fx = l == 1 ? c->nx : F.nx, fy = l == 1 ? c->ny : F.ny;
-    inject_kernel<<<blocks_for(L.N), 256, 0, c->stream>>>(vf, bcf, fx, fy, L.v64, L.bc, L.nx, L.ny,
-                                                          L.nz);
+    const int fx = l == 1 ? c->nx : F.nx, fy = l == 1 ? c->ny : F.ny, fz = l == 1 ? c->nz : F.nz;
+    inject_kernel<<<blocks_for(L.N), 256, 0, c->stream>>>(vf, bcf, fx, fy, fz, L.v64, L.bc, L.nx,
+                                                          L.ny, L.nz);
     e = cudaGetLastError();
     if (e == cudaSuccess && f32) e = convert_f64_f32(L.v64, (float*)L.v, L.N, c->stream);
+    // element layer of the lowest fine layer in each coarse layer, followed down to level 0
     std::vector<uint8_t> lc(L.nz - 1);
-    for (int k = 0; k < L.nz - 1; k++) lc[k] = el[(size_t)k << l];  // lowest child layer
+    for (int k = 0; k < L.nz - 1; k++) {
+      int kk = k;
+      for (int m = l; m >= 1; m--) {
+        const int ncf = (m == 1 ? c->nz : c->mg[m - 1].nz) - 1, ncc = c->mg[m].nz - 1;
+        kk = first_fine_cell(kk, ncf, ncc);
+      }
+      lc[k] = el[std::min<size_t>(kk, el.size() - 1)];
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(L.elayer, lc.data(), lc.size(), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // lc leaves scope
     if (e == cudaSuccess && c->d_cellE) {
-      cell_mean_kernel<<<blocks_for(L.NC), 256, 0, c->stream>>>(cellEf, fx - 1, fy - 1, L.cellE,
-                                                               L.nx - 1, L.ny - 1, L.nz - 1);
+      cell_mean_kernel<<<blocks_for(L.NC), 256, 0, c->stream>>>(cellEf, fx - 1, fy - 1, fz - 1,
+                                                               L.cellE, L.nx - 1, L.ny - 1,
+                                                               L.nz - 1);
       e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
-      // FP64 diagonal; FP32 hierarchy: computed in the fine level's FP32 work vectors,
-      // which hold 12 N_0 >= 24 N_l bytes each
+      // FP64 diagonal; FP32 hierarchy: computed in the fine level's FP32 work vectors r
+      // and d, allocated with >= 24 N_1 bytes each
       double* diag = f32 ? (double*)c->mg[0].r : (double*)L.t;
       double* dinv64 = f32 ? (double*)c->mg[0].d : (double*)L.dinv;
       ElemArgs E{};
@@ -724,14 +818,14 @@ void free_mg(vfgpu_ctx* c) {
 
 long long mg_memory_bytes(int nx, int ny, int nz, int bytes) {
   const long long N = (long long)nx * ny * nz;
-  long long b = 5 * 3 * N * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine work vectors
-  int nlev = 1;
-  while ((nx - 1) % 2 == 0 && (ny - 1) % 2 == 0 && (nz - 1) % 2 == 0 && (nx - 1) / 2 + 1 >= 5 &&
-         (ny - 1) / 2 + 1 >= 5 && (nz - 1) / 2 + 1 >= 5) {
-    nx = (nx - 1) / 2 + 1;
-    ny = (ny - 1) / 2 + 1;
-    nz = (nz - 1) / 2 + 1;
-    nlev++;
+  const long long N1 = (long long)coarser(nx) * coarser(ny) * coarser(nz);
+  const long long nrd = bytes == 4 ? std::max(3 * N, 6 * N1) : 3 * N;
+  long long b = (3 * 3 * N + 2 * nrd) * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine vectors
+  const int nlev = mg_levels(nx, ny, nz);
+  for (int l = 1; l < nlev; l++) {
+    nx = coarser(nx);
+    ny = coarser(ny);
+    nz = coarser(nz);
     const long long Nl = (long long)nx * ny * nz, NCl = (long long)(nx - 1) * (ny - 1) * (nz - 1);
     const TilePlan p = u_plan(nx, ny, nz, bytes, 148);
     b += (long long)(p.seamX + p.seamY) * bytes + 7 * 3 * Nl * bytes + Nl * 8 +
