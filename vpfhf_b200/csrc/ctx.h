@@ -85,6 +85,8 @@ struct vfgpu_ctx {
     double* v64 = nullptr;                     // coarse phase field in FP64 (the diagonal's input)
     uint8_t *bc = nullptr, *elayer = nullptr;
     float* cellE = nullptr;
+    int* xi = nullptr;     // transfer from the finer level: pI (x, y, z), rlo (x, y, z), rn (x, y, z)
+    double* xw = nullptr;  // pw (x, y, z)
     vfgpu::ETab tab{};
     double* coef = nullptr;  // device, 64: lmax, 1/theta, Chebyshev (c1, c2) pairs, scratch
   };

@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "abi_util.h"
+#include "ops.cuh"
 #include "solver.h"
 #include "vec.h"
 
@@ -63,7 +64,7 @@ struct Lin {
   int I;
   double whi;
 };
-__device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
+__host__ __device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
   const long long num = (long long)i * (nc - 1), den = nf - 1;
   Lin l;
   l.I = (int)(num / den);
@@ -71,22 +72,24 @@ __device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
   return l;
 }
 
-// The fine nodes of one axis that coarse node I's hat function covers, with its weights
-// (the entries of the prolongation's column I); at most 5 for a ratio of <= 2.
-__device__ __forceinline__ int coarse_support(int I, int nf, int nc, int (&idx)[6], double (&w)[6]) {
-  int n = 0;
-  const int lo = I > 0 ? (int)(((long long)(I - 1) * (nf - 1)) / (nc - 1)) : 0;
-  const int hi = min(nf - 1, (int)(((long long)(I + 1) * (nf - 1) + (nc - 2)) / (nc - 1)));
-  for (int i = lo; i <= hi && n < 6; i++) {
-    const Lin l = fine_in_coarse(i, nf, nc);
-    const double wt = l.I == I ? 1.0 - l.whi : (l.I + 1 == I ? l.whi : 0.0);
-    if (wt != 0.0) {
-      idx[n] = i;
-      w[n] = wt;
-      n++;
-    }
-  }
-  return n;
+// One axis of the transfer between a level and the next coarser one, tabulated at the
+// hierarchy's build: fine node i lies in coarse cell pI[i] with upper weight pw[i]
+// (fine_in_coarse), and coarse node I's hat function covers the fine nodes
+// [rlo[I], rlo[I] + rn[I]) (<= 5 for a ratio of <= 2) with nonzero weight.
+struct XferAxis {
+  const int* pI;
+  const double* pw;
+  const int* rlo;
+  const int* rn;
+};
+struct Xfer {
+  XferAxis a[3];
+};
+
+// Weight of coarse node I at fine node i (the prolongation's entry).
+__device__ __forceinline__ double hat(const XferAxis& A, int i, int I) {
+  const double w = A.pw[i];
+  return A.pI[i] == I ? 1.0 - w : w;
 }
 
 // Restriction of the residual b - t (the transpose of prolong_add_kernel): coarse node I
@@ -94,26 +97,37 @@ __device__ __forceinline__ int coarse_support(int I, int nf, int nc, int (&idx)[
 // fine Dirichlet dofs; coarse Dirichlet dofs are zeroed.
 template <typename T>
 __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ tf,
-                                const uint8_t* __restrict__ bc_f, int fx, int fy, int fz,
+                                const uint8_t* __restrict__ bc_f, int fx, int fy, const Xfer X,
                                 T* __restrict__ rc, int cx, int cy, int cz,
                                 const uint8_t* __restrict__ bc_c) {
   const int64_t Nc = (int64_t)cx * cy * cz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % cx), J = (int)((q / cx) % cy), K = (int)(q / ((int64_t)cx * cy));
-    int ix[6], iy[6], iz[6];
-    double wx[6], wy[6], wz[6];
-    const int nxs = coarse_support(I, fx, cx, ix, wx), nys = coarse_support(J, fy, cy, iy, wy),
-              nzs = coarse_support(K, fz, cz, iz, wz);
+    const int x0 = X.a[0].rlo[I], nxs = X.a[0].rn[I];
+    const int y0 = X.a[1].rlo[J], nys = X.a[1].rn[J];
+    const int z0 = X.a[2].rlo[K], nzs = X.a[2].rn[K];
+    double wx[5];
+#pragma unroll
+    for (int c1 = 0; c1 < 5; c1++) wx[c1] = c1 < nxs ? hat(X.a[0], x0 + c1, I) : 0.0;
     T acc[3] = {T(0), T(0), T(0)};
-    for (int c3 = 0; c3 < nzs; c3++)
-      for (int c2 = 0; c2 < nys; c2++)
-        for (int c1 = 0; c1 < nxs; c1++) {
-          const T w = T(wz[c3] * wy[c2] * wx[c1]);
-          const int64_t n = node_index(ix[c1], iy[c2], iz[c3], fx, fy);
-          const unsigned bf_bits = bc_f[n];
-          for (int c = 0; c < 3; c++)
-            if (!((bf_bits >> c) & 1u)) acc[c] += w * (bf[3 * n + c] - tf[3 * n + c]);
+    for (int c3 = 0; c3 < nzs; c3++) {
+      const double wz = hat(X.a[2], z0 + c3, K);
+      for (int c2 = 0; c2 < nys; c2++) {
+        const double wzy = wz * hat(X.a[1], y0 + c2, J);
+        const int64_t row = node_index(x0, y0 + c2, z0 + c3, fx, fy);
+#pragma unroll
+        for (int c1 = 0; c1 < 5; c1++) {
+          if (c1 < nxs) {
+            const T w = T(wzy * wx[c1]);
+            const int64_t n = row + c1;
+            const unsigned bf_bits = bc_f[n];
+#pragma unroll
+            for (int c = 0; c < 3; c++)
+              if (!((bf_bits >> c) & 1u)) acc[c] += w * (bf[3 * n + c] - tf[3 * n + c]);
+          }
         }
+      }
+    }
     const unsigned b = bc_c[q];
     for (int c = 0; c < 3; c++) rc[3 * q + c] = ((b >> c) & 1u) ? T(0) : acc[c];
   }
@@ -121,26 +135,26 @@ __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ 
 
 // x_f += trilinear interpolation of e_c; fine Dirichlet dofs untouched.
 template <typename T>
-__global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy, int cz,
+__global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy, const Xfer X,
                                    T* __restrict__ xf, int fx, int fy, int fz,
                                    const uint8_t* __restrict__ bc_f) {
   const int64_t Nf = (int64_t)fx * fy * fz;
   GRID_STRIDE(q, Nf) {
     const int i = (int)(q % fx), j = (int)((q / fx) % fy), k = (int)(q / ((int64_t)fx * fy));
-    const Lin lx = fine_in_coarse(i, fx, cx), ly = fine_in_coarse(j, fy, cy),
-              lz = fine_in_coarse(k, fz, cz);
+    const int Ix = X.a[0].pI[i], Iy = X.a[1].pI[j], Iz = X.a[2].pI[k];
+    const double hx = X.a[0].pw[i], hy = X.a[1].pw[j], hz = X.a[2].pw[k];
     T acc[3] = {T(0), T(0), T(0)};
     for (int dk = 0; dk < 2; dk++) {
-      const double wzk = dk ? lz.whi : 1.0 - lz.whi;
+      const double wzk = dk ? hz : 1.0 - hz;
       if (wzk == 0.0) continue;
       for (int dj = 0; dj < 2; dj++) {
-        const double wyj = dj ? ly.whi : 1.0 - ly.whi;
+        const double wyj = dj ? hy : 1.0 - hy;
         if (wyj == 0.0) continue;
         for (int di = 0; di < 2; di++) {
-          const double wxi = di ? lx.whi : 1.0 - lx.whi;
+          const double wxi = di ? hx : 1.0 - hx;
           if (wxi == 0.0) continue;
           const T w = T(wzk * wyj * wxi);
-          const int64_t n = node_index(lx.I + di, ly.I + dj, lz.I + dk, cx, cy);
+          const int64_t n = node_index(Ix + di, Iy + dj, Iz + dk, cx, cy);
           for (int c = 0; c < 3; c++) acc[c] += w * ec[3 * n + c];
         }
       }
@@ -245,6 +259,107 @@ __global__ void cheb_step_kernel(T* __restrict__ x, T* __restrict__ d, T* __rest
   }
 }
 
+// Degree 1 (a Jacobi step weighted 1/theta) in one pass: x += dinv (b - t) / theta, or
+// x = dinv b / theta from x = 0 (t null) -- cheb_init_kernel and the last
+// cheb_step_kernel's arithmetic (the product rounded before the add, as there) without
+// the r and d vectors.
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+template <typename T>
+__global__ void jacobi1_kernel(const T* __restrict__ b, const T* __restrict__ t,
+                               const T* __restrict__ dinv, T* __restrict__ x,
+                               const double* __restrict__ coef, int64_t n) {
+  const T inv_theta = T(coef[1]);
+  GRID_STRIDE(i, n) {
+    const T di = mul_rn(dinv[i] * (t ? b[i] - t[i] : b[i]), inv_theta);
+    x[i] = t ? x[i] + di : di;
+  }
+}
+
+// The coarsest level's Chebyshev solve from x = 0 in one CTA (the level has <= 8 nodes
+// per axis): the same iteration as chebyshev() with zero_start, its operator applied as
+// one element per thread into shared memory (ncell x 8 x 3 values) and gathered per node
+// in a fixed order, so the result is deterministic.  Replaces 2 deg launches.
+constexpr int kCoarseThreads = 256, kCoarseMaxNodes = 8 * 8 * 8;
+template <typename Op>
+__global__ void __launch_bounds__(kCoarseThreads, 1)
+    coarse_cheb_kernel(const typename Op::Args A0, const LayerTable L,
+                       const typename Op::T* __restrict__ b, typename Op::T* __restrict__ x,
+                       typename Op::T* __restrict__ r, typename Op::T* __restrict__ d,
+                       const typename Op::T* __restrict__ dinv, const double* __restrict__ coef,
+                       int deg) {
+  using T = typename Op::T;
+  extern __shared__ __align__(16) unsigned char coarse_smem[];
+  T* yc = reinterpret_cast<T*>(coarse_smem);  // [cell][corner][component]
+  typename Op::Args A = A0;
+  A.x = d;
+  const int nx = A.nx, ny = A.ny, nz = A.nz, cx = nx - 1, cy = ny - 1, cz = nz - 1;
+  const int N = nx * ny * nz, ncell = cx * cy * cz;
+  const T inv_theta = T(coef[1]);
+  for (int n = threadIdx.x; n < N; n += blockDim.x)
+    for (int c = 0; c < 3; c++) {
+      const int i = 3 * n + c;
+      const T ri = dinv[i] * b[i];
+      r[i] = ri;
+      d[i] = ri * inv_theta;
+      x[i] = T(0);
+    }
+  for (int k = 0; k < deg; k++) {
+    const bool last = k == deg - 1;
+    if (!last) {
+      __syncthreads();  // d complete
+      for (int e = threadIdx.x; e < ncell; e += blockDim.x) {
+        const int ex = e % cx, ey = (e / cx) % cy, ez = e / (cx * cy);
+        T in[8][Op::NIN], out[8][Op::NC];
+#pragma unroll
+        for (int a = 0; a < 8; a++) {
+          const typename Op::T* src[Op::NIN];
+          Op::node_src(A, node_index(ex + (a & 1), ey + ((a >> 1) & 1), ez + (a >> 2), nx, ny), src);
+#pragma unroll
+          for (int q = 0; q < Op::NIN; q++) in[a][q] = *src[q];
+        }
+        Op::element(A, L, ex, ey, ez, in, out);
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+#pragma unroll
+          for (int c = 0; c < 3; c++) yc[(e * 8 + a) * 3 + c] = out[a][c];
+      }
+      __syncthreads();  // element values complete
+    }
+    const T c1 = last ? T(0) : T(coef[2 + 2 * k]), c2 = last ? T(0) : T(coef[3 + 2 * k]);
+    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+      const int i0 = n % nx, j0 = (n / nx) % ny, k0 = n / (nx * ny);
+      T val[3] = {T(0), T(0), T(0)};
+      if (!last)
+        for (int dk = 0; dk < 2; dk++)
+          for (int dj = 0; dj < 2; dj++)
+            for (int di = 0; di < 2; di++) {
+              const int ci = i0 - 1 + di, cj = j0 - 1 + dj, ck = k0 - 1 + dk;
+              if (ci < 0 || cj < 0 || ck < 0 || ci >= cx || cj >= cy || ck >= cz) continue;
+              const int a = (1 - di) + 2 * (1 - dj) + 4 * (1 - dk);
+              const int e = (ck * cy + cj) * cx + ci;
+              for (int c = 0; c < 3; c++) val[c] += yc[(e * 8 + a) * 3 + c];
+            }
+      const unsigned bb = A.bc ? A.bc[n] : 0u;
+      for (int c = 0; c < 3; c++) {
+        const int i = 3 * n + c;
+        const T di = d[i];
+        x[i] += di;
+        if (!last) {
+          const T t = ((bb >> c) & 1u) ? di : val[c];  // Dirichlet rows: t = d
+          const T ri = r[i] - dinv[i] * t;
+          r[i] = ri;
+          d[i] = c1 * di + c2 * ri;
+        }
+      }
+    }
+  }
+}
+
+template <typename Op> size_t coarse_smem_bytes(int ncell) {
+  return (size_t)ncell * 8 * 3 * sizeof(typename Op::T);
+}
+
 // Deterministic start vector of the power iteration in (-1/2, 1/2), 0 on Dirichlet dofs.
 template <typename T>
 __global__ void seed_kernel(T* __restrict__ x, const uint8_t* __restrict__ bc, int64_t N) {
@@ -333,6 +448,78 @@ __global__ void cheb_coef_kernel(double* __restrict__ coef, int deg, double lo, 
 
 // ---------------------------------------------------------------------------------
 // A level seen as a U operator in precision T.
+template <typename T> void* dalloc(int64_t n, cudaError_t& e) {
+  void* p = nullptr;
+  if (e == cudaSuccess) e = cudaMalloc(&p, std::max<int64_t>(1, n) * sizeof(T));
+  return p;
+}
+
+// Tabulates the transfer into level L from its finer neighbour (f nodes per axis):
+// per axis pI, pw (f entries) and rlo, rn (L's node count entries), in L.xi / L.xw.
+cudaError_t build_xfer(vfgpu_ctx::MGLevel& L, const int (&f)[3]) {
+  const int c[3] = {L.nx, L.ny, L.nz};
+  std::vector<int> xi;
+  std::vector<double> xw;
+  for (int d = 0; d < 3; d++) {  // pI, pw
+    for (int i = 0; i < f[d]; i++) {
+      const Lin l = fine_in_coarse(i, f[d], c[d]);
+      xi.push_back(l.I);
+      xw.push_back(l.whi);
+    }
+  }
+  std::vector<int> rn;
+  for (int d = 0; d < 3; d++) {  // rlo, rn: the fine nodes with a nonzero weight, an interval
+    std::vector<int> lo(c[d], f[d]), hi(c[d], -1);
+    for (int i = 0; i < f[d]; i++) {
+      const Lin l = fine_in_coarse(i, f[d], c[d]);
+      lo[l.I] = std::min(lo[l.I], i);
+      hi[l.I] = std::max(hi[l.I], i);
+      if (l.whi > 0.0) {
+        lo[l.I + 1] = std::min(lo[l.I + 1], i);
+        hi[l.I + 1] = std::max(hi[l.I + 1], i);
+      }
+    }
+    for (int I = 0; I < c[d]; I++) {
+      if (hi[I] < lo[I] || hi[I] - lo[I] >= 5) return cudaErrorInvalidValue;
+      xi.push_back(lo[I]);
+      rn.push_back(hi[I] - lo[I] + 1);
+    }
+  }
+  xi.insert(xi.end(), rn.begin(), rn.end());  // the order xfer_of reads
+  if (xi.size() != (size_t)(f[0] + f[1] + f[2]) + 2 * (size_t)(c[0] + c[1] + c[2]))
+    return cudaErrorInvalidValue;
+  cudaError_t e = cudaSuccess;
+  L.xi = (int*)dalloc<int>((int64_t)xi.size(), e);
+  L.xw = (double*)dalloc<double>((int64_t)xw.size(), e);
+  if (e == cudaSuccess) e = cudaMemcpy(L.xi, xi.data(), xi.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(L.xw, xw.data(), xw.size() * sizeof(double), cudaMemcpyHostToDevice);
+  return e;
+}
+
+// The transfer tables of level l (from level l - 1) as kernel arguments.
+Xfer xfer_of(vfgpu_ctx* c, int l) {
+  const auto& L = c->mg[l];
+  const auto& F = c->mg[l - 1];
+  const int f[3] = {F.nx, F.ny, F.nz}, n[3] = {L.nx, L.ny, L.nz};
+  Xfer X;
+  int oi = 0, ow = 0;
+  for (int d = 0; d < 3; d++) {
+    X.a[d].pI = L.xi + oi;
+    X.a[d].pw = L.xw + ow;
+    oi += f[d];
+    ow += f[d];
+  }
+  for (int d = 0; d < 3; d++) {
+    X.a[d].rlo = L.xi + oi;
+    oi += n[d];
+  }
+  for (int d = 0; d < 3; d++) {
+    X.a[d].rn = L.xi + oi;
+    oi += n[d];
+  }
+  return X;
+}
+
 template <typename T> struct LevelT {
   int nx, ny, nz;
   double hx, hy, hz;
@@ -440,6 +627,15 @@ cudaError_t level_apply(vfgpu_ctx* c, const LevelT<T>& V, const T* x, T* y) {
 template <typename T>
 cudaError_t chebyshev(vfgpu_ctx* c, const LevelT<T>& V, const T* b, T* x, int deg, bool zero_start) {
   const int64_t n3 = V.n3;
+  if (deg == 1) {
+    cudaError_t e = zero_start ? cudaSuccess : level_apply<T>(c, V, x, V.t);
+    if (e == cudaSuccess) {
+      jacobi1_kernel<T><<<blocks_for(n3), 256, 0, c->stream>>>(b, zero_start ? nullptr : V.t, V.dinv,
+                                                              x, V.coef, n3);
+      e = cudaGetLastError();
+    }
+    return e;
+  }
   cudaError_t e =
       zero_start ? cudaMemsetAsync(x, 0, n3 * sizeof(T), c->stream) : level_apply<T>(c, V, x, V.t);
   if (e == cudaSuccess) {
@@ -459,22 +655,49 @@ cudaError_t chebyshev(vfgpu_ctx* c, const LevelT<T>& V, const T* b, T* x, int de
   return e;
 }
 
+// The coarsest level's solve: kCoarseDeg Chebyshev steps from x = 0, in one CTA.
+template <typename T> cudaError_t coarse_solve(vfgpu_ctx* c, const LevelT<T>& V, const T* b, T* x) {
+  if (V.n3 / 3 > kCoarseMaxNodes || V.cflag) return chebyshev<T>(c, V, b, x, kCoarseDeg, true);
+  const UApplyArgs<T> A = level_args<T>(c, V, V.d, V.t);
+  const int ncell = (V.nx - 1) * (V.ny - 1) * (V.nz - 1);
+  if (A.ihx == A.ihy && A.ihy == A.ihz)
+    coarse_cheb_kernel<UOp<T, true>>
+        <<<1, kCoarseThreads, coarse_smem_bytes<UOp<T, true>>(ncell), c->stream>>>(
+            A, c->layers, b, x, V.r, V.d, V.dinv, V.coef, kCoarseDeg);
+  else
+    coarse_cheb_kernel<UOp<T>><<<1, kCoarseThreads, coarse_smem_bytes<UOp<T>>(ncell), c->stream>>>(
+        A, c->layers, b, x, V.r, V.d, V.dinv, V.coef, kCoarseDeg);
+  return cudaGetLastError();
+}
+
+// Lets the coarsest solve take the shared memory of an 8 x 8 x 8 level.
+template <typename T> cudaError_t coarse_attributes() {
+  const int ncell = (8 - 1) * (8 - 1) * (8 - 1);
+  cudaError_t e = cudaFuncSetAttribute(coarse_cheb_kernel<UOp<T, true>>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)coarse_smem_bytes<UOp<T, true>>(ncell));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(coarse_cheb_kernel<UOp<T>>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)coarse_smem_bytes<UOp<T>>(ncell));
+  return e;
+}
+
 // z = V-cycle(b) from level l down.
 template <typename T> cudaError_t vcycle(vfgpu_ctx* c, int l, const T* b, T* z) {
   const LevelT<T> V = view<T>(c, l);
-  if (l == (int)c->mg.size() - 1) return chebyshev<T>(c, V, b, z, kCoarseDeg, true);
+  if (l == (int)c->mg.size() - 1) return coarse_solve<T>(c, V, b, z);
   const LevelT<T> C = view<T>(c, l + 1);
   cudaError_t e = chebyshev<T>(c, V, b, z, kSmoothDeg, true);
   if (e == cudaSuccess) e = level_apply<T>(c, V, z, V.t);
   if (e == cudaSuccess) {
-    restrict_kernel<T><<<blocks_for(C.n3 / 3), 256, 0, c->stream>>>(b, V.t, V.bc, V.nx, V.ny, V.nz,
-                                                                    C.b, C.nx, C.ny, C.nz, C.bc);
+    restrict_kernel<T><<<blocks_for(C.n3 / 3), 256, 0, c->stream>>>(
+        b, V.t, V.bc, V.nx, V.ny, xfer_of(c, l + 1), C.b, C.nx, C.ny, C.nz, C.bc);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = vcycle<T>(c, l + 1, C.b, C.x);
   if (e == cudaSuccess) {
-    prolong_add_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(C.x, C.nx, C.ny, C.nz, z,
-                                                                      V.nx, V.ny, V.nz, V.bc);
+    prolong_add_kernel<T><<<blocks_for(V.n3 / 3), 256, 0, c->stream>>>(
+        C.x, C.nx, C.ny, xfer_of(c, l + 1), z, V.nx, V.ny, V.nz, V.bc);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = chebyshev<T>(c, V, b, z, kSmoothDeg, false);
@@ -502,19 +725,13 @@ inline int first_fine_cell(int k, int ncf, int ncc) {
   return a <= 0 ? 0 : (int)((a + b - 1) / b);
 }
 
-template <typename T> void* dalloc(int64_t n, cudaError_t& e) {
-  void* p = nullptr;
-  if (e == cudaSuccess) e = cudaMalloc(&p, std::max<int64_t>(1, n) * sizeof(T));
-  return p;
-}
-
 // Allocates the hierarchy in precision T (rebuilt when the precision changes).
 template <typename T> int mg_build(vfgpu_ctx* c) {
   if (!c->mg.empty() && c->mg_bytes == (int)sizeof(T)) return VFGPU_OK;
   free_mg(c);
   const int nlev = mg_levels(c->nx, c->ny, c->nz);
   if (nlev < 2) return fail(VFGPU_ERR_INVALID, "multigrid needs >= 9 nodes along some axis");
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = coarse_attributes<T>();
   c->mg_coef = (double*)dalloc<double>((int64_t)kCoefPerLevel * nlev, e);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->mg_coef, 0, sizeof(double) * kCoefPerLevel * nlev, c->stream);
   const bool f32 = sizeof(T) == 4;
@@ -543,6 +760,7 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
   }
   int nx = c->nx, ny = c->ny, nz = c->nz;
   for (int l = 1; l < nlev && e == cudaSuccess; l++) {
+    const int f[3] = {nx, ny, nz};
     nx = coarser(nx);
     ny = coarser(ny);
     nz = coarser(nz);
@@ -566,6 +784,7 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
     if (c->d_cellE) L.cellE = (float*)dalloc<float>(L.NC, e);
     etab_host(hx, hy, hz, &L.tab);
     L.coef = c->mg_coef + (int64_t)kCoefPerLevel * l;
+    if (e == cudaSuccess) e = build_xfer(L, f);
   }
   c->mg_bytes = (int)sizeof(T);
   c->mg_ready = false;
@@ -801,7 +1020,8 @@ void free_mg(vfgpu_ctx* c) {
     }
   }
   for (auto& L : c->mg) {
-    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.ev, L.bc, L.elayer, L.cellE};
+    void* bufs[] = {L.seam, L.x, L.b, L.r, L.d, L.t, L.dinv, L.ev, L.bc, L.elayer, L.cellE,
+                    L.xi, L.xw};
     for (void* p : bufs) cudaFree(p);
     if (L.v != (void*)L.v64) cudaFree(L.v);
     cudaFree(L.v64);
@@ -823,9 +1043,11 @@ long long mg_memory_bytes(int nx, int ny, int nz, int bytes) {
   long long b = (3 * 3 * N + 2 * nrd) * bytes + (bytes == 4 ? 3 * N * (4 + 8) : 0);  // fine vectors
   const int nlev = mg_levels(nx, ny, nz);
   for (int l = 1; l < nlev; l++) {
+    b += (long long)(nx + ny + nz) * (4 + 8);  // transfer tables
     nx = coarser(nx);
     ny = coarser(ny);
     nz = coarser(nz);
+    b += (long long)(nx + ny + nz) * 8;
     const long long Nl = (long long)nx * ny * nz, NCl = (long long)(nx - 1) * (ny - 1) * (nz - 1);
     const TilePlan p = u_plan(nx, ny, nz, bytes, 148);
     b += (long long)(p.seamX + p.seamY) * bytes + 7 * 3 * Nl * bytes + Nl * 8 +
