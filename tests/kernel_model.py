@@ -424,49 +424,41 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None):
 
 def v_element(xn, cg, aeps, h):
     """xn[8], cg[27] (weight-premultiplied mass coefficient) -> y[8]; the arithmetic of
-    v_element<T> in ops.cuh."""
+    v_element<T> in ops.cuh: closed-form stiffness moments, sum-factorised mass moments."""
     ihx, ihy, ihz = 1 / h[0], 1 / h[1], 1 / h[2]
     vol = h[0] * h[1] * h[2]
     m = modal8(xn)
-    QX, QY, QZ = np.zeros(4), np.zeros(4), np.zeros(4)
-    M = np.zeros(8)
-    SZ = np.zeros((3, 3))
-    for gz in range(3):
-        tz = GT[gz]
-        SY = np.zeros(3)
-        for gy in range(3):
-            ty = GT[gy]
-            SX = 0.0
-            for gx in range(3):
-                tx = GT[gx]
-                g = gx + 3 * gy + 9 * gz
-                Gx = (m[1] + m[3] * ty + m[5] * tz + m[7] * ty * tz) * ihx
-                Gy = (m[2] + m[3] * tx + m[6] * tz + m[7] * tx * tz) * ihy
-                Gz = (m[4] + m[5] * tx + m[6] * ty + m[7] * tx * ty) * ihz
-                xg = (m[0] + m[1] * tx + m[2] * ty + m[3] * tx * ty + m[4] * tz + m[5] * tx * tz
-                      + m[6] * ty * tz + m[7] * tx * ty * tz)
-                wa = aeps * vol * GW[gx] * GW[gy] * GW[gz]
-                SX += wa * Gx
-                SY[gx] += wa * Gy
-                SZ[gy, gx] += wa * Gz
-                psi = cg[g] * xg
-                M += psi * np.array([1, tx, ty, tx * ty, tz, tx * tz, ty * tz, tx * ty * tz])
-            QX += SX * np.array([1, ty, tz, ty * tz])
-        for gx in range(3):
-            QY += SY[gx] * np.array([1, GT[gx], tz, GT[gx] * tz])
-    for gy in range(3):
-        for gx in range(3):
-            QZ += SZ[gy, gx] * np.array([1, GT[gx], GT[gy], GT[gx] * GT[gy]])
+    av = aeps * vol
+    kx, ky, kz = av * ihx * ihx, av * ihy * ihy, av * ihz * ihz
 
-    def inv(Q, ih):
+    def bfly(q0, q1, q2, q3):
         A = np.empty((2, 2))
         for s1 in range(2):
             for s2 in range(2):
                 a, b = 2 * s1 - 1, 2 * s2 - 1
-                A[s1, s2] = (Q[0] / 4 + a * Q[1] / 2 + b * Q[2] / 2 + a * b * Q[3]) * ih
+                A[s1, s2] = q0 + a * q1 + b * q2 + a * b * q3
         return A
 
-    AX, AY, AZ = inv(QX, ihx), inv(QY, ihy), inv(QZ, ihz)
+    AX = bfly(kx / 4 * m[1], kx / 24 * m[3], kx / 24 * m[5], kx / 144 * m[7])
+    AY = bfly(ky / 4 * m[2], ky / 24 * m[3], ky / 24 * m[6], ky / 144 * m[7])
+    AZ = bfly(kz / 4 * m[4], kz / 24 * m[5], kz / 24 * m[6], kz / 144 * m[7])
+    P00, P01, P10, P11 = np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3)
+    for gz in range(3):
+        tz = GT[gz]
+        p = [m[0] + m[4] * tz, m[1] + m[5] * tz, m[2] + m[6] * tz, m[3] + m[7] * tz]
+        L0, L1 = np.zeros(3), np.zeros(3)
+        for gy in range(3):
+            ty = GT[gy]
+            q0, q1 = p[0] + p[2] * ty, p[1] + p[3] * ty
+            psi = [cg[gx + 3 * gy + 9 * gz] * (q0 + q1 * GT[gx]) for gx in range(3)]
+            L0[gy] = psi[0] + psi[1] + psi[2]
+            L1[gy] = psi[2] - psi[0]
+        P00[gz], P01[gz] = L0.sum(), L0[2] - L0[0]
+        P10[gz], P11[gz] = L1.sum(), L1[2] - L1[0]
+    t = GT[2]
+    M = np.array([P00.sum(), t * P10.sum(), t * P01.sum(), t * t * P11.sum(),
+                  t * (P00[2] - P00[0]), t * t * (P10[2] - P10[0]), t * t * (P01[2] - P01[0]),
+                  t ** 3 * (P11[2] - P11[0])])
     y = np.zeros(8)
     for k in range(2):
         for j in range(2):

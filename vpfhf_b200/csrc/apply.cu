@@ -7,7 +7,10 @@
 
 namespace vfgpu {
 
-constexpr int U_TY = 8, V_TY = 8;
+constexpr int U_TY = 8, V_TY = kVTileY;
+// V tiles carry 2 stages of 27 coefficients per cell in shared memory: 75 KB (FP32,
+// 2 CTAs per SM) or 150 KB (FP64, 1 CTA per SM).
+constexpr int V64_MINB = 1, V32_MINB = 2;
 // FP32 U operator: scalar UOp<float> (2 CTAs of 8 warps per SM) by default.  The
 // packed two-lane variant (UOpF2: two elements per thread, half the arithmetic
 // instructions) is kept as a build option; it needs 242 registers, so one CTA of
@@ -37,9 +40,35 @@ cudaError_t apply_kernel_attributes() {
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<float>, U_TY, 2>();
-  if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, 2>();
-  if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, 3>();
+  if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, V64_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, V32_MINB>();
   return e;
+}
+
+cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int nex, int ney, int nez) {
+  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                              CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                              CUtensorMapFloatOOBfill);
+  static const Encode encode = []() -> Encode {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return nullptr;
+    return reinterpret_cast<Encode>(fn);
+  }();
+  if (!encode) return cudaErrorNotSupported;
+  const int pitch = vcoef_pitch(nex);
+  const cuuint64_t dims[3] = {(cuuint64_t)nex, (cuuint64_t)ney, (cuuint64_t)27 * nez};
+  const cuuint64_t strides[2] = {(cuuint64_t)pitch * bytes, (cuuint64_t)pitch * ney * bytes};
+  const cuuint32_t box[3] = {32, (cuuint32_t)kVTileY, 27}, estride[3] = {1, 1, 1};
+  const CUresult r =
+      encode(map, bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3,
+             const_cast<void*>(coef), dims, strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
@@ -47,7 +76,7 @@ TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
 }
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
-  return tile_plan(nx, ny, nz, V_TY, 1, prec_bytes == 8 ? 2 : 3, num_sms);
+  return tile_plan(nx, ny, nz, V_TY, 1, prec_bytes == 8 ? V64_MINB : V32_MINB, num_sms);
 }
 
 template <>
@@ -69,12 +98,12 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
 template <>
 cudaError_t launch_v_apply<double>(const VApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
-  return launch_tile_apply<VOp<double>, V_TY, 2>(A, p, L, s);
+  return launch_tile_apply<VOp<double>, V_TY, V64_MINB>(A, p, L, s);
 }
 template <>
 cudaError_t launch_v_apply<float>(const VApplyArgs<float>& A, const TilePlan& p,
                                   const LayerTable& L, cudaStream_t s) {
-  return launch_tile_apply<VOp<float>, V_TY, 3>(A, p, L, s);
+  return launch_tile_apply<VOp<float>, V_TY, V32_MINB>(A, p, L, s);
 }
 
 }  // namespace vfgpu

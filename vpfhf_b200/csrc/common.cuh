@@ -1,6 +1,7 @@
 // common.cuh -- shared helpers for the vfgpu kernels (sm_100a).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -40,6 +41,18 @@ __host__ __device__ inline int64_t node_index(int i, int j, int k, int nx, int n
 }
 
 inline int ceil_div(int a, int b) { return (a + b - 1) / b; }
+
+// The V coupling coefficient (27 Gauss-point values per cell) is stored per element
+// layer as 27 planes of the layer's cells, [ez][g][ey][ex], with rows padded to a
+// multiple of 4 cells (16-byte row strides, the tensor-copy rule), so that the 27
+// values of a 32 x TY tile of cells are one box of a 3-D tensor copy.
+__host__ __device__ inline int vcoef_pitch(int nex) { return (nex + 3) & ~3; }
+__host__ __device__ inline int64_t vcoef_index(int g, int ex, int ey, int ez, int pitch, int ney) {
+  return (((int64_t)ez * 27 + g) * ney + ey) * pitch + ex;
+}
+__host__ __device__ inline int64_t vcoef_size(int nex, int ney, int nez) {
+  return (int64_t)27 * nez * ney * vcoef_pitch(nex);
+}
 
 // Deterministic sum of one double per thread over a block (any 1-3D shape with a
 // multiple of 32 threads): warp shuffle trees, then warp 0 sums the warp totals in

@@ -59,8 +59,10 @@ struct vfgpu_ctx {
   static constexpr int NP64 = 9, NP32 = 5;
   double* p64[NP64] = {nullptr};  // 3N + kPoolSlack doubles each
   float* p32[NP32] = {nullptr};   // 3N + kPoolSlack floats each
-  double* coef64 = nullptr;       // 27 per cell: V coupling coefficient
+  double* coef64 = nullptr;       // 27 per cell: V coupling coefficient (vcoef_index layout)
   float* coef32 = nullptr;
+  CUtensorMap vmap64{}, vmap32{}; // coef64 / coef32 as the V apply's tensor copies see them
+  unsigned* d_cerr = nullptr;     // set by a V apply whose coefficient copy timed out
   uint8_t* vmask = nullptr;       // N
   vfgpu::ETab h_tab{};            // element tables of the uniform element (kernel parameter)
   vfgpu::CGState* d_cg = nullptr; // device CG scalars

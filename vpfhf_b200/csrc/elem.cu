@@ -490,6 +490,7 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
   const int ei = (int)(cell % (E.nx - 1));
   const int ej = (int)((cell / (E.nx - 1)) % (E.ny - 1));
   const int ek = (int)(cell / ((int64_t)(E.nx - 1) * (E.ny - 1)));
+  const int pitch = vcoef_pitch(E.nx - 1);
   const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
@@ -524,8 +525,8 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
       const double tr = f11 + f22 + f33;
       const double S = tr < 0. ? 0. : kappa * tr * tr * .5, D = Wf - kappa * tr * tr * .5;
       const double cgv = e.w[g] * (2. * (S + D) + mass);
-      coef[(int64_t)g * NCELL + cell] = cgv;
-      if (coef32) coef32[(int64_t)g * NCELL + cell] = (float)cgv;
+      coef[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = cgv;
+      if (coef32) coef32[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = (float)cgv;
       continue;
     }
     double e11 = 0, e22 = 0, e33 = 0, e12 = 0, e23 = 0, e13 = 0;
@@ -545,8 +546,8 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
     const double s33 = l * e11 + l * e22 + (l + 2. * mu) * e33;
     const double W = (s11 * e11 + s22 * e22 + s33 * e33) * .5 + 2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
     const double cgv = e.w[g] * (2. * W + mass);
-    coef[(int64_t)g * NCELL + cell] = cgv;
-    if (coef32) coef32[(int64_t)g * NCELL + cell] = (float)cgv;
+    coef[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = cgv;
+    if (coef32) coef32[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = (float)cgv;
   }
 }
 
@@ -617,8 +618,7 @@ __global__ void v_diag_tp_kernel(const __grid_constant__ ElemArgs E, int color,
   const CellMat m = cell_mat(E, ei, ej, ek);
   const double aeps = m.Gc / E.atcv * .5 * E.epsilon;
   const double vol = E.hx * E.hy * E.hz;
-  const int64_t cell = ((int64_t)ek * (E.ny - 1) + ej) * (E.nx - 1) + ei;
-  const int64_t ncell = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  const int pitch = vcoef_pitch(E.nx - 1);
   double w27[27], c27[27], J[3][2][2], M[8];
 #pragma unroll
   for (int gz = 0; gz < 3; gz++)
@@ -628,7 +628,7 @@ __global__ void v_diag_tp_kernel(const __grid_constant__ ElemArgs E, int color,
       for (int gx = 0; gx < 3; gx++) {
         const int g = gx + 3 * gy + 9 * gz;
         w27[g] = vol * (w1(gx) * w1(gy) * w1(gz));
-        c27[g] = coef[(int64_t)g * ncell + cell];
+        c27[g] = coef[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)];
       }
   face_moments<true>(w27, J);
   contract27sq(c27, M);

@@ -6,7 +6,9 @@
 //        VF_BilinearFormVCoupling3D_local (VFMech.c:2040-2115):
 //        (Gc/(2 c_w)) eps int grad(phi_a).grad(phi_b) + int c(x) phi_a phi_b,
 //        c = 2 W(u) [+ Gc/(2 c_w)/eps for AT2], with c premultiplied by the Gauss
-//        weight and stored per element and Gauss point (vfgpu v_coef kernel).
+//        weight and stored per element and Gauss point (vfgpu v_coef kernel); the
+//        tile engine stages each element layer's 27 values per cell into shared
+//        memory with one 3-D tensor copy (cmap), two layers ahead of use.
 //        An optional mask removes dofs (row and column) for the reduced-space
 //        solves of the VI Newton method and the rows+columns Dirichlet/irreversibility
 //        treatment (VFCartFE.c:1305-1454, VFMech.c:2637-2682).
@@ -22,7 +24,7 @@ namespace vfgpu {
 template <typename T_, bool CUBIC = false> struct UOp {
   using T = T_;
   using Args = UApplyArgs<T>;
-  static constexpr int NC = 3, NIN = 4, EPT = 1;
+  static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + 3 * n;
     src[1] = A.x + 3 * n + 1;
@@ -75,7 +77,7 @@ template <typename T_, bool CUBIC = false> struct UOp {
 template <typename T_> struct UOpNC {
   using T = T_;
   using Args = UApplyArgs<T>;
-  static constexpr int NC = 3, NIN = 4, EPT = 1;
+  static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<T>::node_src(A, n, src);
   }
@@ -117,7 +119,7 @@ template <typename T_> struct UOpNC {
 struct UOpF2 {
   using T = float;
   using Args = UApplyArgs<float>;
-  static constexpr int NC = 3, NIN = 4, EPT = 2;
+  static constexpr int NC = 3, NIN = 4, EPT = 2, CV = 0;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<float>::node_src(A, n, src);
   }
@@ -164,12 +166,14 @@ struct UOpF2 {
 };
 
 template <typename T> struct VApplyArgs {
+  CUtensorMap cmap;                   // the coefficient as a 3-D tensor (ex, ey, 27 ez + g),
+                                      // box 32 x TY x 27 (vcoef_index layout)
+  unsigned* __restrict__ cerr;        // set to 1 when a coefficient copy was not seen in time
   const T* __restrict__ x;            // N input; must be 0 on masked dofs (the reduced-space
                                       // CG keeps its directions 0 there), which makes the
                                       // masked columns drop out
   T* __restrict__ y;                  // N output
   const uint8_t* __restrict__ mask;   // N: nonzero => dof removed (y = 0); or null
-  const T* __restrict__ coef;         // 27 per cell: w_g (2 W_g [+ A/eps]), coef[g * ncell + cell]
   const uint8_t* __restrict__ elayer; // nz-1 or null
   T* __restrict__ seamX;
   T* __restrict__ seamY;
@@ -180,63 +184,70 @@ template <typename T> struct VApplyArgs {
   T ihx, ihy, ihz, vol;
 };
 
-// y[a] = (K_V,e x_e)[a] for one element (same modal scheme as u_element).
+// A[s1][s2] = q0 + s1 q1 + s2 q2 + s1 s2 q3, s = -1 (index 0) or +1 (index 1).
 template <typename T>
-__device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict__ cg, int64_t cs,
+__device__ __forceinline__ void butterfly4(T q0, T q1, T q2, T q3, T (&A)[2][2]) {
+  const T r0m = q0 - q2, r0p = q0 + q2, r1m = q1 - q3, r1p = q1 + q3;
+  A[0][0] = r0m - r1m;
+  A[1][0] = r0m + r1m;
+  A[0][1] = r0p - r1p;
+  A[1][1] = r0p + r1p;
+}
+
+// y[a] = (K_V,e x_e)[a] for one element, in the modal form x = sum_p m_p t^p on the
+// unit cell t in [-1/2, 1/2]^3 (modal8, as u_element):
+//  - stiffness aeps int grad(phi_a).grad(x): the x-derivative is ihx (m1 + m3 ty +
+//    m5 tz + m7 ty tz), and its moments against {1, ty, tz, ty tz} are exactly
+//    {m1, m3 / 12, m5 / 12, m7 / 144} ihx (<t> = 0, <t^2> = 1/12), which is what the
+//    reference's 27-point Gauss sum gives for this integrand (VF_BilinearFormVAT1/
+//    AT23D_local, VFMech.c:2040-2115; 3 points per axis are exact for it), so the
+//    closed form replaces the sum; likewise y and z;
+//  - mass int c phi_a x with c given per Gauss point: x at the 27 points by sum
+//    factorisation of the modal form, psi_g = c_g x_g, and the moments
+//    M_p = sum_g psi_g t^p by sum factorisation along x, then y, then z.
+template <typename T>
+__device__ __forceinline__ void v_element(const T (&xn)[8], const T* __restrict__ cg, int cs,
                                           T aeps, T ihx, T ihy, T ihz, T vol, T (&y)[8]) {
   T m[8];
   modal8(xn, m);
-  const T Ax = m[1] * ihx, Bx = m[3] * ihx, Cx = m[5] * ihx, Dx = m[7] * ihx;
-  const T Ay = m[2] * ihy, By = m[3] * ihy, Cy = m[6] * ihy, Dy = m[7] * ihy;
-  const T Az = m[4] * ihz, Bz = m[5] * ihz, Cz = m[6] * ihz, Dz = m[7] * ihz;
-  T QX[4] = {0, 0, 0, 0}, QY[4] = {0, 0, 0, 0}, QZ[4] = {0, 0, 0, 0}, SZ[3][3];
-  T M[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // value moments sum psi P_a(tx) P_b(ty) P_c(tz)
   const T av = aeps * vol;
+  const T kx = av * ihx * ihx, ky = av * ihy * ihy, kz = av * ihz * ihz;
+  const T c4 = T(0.25), c24 = T(1.0 / 24.0), c144 = T(1.0 / 144.0);
+  T AX[2][2], AY[2][2], AZ[2][2];
+  butterfly4((kx * c4) * m[1], (kx * c24) * m[3], (kx * c24) * m[5], (kx * c144) * m[7], AX);
+  butterfly4((ky * c4) * m[2], (ky * c24) * m[3], (ky * c24) * m[6], (ky * c144) * m[7], AY);
+  butterfly4((kz * c4) * m[4], (kz * c24) * m[5], (kz * c24) * m[6], (kz * c144) * m[7], AZ);
+  // per gz: sums over the (gx, gy) points of psi {1, ty, tx, tx ty}, each t as its sign
+  T P00[3], P01[3], P10[3], P11[3];
 #pragma unroll
   for (int gz = 0; gz < 3; gz++) {
-    const T ax = lin(gz, Ax, Cx), bx = lin(gz, Bx, Dx), ay = lin(gz, Ay, Cy), by = lin(gz, By, Dy);
     const T p0 = lin(gz, m[0], m[4]), p1 = lin(gz, m[1], m[5]);
     const T p2 = lin(gz, m[2], m[6]), p3 = lin(gz, m[3], m[7]);
-    T SY[3];
+    T L0[3], L1[3];
 #pragma unroll
     for (int gy = 0; gy < 3; gy++) {
-      const T Gx = lin(gy, ax, bx), al = lin(gy, Az, Cz), be = lin(gy, Bz, Dz);
       const T q0 = lin(gy, p0, p2), q1 = lin(gy, p1, p3);
-      T SX = T(0);
+      T psi[3];
 #pragma unroll
-      for (int gx = 0; gx < 3; gx++) {
-        const int g = gx + 3 * gy + 9 * gz;
-        const T Gy = lin(gx, ay, by), Gz = lin(gx, al, be), xg = lin(gx, q0, q1);
-        const T wa = av * (gw<T>(gx) * gw<T>(gy) * gw<T>(gz));
-        const T fx = wa * Gx, fy = wa * Gy, fz = wa * Gz;
-        const T psi = cg[g * cs] * xg;
-        SX = gx == 0 ? fx : SX + fx;
-        SY[gx] = gy == 0 ? fy : SY[gx] + fy;
-        SZ[gy][gx] = gz == 0 ? fz : SZ[gy][gx] + fz;
-        // value moments
-        const T tx = gt<T>(gx), ty = gt<T>(gy), tz = gt<T>(gz);
-        M[0] += psi;
-        if (gx != 1) M[1] = fma(tx, psi, M[1]);
-        if (gy != 1) M[2] = fma(ty, psi, M[2]);
-        if (gx != 1 && gy != 1) M[3] = fma(tx * ty, psi, M[3]);
-        if (gz != 1) M[4] = fma(tz, psi, M[4]);
-        if (gx != 1 && gz != 1) M[5] = fma(tx * tz, psi, M[5]);
-        if (gy != 1 && gz != 1) M[6] = fma(ty * tz, psi, M[6]);
-        if (gx != 1 && gy != 1 && gz != 1) M[7] = fma(tx * ty * tz, psi, M[7]);
-      }
-      moment4(QX, gy, gz, SX);
+      for (int gx = 0; gx < 3; gx++) psi[gx] = cg[(gx + 3 * gy + 9 * gz) * cs] * lin(gx, q0, q1);
+      L0[gy] = (psi[0] + psi[1]) + psi[2];
+      L1[gy] = psi[2] - psi[0];
     }
-#pragma unroll
-    for (int gx = 0; gx < 3; gx++) moment4(QY, gx, gz, SY[gx]);
+    P00[gz] = (L0[0] + L0[1]) + L0[2];
+    P01[gz] = L0[2] - L0[0];
+    P10[gz] = (L1[0] + L1[1]) + L1[2];
+    P11[gz] = L1[2] - L1[0];
   }
-#pragma unroll
-  for (int gy = 0; gy < 3; gy++)
-#pragma unroll
-    for (int gx = 0; gx < 3; gx++) moment4(QZ, gx, gy, SZ[gy][gx]);
-  T AX[2][2], AY[2][2], AZ[2][2];
-  inv_butterfly(QX, ihx, AX);
-  inv_butterfly(QY, ihy, AY);
-  inv_butterfly(QZ, ihz, AZ);
+  const T t1 = T(VF_TAU), t2 = T(VF_TAU * VF_TAU), t3 = T(VF_TAU * VF_TAU * VF_TAU);
+  T M[8];  // value moments sum psi P_a(tx) P_b(ty) P_c(tz)
+  M[0] = (P00[0] + P00[1]) + P00[2];
+  M[1] = t1 * ((P10[0] + P10[1]) + P10[2]);
+  M[2] = t1 * ((P01[0] + P01[1]) + P01[2]);
+  M[3] = t2 * ((P11[0] + P11[1]) + P11[2]);
+  M[4] = t1 * (P00[2] - P00[0]);
+  M[5] = t2 * (P10[2] - P10[0]);
+  M[6] = t2 * (P01[2] - P01[0]);
+  M[7] = t3 * (P11[2] - P11[0]);
   // value part: sum_g psi prod_d (1/2 + s_d t_d) -> 3 inverse butterflies over M
   T b1[8], b2[8], b3[8];
 #pragma unroll
@@ -275,19 +286,21 @@ template <typename T_> struct VOp {
   using T = T_;
   using Args = VApplyArgs<T>;
   static constexpr int NC = 1, NIN = 1, EPT = 1;
+  static constexpr int CV = 27;  // per-cell values staged by the engine (the coefficient)
+  __device__ __forceinline__ static const CUtensorMap* cell_map(const Args& A) { return &A.cmap; }
+  __device__ __forceinline__ static unsigned* cell_err(const Args& A) { return A.cerr; }
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + n;
   }
+  // cc: the element's 27 coefficients in shared memory, cs apart
   __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
                                                  int ey, int ez, const T (&in)[8][NIN],
-                                                 T (&out)[8][NC]) {
+                                                 T (&out)[8][NC], const T* cc, int cs) {
     T xn[8], yn[8];
 #pragma unroll
     for (int a = 0; a < 8; a++) xn[a] = in[a][0];
     const int layer = A.elayer ? A.elayer[ez] : 0;
-    const int64_t cell = ((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex;
-    const int64_t ncell = (int64_t)(A.nx - 1) * (A.ny - 1) * (A.nz - 1);
-    v_element<T>(xn, A.coef + cell, ncell, T(A.P->aeps[layer]), A.ihx, A.ihy, A.ihz, A.vol, yn);
+    v_element<T>(xn, cc, cs, T(A.P->aeps[layer]), A.ihx, A.ihy, A.ihz, A.vol, yn);
 #pragma unroll
     for (int a = 0; a < 8; a++) out[a][0] = yn[a];
   }

@@ -17,6 +17,8 @@ void free_solver(vfgpu_ctx* c) {
   for (auto& p : c->p32) cudaFree(p), p = nullptr;
   cudaFree(c->coef64);
   cudaFree(c->coef32);
+  cudaFree(c->d_cerr);
+  c->d_cerr = nullptr;
   cudaFree(c->vmask);
   cudaFree(c->d_cg);
   cudaFree(c->d_red);
@@ -43,8 +45,18 @@ static int solve_buffers(vfgpu_ctx* c) {
     if (e == cudaSuccess) e = cudaMalloc((void**)&p, n3 * sizeof(double));
   for (auto& p : c->p32)
     if (e == cudaSuccess) e = cudaMalloc((void**)&p, n3 * sizeof(float));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef64, 27 * (size_t)c->NC * sizeof(double));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef32, 27 * (size_t)c->NC * sizeof(float));
+  const size_t ncoef = (size_t)vcoef_size(c->nx - 1, c->ny - 1, c->nz - 1);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef64, ncoef * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->coef32, ncoef * sizeof(float));
+  // row padding is copied but never used; keep it defined
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->coef64, 0, ncoef * sizeof(double), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->coef32, 0, ncoef * sizeof(float), c->stream);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cerr, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
+  if (e == cudaSuccess)
+    e = vcoef_tensor_map(&c->vmap64, c->coef64, 8, c->nx - 1, c->ny - 1, c->nz - 1);
+  if (e == cudaSuccess)
+    e = vcoef_tensor_map(&c->vmap32, c->coef32, 4, c->nx - 1, c->ny - 1, c->nz - 1);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->vmask, (size_t)c->N);
   if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cg, sizeof(CGState));
   if (e == cudaSuccess)
@@ -117,13 +129,14 @@ static cudaError_t u_load(vfgpu_ctx* c, const ElemArgs& E, double* f, const doub
 }
 
 template <typename T>
-static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask, const T* coef,
-                            T* seam, const TilePlan& p) {
+static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask,
+                            const CUtensorMap& cmap, T* seam, const TilePlan& p) {
   VApplyArgs<T> A{};
+  A.cmap = cmap;
+  A.cerr = c->d_cerr;
   A.x = x;
   A.y = y;
   A.mask = mask;
-  A.coef = coef;
   A.elayer = c->d_elayer;
   A.seamX = seam;
   A.seamY = seam + p.seamX;
@@ -136,6 +149,18 @@ static VApplyArgs<T> v_args(vfgpu_ctx* c, const T* x, T* y, const uint8_t* mask,
   A.vol = T(c->hx * c->hy * c->hz);
   A.P = c->d_params;
   return A;
+}
+
+// VFGPU_ERR_CUDA when a V apply gave up waiting for its coefficient copies (the
+// flag is cleared for the next solve).
+static int check_cell_copies(vfgpu_ctx* c) {
+  unsigned flag = 0;
+  cudaError_t e = cudaMemcpyAsync(&flag, c->d_cerr, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+  if (!flag) return VFGPU_OK;
+  cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
+  return fail(VFGPU_ERR_CUDA, "V apply: a coefficient tensor copy did not complete in time");
 }
 
 // Reads n doubles of d_out into h_out (synchronising the stream).
@@ -494,14 +519,14 @@ namespace vfgpu {
 // ---------------------------------------------------------------------------- V
 static cudaError_t v_apply64(vfgpu_ctx* c, const double* x, double* y, const uint8_t* mask,
                              const int* skip, double* dot = nullptr) {
-  VApplyArgs<double> A = v_args<double>(c, x, y, mask, c->coef64, c->seam64, c->vplan64);
+  VApplyArgs<double> A = v_args<double>(c, x, y, mask, c->vmap64, c->seam64, c->vplan64);
   A.skip = skip;
   A.dot = dot;
   return launch_v_apply<double>(A, c->vplan64, c->layers, c->stream);
 }
 static cudaError_t v_apply32(vfgpu_ctx* c, const float* x, float* y, const uint8_t* mask,
                              const int* skip, double* dot = nullptr) {
-  VApplyArgs<float> A = v_args<float>(c, x, y, mask, c->coef32, c->seam32, c->vplan32);
+  VApplyArgs<float> A = v_args<float>(c, x, y, mask, c->vmap32, c->seam32, c->vplan32);
   A.skip = skip;
   A.dot = dot;
   return launch_v_apply<float>(A, c->vplan32, c->layers, c->stream);
@@ -662,6 +687,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   }
   if (!reason) reason = -5;
   c->v32_stale = true;
+  if (int rc2 = check_cell_copies(c)) return rc2;
   S.reason = reason;
   S.fnorm = fnorm;
   S.seconds = w.seconds();
@@ -773,7 +799,7 @@ int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
   b += (long long)(p64.seamX + p64.seamY) * 8 + (long long)(p32.seamX + p32.seamY) * 4;
   b += 3 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
   b += vfgpu_ctx::NP64 * (3 * N + kPoolSlack) * 8 + vfgpu_ctx::NP32 * (3 * N + kPoolSlack) * 4;
-  b += 27 * NC * 12 + N;                                 // V coefficient (FP64 + FP32), mask
+  b += vcoef_size(g->nx - 1, g->ny - 1, g->nz - 1) * 12 + N;  // V coefficient (FP64 + FP32), mask
   b += (RED_BLOCKS + energy_blocks()) * 4 * 8 + 4096;    // reductions, scalars
   *bytes = b;
   return VFGPU_OK;

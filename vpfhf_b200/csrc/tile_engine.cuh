@@ -25,6 +25,12 @@
 //   DOT returns the node's x.y), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
 //   so that a queued batch of iterations costs nothing once it is done).
+// An Op with CV > 0 per-cell values (the V operator's 27 Gauss-point coefficients)
+//   supplies cell_map(A) (a 3-D tensor map, box 32 x TY x CV over (ex, ey, CV ez + g))
+//   and cell_err(A), and element(..., cc, cs) reads its cell's values from shared
+//   memory (cc[g cs]): one thread issues the tensor copy of element layer k + 2 into a
+//   2-stage buffer while layer k is computed, completion tracked by an mbarrier per
+//   stage (a bounded wait; on time-out *cell_err is set and the launch finishes).
 #pragma once
 
 #include <algorithm>
@@ -43,9 +49,65 @@ template <int TY, int EPT = 1> struct Tile {
 
 // Shared memory: a ring of 3 node planes [3][NIN][BY][BX] (planes k, k+1 in use,
 // k+2 in flight) and 2 buffers of element corner contributions [2][8*NC][TY][32].
-template <class Op, int TY> constexpr size_t tile_smem_bytes() {
+template <class Op, int TY> constexpr size_t tile_base_bytes() {
   using T = typename Op::T;
   return sizeof(T) * (3 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + 2 * 8 * Op::NC * 32 * TY);
+}
+// Per-cell value stages (Op::CV > 0): [kCellStages][CV][TY][32] at a 128-byte aligned
+// offset, then one 8-byte mbarrier per stage.
+constexpr int kCellStages = 2;
+template <class Op, int TY> constexpr size_t cell_off() { return (tile_base_bytes<Op, TY>() + 127) & ~size_t(127); }
+template <class Op, int TY> constexpr size_t cell_stage_bytes() {
+  return sizeof(typename Op::T) * Op::CV * TY * 32;
+}
+template <class Op, int TY> constexpr size_t tile_smem_bytes() {
+  if constexpr (Op::CV > 0)
+    return cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>() + kCellStages * 8;
+  else
+    return tile_base_bytes<Op, TY>();
+}
+
+// mbarrier and tensor-copy primitives (one thread issues; every thread may wait).
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"((unsigned)__cvta_generic_to_shared(bar)),
+               "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(bar)),
+               "r"(bytes) : "memory");
+}
+// Waits for the phase with the given parity to complete; gives up after ~2e9 cycles
+// (about a second), flags *err and returns.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return;
+    if (clock64() - t0 > 2000000000ll) {
+      if (err) atomicOr(err, 1u);
+      return;
+    }
+  }
+}
+// 3-D tiled tensor copy global -> shared (no multicast), completion on bar.
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"((unsigned)__cvta_generic_to_shared(bar))
+      : "memory");
 }
 
 // Asynchronous global -> shared copy of one 4- or 8-byte value (LDGSTS); with
@@ -68,7 +130,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // instantiation, so that plain applies carry none of its registers.
 template <class Op, int TY, int MINB, bool DOT>
 __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
-    tile_apply_kernel(const typename Op::Args A, const LayerTable L) {
+    tile_apply_kernel(const __grid_constant__ typename Op::Args A, const LayerTable L) {
   using T = typename Op::T;
   using G = Tile<TY, Op::EPT>;
   constexpr int EPT = Op::EPT;
@@ -137,6 +199,26 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   // the corner contributions of layer k together.
   fetch_plane(0, kf);
   fetch_plane(1, kf + 1);
+  // per-cell values of layers kf, kf + 1 (CV > 0): issued before the first barrier,
+  // which also publishes the mbarrier initialisation
+  [[maybe_unused]] T* cbuf = nullptr;
+  [[maybe_unused]] uint64_t* cbar = nullptr;
+  [[maybe_unused]] auto fetch_cells = [&](int st, int kz) {
+    if constexpr (Op::CV > 0) {
+      mbar_expect_tx(&cbar[st], (unsigned)cell_stage_bytes<Op, TY>());
+      tma_load_3d(cbuf + (size_t)st * Op::CV * TY * 32, Op::cell_map(A), X0, Y0, Op::CV * kz, &cbar[st]);
+    }
+  };
+  if constexpr (Op::CV > 0) {
+    cbuf = reinterpret_cast<T*>(smem_raw + cell_off<Op, TY>());
+    cbar = reinterpret_cast<uint64_t*>(smem_raw + cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>());
+    if (tid == 0) {
+      for (int st = 0; st < kCellStages; st++) mbar_init(&cbar[st], 1);
+      mbar_fence_init();
+      for (int st = 0; st < kCellStages; st++)
+        if (kf + st <= kl) fetch_cells(st, kf + st);
+    }
+  }
   cp_async_wait_all();
   __syncthreads();
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
@@ -146,6 +228,8 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     if constexpr (EPT == 1) {
       const int ey = Y0 + wy;
       T yc[8][NC];
+      if constexpr (Op::CV > 0)
+        mbar_wait(&cbar[(k - kf) % kCellStages], ((k - kf) / kCellStages) & 1, Op::cell_err(A));
       if (ex < nex && ey < ney) {
         T in[8][NIN];
 #pragma unroll
@@ -158,7 +242,12 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
 #pragma unroll
               for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
             }
-        Op::element(A, L, ex, ey, k, in, yc);
+        if constexpr (Op::CV > 0)
+          Op::element(A, L, ex, ey, k, in, yc,
+                      cbuf + (size_t)((k - kf) % kCellStages) * Op::CV * TY * 32 + wy * 32 + lane,
+                      TY * 32);
+        else
+          Op::element(A, L, ex, ey, k, in, yc);
       } else {
 #pragma unroll
         for (int a = 0; a < 8; a++)
@@ -213,6 +302,8 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     cp_async_wait_all();  // this thread's copies of plane k+2 have landed
     __syncthreads();      // ... and everyone's; corner contributions of layer k visible
     if (k + 3 <= kl + 1) fetch_plane(r0, k + 3);  // plane k is no longer read
+    if constexpr (Op::CV > 0)  // layer k's stage is no longer read
+      if (tid == 0 && k + kCellStages <= kl) fetch_cells((k - kf) % kCellStages, k + kCellStages);
 #pragma unroll
     for (int si = 0; si < G::NSLOT; si++) {
       const int s = tid + si * G::NT;
