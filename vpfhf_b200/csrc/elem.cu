@@ -117,6 +117,50 @@ __device__ __forceinline__ constexpr double bas(int i, int g) {
 }
 __device__ __forceinline__ constexpr double w1(int g) { return g == 1 ? 8.0 / 18.0 : 5.0 / 18.0; }
 
+// Modal form of a trilinear field on the unit cell t in [-1/2, 1/2]^3: f = sum_p m_p t^p
+// (p = px + 2 py + 4 pz; m_0 the mean, m_1 the x slope, ...), and its value and
+// gradient at the Gauss point (gx, gy, gz), t = -tau, 0, +tau.  With the point
+// indices known at compile time (unrolled loops) each is a short chain of FMAs, and
+// the compiler shares the partial sums between points.
+__device__ __forceinline__ void modal_of(const double (&f)[8], double (&m)[8]) {
+  double a[8], b[8];
+#pragma unroll
+  for (int p = 0; p < 4; p++) {
+    a[2 * p] = 0.5 * (f[2 * p] + f[2 * p + 1]);
+    a[2 * p + 1] = f[2 * p + 1] - f[2 * p];
+  }
+#pragma unroll
+  for (int k = 0; k < 2; k++)
+#pragma unroll
+    for (int al = 0; al < 2; al++) {
+      const double lo = a[al + 4 * k], hi = a[al + 2 + 4 * k];
+      b[al + 4 * k] = 0.5 * (lo + hi);
+      b[al + 2 + 4 * k] = hi - lo;
+    }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const double lo = b[q], hi = b[q + 4];
+    m[q] = 0.5 * (lo + hi);
+    m[q + 4] = hi - lo;
+  }
+}
+__device__ __forceinline__ double mlin(int g, double a, double b) {
+  return g == 1 ? a : (g == 0 ? fma(b, -VF_TAU, a) : fma(b, VF_TAU, a));
+}
+__device__ __forceinline__ double mval(const double (&m)[8], int gx, int gy, int gz) {
+  return mlin(gz, mlin(gy, mlin(gx, m[0], m[1]), mlin(gx, m[2], m[3])),
+              mlin(gy, mlin(gx, m[4], m[5]), mlin(gx, m[6], m[7])));
+}
+__device__ __forceinline__ double mdx(const double (&m)[8], int gx, int gy, int gz, double ih) {
+  return ih * mlin(gy, mlin(gz, m[1], m[5]), mlin(gz, m[3], m[7]));
+}
+__device__ __forceinline__ double mdy(const double (&m)[8], int gx, int gy, int gz, double ih) {
+  return ih * mlin(gx, mlin(gz, m[2], m[6]), mlin(gz, m[3], m[7]));
+}
+__device__ __forceinline__ double mdz(const double (&m)[8], int gx, int gy, int gz, double ih) {
+  return ih * mlin(gx, mlin(gy, m[4], m[6]), mlin(gy, m[5], m[7]));
+}
+
 // Trilinear field at the 27 points, g = gx + 3 gy + 9 gz.
 __device__ __forceinline__ void interp27(const double (&f)[8], double (&o)[27]) {
   double fx[4][3], fy[2][3][3];
@@ -480,10 +524,15 @@ __global__ void bc_diag_kernel(const uint8_t* __restrict__ bcbits, double* __res
 }
 
 // ElasticEnergyDensity3D_local (VFMech.c:32-106) at every Gauss point, times 2 and
-// the Gauss weight, plus the AT2 mass coefficient (VFMech.c:2040-2058).
-__global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* __restrict__ u,
-                              const double* __restrict__ theta, const double* __restrict__ thetaRef,
-                              double* __restrict__ coef, float* __restrict__ coef32) {
+// the Gauss weight, plus the AT2 mass coefficient (VFMech.c:2040-2058).  The strain at
+// the points comes from the modal form of u (the same trilinear interpolant the
+// reference's basis-function sums evaluate).
+__global__ void __launch_bounds__(128) v_coef_kernel(const __grid_constant__ ElemArgs E,
+                                                     const double* __restrict__ u,
+                                                     const double* __restrict__ theta,
+                                                     const double* __restrict__ thetaRef,
+                                                     double* __restrict__ coef,
+                                                     float* __restrict__ coef32) {
   const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
   const int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (cell >= NCELL) return;
@@ -494,62 +543,64 @@ __global__ void v_coef_kernel(const __grid_constant__ ElemArgs E, const double* 
   const ETab& e = E.tab;
   int64_t n[8];
   cell_nodes(E, ei, ej, ek, n);
-  double u8[8][3], th8[8];
-  for (int a = 0; a < 8; a++) {
-    for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
-    th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+  double mu3[3][8], mth[8];
+  {
+    double f[3][8], th8[8];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) f[c][a] = u[3 * n[a] + c];
+      th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) modal_of(f[c], mu3[c]);
+    modal_of(th8, mth);
   }
+  const double ihx = 1. / E.hx, ihy = 1. / E.hy, ihz = 1. / E.hz;
   const CellMat m = cell_mat(E, ei, ej, ek);
   const double mass = E.atnum == 2 ? m.Gc / E.atcv * .5 / E.epsilon : 0.;
-  for (int g = 0; g < 27; g++) {
-    if (E.unilateral) {
-      // ElasticEnergyDensitySphericalDeviatoricNoCompression3D_local (VFMech.c:115-218):
-      // W = sigma(eps - e0) : eps, less (kappa/2) tr^2 where tr < 0
-      double f11 = 0, f22 = 0, f33 = 0, f12 = 0, f23 = 0, f13 = 0, e0 = 0;
-      for (int a = 0; a < 8; a++) {
-        const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
-        f11 += d0 * u8[a][0];
-        f22 += d1 * u8[a][1];
-        f33 += d2 * u8[a][2];
-        f12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
-        f23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
-        f13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
-        e0 += m.alpha * e.phi[a][g] * th8[a];
+  const double l = m.lambda, mu = m.mu;
+#pragma unroll
+  for (int gz = 0; gz < 3; gz++)
+#pragma unroll
+    for (int gy = 0; gy < 3; gy++)
+#pragma unroll
+      for (int gx = 0; gx < 3; gx++) {
+        const int g = gx + 3 * gy + 9 * gz;
+        const double uxx = mdx(mu3[0], gx, gy, gz, ihx), uyy = mdy(mu3[1], gx, gy, gz, ihy);
+        const double uzz = mdz(mu3[2], gx, gy, gz, ihz);
+        const double e12 = (mdx(mu3[1], gx, gy, gz, ihx) + mdy(mu3[0], gx, gy, gz, ihy)) * .5;
+        const double e23 = (mdy(mu3[2], gx, gy, gz, ihy) + mdz(mu3[1], gx, gy, gz, ihz)) * .5;
+        const double e13 = (mdx(mu3[2], gx, gy, gz, ihx) + mdz(mu3[0], gx, gy, gz, ihz)) * .5;
+        const double at = m.alpha * mval(mth, gx, gy, gz);
+        double cgv;
+        if (E.unilateral) {
+          // ElasticEnergyDensitySphericalDeviatoricNoCompression3D_local (VFMech.c:115-218):
+          // W = sigma(eps - e0) : eps, less (kappa/2) tr^2 where tr < 0
+          const double kappa = l + 2. * mu / 3.;
+          const double s11 = (l + 2. * mu) * (uxx - at) + l * (uyy - at) + l * (uzz - at);
+          const double s22 = l * (uxx - at) + (l + 2. * mu) * (uyy - at) + l * (uzz - at);
+          const double s33 = l * (uxx - at) + l * (uyy - at) + (l + 2. * mu) * (uzz - at);
+          const double Wf = (s11 * uxx + s22 * uyy + s33 * uzz) * .5 +
+                            2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
+          const double tr = uxx + uyy + uzz;
+          const double S = tr < 0. ? 0. : kappa * tr * tr * .5, D = Wf - kappa * tr * tr * .5;
+          cgv = e.w[g] * (2. * (S + D) + mass);
+        } else {
+          const double e11 = uxx - at, e22 = uyy - at, e33 = uzz - at;
+          const double s11 = (l + 2. * mu) * e11 + l * e22 + l * e33;
+          const double s22 = l * e11 + (l + 2. * mu) * e22 + l * e33;
+          const double s33 = l * e11 + l * e22 + (l + 2. * mu) * e33;
+          const double W = (s11 * e11 + s22 * e22 + s33 * e33) * .5 +
+                           2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
+          cgv = e.w[g] * (2. * W + mass);
+        }
+        const int64_t ci = vcoef_index(g, ei, ej, ek, pitch, E.ny - 1);
+        coef[ci] = cgv;
+        if (coef32) coef32[ci] = (float)cgv;
       }
-      const double l = m.lambda, mu = m.mu, kappa = l + 2. * mu / 3.;
-      const double s11 = (l + 2. * mu) * (f11 - e0) + l * (f22 - e0) + l * (f33 - e0);
-      const double s22 = l * (f11 - e0) + (l + 2. * mu) * (f22 - e0) + l * (f33 - e0);
-      const double s33 = l * (f11 - e0) + l * (f22 - e0) + (l + 2. * mu) * (f33 - e0);
-      const double Wf = (s11 * f11 + s22 * f22 + s33 * f33) * .5 +
-                        2. * mu * (f12 * f12 + f23 * f23 + f13 * f13);
-      const double tr = f11 + f22 + f33;
-      const double S = tr < 0. ? 0. : kappa * tr * tr * .5, D = Wf - kappa * tr * tr * .5;
-      const double cgv = e.w[g] * (2. * (S + D) + mass);
-      coef[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = cgv;
-      if (coef32) coef32[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = (float)cgv;
-      continue;
-    }
-    double e11 = 0, e22 = 0, e33 = 0, e12 = 0, e23 = 0, e13 = 0;
-    for (int a = 0; a < 8; a++) {
-      const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
-      const double at = m.alpha * e.phi[a][g] * th8[a];
-      e11 += d0 * u8[a][0] - at;
-      e22 += d1 * u8[a][1] - at;
-      e33 += d2 * u8[a][2] - at;
-      e12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
-      e23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
-      e13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
-    }
-    const double l = m.lambda, mu = m.mu;
-    const double s11 = (l + 2. * mu) * e11 + l * e22 + l * e33;
-    const double s22 = l * e11 + (l + 2. * mu) * e22 + l * e33;
-    const double s33 = l * e11 + l * e22 + (l + 2. * mu) * e33;
-    const double W = (s11 * e11 + s22 * e22 + s33 * e33) * .5 + 2. * mu * (e12 * e12 + e23 * e23 + e13 * e13);
-    const double cgv = e.w[g] * (2. * W + mass);
-    coef[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = cgv;
-    if (coef32) coef32[vcoef_index(g, ei, ej, ek, pitch, E.ny - 1)] = (float)cgv;
-  }
 }
+
 
 // V load (VF_ResidualVAT1/AT23D_local and VF_ResidualVCrackPressure3D_local,
 // VFMech.c:2294-2384) in tensor form: the AT term coef sum_g w phi_a = coef vol / 8 per
