@@ -10,12 +10,14 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def _penny(oracle_mod, n, atnum=1, alpha=0.0, beta=0.0, seed=0):
+    """n nodes per axis, or an (nx, ny, nz) shape over the same 4 x 4 x 4 box."""
     import vpfhf_b200 as vg
     L = 4.0
-    h = L / (n - 1)
+    shape = (n, n, n) if np.isscalar(n) else tuple(n)
+    h = max(L / (m - 1) for m in shape)
     kw = dict(E=1e10, nu=0.25, Gc=100.0, epsilon=2 * h, eta=1e-8, atnum=atnum)
-    o = oracle_mod.Oracle((n, n, n), (L, L, L), alpha=alpha, beta=beta, pressurize=True, **kw)
-    ctx = vg.VFContext((n, n, n), (L, L, L),
+    o = oracle_mod.Oracle(shape, (L, L, L), alpha=alpha, beta=beta, pressurize=True, **kw)
+    ctx = vg.VFContext(shape, (L, L, L),
                        dict(E=kw["E"], nu=kw["nu"], Gc=kw["Gc"], alpha=alpha, beta=beta),
                        epsilon=kw["epsilon"], eta=kw["eta"], atnum=atnum, pressurize=True)
     ctx.set_bc(vg.rollers())
@@ -44,11 +46,15 @@ def test_u_residual(cuda, oracle_mod):
     ctx.close()
 
 
-@pytest.mark.parametrize("atnum", [1, 2])
-def test_v_residual(cuda, oracle_mod, atnum):
+@pytest.mark.parametrize("atnum,shape", [(1, 17), (2, 17), (1, (23, 18, 11)), (2, (38, 9, 14))])
+def test_v_residual(cuda, oracle_mod, atnum, shape):
+    """The V residual (K_V v - b with the masks) against the oracle; the unequal grids
+    have cell rows that are not a multiple of the coefficient's 4-cell row padding nor
+    of the 32 x 8 tile, so the tensor copies of the coefficient read padded rows and
+    zero-filled boxes."""
     import vpfhf_b200 as vg
     rng = np.random.default_rng(2)
-    o, ctx, v, p, mask, val = _penny(oracle_mod, 17, atnum=atnum, alpha=1e-5, beta=0.7)
+    o, ctx, v, p, mask, val = _penny(oracle_mod, shape, atnum=atnum, alpha=1e-5, beta=0.7)
     u = rng.standard_normal(3 * o.N) * 1e-4
     theta = rng.uniform(0, 10, o.N)
     virrev = np.clip(v + 0.02 * rng.standard_normal(o.N), 0, 1)
@@ -66,9 +72,10 @@ def test_v_residual(cuda, oracle_mod, atnum):
     ctx.close()
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_step_u_and_v(cuda, oracle_mod, precision):
-    o, ctx, v, p, mask, val = _penny(oracle_mod, 17)
+@pytest.mark.parametrize("precision,shape", [("fp64", 17), ("mixed", 17), ("fp64", (23, 18, 11)),
+                                             ("mixed", (23, 18, 11))])
+def test_step_u_and_v(cuda, oracle_mod, precision, shape):
+    o, ctx, v, p, mask, val = _penny(oracle_mod, shape)
     u = np.zeros(3 * o.N)
     rc, st = ctx.step_u(dict(precision=precision))
     assert rc == 0 and st["reason"] > 0, st

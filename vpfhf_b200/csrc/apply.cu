@@ -7,7 +7,13 @@
 
 namespace vfgpu {
 
-constexpr int U_TY = 8, V_TY = kVTileY;
+// FP64 U operator tiles: 32 x U64_TY elements (1 CTA per SM: ~250 registers per thread).
+// 12 rows (12 warps per SM at 168 registers, with 288 bytes of spills) measured slower
+// on B200: 0.280 against 0.253 ms at 129^3, 0.814 against 0.733 ms at 193^3.
+#ifndef VFGPU_U64_TY
+#define VFGPU_U64_TY 8
+#endif
+constexpr int U_TY = 8, U64_TY = VFGPU_U64_TY, V_TY = kVTileY;
 // V tiles carry 2 stages of 27 coefficients per cell in shared memory: 75 KB (FP32,
 // 2 CTAs per SM) or 150 KB (FP64, 1 CTA per SM).
 constexpr int V64_MINB = 1, V32_MINB = 2;
@@ -34,11 +40,11 @@ template <typename T> bool cubic(const UApplyArgs<T>& A) { return A.ihx == A.ihy
 cudaError_t apply_kernel_attributes() {
   static std::mutex m;  // contexts may be created from several threads
   std::lock_guard<std::mutex> lk(m);
-  cudaError_t e = set_tile_attributes<UOp<double>, U_TY, 1>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U_TY, 1>();
+  cudaError_t e = set_tile_attributes<UOp<double>, U64_TY, 1>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U64_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U_TY, 1>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U64_TY, 1>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<float>, U_TY, 2>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<double>, V_TY, V64_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<VOp<float>, V_TY, V32_MINB>();
@@ -72,7 +78,7 @@ cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int 
 }
 
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
-  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U_TY, 3, 1, num_sms);
+  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, 1, num_sms);
   return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
 }
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
@@ -82,9 +88,9 @@ TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
 template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
-  if (A.cflag) return launch_tile_apply<UOpNC<double>, U_TY, 1>(A, p, L, s);
-  if (cubic(A)) return launch_tile_apply<UOp<double, true>, U_TY, 1>(A, p, L, s);
-  return launch_tile_apply<UOp<double>, U_TY, 1>(A, p, L, s);
+  if (A.cflag) return launch_tile_apply<UOpNC<double>, U64_TY, 1>(A, p, L, s);
+  if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, 1>(A, p, L, s);
+  return launch_tile_apply<UOp<double>, U64_TY, 1>(A, p, L, s);
 }
 template <>
 cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
