@@ -96,6 +96,7 @@ struct vfgpu_ctx {
   int mg_bytes = 0;
   bool mg_ready = false;          // coarse fields, diagonals and eigenvalue bounds are current
   bool mg_ev = false;             // the levels' ev vectors hold earlier eigenvector estimates
+  bool mg_layers = false;         // the coarse levels' element layers match d_elayer
   double* mg_coef = nullptr;      // 64 doubles per level (MGLevel::coef points into it)
   double* mg_z = nullptr;         // FP32 V-cycle: the preconditioned residual in FP64 (3N)
   const void* mg_dinv0 = nullptr; // fine inverse diagonal in the V-cycle's precision

@@ -788,6 +788,7 @@ template <typename T> int mg_build(vfgpu_ctx* c) {
   }
   c->mg_bytes = (int)sizeof(T);
   c->mg_ready = false;
+  c->mg_layers = false;
   if (e != cudaSuccess) {
     free_mg(c);
     return cuda_fail(e, "multigrid hierarchy");
@@ -805,9 +806,26 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
     auto& L = c->mg[l];
     if (c->d_cellE && !L.cellE) e = cudaMalloc((void**)&L.cellE, L.NC * sizeof(float));
   }
-  std::vector<uint8_t> el(std::max(1, c->nz - 1));
-  if (e == cudaSuccess) e = cudaMemcpyAsync(el.data(), c->d_elayer, el.size(), cudaMemcpyDeviceToHost, c->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  // element layers of the coarse levels: the layer of the lowest fine layer in each
+  // coarse layer, followed down to level 0 (uploaded once per hierarchy and material)
+  if (!c->mg_layers) {
+    std::vector<uint8_t> el(std::max(1, c->nz - 1));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(el.data(), c->d_elayer, el.size(), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    std::vector<std::vector<uint8_t>> all(nlev);
+    for (int l = 1; l < nlev && e == cudaSuccess; l++) {
+      auto& L = c->mg[l];
+      all[l].resize(L.nz - 1);
+      for (int k = 0; k < L.nz - 1; k++) {
+        int kk = k;
+        for (int m = l; m >= 1; m--) kk = first_fine_cell(kk, c->mg[m - 1].nz - 1, c->mg[m].nz - 1);
+        all[l][k] = el[std::min<size_t>(kk, el.size() - 1)];
+      }
+      e = cudaMemcpyAsync(L.elayer, all[l].data(), all[l].size(), cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // the host copies leave scope
+    if (e == cudaSuccess) c->mg_layers = true;
+  }
   for (int l = 1; l < nlev && e == cudaSuccess; l++) {
     auto& L = c->mg[l];
     auto& F = c->mg[l - 1];
@@ -819,18 +837,6 @@ template <typename T> int mg_setup(vfgpu_ctx* c) {
                                                           L.ny, L.nz);
     e = cudaGetLastError();
     if (e == cudaSuccess && f32) e = convert_f64_f32(L.v64, (float*)L.v, L.N, c->stream);
-    // element layer of the lowest fine layer in each coarse layer, followed down to level 0
-    std::vector<uint8_t> lc(L.nz - 1);
-    for (int k = 0; k < L.nz - 1; k++) {
-      int kk = k;
-      for (int m = l; m >= 1; m--) {
-        const int ncf = (m == 1 ? c->nz : c->mg[m - 1].nz) - 1, ncc = c->mg[m].nz - 1;
-        kk = first_fine_cell(kk, ncf, ncc);
-      }
-      lc[k] = el[std::min<size_t>(kk, el.size() - 1)];
-    }
-    if (e == cudaSuccess) e = cudaMemcpyAsync(L.elayer, lc.data(), lc.size(), cudaMemcpyHostToDevice, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // lc leaves scope
     if (e == cudaSuccess && c->d_cellE) {
       cell_mean_kernel<<<blocks_for(L.NC), 256, 0, c->stream>>>(cellEf, fx - 1, fy - 1, fz - 1,
                                                                L.cellE, L.nx - 1, L.ny - 1,

@@ -281,6 +281,7 @@ int vfgpu_set_matprop(vfgpu_ctx* c, int nlayer, const vfgpu_matprop* mp, const i
     return fail(VFGPU_ERR_INVALID, "vfgpu_set_matprop: nlayer must be in [1,%d]", VF_MAXLAYER);
   cudaSetDevice(c->dev);
   c->mg_ev = false;  // a new material starts the multigrid eigenvalue estimates afresh
+  c->mg_layers = false;  // ... and may move the element layers
   LayerTable L{};
   for (int l = 0; l < nlayer; l++) {
     const double E = mp[l].E, nu = mp[l].nu;
