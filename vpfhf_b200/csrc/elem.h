@@ -38,9 +38,9 @@ cudaError_t launch_u_diag(const ElemArgs& E, const double* v, const uint8_t* bcb
                           cudaStream_t s, const double* u0 = nullptr);
 // NOCOMPRESSION sign pattern: flags[cell] bit g = (tr(eps(u)) < 0 at Gauss point g).
 cudaError_t launch_nc_flags(const ElemArgs& E, const double* u, uint32_t* flags, cudaStream_t s);
-// coef (27 per cell, Gauss-point-major: coef[g * ncell + cell], so that the V apply's
-// loads of one Gauss point over a warp's cells are contiguous) = w_g (2 W_g(u,theta)
-// [+ Gc/(2c_w)/eps for AT2]) in FP64 and, if coef32 is not null, FP32.
+// coef (27 per cell in the vcoef_index layout: per element layer, 27 planes of the
+// layer's cells, so that a tile's values are one box of a 3-D tensor copy) = w_g
+// (2 W_g(u,theta) [+ Gc/(2c_w)/eps for AT2]) in FP64 and, if coef32 is not null, FP32.
 cudaError_t launch_v_coef(const ElemArgs& E, const double* u, const double* theta,
                           const double* thetaRef, double* coef, float* coef32, cudaStream_t s);
 // b (N) = AT linear term + crack pressure term (VFMech.c:2294-2384).  Overwrites b.
