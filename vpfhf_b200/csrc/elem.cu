@@ -706,17 +706,36 @@ struct KSum {
   __device__ double value() const { return s + c; }
 };
 
-constexpr int EN_THREADS = 256, EN_BLOCKS = 592;
+constexpr int EN_THREADS = 128, EN_BLOCKS = 888;  // 6 blocks per SM of 148
+
+// Value and gradient of a modal form (modal_of) at the point t = (tx, ty, tz).
+__device__ __forceinline__ double mval_t(const double (&m)[8], double tx, double ty, double tz) {
+  return fma(fma(fma(m[7], tx, m[6]), ty, fma(m[5], tx, m[4])), tz,
+             fma(fma(m[3], tx, m[2]), ty, fma(m[1], tx, m[0])));
+}
+__device__ __forceinline__ double mdx_t(const double (&m)[8], double ty, double tz, double ih) {
+  return ih * fma(fma(m[7], tz, m[3]), ty, fma(m[5], tz, m[1]));
+}
+__device__ __forceinline__ double mdy_t(const double (&m)[8], double tx, double tz, double ih) {
+  return ih * fma(fma(m[7], tz, m[3]), tx, fma(m[6], tz, m[2]));
+}
+__device__ __forceinline__ double mdz_t(const double (&m)[8], double tx, double ty, double ih) {
+  return ih * fma(fma(m[7], ty, m[5]), tx, fma(m[6], ty, m[4]));
+}
 
 // One thread per element (grid-stride, fixed assignment), per-thread compensated
-// sums, pairwise tree in shared memory, per-block partials: deterministic.
-__global__ void __launch_bounds__(EN_THREADS) energy_kernel(
+// sums, pairwise tree in shared memory, per-block partials: deterministic.  The fields
+// at the 27 points come from their modal forms (the trilinear interpolants the
+// reference's basis-function sums evaluate); the point loop is not unrolled, which
+// keeps the thread at < 170 registers (3 blocks per SM).
+__global__ void __launch_bounds__(EN_THREADS, 3) energy_kernel(
     const __grid_constant__ ElemArgs E, const double* __restrict__ u, const double* __restrict__ v,
     const double* __restrict__ theta, const double* __restrict__ thetaRef,
     const double* __restrict__ p, double* __restrict__ partial, double* __restrict__ cellcov) {
   __shared__ double red[4][EN_THREADS];
-  const ETab& e = E.tab;
   const int64_t NCELL = (int64_t)(E.nx - 1) * (E.ny - 1) * (E.nz - 1);
+  const double ihx = 1. / E.hx, ihy = 1. / E.hy, ihz = 1. / E.hz;
+  const double vol = E.hx * E.hy * E.hz;
   KSum acc[4];
   for (int64_t cell = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; cell < NCELL;
        cell += (int64_t)gridDim.x * blockDim.x) {
@@ -726,64 +745,67 @@ __global__ void __launch_bounds__(EN_THREADS) energy_kernel(
     int64_t n[8];
     cell_nodes(E, ei, ej, ek, n);
     const CellMat m = cell_mat(E, ei, ej, ek);
-    double u8[8][3], v8[8], th8[8], p8[8];
-    for (int a = 0; a < 8; a++) {
-      for (int c = 0; c < 3; c++) u8[a][c] = u[3 * n[a] + c];
-      v8[a] = v[n[a]];
-      th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
-      p8[a] = p ? p[n[a]] : 0.;
+    double mu3[3][8], mv[8], mp[8], mth[8];
+    {
+      double f[3][8], v8[8], th8[8], p8[8];
+#pragma unroll
+      for (int a = 0; a < 8; a++) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) f[c][a] = u[3 * n[a] + c];
+        v8[a] = v[n[a]];
+        th8[a] = theta ? theta[n[a]] - (thetaRef ? thetaRef[n[a]] : 0.) : 0.;
+        p8[a] = p ? p[n[a]] : 0.;
+      }
+#pragma unroll
+      for (int c = 0; c < 3; c++) modal_of(f[c], mu3[c]);
+      modal_of(v8, mv);
+      modal_of(p8, mp);
+      modal_of(th8, mth);
     }
     const double threekappa = 3. * m.lambda + 2. * m.mu, coefbeta = m.beta / threekappa;
     const double scoef = m.Gc / E.atcv * .25;
-    double el = 0., pw = 0., se = 0., cv = 0.;
+    double el = 0., pw = 0., se = 0., cv = 0., wsum = 0.;
+#pragma unroll 1
     for (int g = 0; g < 27; g++) {
-      double D11 = 0, D22 = 0, D33 = 0, D12 = 0, D23 = 0, D13 = 0, ve = 0, pe = 0, te = 0;
-      double gv[3] = {0, 0, 0}, ue[3] = {0, 0, 0};
-      for (int a = 0; a < 8; a++) {
-        const double d0 = e.dphi[a][0][g], d1 = e.dphi[a][1][g], d2 = e.dphi[a][2][g];
-        const double ph = e.phi[a][g];
-        D11 += d0 * u8[a][0];
-        D22 += d1 * u8[a][1];
-        D33 += d2 * u8[a][2];
-        D12 += (d0 * u8[a][1] + d1 * u8[a][0]) * .5;
-        D23 += (d1 * u8[a][2] + d2 * u8[a][1]) * .5;
-        D13 += (d0 * u8[a][2] + d2 * u8[a][0]) * .5;
-        ve += ph * v8[a];
-        pe += ph * p8[a];
-        te += ph * th8[a];
-        gv[0] += d0 * v8[a];
-        gv[1] += d1 * v8[a];
-        gv[2] += d2 * v8[a];
-        for (int c = 0; c < 3; c++) ue[c] += ph * u8[a][c];
-      }
+      const int gx = g % 3, gy = (g / 3) % 3, gz = g / 9;
+      const double tx = gx == 1 ? 0. : (gx == 0 ? -VF_TAU : VF_TAU);
+      const double ty = gy == 1 ? 0. : (gy == 0 ? -VF_TAU : VF_TAU);
+      const double tz = gz == 1 ? 0. : (gz == 0 ? -VF_TAU : VF_TAU);
+      const double w = vol * (w1(gx) * w1(gy) * w1(gz));
+      double D11 = mdx_t(mu3[0], ty, tz, ihx), D22 = mdy_t(mu3[1], tx, tz, ihy);
+      double D33 = mdz_t(mu3[2], tx, ty, ihz);
+      const double D12 = (mdx_t(mu3[1], ty, tz, ihx) + mdy_t(mu3[0], tx, tz, ihy)) * .5;
+      const double D23 = (mdy_t(mu3[2], tx, tz, ihy) + mdz_t(mu3[1], tx, ty, ihz)) * .5;
+      const double D13 = (mdx_t(mu3[2], ty, tz, ihx) + mdz_t(mu3[0], tx, ty, ihz)) * .5;
+      const double ve = mval_t(mv, tx, ty, tz), pe = mval_t(mp, tx, ty, tz);
+      const double te = mval_t(mth, tx, ty, tz);
+      const double gv0 = mdx_t(mv, ty, tz, ihx), gv1 = mdy_t(mv, tx, tz, ihy), gv2 = mdz_t(mv, tx, ty, ihz);
       // VF_ElasticEnergy3D_local (VFMech.c:725-809), quirk Q2: v^2 (1+eta) on the deviator
       const double tr = D11 + D22 + D33;
       D11 -= tr / 3.;
       D22 -= tr / 3.;
       D33 -= tr / 3.;
       el += (D11 * D11 + D22 * D22 + D33 * D33 + (D12 * D12 + D23 * D23 + D13 * D13) * 2.) * ve * ve *
-            (1. + E.eta) * m.mu * e.w[g];
+            (1. + E.eta) * m.mu * w;
       // NOCOMPRESSION (VF_ElasticEnergyNoCompression3D_local, VFMech.c:819-908): the
       // spherical factor is 1 instead of v where tr < 0
       const double sph = (E.unilateral && tr < 0.) ? 1. : ve;
       const double WD = (tr / 3. - m.alpha * te) * sph - coefbeta * pe;
-      el += 3. * threekappa / 2. * WD * WD * e.w[g];
-      el += threekappa / 6. * tr * tr * E.eta * e.w[g];
-      const double udv = ue[0] * gv[0] + ue[1] * gv[1] + ue[2] * gv[2];
+      el += 3. * threekappa / 2. * WD * WD * w;
+      el += threekappa / 6. * tr * tr * E.eta * w;
+      const double udv = mval_t(mu3[0], tx, ty, tz) * gv0 + mval_t(mu3[1], tx, ty, tz) * gv1 +
+                         mval_t(mu3[2], tx, ty, tz) * gv2;
       // VF_PressureWork3D_local (VFMech.c:920-974)
-      if (E.hasCrackPressure) pw += e.w[g] * pe * udv;
+      if (E.hasCrackPressure) pw += w * pe * udv;
       // VF_AT1/AT2SurfaceEnergy3D_local (VFMech.c:2394-2465)
-      const double g2 = gv[0] * gv[0] + gv[1] * gv[1] + gv[2] * gv[2];
+      const double g2 = gv0 * gv0 + gv1 * gv1 + gv2 * gv2;
       const double om = 1. - ve;
-      se += e.w[g] * ((E.atnum == 1 ? om : om * om) / E.epsilon + g2 * E.epsilon) * scoef;
+      se += w * ((E.atnum == 1 ? om : om * om) / E.epsilon + g2 * E.epsilon) * scoef;
       // VolumetricCrackOpening3D_local (VFPermfield.c:15-73)
-      cv += udv * e.w[g];
+      cv += udv * w;
+      wsum += w;
     }
-    if (cellcov) {
-      double vol = 0.;
-      for (int g = 0; g < 27; g++) vol += e.w[g];
-      cellcov[cell] = cv / vol;
-    }
+    if (cellcov) cellcov[cell] = cv / wsum;
     acc[0].add(el);
     acc[1].add(pw);
     acc[2].add(se);
