@@ -157,7 +157,7 @@ static int check_cell_copies(vfgpu_ctx* c) {
   unsigned flag = 0;
   cudaError_t e = cudaMemcpyAsync(&flag, c->d_cerr, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
+  if (e != cudaSuccess) return cuda_fail(e, "V apply");
   if (!flag) return VFGPU_OK;
   cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
   return fail(VFGPU_ERR_CUDA, "V apply: a coefficient tensor copy did not complete in time");
@@ -839,7 +839,7 @@ int vfgpu_v_residual(vfgpu_ctx* c, double* F) {
   if (e == cudaSuccess) e = copy_out(c, F, Fd, N);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_v_residual");
-  return VFGPU_OK;
+  return check_cell_copies(c);
 }
 
 }  // extern "C"
