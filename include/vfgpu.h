@@ -355,6 +355,13 @@ int vfgpu_u_apply_noalloc(const vfgpu_grid* grid, const vfgpu_matprop* mp, doubl
  * roofline). */
 int vfgpu_fma_peak(int bytes, double* tflops);
 
+/* Diagnostic, no counterpart in the reference: runs the bounded mbarrier wait that the
+ * V apply's coefficient copies use on a phase that completes (complete = 1) or never
+ * does (complete = 0) with a limit of `cycles` (<= 4e9) SM clock cycles, and sets
+ * *timed_out to whether the wait gave up (the kernel then returns normally and the
+ * device stays usable).  Returns 0, or < 0 on a bad argument or CUDA error. */
+int vfgpu_wait_selftest(long long cycles, int complete, int* timed_out);
+
 #ifdef __cplusplus
 }
 #endif

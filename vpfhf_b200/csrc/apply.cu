@@ -77,6 +77,37 @@ cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int 
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
+// One CTA waits on an mbarrier whose phase completes (complete = 1: the arrival is
+// made) or never does (complete = 0: 16 transaction bytes are expected and no copy is
+// issued); the bounded wait sets *err when it gives up.
+__global__ void wait_selftest_kernel(unsigned* err, long long limit, int complete) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    if (complete) mbar_arrive(&bar);
+    else mbar_expect_tx(&bar, 16);
+  }
+  __syncthreads();
+  mbar_wait(&bar, 0, err, limit);
+}
+
+cudaError_t wait_selftest(long long cycles, int complete, int* timed_out) {
+  unsigned* d = nullptr;
+  unsigned h = 0;
+  cudaError_t e = cudaMalloc(&d, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(unsigned));
+  if (e == cudaSuccess) {
+    wait_selftest_kernel<<<1, 64>>>(d, cycles, complete);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(unsigned), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  *timed_out = h ? 1 : 0;
+  return e;
+}
+
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, 1, num_sms);
   return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
@@ -113,3 +144,8 @@ cudaError_t launch_v_apply<float>(const VApplyArgs<float>& A, const TilePlan& p,
 }
 
 }  // namespace vfgpu
+
+extern "C" int vfgpu_wait_selftest(long long cycles, int complete, int* timed_out) {
+  if (!timed_out || cycles < 0 || cycles > 4000000000ll) return -1;
+  return vfgpu::wait_selftest(cycles, complete ? 1 : 0, timed_out) == cudaSuccess ? 0 : -2;
+}

@@ -16,6 +16,9 @@ constexpr int kVTileY = 8;
 // The V coefficient array (vcoef_index layout, 8- or 4-byte values) as the 3-D tensor
 // the V apply stages from: box 32 x kVTileY x 27.
 cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int nex, int ney, int nez);
+// The bounded mbarrier wait of the tensor-copy pipeline, alone: *timed_out = 1 when a
+// wait on a phase that never completes (complete = 0) gave up after `cycles`.
+cudaError_t wait_selftest(long long cycles, int complete, int* timed_out);
 
 template <typename T>
 cudaError_t launch_u_apply(const UApplyArgs<T>& A, const TilePlan& p, const LayerTable& L,

@@ -80,9 +80,14 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
                    (unsigned)__cvta_generic_to_shared(bar)),
                "r"(bytes) : "memory");
 }
-// Waits for the phase with the given parity to complete; gives up after ~2e9 cycles
-// (about a second), flags *err and returns.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err) {
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"((unsigned)__cvta_generic_to_shared(bar))
+               : "memory");
+}
+// Waits for the phase with the given parity to complete; gives up after `limit` cycles
+// (by default ~2e9, about a second), flags *err and returns.
+__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err,
+                                          long long limit = 2000000000ll) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
   const long long t0 = clock64();
   for (;;) {
@@ -94,7 +99,7 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsign
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return;
-    if (clock64() - t0 > 2000000000ll) {
+    if (clock64() - t0 > limit) {
       if (err) atomicOr(err, 1u);
       return;
     }
