@@ -127,6 +127,9 @@ struct vfgpu_ctx {
   std::vector<Graph> graphs;
   uint64_t gen = 1;
   bool use_graphs = true;
+  // per CG call site (run_cg kind 1..4): iterations of its last solve, the size of
+  // the first batch of the next one
+  int cg_last_its[8] = {0};
 };
 
 namespace vfgpu {

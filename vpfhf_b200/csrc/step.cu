@@ -238,7 +238,13 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
                   double atol, double dtol, int maxit, const Watch& w, int* its, int* reason,
                   bool* timeout) {
   cudaError_t e = cg_init<T>(v, c->d_cg, c->d_red, rtol, atol, dtol, maxit, c->stream);
+  // Batches of iterations are queued without a host round trip; a converged CG turns
+  // the rest of a batch into no-ops (skip flag), so the batch sizes do not change the
+  // result.  The first batch is as long as the call site's last solve (a power of two,
+  // 4..64), and is queued before the first host check.
   int batch = 4;
+  while (batch < 64 && batch < c->cg_last_its[kind & 7]) batch *= 2;
+  bool first = true;
   *timeout = false;
   auto body = [&](int nb) {
     cudaError_t eb = cudaSuccess;
@@ -249,20 +255,24 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
     return eb;
   };
   while (e == cudaSuccess) {
-    e = cudaMemcpyAsync(c->h_cg, c->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess || c->h_cg->done) break;
-    if (w.expired()) {
-      *timeout = true;
-      break;
+    if (!first) {
+      e = cudaMemcpyAsync(c->h_cg, c->d_cg, sizeof(CGState), cudaMemcpyDeviceToHost, c->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+      if (e != cudaSuccess || c->h_cg->done) break;
+      if (w.expired()) {
+        *timeout = true;
+        break;
+      }
+      batch = std::min(batch * 2, 64);
     }
+    first = false;
     cudaGraphExec_t g = c->use_graphs ? cg_graph(c, kind, batch, [&] { return body(batch); }) : nullptr;
     e = g ? cudaGraphLaunch(g, c->stream) : body(batch);
-    batch = std::min(batch * 2, 64);
   }
   if (e != cudaSuccess) return cuda_fail(e, "CG");
   *its = c->h_cg->its;
   *reason = c->h_cg->reason;
+  c->cg_last_its[kind & 7] = *its;
   return VFGPU_OK;
 }
 
