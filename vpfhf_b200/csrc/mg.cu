@@ -360,6 +360,23 @@ template <typename Op> size_t coarse_smem_bytes(int ncell) {
   return (size_t)ncell * 8 * 3 * sizeof(typename Op::T);
 }
 
+// The PCG step x += alpha p, r -= alpha w with alpha = rz / (p.w) formed on the device
+// (pw = the dot product just reduced into *pw_in); nothing changes unless p.w > 0 (the
+// host then stops on the indefinite or NaN p.w it reads back from pw_out).
+__global__ void pcg_step_kernel(double* __restrict__ x, double* __restrict__ r,
+                                const double* __restrict__ p, const double* __restrict__ w,
+                                const double* __restrict__ pw_in, double* __restrict__ pw_out,
+                                double rz, int64_t n) {
+  const double pw = *pw_in;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *pw_out = pw;
+  if (!(pw > 0.)) return;
+  const double alpha = rz / pw;
+  GRID_STRIDE(i, n) {
+    x[i] += alpha * p[i];
+    r[i] += (-alpha) * w[i];
+  }
+}
+
 // Deterministic start vector of the power iteration in (-1/2, 1/2), 0 on Dirichlet dofs.
 template <typename T>
 __global__ void seed_kernel(T* __restrict__ x, const uint8_t* __restrict__ bc, int64_t N) {
@@ -942,14 +959,14 @@ int mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double*
   double* z = sizeof(T) == 8 ? (double*)c->mg[0].x : c->mg_z;
   cudaError_t e = cudaMemsetAsync(x, 0, n3 * sizeof(double), c->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(r, b, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
-  // h[0] = r.z, h[2] = ||D^-1 r||^2
-  double h[3] = {0., 0., 0.};
+  // h[0] = r.z, h[2] = ||D^-1 r||^2, h[8] = the step's p.w (one host read per iteration)
+  double h[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
   auto scalars = [&]() {
     const double* pa[1] = {r};
     const double* pb[1] = {z};
     if (e == cudaSuccess) e = dev_dots(pa, pb, 1, n3, c->d_red, c->d_out, c->stream);
     if (e == cudaSuccess) e = dev_znorm2(r, dinv0, n3, c->d_red, c->d_out + 2, c->stream);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(h, c->d_out, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, c->d_out, 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   };
   if (e == cudaSuccess) e = precondition<T>(c, r, z);
@@ -982,20 +999,18 @@ int mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double*
     const double* pa[1] = {p};
     const double* pb[1] = {w};
     if (e == cudaSuccess) e = dev_dots(pa, pb, 1, n3, c->d_red, c->d_out, c->stream);
-    double pw = 0.;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&pw, c->d_out, sizeof pw, cudaMemcpyDeviceToHost, c->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-    if (e != cudaSuccess) break;
-    if (!(pw > 0.)) {
-      *reason = (pw == pw) ? CG_DIVERGED_INDEFINITE : CG_DIVERGED_NAN;
-      break;
+    if (e == cudaSuccess) {
+      pcg_step_kernel<<<blocks_for(n3), 256, 0, c->stream>>>(x, r, p, w, c->d_out, c->d_out + 8, rz, n3);
+      e = cudaGetLastError();
     }
-    const double alpha = rz / pw;
-    e = dev_axpy(x, alpha, p, n3, c->stream);
-    if (e == cudaSuccess) e = dev_axpy(r, -alpha, w, n3, c->stream);
     if (e == cudaSuccess) e = precondition<T>(c, r, z);
     scalars();
     if (e != cudaSuccess) break;
+    const double pw = h[8];
+    if (!(pw > 0.)) {  // x and r were left unchanged
+      *reason = (pw == pw) ? CG_DIVERGED_INDEFINITE : CG_DIVERGED_NAN;
+      break;
+    }
     *its += 1;
     const double dp = sqrt(h[2]);
     if (!(dp == dp)) *reason = CG_DIVERGED_NAN;
