@@ -75,7 +75,8 @@ __host__ __device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
 // One axis of the transfer between a level and the next coarser one, tabulated at the
 // hierarchy's build: fine node i lies in coarse cell pI[i] with upper weight pw[i]
 // (fine_in_coarse), and coarse node I's hat function covers the fine nodes
-// [rlo[I], rlo[I] + rn[I]) (<= 5 for a ratio of <= 2) with nonzero weight.
+// [rlo[I], rlo[I] + rn[I]) (<= 4 for the ratios ceil(cells / 2) gives: the open
+// interval of two coarse cells holds at most 4 fine nodes) with nonzero weight.
 struct XferAxis {
   const int* pI;
   const double* pw;
@@ -106,17 +107,22 @@ __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ 
     const int x0 = X.a[0].rlo[I], nxs = X.a[0].rn[I];
     const int y0 = X.a[1].rlo[J], nys = X.a[1].rn[J];
     const int z0 = X.a[2].rlo[K], nzs = X.a[2].rn[K];
-    double wx[5];
+    double wx[4];
 #pragma unroll
-    for (int c1 = 0; c1 < 5; c1++) wx[c1] = c1 < nxs ? hat(X.a[0], x0 + c1, I) : 0.0;
+    for (int c1 = 0; c1 < 4; c1++) wx[c1] = c1 < nxs ? hat(X.a[0], x0 + c1, I) : 0.0;
     T acc[3] = {T(0), T(0), T(0)};
-    for (int c3 = 0; c3 < nzs; c3++) {
+    // fully unrolled (predicated) so that the row loads of the support issue together
+#pragma unroll
+    for (int c3 = 0; c3 < 4; c3++) {
+      if (c3 >= nzs) continue;
       const double wz = hat(X.a[2], z0 + c3, K);
-      for (int c2 = 0; c2 < nys; c2++) {
+#pragma unroll
+      for (int c2 = 0; c2 < 4; c2++) {
+        if (c2 >= nys) continue;
         const double wzy = wz * hat(X.a[1], y0 + c2, J);
         const int64_t row = node_index(x0, y0 + c2, z0 + c3, fx, fy);
 #pragma unroll
-        for (int c1 = 0; c1 < 5; c1++) {
+        for (int c1 = 0; c1 < 4; c1++) {
           if (c1 < nxs) {
             const T w = T(wzy * wx[c1]);
             const int64_t n = row + c1;
@@ -497,7 +503,7 @@ cudaError_t build_xfer(vfgpu_ctx::MGLevel& L, const int (&f)[3]) {
       }
     }
     for (int I = 0; I < c[d]; I++) {
-      if (hi[I] < lo[I] || hi[I] - lo[I] >= 5) return cudaErrorInvalidValue;
+      if (hi[I] < lo[I] || hi[I] - lo[I] >= 4) return cudaErrorInvalidValue;
       xi.push_back(lo[I]);
       rn.push_back(hi[I] - lo[I] + 1);
     }
