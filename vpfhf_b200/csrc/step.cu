@@ -240,10 +240,10 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
   cudaError_t e = cg_init<T>(v, c->d_cg, c->d_red, rtol, atol, dtol, maxit, c->stream);
   // Batches of iterations are queued without a host round trip; a converged CG turns
   // the rest of a batch into no-ops (skip flag), so the batch sizes do not change the
-  // result.  The first batch is as long as the call site's last solve (a power of two,
-  // 4..64), and is queued before the first host check.
+  // result.  The first batch is the largest power of two (4..64) not above the call
+  // site's last iteration count, and is queued before the first host check.
   int batch = 4;
-  while (batch < 64 && batch < c->cg_last_its[kind & 7]) batch *= 2;
+  while (batch < 64 && 2 * batch <= c->cg_last_its[kind & 7]) batch *= 2;
   bool first = true;
   *timeout = false;
   auto body = [&](int nb) {
