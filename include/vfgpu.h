@@ -125,6 +125,15 @@ int vfgpu_destroy(vfgpu_ctx* ctx);
  * problems in the serving loop. */
 int vfgpu_memory_estimate(const vfgpu_grid* grid, long long* bytes);
 
+/* The multigrid hierarchy a solve with pc = VFGPU_PC_MG builds for this grid (host
+ * only, no counterpart in the reference): *nlevels levels (1: the grid cannot be
+ * coarsened and such a solve is refused), their node counts in dims[3 l .. 3 l + 2]
+ * for l < min(*nlevels, max_levels), and the extra device bytes of the hierarchy in
+ * precision `bytes` (8: FP64 V-cycle, 4: the FP32 one of VFGPU_MIXED) in *mg_bytes
+ * (may be NULL). */
+int vfgpu_mg_hierarchy(const vfgpu_grid* grid, int bytes, int max_levels, int* dims, int* nlevels,
+                       long long* mg_bytes);
+
 /* Per-layer material (VFMatPropGet, VFCommon.c:506-588); layer[ek] for the
  * nz-1 element layers (VFLayerInit, VFCommon.c:1099-1120), NULL = all layer 0. */
 int vfgpu_set_matprop(vfgpu_ctx* ctx, int nlayer, const vfgpu_matprop* mp, const int* layer);

@@ -35,3 +35,20 @@ def test_solve_opts_defaults():
     o = vg.solve_opts(precision="mixed", ksp_maxit=77)
     assert o.precision == vg.MIXED and o.ksp_maxit == 77
     assert o.ksp_rtol == 1e-8 and o.ksp_atol == 1e-10 and o.snes_rtol == 1e-8
+
+
+def test_mg_hierarchy_levels():
+    """The multigrid hierarchy: an axis with >= 9 nodes goes to n/2 + 1 nodes
+    (ceil(cells / 2) cells), the others keep theirs, until no axis has 9 nodes."""
+    import vpfhf_b200 as vg
+    lv, nb = vg.mg_hierarchy((129, 129, 129))
+    assert lv == [(129,) * 3, (65,) * 3, (33,) * 3, (17,) * 3, (9,) * 3, (5,) * 3] and nb > 0
+    assert [d[0] for d in vg.mg_hierarchy((128, 128, 128))[0]] == [128, 65, 33, 17, 9, 5]
+    assert [d[0] for d in vg.mg_hierarchy((48, 48, 48))[0]] == [48, 25, 13, 7]
+    assert vg.mg_hierarchy((40, 33, 12))[0] == [(40, 33, 12), (21, 17, 7), (11, 9, 7), (6, 5, 7)]
+    assert vg.mg_hierarchy((8, 8, 8))[0] == [(8, 8, 8)]  # refused by a pc="mg" solve
+    # FP64 hierarchy holds more bytes than the FP32 one; the estimate grows with the grid
+    n32 = vg.mg_hierarchy((65, 65, 65), precision=vg.MIXED)[1]
+    n64 = vg.mg_hierarchy((65, 65, 65), precision=vg.FP64)[1]
+    assert n64 > n32 > vg.mg_hierarchy((33, 33, 33))[1] > 0
+    assert vg.mg_hierarchy((8, 8, 8))[1] == 0

@@ -285,6 +285,19 @@ def solve_opts(**kw):
     return o
 
 
+def mg_hierarchy(shape, lengths=(1.0, 1.0, 1.0), precision=MIXED):
+    """The multigrid levels (node counts per axis) a pc="mg" solve builds for this grid,
+    and the hierarchy's extra device bytes for the V-cycle precision (FP32 under MIXED,
+    FP64 under FP64).  Host only.  One level: the grid cannot be coarsened."""
+    g = _abi.Grid(*shape, *lengths)
+    dims = (C.c_int * 96)()
+    nlev, nbytes = C.c_int(0), C.c_longlong(0)
+    _abi.check(_abi.lib().vfgpu_mg_hierarchy(C.byref(g), 4 if precision == MIXED else 8, 32, dims,
+                                               C.byref(nlev), C.byref(nbytes)),
+               "vfgpu_mg_hierarchy")
+    return [tuple(dims[3 * l:3 * l + 3]) for l in range(min(nlev.value, 32))], nbytes.value
+
+
 def penny_crack_v(n, l, center, r, theta=0.0, phi=0.0, thickness=0.0, epsilon=0.2, atnum=1):
     """Initial phase field of one penny-shaped crack, VFPennyCrackBuildVAT1/2
     (VFCracks.c:136-227) with the distance of VFDistanceToPennyCrack (VFCracks.c:101-126):

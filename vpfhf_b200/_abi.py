@@ -126,6 +126,8 @@ _SIGS = {
     "vfgpu_create": [C.POINTER(Grid), C.POINTER(C.c_void_p)],
     "vfgpu_destroy": [C.c_void_p],
     "vfgpu_memory_estimate": [C.POINTER(Grid), C.POINTER(C.c_longlong)],
+    "vfgpu_mg_hierarchy": [C.POINTER(Grid), C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                           C.POINTER(C.c_longlong)],
     "vfgpu_set_matprop": [C.c_void_p, C.c_int, C.POINTER(MatProp), C.c_void_p],
     "vfgpu_set_cell_modulus": [C.c_void_p, C.c_void_p],
     "vfgpu_set_vfprop": [C.c_void_p, C.POINTER(VFProp)],

@@ -1096,3 +1096,24 @@ int run_mgcg(vfgpu_ctx* c, bool fp32, const double* b, double* x, double* r, dou
 }
 
 }  // namespace vfgpu
+
+extern "C" int vfgpu_mg_hierarchy(const vfgpu_grid* g, int bytes, int max_levels, int* dims,
+                                  int* nlevels, long long* mg_bytes) {
+  if (!g || !nlevels || (max_levels > 0 && !dims) || (bytes != 4 && bytes != 8))
+    return vfgpu::fail(VFGPU_ERR_INVALID, "vfgpu_mg_hierarchy: bad argument");
+  if (g->nx < 2 || g->ny < 2 || g->nz < 2)
+    return vfgpu::fail(VFGPU_ERR_INVALID, "vfgpu_mg_hierarchy: bad grid");
+  int nx = g->nx, ny = g->ny, nz = g->nz;
+  const int nlev = vfgpu::mg_levels(nx, ny, nz);
+  for (int l = 0; l < nlev && l < max_levels; l++) {
+    dims[3 * l] = nx;
+    dims[3 * l + 1] = ny;
+    dims[3 * l + 2] = nz;
+    nx = vfgpu::coarser(nx);
+    ny = vfgpu::coarser(ny);
+    nz = vfgpu::coarser(nz);
+  }
+  *nlevels = nlev;
+  if (mg_bytes) *mg_bytes = vfgpu::mg_memory_bytes(g->nx, g->ny, g->nz, bytes);
+  return VFGPU_OK;
+}
