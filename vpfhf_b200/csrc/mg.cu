@@ -79,20 +79,54 @@ __host__ __device__ __forceinline__ Lin fine_in_coarse(int i, int nf, int nc) {
 // (fine_in_coarse), and coarse node I's hat function covers the fine nodes
 // [rlo[I], rlo[I] + rn[I]) (<= 4 for the ratios ceil(cells / 2) gives: the open
 // interval of two coarse cells holds at most 4 fine nodes) with nonzero weight.
+// Two common axes need no table (mode): a nested axis (an even fine cell count, ratio
+// 2: fine node i in coarse cell i / 2 with upper weight 1/2 for odd i, coarse node I
+// covering 2I - 1 .. 2I + 1) and an axis that is not coarsened (identity); both give
+// the table's values exactly.
+constexpr int kXferTable = 0, kXferNested = 1, kXferIdentity = 2;
 struct XferAxis {
   const int* pI;
   const double* pw;
   const int* rlo;
   const int* rn;
+  int nf, mode;
 };
 struct Xfer {
   XferAxis a[3];
 };
 
-// Weight of coarse node I at fine node i (the prolongation's entry).
+// Weight of coarse node I at fine node i of its support (the prolongation's entry).
 __device__ __forceinline__ double hat(const XferAxis& A, int i, int I) {
+  if (A.mode == kXferNested) return i == 2 * I ? 1.0 : 0.5;
+  if (A.mode == kXferIdentity) return 1.0;
   const double w = A.pw[i];
   return A.pI[i] == I ? 1.0 - w : w;
+}
+// The support [lo, lo + n) of coarse node I.
+__device__ __forceinline__ void support_of(const XferAxis& A, int I, int& lo, int& n) {
+  if (A.mode == kXferNested) {
+    lo = max(2 * I - 1, 0);
+    n = min(2 * I + 1, A.nf - 1) - lo + 1;
+  } else if (A.mode == kXferIdentity) {
+    lo = I;
+    n = 1;
+  } else {
+    lo = A.rlo[I];
+    n = A.rn[I];
+  }
+}
+// The coarse cell of fine node i and its upper weight.
+__device__ __forceinline__ void cell_of(const XferAxis& A, int i, int& I, double& whi) {
+  if (A.mode == kXferNested) {
+    I = i >> 1;
+    whi = (i & 1) ? 0.5 : 0.0;
+  } else if (A.mode == kXferIdentity) {
+    I = i;
+    whi = 0.0;
+  } else {
+    I = A.pI[i];
+    whi = A.pw[i];
+  }
 }
 
 // Restriction of the residual b - t (the transpose of prolong_add_kernel): coarse node I
@@ -106,9 +140,10 @@ __global__ void restrict_kernel(const T* __restrict__ bf, const T* __restrict__ 
   const int64_t Nc = (int64_t)cx * cy * cz;
   GRID_STRIDE(q, Nc) {
     const int I = (int)(q % cx), J = (int)((q / cx) % cy), K = (int)(q / ((int64_t)cx * cy));
-    const int x0 = X.a[0].rlo[I], nxs = X.a[0].rn[I];
-    const int y0 = X.a[1].rlo[J], nys = X.a[1].rn[J];
-    const int z0 = X.a[2].rlo[K], nzs = X.a[2].rn[K];
+    int x0, nxs, y0, nys, z0, nzs;
+    support_of(X.a[0], I, x0, nxs);
+    support_of(X.a[1], J, y0, nys);
+    support_of(X.a[2], K, z0, nzs);
     double wx[4];
 #pragma unroll
     for (int c1 = 0; c1 < 4; c1++) wx[c1] = c1 < nxs ? hat(X.a[0], x0 + c1, I) : 0.0;
@@ -149,8 +184,11 @@ __global__ void prolong_add_kernel(const T* __restrict__ ec, int cx, int cy, con
   const int64_t Nf = (int64_t)fx * fy * fz;
   GRID_STRIDE(q, Nf) {
     const int i = (int)(q % fx), j = (int)((q / fx) % fy), k = (int)(q / ((int64_t)fx * fy));
-    const int Ix = X.a[0].pI[i], Iy = X.a[1].pI[j], Iz = X.a[2].pI[k];
-    const double hx = X.a[0].pw[i], hy = X.a[1].pw[j], hz = X.a[2].pw[k];
+    int Ix, Iy, Iz;
+    double hx, hy, hz;
+    cell_of(X.a[0], i, Ix, hx);
+    cell_of(X.a[1], j, Iy, hy);
+    cell_of(X.a[2], k, Iz, hz);
     T acc[3] = {T(0), T(0), T(0)};
     for (int dk = 0; dk < 2; dk++) {
       const double wzk = dk ? hz : 1.0 - hz;
@@ -541,6 +579,10 @@ Xfer xfer_of(vfgpu_ctx* c, int l) {
   for (int d = 0; d < 3; d++) {
     X.a[d].rn = L.xi + oi;
     oi += n[d];
+  }
+  for (int d = 0; d < 3; d++) {
+    X.a[d].nf = f[d];
+    X.a[d].mode = n[d] == f[d] ? kXferIdentity : (f[d] - 1 == 2 * (n[d] - 1) ? kXferNested : kXferTable);
   }
   return X;
 }
