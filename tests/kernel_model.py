@@ -277,8 +277,24 @@ def plan(nx, ny, nz, TY, zc):
                 seamX=(ntx - 1) * nz * ny * 12, seamY=(nty - 1) * nz * nx * 6)
 
 
-def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None):
-    """Replays u_apply_kernel + u_seam_fixup_kernel; returns y (3N)."""
+def segments(ntx, nty, nz, ncta, b):
+    """Block b's share of the tile engine's work: node planes [U b / ncta, U (b+1) / ncta)
+    of the U = ntx nty nz (column, plane) units, column-major, cut at column ends into
+    (bx, by, z0, z1) chunks (tile_apply_kernel)."""
+    U = ntx * nty * nz
+    u, u1 = U * b // ncta, U * (b + 1) // ncta
+    out = []
+    while u < u1:
+        col, z0 = u // nz, u % nz
+        z1 = min(nz, z0 + (u1 - u))
+        out.append((col % ntx, col // ntx, z0, z1))
+        u += z1 - z0
+    return out
+
+
+def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, ncta=None):
+    """Replays u_apply_kernel + u_seam_fixup_kernel; returns y (3N).  ncta: the kernel's
+    balanced segments over ncta blocks instead of z-chunks of zc planes."""
     nx, ny, nz = n
     nex, ney = nx - 1, ny - 1
     P = plan(nx, ny, nz, TY, zc)
@@ -296,101 +312,101 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None):
         assert 0 <= i < nx and 0 <= j < ny and 0 <= k < nz
         return (k * ny + j) * nx + i
 
-    for bz in range(P["nzc"]):
-        for by in range(nty):
-            for bx in range(ntx):
-                X0, Y0, z0 = 32 * bx, TY * by, bz * zc
-                if z0 >= nz:
-                    continue
-                z1 = min(z0 + zc, nz)
-                kf, kl = max(z0 - 1, 0), min(z1, nz - 1) - 1
-                carry = np.zeros((32 * TY, nslot, 3))
+    if ncta is None:  # z-chunks of zc planes per xy tile
+        chunks = [(bx, by, bz * zc, min(bz * zc + zc, nz)) for bz in range(P["nzc"])
+                  for by in range(nty) for bx in range(ntx) if bz * zc < nz]
+    else:  # the kernel's balanced segments
+        chunks = [c for b in range(ncta) for c in segments(ntx, nty, nz, ncta, b)]
+    for bx, by, z0, z1 in chunks:
+        X0, Y0 = 32 * bx, TY * by
+        kf, kl = max(z0 - 1, 0), min(z1, nz - 1) - 1
+        carry = np.zeros((32 * TY, nslot, 3))
 
-                def emit(l, w, X, Y, z, val):
-                    left, right = (l == 0 and bx > 0), (l == 32 and bx < ntx - 1)
-                    bot, top = (w == 0 and by > 0), (w == TY and by < nty - 1)
-                    nn = nid(X, Y, z)
-                    if not (left or right or bot or top):
-                        for c in range(3):
-                            y[3 * nn + c] = x[3 * nn + c] if (bcbits[nn] >> c) & 1 else val[c]
-                            written[3 * nn + c] += 1
-                    elif left or right:
-                        i = bx if left else bx + 1
-                        slot = (2 if bot else 0) + (1 if left else 0)
-                        base = ((((i - 1) * nz + z) * ny + Y) * 4 + slot) * 3
-                        assert 0 <= base and base + 3 <= P["seamX"]
-                        assert np.isnan(seamX[base:base + 3]).all()
-                        seamX[base:base + 3] = val
-                    else:
-                        j = by if bot else by + 1
-                        base = ((((j - 1) * nz + z) * nx + X) * 2 + (1 if bot else 0)) * 3
-                        assert 0 <= base and base + 3 <= P["seamY"]
-                        assert np.isnan(seamY[base:base + 3]).all()
-                        seamY[base:base + 3] = val
+        def emit(l, w, X, Y, z, val):
+            left, right = (l == 0 and bx > 0), (l == 32 and bx < ntx - 1)
+            bot, top = (w == 0 and by > 0), (w == TY and by < nty - 1)
+            nn = nid(X, Y, z)
+            if not (left or right or bot or top):
+                for c in range(3):
+                    y[3 * nn + c] = x[3 * nn + c] if (bcbits[nn] >> c) & 1 else val[c]
+                    written[3 * nn + c] += 1
+            elif left or right:
+                i = bx if left else bx + 1
+                slot = (2 if bot else 0) + (1 if left else 0)
+                base = ((((i - 1) * nz + z) * ny + Y) * 4 + slot) * 3
+                assert 0 <= base and base + 3 <= P["seamX"]
+                assert np.isnan(seamX[base:base + 3]).all()
+                seamX[base:base + 3] = val
+            else:
+                j = by if bot else by + 1
+                base = ((((j - 1) * nz + z) * nx + X) * 2 + (1 if bot else 0)) * 3
+                assert 0 <= base and base + 3 <= P["seamY"]
+                assert np.isnan(seamY[base:base + 3]).all()
+                seamY[base:base + 3] = val
 
-                def plane(kz):
-                    sx = np.zeros((4, BY, BX))
-                    for w in range(BY):
-                        for l in range(BX):
-                            X, Y = X0 + l, Y0 + w
-                            if X < nx and Y < ny:
-                                nn = nid(X, Y, kz)
-                                sx[0:3, w, l] = x[3 * nn:3 * nn + 3]
-                                sx[3, w, l] = v[nn]
-                    return sx
+        def plane(kz):
+            sx = np.zeros((4, BY, BX))
+            for w in range(BY):
+                for l in range(BX):
+                    X, Y = X0 + l, Y0 + w
+                    if X < nx and Y < ny:
+                        nn = nid(X, Y, kz)
+                        sx[0:3, w, l] = x[3 * nn:3 * nn + 3]
+                        sx[3, w, l] = v[nn]
+            return sx
 
-                buf = {kf: plane(kf)}
-                for k in range(kf, kl + 1):
-                    buf[k + 1] = plane(k + 1)
-                    sc = np.zeros((24, TY, 32))
-                    for wy in range(TY):
-                        for lane in range(32):
-                            ex, ey = X0 + lane, Y0 + wy
-                            if ex < nex and ey < ney:
-                                xn = np.zeros((8, 3))
-                                vn = np.zeros(8)
-                                for kk in range(2):
-                                    for j in range(2):
-                                        for i in range(2):
-                                            a = i + 2 * j + 4 * kk
-                                            xn[a] = buf[k + kk][0:3, wy + j, lane + i]
-                                            vn[a] = buf[k + kk][3, wy + j, lane + i]
-                                yc = el_fn(xn, vn)
-                                sc[:, wy, lane] = yc.reshape(24)
-                    for tid in range(32 * TY):
-                        for si in range(nslot):
-                            s = tid + si * 32 * TY
-                            if s >= BX * BY:
+        buf = {kf: plane(kf)}
+        for k in range(kf, kl + 1):
+            buf[k + 1] = plane(k + 1)
+            sc = np.zeros((24, TY, 32))
+            for wy in range(TY):
+                for lane in range(32):
+                    ex, ey = X0 + lane, Y0 + wy
+                    if ex < nex and ey < ney:
+                        xn = np.zeros((8, 3))
+                        vn = np.zeros(8)
+                        for kk in range(2):
+                            for j in range(2):
+                                for i in range(2):
+                                    a = i + 2 * j + 4 * kk
+                                    xn[a] = buf[k + kk][0:3, wy + j, lane + i]
+                                    vn[a] = buf[k + kk][3, wy + j, lane + i]
+                        yc = el_fn(xn, vn)
+                        sc[:, wy, lane] = yc.reshape(24)
+            for tid in range(32 * TY):
+                for si in range(nslot):
+                    s = tid + si * 32 * TY
+                    if s >= BX * BY:
+                        continue
+                    l, w = s % BX, s // BX
+                    X, Y = X0 + l, Y0 + w
+                    if X >= nx or Y >= ny:
+                        continue
+                    p0 = np.zeros(3)
+                    p1 = np.zeros(3)
+                    for dw in range(2):
+                        ew, j = w - 1 + dw, 1 - dw
+                        if ew < 0 or ew >= TY:
+                            continue
+                        for dl in range(2):
+                            el, i = l - 1 + dl, 1 - dl
+                            if el < 0 or el >= 32:
                                 continue
-                            l, w = s % BX, s // BX
-                            X, Y = X0 + l, Y0 + w
-                            if X >= nx or Y >= ny:
-                                continue
-                            p0 = np.zeros(3)
-                            p1 = np.zeros(3)
-                            for dw in range(2):
-                                ew, j = w - 1 + dw, 1 - dw
-                                if ew < 0 or ew >= TY:
-                                    continue
-                                for dl in range(2):
-                                    el, i = l - 1 + dl, 1 - dl
-                                    if el < 0 or el >= 32:
-                                        continue
-                                    p0 += sc[(i + 2 * j) * 3:(i + 2 * j) * 3 + 3, ew, el]
-                                    p1 += sc[(i + 2 * j + 4) * 3:(i + 2 * j + 4) * 3 + 3, ew, el]
-                            if k >= z0:
-                                emit(l, w, X, Y, k, carry[tid, si] + p0)
-                            carry[tid, si] = p1
-                if z1 == nz:
-                    for tid in range(32 * TY):
-                        for si in range(nslot):
-                            s = tid + si * 32 * TY
-                            if s >= BX * BY:
-                                continue
-                            l, w = s % BX, s // BX
-                            X, Y = X0 + l, Y0 + w
-                            if X < nx and Y < ny:
-                                emit(l, w, X, Y, nz - 1, carry[tid, si])
+                            p0 += sc[(i + 2 * j) * 3:(i + 2 * j) * 3 + 3, ew, el]
+                            p1 += sc[(i + 2 * j + 4) * 3:(i + 2 * j + 4) * 3 + 3, ew, el]
+                    if k >= z0:
+                        emit(l, w, X, Y, k, carry[tid, si] + p0)
+                    carry[tid, si] = p1
+        if z1 == nz:
+            for tid in range(32 * TY):
+                for si in range(nslot):
+                    s = tid + si * 32 * TY
+                    if s >= BX * BY:
+                        continue
+                    l, w = s % BX, s // BX
+                    X, Y = X0 + l, Y0 + w
+                    if X < nx and Y < ny:
+                        emit(l, w, X, Y, nz - 1, carry[tid, si])
     # seam fix-up
     nxs = (ntx - 1) * nz * ny
     nys = (nty - 1) * nz * nx

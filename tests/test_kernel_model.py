@@ -46,6 +46,30 @@ def test_tiled_schedule_matches_oracle(oracle_mod, n, TY, zc):
     assert np.abs(y - yref).max() <= 1e-13 * np.abs(yref).max()
 
 
+@pytest.mark.parametrize("n,TY,ncta", [((37, 21, 13), 8, 7), ((34, 10, 7), 4, 5), ((3, 2, 4), 8, 3),
+                                       ((37, 21, 13), 8, 1), ((37, 21, 13), 8, 78), ((3, 2, 4), 8, 4)])
+def test_balanced_segments_match_chunks(oracle_mod, n, TY, ncta):
+    """The kernel's balanced split of the (column, node plane) units over ncta blocks,
+    cut at column ends: segments cover every unit once, and the tiled apply over them is
+    bit-identical to the z-chunked one (a segment recomputes the element layer below its
+    first plane, so each node's sum order does not depend on the split)."""
+    rng = np.random.default_rng(sum(n) + ncta)
+    o = oracle_mod.Oracle(n, (1.1, 0.9, 0.7), E=3.0, nu=0.2, eta=1e-2)
+    lam, mu = 3.0 * 0.2 / 1.2 / 0.6, 3.0 / 1.2 * 0.5
+    v, x = rng.uniform(0, 1, o.N), rng.standard_normal(3 * o.N)
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    bits = (mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)
+    h = tuple(L / (k - 1) for L, k in zip((1.1, 0.9, 0.7), n))
+    ntx, nty = -(-(n[0] - 1) // 32), -(-(n[1] - 1) // TY)
+    units = [(bx, by, z) for b in range(ncta) for bx, by, z0, z1 in km.segments(ntx, nty, n[2], ncta, b)
+             for z in range(z0, z1)]
+    assert sorted(units) == sorted((bx, by, z) for bx in range(ntx) for by in range(nty)
+                                   for z in range(n[2]))
+    ys = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, ncta=ncta)
+    yc = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, zc=n[2])
+    assert np.array_equal(ys, yc)
+
+
 def test_modal_v_element_matches_gauss_sum(oracle_mod):
     """K_V,e x = sum_g [aeps w grad(phi_a).grad(x) + c_g phi_a x] from the element tables."""
     rng = np.random.default_rng(5)

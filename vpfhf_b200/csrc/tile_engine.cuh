@@ -72,6 +72,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"((unsigned)__cvta_generic_to_shared(bar)),
                "r"(count) : "memory");
 }
+__device__ __forceinline__ void mbar_inval(uint64_t* bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"((unsigned)__cvta_generic_to_shared(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_fence_init() {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
@@ -144,17 +147,28 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   T* sx = reinterpret_cast<T*>(smem_raw);  // [3 ring][NIN][BY][BX]
   T* sc = sx + 3 * NIN * G::BY * G::BX;    // [2][8*NC][TY][32]
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
-  const int bx = blockIdx.x, by = blockIdx.y, bz = blockIdx.z;
-  const int X0 = bx * 32, Y0 = by * TY;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
-  const int z0 = bz * A.zc;
-  const int blin = (bz * gridDim.y + by) * gridDim.x + bx;
-  if (z0 >= nz) {
-    if (DOT && tid == 0) A.dot[blin] = 0.;
+  // This block's share of the work: node planes [U b / n, U (b + 1) / n) of the
+  // U = ntx nty nz (xy tile, node plane) units taken column by column, cut at column
+  // ends into segments (a segment recomputes the element layer below its first plane,
+  // so the result does not depend on the split).
+  const int64_t U = (int64_t)A.ntx * A.nty * nz;
+  const int64_t u_begin = U * blockIdx.x / gridDim.x, u_end = U * (blockIdx.x + 1) / gridDim.x;
+  if (u_begin >= u_end) {
+    if (DOT && threadIdx.x + threadIdx.y == 0) A.dot[blockIdx.x] = 0.;
     return;
   }
   if (A.skip && *A.skip) return;  // converged solve: uniform early exit, before any barrier
-  const int z1 = min(z0 + A.zc, nz);
+  double dacc = 0.;  // this thread's share of x.y over the nodes it finishes (A.dot)
+  [[maybe_unused]] T* cbuf = nullptr;
+  [[maybe_unused]] uint64_t* cbar = nullptr;
+  if constexpr (Op::CV > 0) {
+    cbuf = reinterpret_cast<T*>(smem_raw + cell_off<Op, TY>());
+    cbar = reinterpret_cast<uint64_t*>(smem_raw + cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>());
+  }
+
+  auto run_segment = [&](const int bx, const int by, const int z0, const int z1) {
+  const int X0 = bx * 32, Y0 = by * TY;
   const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
 
 #define SXA(buf, comp, w, l) sx[(((buf) * NIN + (comp)) * G::BY + (w)) * G::BX + (l)]
@@ -173,7 +187,6 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     cp_async_commit();
   };
 
-  double dacc = 0.;  // this thread's share of x.y over the nodes it finishes (A.dot)
   auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC]) {
     const bool left = (l == 0 && bx > 0), right = (l == 32 && bx < A.ntx - 1);
     const bool bot = (w == 0 && by > 0), top = (w == TY && by < A.nty - 1);
@@ -206,8 +219,6 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   fetch_plane(1, kf + 1);
   // per-cell values of layers kf, kf + 1 (CV > 0): issued before the first barrier,
   // which also publishes the mbarrier initialisation
-  [[maybe_unused]] T* cbuf = nullptr;
-  [[maybe_unused]] uint64_t* cbar = nullptr;
   [[maybe_unused]] auto fetch_cells = [&](int st, int kz) {
     if constexpr (Op::CV > 0) {
       mbar_expect_tx(&cbar[st], (unsigned)cell_stage_bytes<Op, TY>());
@@ -215,8 +226,6 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     }
   };
   if constexpr (Op::CV > 0) {
-    cbuf = reinterpret_cast<T*>(smem_raw + cell_off<Op, TY>());
-    cbar = reinterpret_cast<uint64_t*>(smem_raw + cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>());
     if (tid == 0) {
       for (int st = 0; st < kCellStages; st++) mbar_init(&cbar[st], 1);
       mbar_fence_init();
@@ -353,10 +362,25 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       emit(l, w, X, Y, nz - 1, carry[si]);
     }
   }
+  };  // run_segment
+
+  for (int64_t u = u_begin; u < u_end;) {
+    const int col = (int)(u / nz), z0 = (int)(u % nz);
+    const int64_t left = u_end - u;
+    const int z1 = left < (int64_t)(nz - z0) ? z0 + (int)left : nz;
+    run_segment(col % A.ntx, col / A.ntx, z0, z1);
+    u += z1 - z0;
+    if (u < u_end) {
+      __syncthreads();  // the next segment reuses the shared-memory buffers
+      if constexpr (Op::CV > 0)  // every phase of the stages completed: re-armed by the next init
+        if (tid == 0)
+          for (int st = 0; st < kCellStages; st++) mbar_inval(&cbar[st]);
+    }
+  }
   if constexpr (DOT) {
     __syncthreads();  // the shared-memory buffers are no longer read
     const double bs = block_sum_dbl(dacc, reinterpret_cast<double*>(smem_raw));
-    if (tid == 0) A.dot[blin] = bs;
+    if (tid == 0) A.dot[blockIdx.x] = bs;
   }
 #undef SXA
 #undef SCA
@@ -413,6 +437,7 @@ __global__ void __launch_bounds__(256) seam_fixup_kernel(const typename Op::Args
 // the SMs in whole waves), and the seam buffer sizes in elements of T.
 struct TilePlan {
   int ty, ntx, nty, zc, nzc;
+  int ncta;  // blocks of a launch: one wave, or one node plane per block on small grids
   size_t seamX, seamY;
 };
 
@@ -434,6 +459,8 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
     }
   }
   p.nzc = (nz + p.zc - 1) / p.zc;
+  const int64_t units = (int64_t)tiles * nz;
+  p.ncta = (int)std::max<int64_t>(1, std::min<int64_t>(slots, units));
   p.seamX = (size_t)(p.ntx - 1) * nz * ny * 4 * nc;
   p.seamY = (size_t)(p.nty - 1) * nz * nx * 2 * nc;
   return p;
@@ -447,7 +474,7 @@ inline int seam_blocks(const TilePlan& p, int nx, int ny, int nz) {
   return (int)std::min<int64_t>((nseam + 255) / 256, 148 * 8);
 }
 inline int tile_dot_count(const TilePlan& p, int nx, int ny, int nz) {
-  return p.ntx * p.nty * p.nzc + seam_blocks(p, nx, ny, nz);
+  return p.ncta + seam_blocks(p, nx, ny, nz);
 }
 
 // Opt-in to the dynamic shared memory the kernel needs; done once per device (and
@@ -479,8 +506,8 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
   constexpr size_t smem = tile_smem_bytes<Op, TY>();
   cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
   if (ea != cudaSuccess) return ea;
-  dim3 grid(p.ntx, p.nty, p.nzc), block(32, TY / Op::EPT);
-  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = p.ntx * p.nty * p.nzc;
+  dim3 grid(p.ncta), block(32, TY / Op::EPT);
+  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = p.ncta;
   if (A.dot) {
     tile_apply_kernel<Op, TY, MINB, true><<<grid, block, smem, s>>>(A, L);
     if (sblocks > 0) seam_fixup_kernel<Op, true><<<sblocks, 256, 0, s>>>(A, TY, base);
