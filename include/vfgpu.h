@@ -347,12 +347,14 @@ int vfgpu_server_destroy(vfgpu_server* s);
  * waiting.  The only scratch (the seam partial sums) is a fixed 32 MiB array
  * inside the library (VFGPU_NOALLOC_SCRATCH_DOUBLES doubles; every GPU that
  * loads the library holds it until exit); grids whose seams need more are
- * rejected with VFGPU_ERR_INVALID (129^3 fits, 161^3 does not).  The first call
- * on a device looks up the array's device address (cudaGetSymbolAddress): make
- * that first call before any stream capture.  All calls share the one array, so
- * calls whose work overlaps on the GPU (different streams, different threads)
- * race; serialise them.  Every scratch slot read is written earlier in the same
- * call, so no clearing is needed between calls. */
+ * rejected with VFGPU_ERR_INVALID (129^3 fits, 161^3 does not), and so are x and y
+ * that overlap (the apply is out of place).  Every call looks up the array's device
+ * address in the current context (cudaGetSymbolAddress, host-side) and, on the first
+ * call on a device, opts the kernels in to their shared memory: make that first call
+ * before any stream capture.  All calls share the one array, so calls whose work
+ * overlaps on the GPU (different streams, different threads) race; serialise them.
+ * Every scratch slot read is written earlier in the same call, so no clearing is
+ * needed between calls. */
 #define VFGPU_NOALLOC_SCRATCH_DOUBLES 4194304
 int vfgpu_u_apply_noalloc(const vfgpu_grid* grid, const vfgpu_matprop* mp, double eta,
                           const double* v, const unsigned char* bcbits, const double* x,

@@ -28,7 +28,7 @@ PARAMS = dict(n=(41, 41, 41), l=(4.0, 4.0, 4.0), E=1e10, nu=0.25, Gc=100.0, atnu
 
 def run(P=PARAMS, log=print):
     o = vo.Oracle(P["n"], P["l"], E=P["E"], nu=P["nu"], Gc=P["Gc"], epsilon=P["epsilon"],
-                  eta=P["eta"], atnum=P["atnum"], pressurize=True)
+                  eta=P["eta"], atnum=P["atnum"], pressurize=True, nthreads=P.get("nthreads", 0))
     N = o.N
     V = o.penny_v(P["center"], P["r"])
     virrev = V.copy()
@@ -45,7 +45,7 @@ def run(P=PARAMS, log=print):
         sv = o.step_v(V, U, lb, ub, p=p)
         el, pw = o.u_energy(U, V, p=p)
         rec.append([el, pw, o.v_energy(V), o.cov(U, V), np.abs(V - vold).max(),
-                    su.ksp_its, su.newton_its, sv.ksp_its, sv.newton_its])
+                    su.ksp_its, su.newton_its, sv.ksp_its, sv.newton_its, time.time() - t0])
         log(f"AM {it}: elastic {el:.9e} pw {pw:.9e} surf {rec[-1][2]:.9e} cov {rec[-1][3]:.9e} "
             f"errV {rec[-1][4]:.3e} kspU {su.ksp_its} kspV {sv.ksp_its} ({time.time() - t0:.1f}s)")
     return np.array(rec), U, V
@@ -55,4 +55,4 @@ if __name__ == "__main__":
     rec, U, V = run()
     np.savez_compressed(os.path.join(HERE, "penny41.npz"), rec=rec, V=V, U=U,
                         columns=np.array(["elastic", "pressure_work", "surface", "cov", "errV",
-                                          "kspU", "newtonU", "kspV", "newtonV"]))
+                                          "kspU", "newtonU", "kspV", "newtonV", "seconds"]))

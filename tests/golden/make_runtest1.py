@@ -5,12 +5,17 @@ ValidationTests/test1.c run by `make runtest1`, arguments at
 ValidationTests/makefile:196-198).  Run from the repository root:
 
     python tests/golden/make_runtest1.py /path/to/VPFHF
+
+(or with the path of the VPFHF source tree in the VPFHF_REFERENCE environment variable).
 """
 import json
+import os
 import re
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VPFHF_REFERENCE")
+if not ref:
+    sys.exit("usage: make_runtest1.py /path/to/VPFHF (or set VPFHF_REFERENCE)")
 text = open(f"{ref}/ValidationTests/results/runtest1.out").read()
 steps = []
 for block in re.split(r"==== time step ", text)[1:]:

@@ -48,7 +48,8 @@ def test_device_cracks_match_oracle(cuda, oracle_mod, atnum, with_rects):
 
 
 def _oracle_am(oracle_mod, p, its):
-    """The oracle's AM loop for an AT1 pressurised-crack problem on rollers."""
+    """The oracle's AM loop for a pressurised-crack problem on rollers: AT1 bounds
+    [0, VIrrev]; AT2 bounds [0, 1] with the nodes whose VIrrev <= irrevtol pinned."""
     o = oracle_mod.Oracle(p.n, p.l, E=p.E, nu=p.nu, Gc=p.Gc, epsilon=p.eps, eta=p.eta,
                           atnum=p.atnum, pressurize=True)
     pr, rr = _rows(p.pennies, p.rects)
@@ -56,19 +57,21 @@ def _oracle_am(oracle_mod, p, its):
     U = np.zeros(3 * o.N)
     pres = np.full(o.N, p.pressure)
     umask, uval = o.bc(oracle_mod.rollers_face())
-    lb, ub = np.zeros(o.N), V.copy()
+    virrev = V.copy()
+    lb, ub = np.zeros(o.N), (virrev.copy() if p.atnum == 1 else np.ones(o.N))
     for _ in range(its):
         o.step_u(U, V, p=pres, mask=umask, value=uval)
-        o.step_v(V, U, lb, ub, p=pres)
+        o.step_v(V, U, lb, ub, p=pres, virrev=virrev if p.atnum == 2 else None)
     el, pw = o.u_energy(U, V, p=pres)
     return dict(elastic=el, pressure_work=pw, surface=o.v_energy(V), cov=o.cov(U, V)), V
 
 
+@pytest.mark.parametrize("atnum", [1, 2])
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_server_matches_direct_and_oracle(cuda, oracle_mod, precision):
+def test_server_matches_direct_and_oracle(cuda, oracle_mod, precision, atnum):
     import vpfhf_b200 as vg
     from vpfhf_b200.serve import Problem, Server
-    p = Problem(n=(17, 17, 17), E=1.2e10, nu=0.22, atnum=1, pennies=PENNIES[:2], am_its=3,
+    p = Problem(n=(17, 17, 17), E=1.2e10, nu=0.22, atnum=atnum, pennies=PENNIES[:2], am_its=3,
                 precision=precision)
     vs = np.empty(p.nodes)
     with Server(workers=2) as srv:

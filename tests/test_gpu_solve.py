@@ -97,6 +97,88 @@ def test_step_u_and_v(cuda, oracle_mod, precision, shape):
     ctx.close()
 
 
+@pytest.mark.parametrize("precision,shape", [("fp64", 17), ("mixed", 17), ("fp64", (23, 18, 11)),
+                                             ("mixed", (23, 18, 11))])
+def test_step_v_at2(cuda, oracle_mod, precision, shape):
+    """AT2 StepV against the oracle: the VI Newton solve with bounds [0, 1]
+    (VFCommon.c:1065) and the irreversibility pin of the nodes whose VIrrev <= irrevtol
+    (VF_IrrevApplyEQVec / EQMat, VFMech.c:2597-2682), from the solved U; the AT2 surface
+    energy (VF_AT2SurfaceEnergy3D_local, VFMech.c:2394-2425) of the result."""
+    o, ctx, v, p, mask, val = _penny(oracle_mod, shape, atnum=2)
+    N = o.N
+    pinned = v <= 5e-2
+    assert pinned.any() and not pinned.all()
+    rc, st = ctx.step_u(dict(precision=precision))
+    assert rc == 0 and st["reason"] > 0, st
+    u = np.zeros(3 * N)
+    o.step_u(u, v, p=p, mask=mask, value=val)
+    assert np.linalg.norm(ctx.get_field("U") - u) <= 1e-6 * np.linalg.norm(u)
+    assert ctx.v_energy() == pytest.approx(o.v_energy(v), rel=1e-10)
+    rc, sv = ctx.step_v(dict(precision=precision))
+    assert rc == 0 and sv["reason"] > 0, sv
+    vo_ = v.copy()
+    so = o.step_v(vo_, u, np.zeros(N), np.ones(N), p=p, virrev=v)
+    assert so.reason > 0
+    vg_ = ctx.get_field("V")
+    assert np.abs(vg_ - vo_).max() <= 1e-6
+    assert np.array_equal(vg_[pinned], v[pinned])          # pinned nodes keep their value
+    assert vg_.min() >= 0.0 and vg_.max() <= 1.0            # AT2 bounds [0, 1], not [0, VIrrev]
+    assert (vg_ > v + 1e-3).any()                           # ... which this solve uses
+    assert ctx.v_energy() == pytest.approx(o.v_energy(vo_), rel=1e-7)
+    ctx.close()
+
+
+def _oracle_am_loop(oracle_mod, o, V, p, its, atnum):
+    """The oracle's AM loop (ValidationTests/test18.c:196-205) from the crack state V on
+    rollers: VFTimeStepPrepare (VIrrev = V), then StepU / StepV with the AT bounds
+    (AT1 [0, VIrrev], AT2 [0, 1] with the VIrrev <= irrevtol pin)."""
+    N = o.N
+    U = np.zeros(3 * N)
+    V = V.copy()
+    virrev = V.copy()
+    umask, uval = o.bc(oracle_mod.rollers_face())
+    lb = np.zeros(N)
+    ub = virrev.copy() if atnum == 1 else np.ones(N)
+    recs = []
+    for _ in range(its):
+        o.step_u(U, V, p=p, mask=umask, value=uval)
+        o.step_v(V, U, lb, ub, p=p, virrev=virrev if atnum == 2 else None)
+        el, pw = o.u_energy(U, V, p=p)
+        recs.append((el, pw, o.v_energy(V), o.cov(U, V)))
+    return recs, U, V
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_at2_am_loop(cuda, oracle_mod, precision):
+    """4 AM iterations of an AT2 pressurised penny crack (25^3, eps = 2h) against the
+    oracle's AM loop: every iteration's elastic energy, pressure work, AT2 surface
+    energy and crack opening within 1e-6 relative, V L-inf <= 1e-4 at the end."""
+    import vpfhf_b200 as vg
+    n, L = (25, 25, 25), (4.0, 4.0, 4.0)
+    h = 4.0 / 24
+    kw = dict(E=1e10, nu=0.25, Gc=100.0)
+    o = oracle_mod.Oracle(n, L, epsilon=2 * h, eta=1e-8, atnum=2, pressurize=True, **kw)
+    V0 = o.penny_v((2.0, 2.0, 2.0), 0.9)
+    p = np.full(o.N, 1e6)
+    ref, Uo, Vo = _oracle_am_loop(oracle_mod, o, V0, p, 4, 2)
+    ctx = vg.VFContext(n, L, kw, epsilon=2 * h, eta=1e-8, atnum=2, pressurize=True)
+    ctx.set_bc(vg.rollers())
+    ctx.set_field("V", V0)
+    ctx.set_field("pressure", p)
+    ctx.time_step_prepare()
+    for it in range(4):
+        rc, err, su, sv = ctx.am_step(dict(precision=precision))
+        assert rc == 0, (su, sv)
+        el, _, pw = ctx.u_energy()
+        got = (el, pw, ctx.v_energy(), ctx.crack_opening())
+        for g, r in zip(got, ref[it]):
+            assert g == pytest.approx(r, rel=1e-6), (it, got, ref[it])
+    Vg = ctx.get_field("V")
+    assert np.abs(Vg - Vo).max() <= 1e-4
+    assert np.array_equal(Vg[V0 <= 5e-2], V0[V0 <= 5e-2])
+    ctx.close()
+
+
 def runtest1_gpu(vg, precision, steps=11, altmintol=1e-3):
     """ValidationTests/test1.c (make runtest1 arguments) through the product path."""
     n = (101, 5, 5)

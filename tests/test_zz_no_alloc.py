@@ -1,9 +1,9 @@
 """vfgpu_u_apply_noalloc: the U apply for callers that cannot allocate device memory
 while they run (it keeps its seam scratch in a fixed array inside the library).
 
-Checked through the C ABI against the ctx-based vfgpu_u_apply on two calls in a row
-(the second call reuses the scratch the first one left behind).  This file is named
-to be collected last."""
+Checked through the C ABI against the ctx-based vfgpu_u_apply and against the oracle's
+matrix-free apply on two calls in a row (the second call reuses the scratch the first
+one left behind).  This file is named to be collected last."""
 import ctypes as C
 
 import numpy as np
@@ -47,7 +47,29 @@ def test_noalloc_matches_ctx_apply_twice(cuda, oracle_mod, n, l):
         torch.cuda.synchronize()
         y = yd.cpu().numpy()
         assert np.abs(y - ref).max() <= 1e-12 * np.abs(ref).max(), call
+        if o.N <= 65 ** 3:  # the oracle's apply (Dirichlet rows y = x) at the same tolerance
+            mask, _ = o.bc(oracle_mod.rollers_face())
+            yo = oracle_mod.Oracle(n, l, E=E, nu=nu, eta=eta).u_apply(v, x, mask)
+            assert np.abs(y - yo).max() <= 1e-12 * np.abs(yo).max(), call
     ctx.close()
+
+
+def test_noalloc_rejects_overlapping_x_and_y(cuda):
+    """The apply is out of place: x and y that share memory are refused before any launch."""
+    from vpfhf_b200 import _abi
+    torch = cuda
+    n = (9, 9, 9)
+    grid = _abi.Grid(*n, 1.0, 1.0, 1.0)
+    mp = _abi.MatProp(1e10, 0.25, 0.0, 0.0, 1.0)
+    N = 9 ** 3
+    v = torch.ones(N, dtype=torch.float64, device="cuda")
+    buf = torch.zeros(3 * N + 8, dtype=torch.float64, device="cuda")
+    L = _abi.lib()
+    for off in (0, 8):  # the same array, and an array shifted by 8 doubles
+        rc = L.vfgpu_u_apply_noalloc(C.byref(grid), C.byref(mp), 1e-8, v.data_ptr(), None,
+                                     buf.data_ptr(), buf.data_ptr() + off * 8, None)
+        assert rc == _abi.ERR_INVALID
+        assert "overlap" in L.vfgpu_last_error().decode()
 
 
 def test_noalloc_rejects_grids_beyond_the_fixed_scratch(cuda):

@@ -22,21 +22,15 @@ constexpr size_t kScratchDoubles = VFGPU_NOALLOC_SCRATCH_DOUBLES;
 // earlier in the same call, so nothing has to be cleared between calls.
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-static double* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (looked up once per
-// device with that device current; the host-side symbol is not a device address).
-int scratch_address(int dev, double** out) {
-  if (dev < 0 || dev >= kMaxDevices)
-    return vfgpu::fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: device %d out of range", dev);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return vfgpu::cuda_fail(e, "vfgpu_u_apply_noalloc: cudaGetSymbolAddress");
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
+// Device address of the scratch array in the current device's context.  Looked up on
+// every call (a host-side table lookup, no device work): the host-side symbol is not
+// a device address, and a cached address would go stale when the context is rebuilt
+// (cudaDeviceReset, or another primary context after a reset elsewhere in the process).
+int scratch_address(double** out) {
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return vfgpu::cuda_fail(e, "vfgpu_u_apply_noalloc: cudaGetSymbolAddress");
+  *out = static_cast<double*>(p);
   return VFGPU_OK;
 }
 
@@ -57,6 +51,14 @@ extern "C" int vfgpu_u_apply_noalloc(const vfgpu_grid* g, const vfgpu_matprop* m
   if (!is_device_ptr(v) || !is_device_ptr(x) || !is_device_ptr(y) ||
       (bcbits && !is_device_ptr(bcbits)))
     return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: v, x, y, bcbits must be device pointers");
+  {
+    // out of place only: the tiles read x planes and Dirichlet rows copy x while other
+    // blocks write y
+    const uintptr_t n3 = (uintptr_t)g->nx * g->ny * g->nz * 3 * sizeof(double);
+    const uintptr_t xb = reinterpret_cast<uintptr_t>(x), yb = reinterpret_cast<uintptr_t>(y);
+    if (xb < yb + n3 && yb < xb + n3)
+      return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: x and y overlap (the apply is out of place)");
+  }
   int dev = 0, nsm = 148;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_noalloc: cudaGetDevice");
@@ -68,8 +70,11 @@ extern "C" int vfgpu_u_apply_noalloc(const vfgpu_grid* g, const vfgpu_matprop* m
                 "scratch holds %zu (use vfgpu_u_apply with a vfgpu_ctx)",
                 g->nx, g->ny, g->nz, p.seamX + p.seamY, kScratchDoubles);
   double* scratch = nullptr;
-  int rc = scratch_address(dev, &scratch);
+  int rc = scratch_address(&scratch);
   if (rc) return rc;
+  // the kernels' shared-memory opt-in, under the same lock vfgpu_create takes
+  e = apply_kernel_attributes();
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_noalloc: kernel attributes");
   LayerTable L{};
   L.lambda[0] = mp->E * mp->nu / (1. + mp->nu) / (1. - 2. * mp->nu);  // VFCommon.c:584
   L.mu[0] = mp->E / (1. + mp->nu) * .5;                                // VFCommon.c:585

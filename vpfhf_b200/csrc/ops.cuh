@@ -180,7 +180,7 @@ template <typename T> struct VApplyArgs {
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   const DevParams* __restrict__ P;    // Gc/(2 c_w) eps per layer
   double* __restrict__ dot;           // if non-null: per-block partials of x.y
-  int nx, ny, nz, ntx, nty, zc;
+  int nx, ny, nz, ntx, nty;
   T ihx, ihy, ihz, vol;
 };
 

@@ -1,22 +1,25 @@
 // tile_engine.cuh -- the z-marching tile schedule shared by the matrix-free
 // operators (U: 3 dofs per node, V: 1 dof per node).
 //
-// A CTA owns 32 (x, one warp) x TY (y, TY warps) elements and marches up a chunk
-// of node planes in z.  Per element layer: node planes of the tile's 33 x (TY+1)
-// node box stream through a 3-slot shared-memory ring by asynchronous copies
-// (cp.async, two planes ahead), each thread computes its
-// element's 8 x NC corner contributions (Op::element), those go to shared
-// memory, and node-owner threads sum the (up to 4) xy-contributions in a fixed
-// order; the z-direction sum is carried in registers.  A z-chunk recomputes the
-// element layer below its first plane.  Nodes on the seams between xy-tiles get
-// partial sums from 2 or 4 tiles, written to a seam buffer and summed in a
-// fixed order by seam_fixup_kernel.  The result is deterministic (no atomics)
-// and independent of the chunking in z.
+// The grid's elements are cut into xy tiles of 32 (x, one warp) x TY (y, TY warps)
+// elements; a (tile, node plane) pair is one unit of work, and the ntx nty nz units,
+// taken column by column (all planes of tile 0, then tile 1, ...), are shared evenly
+// by one wave of blocks: block b takes units [U b / n, U (b + 1) / n), cut at column
+// ends into segments.  A segment marches up its planes: per element layer, node
+// planes of the tile's 33 x (TY+1) node box stream through a 3-slot shared-memory
+// ring by asynchronous copies (cp.async, two planes ahead), each thread computes its
+// element's 8 x NC corner contributions (Op::element), those go to shared memory,
+// and node-owner threads sum the (up to 4) xy-contributions in a fixed order; the
+// z-direction sum is carried in registers.  A segment recomputes the element layer
+// below its first plane, so the result does not depend on the split.  Nodes on the
+// seams between xy-tiles get partial sums from 2 or 4 tiles, written to a seam buffer
+// and summed in a fixed order by seam_fixup_kernel.  The result is deterministic (no
+// atomics).
 //
 // Op supplies:  NC, NIN (per-node inputs staged in smem), EPT (elements per
 //   thread: 1, or 2 for an operator that evaluates two y-adjacent elements at once
 //   in the two lanes of packed FP32 instructions), the Args type with
-//   x/y/seamX/seamY/nx/ny/nz/ntx/nty/zc members, and
+//   x/y/seamX/seamY/nx/ny/nz/ntx/nty members, and
 //   node_src(A, n, src[NIN]) (global addresses of a node's inputs),
 //   element(A, L, ex, ey, ez, in[8][NIN], out[8][NC]) (EPT = 1) or
 //   element_multi(A, L, ex, ey[EPT], ez, ok[EPT], in[EPT][8][NIN], out[EPT][8][NC])
@@ -30,10 +33,14 @@
 //   and cell_err(A), and element(..., cc, cs) reads its cell's values from shared
 //   memory (cc[g cs]): one thread issues the tensor copy of element layer k + 2 into a
 //   2-stage buffer while layer k is computed, completion tracked by an mbarrier per
-//   stage (a bounded wait; on time-out *cell_err is set and the launch finishes).
+//   stage.  The wait is bounded: a thread whose wait gives up sets *cell_err, the
+//   block stops at that layer's barrier (no further copy is issued), thread 0 waits
+//   (bounded again) for the copies still in flight into its stages, and the block
+//   returns.
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 
 #include "common.cuh"
 
@@ -88,8 +95,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
                : "memory");
 }
 // Waits for the phase with the given parity to complete; gives up after `limit` cycles
-// (by default ~2e9, about a second), flags *err and returns.
-__device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsigned* err,
+// (by default ~2e9, about a second), flags *err and returns false.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, unsigned* err,
                                           long long limit = 2000000000ll) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
   const long long t0 = clock64();
@@ -101,10 +108,10 @@ __device__ __forceinline__ void mbar_wait(uint64_t* bar, unsigned parity, unsign
         : "=r"(done)
         : "r"(a), "r"(parity)
         : "memory");
-    if (done) return;
+    if (done) return true;
     if (clock64() - t0 > limit) {
       if (err) atomicOr(err, 1u);
-      return;
+      return false;
     }
   }
 }
@@ -167,7 +174,9 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     cbar = reinterpret_cast<uint64_t*>(smem_raw + cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>());
   }
 
-  auto run_segment = [&](const int bx, const int by, const int z0, const int z1) {
+  // Returns false if a bounded wait on the per-cell copies gave up (the block then
+  // stops: see the layer barrier).
+  auto run_segment = [&](const int bx, const int by, const int z0, const int z1) -> bool {
   const int X0 = bx * 32, Y0 = by * TY;
   const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
 
@@ -236,6 +245,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   cp_async_wait_all();
   __syncthreads();
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
+  [[maybe_unused]] bool gave_up = false;
   for (int k = kf; k <= kl; k++) {
     const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = (k - kf) & 1;
     const int ex = X0 + lane;
@@ -243,7 +253,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       const int ey = Y0 + wy;
       T yc[8][NC];
       if constexpr (Op::CV > 0)
-        mbar_wait(&cbar[(k - kf) % kCellStages], ((k - kf) / kCellStages) & 1, Op::cell_err(A));
+        gave_up = !mbar_wait(&cbar[(k - kf) % kCellStages], ((k - kf) / kCellStages) & 1, Op::cell_err(A));
       if (ex < nex && ey < ney) {
         T in[8][NIN];
 #pragma unroll
@@ -314,7 +324,23 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
           for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, EPT * wy + e, lane) = yc[e][a][c];
     }
     cp_async_wait_all();  // this thread's copies of plane k+2 have landed
-    __syncthreads();      // ... and everyone's; corner contributions of layer k visible
+    if constexpr (Op::CV > 0) {
+      // ... and everyone's; corner contributions of layer k visible.  If any thread's
+      // wait on layer k's values gave up, the whole block stops here: no further copy
+      // is issued, thread 0 waits (bounded) for the tensor copies still in flight into
+      // the stages of layers k and k + 1, and the launch's results are void (the host
+      // sees *cell_err).
+      if (__syncthreads_or(gave_up)) {
+        if (tid == 0) {
+          mbar_wait(&cbar[(k - kf) % kCellStages], ((k - kf) / kCellStages) & 1, nullptr);
+          if (k + 1 <= kl)
+            mbar_wait(&cbar[(k + 1 - kf) % kCellStages], ((k + 1 - kf) / kCellStages) & 1, nullptr);
+        }
+        return false;
+      }
+    } else {
+      __syncthreads();    // ... and everyone's; corner contributions of layer k visible
+    }
     if (k + 3 <= kl + 1) fetch_plane(r0, k + 3);  // plane k is no longer read
     if constexpr (Op::CV > 0)  // layer k's stage is no longer read
       if (tid == 0 && k + kCellStages <= kl) fetch_cells((k - kf) % kCellStages, k + kCellStages);
@@ -362,13 +388,14 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       emit(l, w, X, Y, nz - 1, carry[si]);
     }
   }
+  return true;
   };  // run_segment
 
   for (int64_t u = u_begin; u < u_end;) {
     const int col = (int)(u / nz), z0 = (int)(u % nz);
     const int64_t left = u_end - u;
     const int z1 = left < (int64_t)(nz - z0) ? z0 + (int)left : nz;
-    run_segment(col % A.ntx, col / A.ntx, z0, z1);
+    if (!run_segment(col % A.ntx, col / A.ntx, z0, z1)) break;  // block-uniform
     u += z1 - z0;
     if (u < u_end) {
       __syncthreads();  // the next segment reuses the shared-memory buffers
@@ -433,11 +460,12 @@ __global__ void __launch_bounds__(256) seam_fixup_kernel(const typename Op::Args
 }
 
 
-// Launch plan: xy tiles of 32 x ty elements, z-chunks of zc planes (chosen to fill
-// the SMs in whole waves), and the seam buffer sizes in elements of T.
+// Launch plan: xy tiles of 32 x ty elements, the blocks of one launch (one wave of
+// ctas_per_sm blocks per SM, or one unit per block on small grids) and the seam buffer
+// sizes in elements of T.
 struct TilePlan {
-  int ty, ntx, nty, zc, nzc;
-  int ncta;  // blocks of a launch: one wave, or one node plane per block on small grids
+  int ty, ntx, nty;
+  int ncta;
   size_t seamX, seamY;
 };
 
@@ -447,18 +475,6 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
   p.ntx = (nx - 1 + 31) / 32;
   p.nty = (ny - 1 + ty - 1) / ty;
   const int slots = num_sms * ctas_per_sm, tiles = p.ntx * p.nty;
-  double best = 1e300;
-  p.zc = nz;
-  for (int nzc = 1; nzc <= nz; nzc++) {
-    const int zc = (nz + nzc - 1) / nzc, chunks = (nz + zc - 1) / zc;
-    const int waves = (tiles * chunks + slots - 1) / slots;
-    const double cost = (double)waves * (zc + 1 + 2);  // +1 halo layer, +2 fill/drain
-    if (cost < best - 1e-9) {
-      best = cost;
-      p.zc = zc;
-    }
-  }
-  p.nzc = (nz + p.zc - 1) / p.zc;
   const int64_t units = (int64_t)tiles * nz;
   p.ncta = (int)std::max<int64_t>(1, std::min<int64_t>(slots, units));
   p.seamX = (size_t)(p.ntx - 1) * nz * ny * 4 * nc;
@@ -479,21 +495,22 @@ inline int tile_dot_count(const TilePlan& p, int nx, int ny, int nz) {
 
 // Opt-in to the dynamic shared memory the kernel needs; done once per device (and
 // up front, from vfgpu_create, so that no attribute call happens inside a capture).
-// Callers serialise (apply_kernel_attributes holds a mutex).
-template <class Op, int TY, int MINB> inline unsigned long long g_tile_attr_set = 0;  // device bits
+// The per-device bits are atomic, so concurrent callers at worst repeat the
+// (idempotent) attribute call.
+template <class Op, int TY, int MINB> inline std::atomic<unsigned long long> g_tile_attr_set{0};
 template <class Op, int TY, int MINB> cudaError_t set_tile_attributes() {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
-  if (g_tile_attr_set<Op, TY, MINB> & bit) return cudaSuccess;
+  if (g_tile_attr_set<Op, TY, MINB>.load(std::memory_order_acquire) & bit) return cudaSuccess;
   const int smem = (int)tile_smem_bytes<Op, TY>();
   e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB, false>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB, true>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-  if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB> |= bit;
+  if (e == cudaSuccess) g_tile_attr_set<Op, TY, MINB>.fetch_or(bit, std::memory_order_release);
   return e;
 }
 
@@ -502,7 +519,6 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
                               cudaStream_t s) {
   A.ntx = p.ntx;
   A.nty = p.nty;
-  A.zc = p.zc;
   constexpr size_t smem = tile_smem_bytes<Op, TY>();
   cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
   if (ea != cudaSuccess) return ea;

@@ -44,7 +44,7 @@ template <typename T> struct UApplyArgs {
   const uint32_t* __restrict__ cflag; // NOCOMPRESSION: per cell, bit g = tr(eps(u0)) < 0 at Gauss
                                       // point g (u_element_nc); null = the plain operator
   int nx, ny, nz;
-  int ntx, nty, zc;                   // tiles in x, y; owned node planes per z-chunk
+  int ntx, nty;                       // tiles in x, y
   T ihx, ihy, ihz, vol, eta;
 };
 

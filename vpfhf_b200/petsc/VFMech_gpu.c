@@ -5,7 +5,8 @@
  * UpdateFractureWidth) that run on a B200 through the vfgpu C ABI (include/vfgpu.h).
  *
  * Build it into VPFHF instead of VFMech.c's versions of these four functions
- * (see INTEGRATION.md): the callers (VPFHF.c, VFCommon.c:1166-1231 and the
+ * (compile this file with -I<repo>/include, link libvfgpu.so, and drop the four
+ * definitions from VFMech.c): the callers (VPFHF.c, VFCommon.c:1166-1231 and the
  * ValidationTests drivers) link unchanged.  One MPI rank per GPU problem: the
  * DMDA must not be distributed (comm size 1); in-situ tractions and
  * UNILATERAL_NOCOMPRESSION are passed on to the device problem.
