@@ -19,8 +19,9 @@ rank runs its own copy of the workload and `value` is the total over ranks.
 
 --impl reference times the reference's CPU algorithm for the same metric: the
 assembled AIJ (CSR, 81 nnz/row) sparse matrix-vector product that KSPCG runs
-(restated in the oracle, oracle/vf_oracle.c) on all host cores, on a bounded
-sample (the 65^3 grid, whose matrix is far larger than the host caches).
+(restated in the oracle, oracle/vf_oracle.c) on all host cores, on the same 129^3
+workload, and beside it the AM step by the reference's method (assembled Jacobians,
+CG on the assembled matrix) on the 41^3 penny crack.
 """
 from __future__ import annotations
 
@@ -278,6 +279,7 @@ def run_gpu(args):
                     zip(names, am[key]["energies"][-1], am["fp64"]["energies"][-1])}
         return rel, rel_last, float(np.abs(vfin[key] - vfin["fp64"]).max())
     rel, rel_last, v_linf = versus_fp64("mixed")
+    am_c1 = gpu_am_c1(vg, barrier)
 
     serving = run_serving(args) if args.serve_problems > 0 else None
 
@@ -349,17 +351,37 @@ def run_gpu(args):
                            "note": "fp64 / mixed: Jacobi-preconditioned U solve (the reference's); "
                                    "mg_*: multigrid-preconditioned U solve, same stopping test",
                            "steps": args.am_steps,
-                           "kspU_last": {k: am[k]["last_kspU"] for k in am}},
+                           "kspU_last": {k: am[k]["last_kspU"] for k in am},
+                           "c1_41": am_c1},
         "clocks": clocks,
     }
     if serving:
         line["serving"] = serving
     if args.cpu_baseline:
-        line["cpu_baseline"] = cpu_reference(args, quick=True)
+        line["cpu_baseline"] = cpu_reference(args)
     print(json.dumps(line))
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def gpu_am_c1(vg, barrier, its=3):
+    """AM steps of the 41^3 penny crack (the CPU AM-step baseline's workload) with the
+    Jacobi U solve, FP64 and mixed; the first iteration (from U = 0) untimed."""
+    out = {}
+    for prec in ("fp64", "mixed"):
+        ctx, _ = setup_problem(vg, 41)
+        times = []
+        for it in range(its):
+            barrier()
+            t0 = time.perf_counter()
+            ctx.am_step(dict(precision=prec))
+            barrier()
+            times.append(time.perf_counter() - t0)
+        ctx.close()
+        out[prec] = round(1.0 / float(np.mean(times[1:])), 3)
+    out["sample"] = f"AM iterations 2..{its} (the first, from U = 0, untimed)"
+    return out
 
 
 def run_serving(args):
@@ -478,29 +500,81 @@ def run_large(args):
         print(json.dumps(out))
 
 
-def cpu_reference(args, quick=False):
-    """The reference's KSP matvec (AIJ SpMV, restated in the oracle) on the host cores."""
+def _cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_reference(args, reps=5):
+    """The reference's method on the host cores, restated in the oracle (oracle/):
+    the KSP matvec -- the assembled DMDA AIJ matrix (CSR, 81 nnz/row) times a vector --
+    on the 129^3 workload itself, and the AM step (StepU + StepV with re-formed element
+    matrices, the Jacobian assembled every Newton iteration and CG + Jacobi on the
+    assembled matrix) on the 41^3 penny crack."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import vforacle as vo
-    n = 65
+    n = N_EDGE
     h = L_BOX / (n - 1)
     cores = os.cpu_count() or 1
     o = vo.Oracle((n, n, n), (L_BOX,) * 3, E=1e10, nu=0.25, Gc=100.0, epsilon=2 * h, eta=1e-8,
                   atnum=1, nthreads=cores)
     v = o.penny_v((L_BOX / 2,) * 3, 0.4)
     mask, _ = o.bc(vo.rollers_face())
+    t0 = time.perf_counter()
     csr = o.u_csr(v, mask)
+    t_asm = time.perf_counter() - t0
     x = np.random.default_rng(7).standard_normal(3 * o.N)
-    reps = 3 if quick else max(3, args.steps)
     o.csr_spmv(csr, x, cores)
     t0 = time.perf_counter()
     for _ in range(reps):
         o.csr_spmv(csr, x, cores)
     dt = (time.perf_counter() - t0) / reps
+    nnz = len(csr[1])
+    del csr
+    am = cpu_am_step(vo, cores)
     return {"value": round(3 * o.N / dt / 1e9, 4), "unit": "GDOF/s", "cores": cores,
-            "kind": "port",
-            "sample": f"AIJ (CSR, 81 nnz/row) SpMV of K(v) on the 65^3 penny-crack grid "
-                      f"({3 * o.N} dofs, {len(csr[1])} nonzeros), {reps} products"}
+            "kind": "port", "cpu": _cpu_model(),
+            "sample": f"AIJ (CSR, 81 nnz/row) SpMV of K(v) on the 129^3 penny-crack grid "
+                      f"({3 * o.N} dofs, {nnz} nonzeros), {reps} products after one untimed",
+            "assembly_s": round(t_asm, 3),
+            "am_step": am}
+
+
+def cpu_am_step(vo, cores, its=3):
+    """AM iterations of the 41^3 pressurised penny crack (E 10 GPa, nu 0.25, Gc 100, AT1,
+    eps 2h, p 1 MPa, rollers) by the reference's method on all host cores; the first
+    iteration (from U = 0) is untimed, the rest averaged."""
+    n, h = 41, L_BOX / 40
+    o = vo.Oracle((n, n, n), (L_BOX,) * 3, E=1e10, nu=0.25, Gc=100.0, epsilon=2 * h, eta=1e-8,
+                  atnum=1, nthreads=cores)
+    V = o.penny_v((L_BOX / 2,) * 3, 0.4)
+    virrev = V.copy()
+    U = np.zeros(3 * o.N)
+    p = np.full(o.N, 1e6)
+    umask, uval = o.bc(vo.rollers_face())
+    lb, ub = np.zeros(o.N), virrev.copy()
+    recs = []
+    for it in range(its):
+        t0 = time.perf_counter()
+        su, ta_u = o.step_u_asm(U, V, p=p, mask=umask, value=uval)
+        t1 = time.perf_counter()
+        sv, ta_v = o.step_v_asm(V, U, lb, ub, p=p)
+        t2 = time.perf_counter()
+        recs.append(dict(s=t2 - t0, u_s=t1 - t0, v_s=t2 - t1, asm_s=ta_u + ta_v,
+                         kspU=su.ksp_its, kspV=sv.ksp_its))
+    timed = recs[1:]
+    s = float(np.mean([r["s"] for r in timed]))
+    return {"workload": "penny crack 41^3 (206,763 U dofs), AT1 eps=2h, rollers, p=1e6",
+            "method": "assembled Jacobians (CSR) + CG/Jacobi, residuals from element matrices",
+            "am_steps_per_s": round(1.0 / s, 4), "s_per_step": round(s, 3),
+            "assembly_share": round(float(np.mean([r["asm_s"] / r["s"] for r in timed])), 3),
+            "kspU": [r["kspU"] for r in recs], "kspV": [r["kspV"] for r in recs],
+            "sample": f"AM iterations 2..{its} (the first, from U = 0, untimed)"}
 
 
 def run_reference(args):
@@ -512,7 +586,7 @@ def run_reference(args):
         "impl": "reference", "metric": "GDOF/s matvec", "value": cb["value"], "unit": "GDOF/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": cb["sample"]},
+        "config": {"workload": WORKLOAD, "grid": [N_EDGE] * 3, "sample": cb["sample"]},
         "cpu_baseline": cb,
         "e2e": {"value": cb["value"], "unit": "GDOF/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))

@@ -181,6 +181,21 @@ int vfo_step_v(const vfo_problem *P, double *v, const double *u, const double *t
                const double *lb, const double *ub, const uint8_t *bcmask,
                const double *bcval, const vfo_solver_opts *o, vfo_stats *st);
 
+/* The same two solves by the reference's method, for the timed CPU AM-step baseline:
+ * residuals from re-formed element matrices, the Jacobian assembled into CSR at every
+ * Newton iteration, KSPCG + Jacobi on the assembled matrix (VFMech.c:1555-1596,
+ * 1897-2029, 2772-2848, 2948-3027); element loops and vector sums on all threads.
+ * *seconds_assembly = time spent assembling the Jacobians.  UNILATERAL_NONE only. */
+int vfo_step_u_asm(const vfo_problem *P, double *u, const double *v, const double *theta,
+                   const double *thetaRef, const double *p, const uint8_t *bcmask,
+                   const double *bcval, const vfo_solver_opts *o, vfo_stats *st,
+                   double *seconds_assembly);
+int vfo_step_v_asm(const vfo_problem *P, double *v, const double *u, const double *theta,
+                   const double *thetaRef, const double *p, const double *virrev,
+                   const double *lb, const double *ub, const uint8_t *bcmask,
+                   const double *bcval, const vfo_solver_opts *o, vfo_stats *st,
+                   double *seconds_assembly);
+
 #ifdef __cplusplus
 }
 #endif

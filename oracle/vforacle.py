@@ -130,6 +130,10 @@ def _declare(L):
                        C.POINTER(Stats)],
         "vfo_step_v": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
                        C.POINTER(SolverOpts), C.POINTER(Stats)],
+        "vfo_step_u_asm": [_P, _dp, _dp, odp, odp, odp, ou8, odp, C.POINTER(SolverOpts),
+                           C.POINTER(Stats), C.POINTER(C.c_double)],
+        "vfo_step_v_asm": [_P, _dp, _dp, odp, odp, odp, odp, _dp, _dp, ou8, odp,
+                           C.POINTER(SolverOpts), C.POINTER(Stats), C.POINTER(C.c_double)],
     }
     for name, args in sig.items():
         f = getattr(L, name)
@@ -385,6 +389,27 @@ class Oracle:
                           np.ascontiguousarray(lb, np.float64), np.ascontiguousarray(ub, np.float64),
                           mask, value, C.byref(o), C.byref(st))
         return st
+
+
+    def step_u_asm(self, u, v, theta=None, thetaRef=None, p=None, mask=None, value=None,
+                   opts=None):
+        """StepU by the reference's method (assembled Jacobian, CG on the CSR matrix);
+        returns (stats, seconds spent assembling)."""
+        st, ta = Stats(), C.c_double()
+        o = opts or default_opts()
+        self.L.vfo_step_u_asm(C.byref(self.P), u, v, theta, thetaRef, p, mask, value, C.byref(o),
+                              C.byref(st), C.byref(ta))
+        return st, ta.value
+
+    def step_v_asm(self, v, u, lb, ub, theta=None, thetaRef=None, p=None, virrev=None,
+                   mask=None, value=None, opts=None):
+        st, ta = Stats(), C.c_double()
+        o = opts or default_opts()
+        self.L.vfo_step_v_asm(C.byref(self.P), v, u, theta, thetaRef, p, virrev,
+                              np.ascontiguousarray(lb, np.float64),
+                              np.ascontiguousarray(ub, np.float64), mask, value, C.byref(o),
+                              C.byref(st), C.byref(ta))
+        return st, ta.value
 
 
 def rollers_face():
