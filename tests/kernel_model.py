@@ -269,6 +269,50 @@ def u_element_sums(xn, vn, lam, mu, eta, h, cubic=False):
     return y
 
 
+def u_element_const(xn, S, lam, mu, h, cubic=False):
+    """xn[8][3] -> y[8][3] for an element whose phase field is the same at its 8 nodes
+    (S = v^2 + eta at every point); same arithmetic as u_element_const<T> in u_apply.cuh.
+    The stress is then the polynomial S D(G) with G bilinear per column, and its moments
+    against {1, s_a, s_b, s_a s_b} (doubled coordinate s = 2t) are exact averages over the
+    cell: E[s^2] = 1/3 and the odd moments vanish, which is also what the 3-point Gauss
+    rule gives for these degrees.  With the modal sums m (modal8s) and k_d = 1/(4 h_d):
+      T_B = sum_{e not in B} m[e][B + e] k_e                  (trace coefficient of s^B)
+      R[c][d][B] = vol S 3^-|B| k_d [lambda [c == d] T_B
+                   + mu (m[c][B + d] k_d + [c not in B] m[d][B + c] k_c)],
+    and the node polynomial's coefficient of the monomial p (a set of axes) is
+    w[p] = sum_{d in p} R[c][d][p - d]."""
+    m = [modal8s(xn[:, c]) for c in range(3)]
+    k = [0.25 / hh for hh in h]
+    vol = h[0] * h[1] * h[2]
+    T = {}
+    for B in range(8):
+        T[B] = sum(m[e][B | (1 << e)] * (1.0 if cubic else k[e]) for e in range(3)
+                   if not (B >> e) & 1)
+    y = np.zeros((8, 3))
+    for c in range(3):
+        w = np.zeros(8)
+        for pset in range(1, 8):
+            for d in range(3):
+                if not (pset >> d) & 1:
+                    continue
+                B = pset & ~(1 << d)
+                nb = bin(B).count("1")
+                kd = 1.0 if cubic else k[d]
+                kc = 1.0 if cubic else k[c]
+                off = m[d][B | (1 << c)] * kc if not (B >> c) & 1 else 0.0
+                if c == d:
+                    inner = lam * T[B] + 2 * mu * m[c][B | (1 << c)] * kd
+                else:
+                    inner = mu * (m[c][B | (1 << d)] * kd + off)
+                scale = vol * S * 3.0 ** -nb * (k[0] ** 2 if cubic else kd)
+                w[pset] += scale * inner
+        for a in range(8):
+            sg = [1 if (a >> b) & 1 else -1 for b in range(3)]
+            y[a, c] = sum(w[p] * np.prod([sg[b] for b in range(3) if (p >> b) & 1])
+                          for p in range(1, 8))
+    return y
+
+
 def plan(nx, ny, nz, TY, zc):
     ntx = -(-(nx - 1) // 32)
     nty = -(-(ny - 1) // TY)

@@ -32,6 +32,23 @@ def test_modal_sum_element_cubic(oracle_mod):
             assert np.abs(y.reshape(24) - yref).max() <= 1e-14 * np.abs(yref).max()
 
 
+@pytest.mark.parametrize("h", [(0.3, 0.5, 0.7), (0.25, 0.25, 0.25)])
+def test_constant_phase_field_element(oracle_mod, h):
+    """Elements whose 8 nodal v are equal: the fixed-weight form (exact cell averages of
+    the polynomial stress moments) against the reference's 27-point element matrix."""
+    rng = np.random.default_rng(6)
+    eta = 1e-3
+    o = oracle_mod.Oracle((2, 2, 2), h, E=2.0, nu=0.3, eta=eta)
+    lam, mu = 2.0 * 0.3 / 1.3 / 0.4, 2.0 / 1.3 * 0.5
+    for vc in (1.0, 0.37, 0.0):
+        v = np.full(8, vc)
+        x = rng.standard_normal(24)
+        yref = o.u_element_matrix(0, 0, 0, v) @ x
+        for cubic in ((False, True) if h[0] == h[1] == h[2] else (False,)):
+            y = km.u_element_const(x.reshape(8, 3), vc * vc + eta, lam, mu, h, cubic=cubic)
+            assert np.abs(y.reshape(24) - yref).max() <= 1e-14 * np.abs(yref).max(), (vc, cubic)
+
+
 @pytest.mark.parametrize("n,TY,zc", [((37, 21, 13), 8, 5), ((34, 10, 7), 4, 3), ((3, 2, 4), 8, 2)])
 def test_tiled_schedule_matches_oracle(oracle_mod, n, TY, zc):
     rng = np.random.default_rng(sum(n))

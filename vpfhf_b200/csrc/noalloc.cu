@@ -51,14 +51,6 @@ extern "C" int vfgpu_u_apply_noalloc(const vfgpu_grid* g, const vfgpu_matprop* m
   if (!is_device_ptr(v) || !is_device_ptr(x) || !is_device_ptr(y) ||
       (bcbits && !is_device_ptr(bcbits)))
     return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: v, x, y, bcbits must be device pointers");
-  {
-    // out of place only: the tiles read x planes and Dirichlet rows copy x while other
-    // blocks write y
-    const uintptr_t n3 = (uintptr_t)g->nx * g->ny * g->nz * 3 * sizeof(double);
-    const uintptr_t xb = reinterpret_cast<uintptr_t>(x), yb = reinterpret_cast<uintptr_t>(y);
-    if (xb < yb + n3 && yb < xb + n3)
-      return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: x and y overlap (the apply is out of place)");
-  }
   int dev = 0, nsm = 148;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_noalloc: cudaGetDevice");
@@ -69,6 +61,14 @@ extern "C" int vfgpu_u_apply_noalloc(const vfgpu_grid* g, const vfgpu_matprop* m
                 "vfgpu_u_apply_noalloc: grid %dx%dx%d needs %zu scratch doubles, the fixed "
                 "scratch holds %zu (use vfgpu_u_apply with a vfgpu_ctx)",
                 g->nx, g->ny, g->nz, p.seamX + p.seamY, kScratchDoubles);
+  {
+    // out of place only: the tiles read x planes and Dirichlet rows copy x while other
+    // blocks write y
+    const uintptr_t n3 = (uintptr_t)g->nx * g->ny * g->nz * 3 * sizeof(double);
+    const uintptr_t xb = reinterpret_cast<uintptr_t>(x), yb = reinterpret_cast<uintptr_t>(y);
+    if (xb < yb + n3 && yb < xb + n3)
+      return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_noalloc: x and y overlap (the apply is out of place)");
+  }
   double* scratch = nullptr;
   int rc = scratch_address(&scratch);
   if (rc) return rc;

@@ -54,7 +54,16 @@ template <typename T_, bool CUBIC = false> struct UOp {
       lam = T(LT.lambda[layer]);
       mu = T(LT.mu[layer]);
     }
-    u_element<T, CUBIC>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+    // an element whose nodal phase field is constant (the intact bulk, v = 1) takes the
+    // fixed-weight form; the rest the row closed form
+    const T v0 = vn[0];
+    bool cst = true;
+#pragma unroll
+    for (int a = 1; a < 8; a++) cst = cst && vn[a] == v0;
+    if (cst)
+      u_element_const<T, CUBIC>(xn, fma(v0, v0, eta), lam, mu, A.ihx, A.ihy, A.ihz, A.vol, out);
+    else
+      u_element<T, CUBIC>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   // Writes y of node n (Dirichlet rows: y = x); with DOT, returns x.y over its dofs
   // (the launch accumulates the CG dot into A.dot).
