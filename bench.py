@@ -387,7 +387,8 @@ def gpu_am_c1(vg, barrier, its=3):
 def run_serving(args):
     """The serving stream: independent pressurised-crack problems (grid edge uniform over
     {17, 33, 65, 97}, 1-4 random penny cracks, E ~ U[5,30] GPa, nu ~ U[0.15,0.35], AT1/AT2,
-    5 AM iterations each) through the library's request loop.  The FP64 capacity is
+    5 AM iterations each, multigrid U solve on the two larger grids) through the library's
+    request loop.  The FP64 capacity is
     measured closed-loop on the first 128 problems; the full stream then arrives as a
     seeded Poisson process at 0.8x that capacity, once in FP64 and once mixed (same
     arrival times).  Latency = completion - arrival."""
@@ -398,6 +399,8 @@ def run_serving(args):
     rate = 0.8 * cap["throughput"]
     arr = poisson_arrivals(count, rate)
     out = {"problems": count, "workers": workers, "am_its_per_problem": 5,
+           "u_solve": "multigrid PCG on the 65^3 / 97^3 problems, Jacobi PCG on 17^3 / 33^3 "
+                      "(solve option pc = auto)",
            "capacity_fp64_per_s": round(cap["throughput"], 3),
            "arrival_rate_per_s": round(rate, 3),
            "grids": "edge uniform over {17,33,65,97}, cube [0,4]^3"}

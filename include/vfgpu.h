@@ -97,10 +97,14 @@ typedef struct {
                           /* VFGPU_PC_MG (geometric multigrid V-cycle, FP32 under       */
                           /* VFGPU_MIXED, FP64 otherwise; FP64 CG with the Jacobi       */
                           /* solve's stopping test; needs >= 9 nodes along some axis)   */
+                          /* or VFGPU_PC_AUTO (multigrid on grids with at least         */
+                          /* VFGPU_PC_AUTO_MG_NODES nodes along some axis, else Jacobi) */
 } vfgpu_solve_opts;
 
 #define VFGPU_PC_JACOBI 0
 #define VFGPU_PC_MG 1
+#define VFGPU_PC_AUTO 2
+#define VFGPU_PC_AUTO_MG_NODES 65
 
 typedef struct {
   int newton_its;         /* SNES iterations                                            */

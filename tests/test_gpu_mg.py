@@ -177,3 +177,18 @@ def test_mg_precision_switch_and_am_loop(cuda):
         ref = run(b, ["fp64", "mixed", "fp64"][:k + 1])[-1]
         b.close()
         assert np.array_equal(got[k][0], ref[0]) and np.array_equal(got[k][1], ref[1]), prec
+
+
+@pytest.mark.parametrize("n,resolved", [(33, "jacobi"), (65, "mg")])
+def test_auto_preconditioner_resolves_by_grid(cuda, n, resolved):
+    """pc="auto" is the Jacobi solve below 65 nodes per axis and the multigrid one from
+    65 on: the same bits as the solve it resolves to."""
+    out = {}
+    for pc in ("auto", resolved):
+        ctx = _penny_ctx(n)
+        rc, st = ctx.step_u(dict(pc=pc, precision="mixed"))
+        assert rc == 0 and st["reason"] > 0, st
+        out[pc] = (ctx.get_field("U"), st["ksp_its"])
+        ctx.close()
+    assert np.array_equal(out["auto"][0], out[resolved][0])
+    assert out["auto"][1] == out[resolved][1]

@@ -273,14 +273,15 @@ class VFContext:
 
 def solve_opts(**kw):
     """SolveOpts with the reference's defaults (vfgpu_default_solve_opts), overridden by kw;
-    `precision` accepts FP64 / MIXED or "fp64" / "mixed", `pc` "jacobi" / "mg"."""
+    `precision` accepts FP64 / MIXED or "fp64" / "mixed", `pc` "jacobi" / "mg" / "auto"
+    (multigrid on grids with >= 65 nodes along some axis, else Jacobi)."""
     o = _abi.SolveOpts()
     _abi.lib().vfgpu_default_solve_opts(C.byref(o))
     for k, v in kw.items():
         if k == "precision" and isinstance(v, str):
             v = {"fp64": FP64, "mixed": MIXED}[v.lower()]
         if k == "pc" and isinstance(v, str):
-            v = {"jacobi": _abi.PC_JACOBI, "mg": _abi.PC_MG}[v.lower()]
+            v = {"jacobi": _abi.PC_JACOBI, "mg": _abi.PC_MG, "auto": _abi.PC_AUTO}[v.lower()]
         setattr(o, k, v)
     return o
 

@@ -17,7 +17,7 @@ OK, NOT_CONVERGED, DIVERGED = 0, 1, 2
 ERR_INVALID, ERR_CUDA, ERR_OOM, ERR_STATE = -1, -2, -3, -4
 FP64, MIXED = 0, 1
 UNILATERAL_NONE, UNILATERAL_NOCOMPRESSION = 0, 1
-PC_JACOBI, PC_MG = 0, 1
+PC_JACOBI, PC_MG, PC_AUTO = 0, 1, 2
 BC_NONE, BC_ZERO, BC_ONE, BC_FIXED = 0, 1, 2, 3
 FIELD_U, FIELD_V, FIELD_VIRREV, FIELD_BCU, FIELD_THETA, FIELD_THETAREF, FIELD_PRESSURE = range(7)
 FIELD_NAMES = {"U": FIELD_U, "V": FIELD_V, "VIrrev": FIELD_VIRREV, "BCU": FIELD_BCU,

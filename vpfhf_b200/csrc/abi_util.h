@@ -6,6 +6,13 @@
 #include "ctx.h"
 
 namespace vfgpu {
+// The StepU preconditioner a solve option resolves to on an nx x ny x nz grid
+// (VFGPU_PC_AUTO: multigrid where some axis has VFGPU_PC_AUTO_MG_NODES nodes or more).
+inline int resolve_pc(int pc, int nx, int ny, int nz) {
+  if (pc != VFGPU_PC_AUTO) return pc;
+  const int m = nx > ny ? (nx > nz ? nx : nz) : (ny > nz ? ny : nz);
+  return m >= VFGPU_PC_AUTO_MG_NODES ? VFGPU_PC_MG : VFGPU_PC_JACOBI;
+}
 int fail(int code, const char* fmt, ...);
 int cuda_fail(cudaError_t e, const char* what);
 bool is_device_ptr(const void* p);

@@ -79,7 +79,8 @@ namespace {
 
 GridKey key_of(const vfgpu_request& q) {
   const vfgpu_grid& g = q.grid;
-  const int mg = q.opts.pc == VFGPU_PC_MG ? (q.opts.precision == VFGPU_MIXED ? 4 : 8) : 0;
+  const int pc = resolve_pc(q.opts.pc, g.nx, g.ny, g.nz);
+  const int mg = pc == VFGPU_PC_MG ? (q.opts.precision == VFGPU_MIXED ? 4 : 8) : 0;
   return {g.nx, g.ny, g.nz, g.lx, g.ly, g.lz, mg};
 }
 

@@ -361,8 +361,9 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   if (o_) o = *o_; else vfgpu_default_solve_opts(&o);
   if (o.precision != VFGPU_FP64 && o.precision != VFGPU_MIXED)
     return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad precision");
-  if (o.pc != VFGPU_PC_JACOBI && o.pc != VFGPU_PC_MG)
+  if (o.pc != VFGPU_PC_JACOBI && o.pc != VFGPU_PC_MG && o.pc != VFGPU_PC_AUTO)
     return fail(VFGPU_ERR_INVALID, "vfgpu_step_u: bad preconditioner");
+  o.pc = resolve_pc(o.pc, c->nx, c->ny, c->nz);
   vfgpu_solve_stats S{};
   cudaSetDevice(c->dev);
   int rc = solve_buffers(c);

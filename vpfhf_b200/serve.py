@@ -158,10 +158,12 @@ def random_penny(rng, L):
 
 
 def serving_stream(count=512, seed=1004, edges=(17, 33, 65, 97), L=4.0, am_its=5,
-                   precision="fp64", pc="jacobi"):
+                   precision="fp64", pc="auto"):
     """`count` independent problems: grid edge uniform over `edges`, 1-4 random penny
     cracks, E ~ U[5, 30] GPa, nu ~ U[0.15, 0.35], AT1 or AT2 with probability 1/2,
-    epsilon = 2h, eta = 1e-8, Gc = 100, 1 MPa crack pressure on rollers."""
+    epsilon = 2h, eta = 1e-8, Gc = 100, 1 MPa crack pressure on rollers.  `pc` "auto"
+    solves the 65^3 and 97^3 problems with the multigrid U solve and the smaller ones
+    with the Jacobi one."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
