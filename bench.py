@@ -196,7 +196,22 @@ def run_gpu(args):
     t32 = timed_applies(vg.MIXED, x32, y32, args.steps, args.warmup)
     ms64 = float(np.mean(t64))
     ms32 = float(np.mean(t32))
-    ms64, ms32 = max_over_ranks([ms64, ms32], dist, "cuda")
+    # the tensor-core element contraction (vfgpu_u_apply_tc), same FP32 inputs
+    for _ in range(args.warmup):
+        ctx.u_apply_tc(x32, y32)
+    evt = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    barrier()
+    for a, b in evt:
+        with torch.cuda.stream(s):
+            flush.zero_()
+        a.record(s)
+        ctx.u_apply_tc(x32, y32)
+        b.record(s)
+    torch.cuda.synchronize()
+    mstc = float(np.mean([a.elapsed_time(b) for a, b in evt]))
+    tc_ok = not ctx.tc_error()
+    ms64, ms32, mstc = max_over_ranks([ms64, ms32, mstc], dist, "cuda")
 
     if args.only_am:
         out = {}
@@ -230,7 +245,8 @@ def run_gpu(args):
 
     if args.only_apply:
         if rank == 0:
-            print(json.dumps({"grid": n, "ms_fp64": ms64, "ms_fp32": ms32, "clocks": clocks}))
+            print(json.dumps({"grid": n, "ms_fp64": ms64, "ms_fp32": ms32, "ms_tc": mstc,
+                              "tc_ok": tc_ok, "clocks": clocks}))
         ctx.close()
         if dist:
             dist.destroy_process_group()
@@ -341,6 +357,12 @@ def run_gpu(args):
                     "instructions issued / (measured DFMA rate), the pipe's occupancy"},
         "mixed": {"value": round(N3 * world / (ms32 * 1e-3) / 1e9, 3), "unit": "GDOF/s",
                   "ms_per_step": round(ms32, 4), "dtype": "f32"},
+        "tensor_core_apply": {
+            "value": round(N3 * world / (mstc * 1e-3) / 1e9, 3), "unit": "GDOF/s",
+            "ms_per_step": round(mstc, 4), "dtype": "f32 (split-tf32 tcgen05.mma)",
+            "ok": tc_ok,
+            "note": "vfgpu_u_apply_tc: element contraction as two GEMMs per 128-element tile on "
+                    "the tensor cores (not used by the solvers); compare with `mixed`"},
         "am_steps_per_s": {**{k: round(1.0 / am[k]["s_per_step"], 3) for k in am},
                            "mixed_vs_fp64_max_rel_energy_diff": rel,
                            "mixed_vs_fp64_rel_at_last_step": rel_last,

@@ -364,6 +364,25 @@ int vfgpu_u_apply_noalloc(const vfgpu_grid* grid, const vfgpu_matprop* mp, doubl
                           const double* v, const unsigned char* bcbits, const double* x,
                           double* y, void* stream);
 
+/* No counterpart in the reference: y = J_U x (FP32 vectors on the device, V from the
+ * ctx) with the element contraction on the tensor cores -- two GEMMs per tile of 128
+ * elements (gradients, strains and v at the 27 Gauss points from the 32 nodal values;
+ * the Gauss-weighted transpose back to the 24 nodal forces) issued as tcgen05.mma in
+ * split TF32 (hi/lo, three products per term, FP32 accumulation in tensor memory), the
+ * pointwise degradation v^2 + eta and Lame factors on the CUDA cores.  Element results
+ * are summed with atomics (not bit-reproducible); Dirichlet rows y = x.  A measured
+ * alternative to vfgpu_u_apply_dev's CUDA-core element, not used by the solvers;
+ * UNILATERAL_NONE only.  Queued on the ctx stream; vfgpu_tc_error reports whether a
+ * bounded wait inside it gave up (its results are then void). */
+int vfgpu_u_apply_tc(vfgpu_ctx* ctx, const float* x, float* y);
+int vfgpu_tc_error(vfgpu_ctx* ctx, int* flagged);
+/* Host only: the two constant matrices of vfgpu_u_apply_tc for an hx x hy x hz cell,
+ * row-major B1[32][224] (K = 24 displacements + 8 phase-field values, N = 27 points x
+ * {tr, 2 e_xx, 2 e_yy, 2 e_zz, g_xy, g_xz, g_yz, v} + 8 zero columns) and B2[192][32]
+ * (K = 3 passes x (9 points x {lambda s tr, mu s E_xx .. E_yz} + 1 zero row), N = 24
+ * dofs + 8 zero columns). */
+int vfgpu_tc_tables(double hx, double hy, double hz, double* B1, double* B2);
+
 /* Measurement utility, no counterpart in the reference: FMA throughput of the
  * current GPU's CUDA cores in TFLOP/s for bytes = 8 (FP64) or 4 (FP32), from a
  * kernel of independent FMA chains (the denominator of the operator's compute

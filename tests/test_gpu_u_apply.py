@@ -93,3 +93,29 @@ def test_u_apply_host_pipeline_matches_device(cuda, oracle_mod, unilateral):
         ctx.u_apply(xp.numpy(), vg.FP64, out=yp.numpy())
         assert np.array_equal(yp.numpy(), y)
     ctx.close()
+
+
+@pytest.mark.parametrize("n,l,cellE", [((41, 41, 41), (4.0, 4.0, 4.0), False),
+                                       ((41, 41, 41), (4.0, 4.0, 4.0), True),
+                                       ((37, 21, 13), (1.1, 0.9, 0.7), False)])
+def test_u_apply_constant_phase_field_elements(cuda, oracle_mod, n, l, cellE):
+    """Mostly intact phase field (v = 1 away from a penny crack, a block of a constant
+    v = 0.4 and a random block): elements whose 8 nodal v are equal take the
+    fixed-weight element, the rest the row closed form; FP64 at 1e-12 and FP32 at
+    2e-6 normwise against the oracle, on cubic and non-cubic cells."""
+    import vpfhf_b200 as vg
+    o, ctx, _, x, mask = _setup(oracle_mod, n, l, 5, cellE=cellE)
+    rng = np.random.default_rng(6)
+    pen = oracle_mod.Oracle(n, l, epsilon=2 * max(li / (ni - 1) for li, ni in zip(l, n)))
+    v = pen.penny_v(tuple(li / 2 for li in l), 0.25 * min(l))
+    vv = v.reshape(n[2], n[1], n[0])
+    vv[:n[2] // 3, :n[1] // 3, :n[0] // 3] = 0.4
+    vv[-n[2] // 4:, -n[1] // 4:, -n[0] // 4:] = rng.uniform(0, 1, vv[-n[2] // 4:, -n[1] // 4:, -n[0] // 4:].shape)
+    v = vv.reshape(-1).copy()
+    ctx.set_field("V", v)
+    yref = o.u_apply(v, x, mask)
+    y = ctx.u_apply(x, vg.FP64)
+    assert np.abs(y - yref).max() <= 1e-12 * np.abs(yref).max()
+    y32 = ctx.u_apply(x, vg.MIXED)
+    assert np.linalg.norm(y32 - yref) <= 2e-6 * np.linalg.norm(yref)
+    ctx.close()

@@ -164,6 +164,16 @@ class VFContext:
         _abi.check(self.L.vfgpu_u_apply_dev(self.h, int(precision), x.data_ptr(), y.data_ptr()),
                    "vfgpu_u_apply_dev")
 
+    def u_apply_tc(self, x, y):
+        """Queues y = J_U x with the tensor-core element contraction (float32 device
+        tensors; vfgpu_u_apply_tc).  Returns immediately."""
+        _abi.check(self.L.vfgpu_u_apply_tc(self.h, x.data_ptr(), y.data_ptr()), "vfgpu_u_apply_tc")
+
+    def tc_error(self):
+        f = C.c_int()
+        _abi.check(self.L.vfgpu_tc_error(self.h, C.byref(f)), "vfgpu_tc_error")
+        return bool(f.value)
+
     @property
     def stream_handle(self):
         s = C.c_void_p()

@@ -161,6 +161,9 @@ _SIGS = {
     "vfgpu_server_info_get": [C.c_void_p, C.POINTER(ServerInfo)],
     "vfgpu_server_destroy": [C.c_void_p],
     "vfgpu_fma_peak": [C.c_int, C.POINTER(C.c_double)],
+    "vfgpu_u_apply_tc": [C.c_void_p, C.c_void_p, C.c_void_p],
+    "vfgpu_tc_error": [C.c_void_p, C.POINTER(C.c_int)],
+    "vfgpu_tc_tables": [C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "vfgpu_wait_selftest": [C.c_longlong, C.c_int, C.POINTER(C.c_int)],
     "vfgpu_u_apply_noalloc": [C.POINTER(Grid), C.POINTER(MatProp), C.c_double, C.c_void_p,
                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p],

@@ -30,6 +30,8 @@ struct vfgpu_ctx {
   // compression bits of the current linearisation point
   int unilateral = 0;
   uint32_t* d_cflag = nullptr;  // NC
+  void* d_tcB = nullptr;        // tensor-core apply: its constant operands (tc_apply.cu)
+  unsigned* d_tcerr = nullptr;  // tensor-core apply: bounded-wait flag
 
   // in-situ stresses (VFCtx.hasInsitu, insitumin, insitumax)
   bool has_insitu = false;

@@ -169,7 +169,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   cudaFree(c->t64c);
-  void* bufs[] = {c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_tcB, c->d_tcerr, c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
