@@ -197,20 +197,22 @@ def run_gpu(args):
     ms64 = float(np.mean(t64))
     ms32 = float(np.mean(t32))
     # the tensor-core element contraction (vfgpu_u_apply_tc), same FP32 inputs
-    for _ in range(args.warmup):
+    mstc, tc_ok = float("nan"), False
+    for _ in range(args.warmup if args.tc else 0):
         ctx.u_apply_tc(x32, y32)
-    evt = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-           for _ in range(args.steps)]
-    barrier()
-    for a, b in evt:
-        with torch.cuda.stream(s):
-            flush.zero_()
-        a.record(s)
-        ctx.u_apply_tc(x32, y32)
-        b.record(s)
-    torch.cuda.synchronize()
-    mstc = float(np.mean([a.elapsed_time(b) for a, b in evt]))
-    tc_ok = not ctx.tc_error()
+    if args.tc:
+        evt = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        barrier()
+        for a, b in evt:
+            with torch.cuda.stream(s):
+                flush.zero_()
+            a.record(s)
+            ctx.u_apply_tc(x32, y32)
+            b.record(s)
+        torch.cuda.synchronize()
+        mstc = float(np.mean([a.elapsed_time(b) for a, b in evt]))
+        tc_ok = not ctx.tc_error()
     ms64, ms32, mstc = max_over_ranks([ms64, ms32, mstc], dist, "cuda")
 
     if args.only_am:
@@ -357,7 +359,7 @@ def run_gpu(args):
                     "instructions issued / (measured DFMA rate), the pipe's occupancy"},
         "mixed": {"value": round(N3 * world / (ms32 * 1e-3) / 1e9, 3), "unit": "GDOF/s",
                   "ms_per_step": round(ms32, 4), "dtype": "f32"},
-        "tensor_core_apply": {
+        "tensor_core_apply": None if not args.tc else {
             "value": round(N3 * world / (mstc * 1e-3) / 1e9, 3), "unit": "GDOF/s",
             "ms_per_step": round(mstc, 4), "dtype": "f32 (split-tf32 tcgen05.mma)",
             "ok": tc_ok,
@@ -628,6 +630,8 @@ def main():
     ap.add_argument("--serve-workers", type=int, default=8)
     ap.add_argument("--impl", default="vfgpu", choices=["vfgpu", "reference"])
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-tc", dest="tc", action="store_false",
+                    help="skip the tensor-core apply timing")
     ap.add_argument("--grid", type=int, default=N_EDGE, help="nodes per axis (profiling runs)")
     ap.add_argument("--only-apply", action="store_true",
                     help="time the operator applications only (profiling runs)")
