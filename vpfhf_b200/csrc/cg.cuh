@@ -18,7 +18,7 @@ enum { CG_RUNNING = 0, CG_CONVERGED_RTOL = 2, CG_CONVERGED_ATOL = 3, CG_DIVERGED
 
 struct CGState {
   double rz, rz_new, pw, zz, alpha, beta, rnorm0, ttol, dtol;
-  double xalpha;  // step of the solution update still to be applied (0: none)
+  double xalpha;  // step of the current iteration (0 if it made none); see cg_after_apply
   int its, maxit, done, reason;
   unsigned int arrive;  // blocks of the running update kernel that have finished
 };
@@ -29,13 +29,6 @@ constexpr int RED_THREADS = 256, RED_BLOCKS = 592;
 
 // The vectors are whole device allocations (16-byte aligned: the kernels use 16-byte
 // loads and stores).
-// With p2 non-null the solution update is fused into the operator apply: iteration i
-// applies the operator to p_i (buffer i % 2: p, p2) and the apply also adds
-// xalpha p_{i-1} (the other buffer) to x for every node it finishes; the update kernel
-// then moves only r, and the direction update writes p_{i+1} into the other buffer.
-// After the last iteration cg_finish_x adds the pending step.  Iteration parity follows
-// the global iteration count, so batches of iterations must be even.  With p2 null
-// (one direction buffer) the update kernel updates x itself.
 template <typename T> struct CGVecs {
   T* x;              // solution
   T* r;              // residual
@@ -47,22 +40,20 @@ template <typename T> struct CGVecs {
   int64_t n;
   const double* dotp;   // the operator's block partials of p.w (written by the apply), or
   int ndot;             // null: cg_after_apply computes p.w in a separate pass
-  T* p2 = nullptr;      // second direction buffer: fused solution update (see above)
-  T* pcur(int parity) const { return (p2 && (parity & 1)) ? p2 : p; }
-  T* pother(int parity) const { return p2 ? ((parity & 1) ? p : p2) : p; }
 };
 
 // Host-side driver pieces (solver.cu).  One iteration is: the operator apply
 // w = A p, which also writes the block partials of p.w to v.dotp (the tile
-// engine's A.dot), then cg_after_apply.
+// engine's A.dot), then cg_after_apply: the update kernel moves r only (r -= alpha w,
+// z = D^-1 r, (r,z), (z,z)), and the direction kernel does x += alpha p together with
+// p = z + beta p, in one pass over p.  The iteration that stops the solve skips the
+// direction kernel, so cg_finish_x adds its step to x after the loop.
 template <typename T>
 cudaError_t cg_init(const CGVecs<T>& v, CGState* st, double* partial, double rtol, double atol,
                     double dtol, int maxit, cudaStream_t s);
 template <typename T>
-cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s,
-                           int parity = 0);
-// Fused mode: x += xalpha p_last, the step of the last iteration (of parity `parity`).
+cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s);
 template <typename T>
-cudaError_t cg_finish_x(const CGVecs<T>& v, const CGState* st, int parity, cudaStream_t s);
+cudaError_t cg_finish_x(const CGVecs<T>& v, const CGState* st, cudaStream_t s);
 
 }  // namespace vfgpu

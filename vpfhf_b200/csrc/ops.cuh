@@ -20,19 +20,6 @@
 
 namespace vfgpu {
 
-// The CG solution update of the previous iteration, x += alpha p_prev, done by the
-// operator apply for the K dofs of each node it finishes (exactly once per node: the
-// tile owner or the seam fix-up); the same arithmetic as the separate update kernel.
-template <int K, typename T, class Args>
-__device__ __forceinline__ void fused_x_update(const Args& A, int64_t n) {
-  if (!A.xacc) return;
-  const double a = *A.xalpha;
-  if (a == 0.) return;
-  const T ta = (T)a;
-#pragma unroll
-  for (int c = 0; c < K; c++) A.xacc[K * n + c] = A.xacc[K * n + c] + ta * A.xdir[K * n + c];
-}
-
 // CUBIC: hx = hy = hz, every 1/h factor folds into the row weight (u_element).
 template <typename T_, bool CUBIC = false> struct UOp {
   using T = T_;
@@ -90,7 +77,6 @@ template <typename T_, bool CUBIC = false> struct UOp {
       A.y[3 * n + c] = y;
       if constexpr (DOT) d += (double)A.x[3 * n + c] * (double)y;
     }
-    fused_x_update<3, T>(A, n);
     return d;
   }
 };
@@ -203,9 +189,6 @@ template <typename T> struct VApplyArgs {
   const int* __restrict__ skip;       // if non-null and *skip != 0 the launch does nothing
   const DevParams* __restrict__ P;    // Gc/(2 c_w) eps per layer
   double* __restrict__ dot;           // if non-null: per-block partials of x.y
-  T* __restrict__ xacc;               // fused CG solution update, as in UApplyArgs
-  const T* __restrict__ xdir;
-  const double* __restrict__ xalpha;
   int nx, ny, nz, ntx, nty;
   T ihx, ihy, ihz, vol;
 };
@@ -334,7 +317,6 @@ template <typename T_> struct VOp {
   __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
     const T y = (A.mask && A.mask[n]) ? T(0) : val[0];
     A.y[n] = y;
-    fused_x_update<1, T>(A, n);
     if constexpr (DOT) return (double)A.x[n] * (double)y;
     return 0.;
   }

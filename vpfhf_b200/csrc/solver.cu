@@ -187,18 +187,18 @@ __device__ __forceinline__ void cg_finish_iteration(CGState* st, double rz, doub
 
 // p.w by blocks (for an operator apply that did not produce it).
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) cg_pw_kernel(CGVecs<T> v, const T* __restrict__ pc,
-                                                            const CGState* st, double* partial) {
+__global__ void __launch_bounds__(RED_THREADS) cg_pw_kernel(CGVecs<T> v, const CGState* st,
+                                                            double* partial) {
   if (st->done) return;
   double acc[1] = {0.};
   pack_loop<T>(
       v.n,
       [&](int64_t c) {
-        const Pack<T> p = ld16(pc, c), w = ld16(v.w, c);
+        const Pack<T> p = ld16(v.p, c), w = ld16(v.w, c);
 #pragma unroll
         for (int k = 0; k < Pack<T>::W; k++) acc[0] += (double)p.e[k] * (double)w.e[k];
       },
-      [&](int64_t i) { acc[0] += (double)pc[i] * (double)v.w[i]; });
+      [&](int64_t i) { acc[0] += (double)v.p[i] * (double)v.w[i]; });
   block_sum<1>(acc, partial);
 }
 
@@ -225,59 +225,31 @@ __global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, CGS
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->pw = pw;
     st->alpha = alpha;
-    st->xalpha = alpha;  // fused mode: the next apply (or cg_finish_x) adds alpha p to x
+    st->xalpha = alpha;  // x += alpha p: in cg_p_kernel, or in cg_finish_x if the solve stops here
   }
   const T a = (T)alpha;
   double acc[2] = {0., 0.};
-  if (v.p2) {  // fused mode: x is updated by the next operator apply
-    pack_loop<T>(
-        v.n,
-        [&](int64_t c) {
-          Pack<T> r = ld16(v.r, c);
-          const Pack<T> w = ld16(v.w, c), d = ld16(v.dinv, c);
+  pack_loop<T>(
+      v.n,
+      [&](int64_t c) {
+        Pack<T> r = ld16(v.r, c);
+        const Pack<T> w = ld16(v.w, c), d = ld16(v.dinv, c);
 #pragma unroll
-          for (int k = 0; k < Pack<T>::W; k++) {
-            r.e[k] = r.e[k] - a * w.e[k];
-            const T z = r.e[k] * d.e[k];
-            acc[0] += (double)z * (double)r.e[k];
-            acc[1] += (double)z * (double)z;
-          }
-          st16(v.r, c, r);
-        },
-        [&](int64_t i) {
-          const T r = v.r[i] - a * v.w[i];
-          const T z = r * v.dinv[i];
-          v.r[i] = r;
-          acc[0] += (double)z * (double)r;
+        for (int k = 0; k < Pack<T>::W; k++) {
+          r.e[k] = r.e[k] - a * w.e[k];
+          const T z = r.e[k] * d.e[k];
+          acc[0] += (double)z * (double)r.e[k];
           acc[1] += (double)z * (double)z;
-        });
-  } else {
-    pack_loop<T>(
-        v.n,
-        [&](int64_t c) {
-          Pack<T> x = ld16(v.x, c), r = ld16(v.r, c);
-          const Pack<T> p = ld16(v.p, c), w = ld16(v.w, c), d = ld16(v.dinv, c);
-#pragma unroll
-          for (int k = 0; k < Pack<T>::W; k++) {
-            x.e[k] = x.e[k] + a * p.e[k];
-            r.e[k] = r.e[k] - a * w.e[k];
-            const T z = r.e[k] * d.e[k];
-            acc[0] += (double)z * (double)r.e[k];
-            acc[1] += (double)z * (double)z;
-          }
-          st16(v.x, c, x);
-          st16(v.r, c, r);
-        },
-        [&](int64_t i) {
-          const T x = v.x[i] + a * v.p[i];
-          const T r = v.r[i] - a * v.w[i];
-          const T z = r * v.dinv[i];
-          v.x[i] = x;
-          v.r[i] = r;
-          acc[0] += (double)z * (double)r;
-          acc[1] += (double)z * (double)z;
-        });
-  }
+        }
+        st16(v.r, c, r);
+      },
+      [&](int64_t i) {
+        const T r = v.r[i] - a * v.w[i];
+        const T z = r * v.dinv[i];
+        v.r[i] = r;
+        acc[0] += (double)z * (double)r;
+        acc[1] += (double)z * (double)z;
+      });
   block_sum<2>(acc, partial);
   __shared__ bool last;
   __threadfence();  // this block's partials are visible before it is counted
@@ -312,26 +284,36 @@ __global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, CGS
   }
 }
 
-// p_next = z + beta p_cur (in place when the two are the same buffer).
+// x += alpha p and p = z + beta p in one pass (the iteration went on: not done).
 template <typename T>
-__global__ void cg_p_kernel(CGVecs<T> v, const T* pc, T* pn, const CGState* st) {
+__global__ void cg_p_kernel(CGVecs<T> v, const CGState* st) {
   if (st->done) return;
-  const T b = (T)st->beta;
+  const T a = (T)st->alpha, b = (T)st->beta;
   pack_loop<T>(
       v.n,
       [&](int64_t c) {
-        Pack<T> p = ld16(pc, c);
+        Pack<T> p = ld16(v.p, c), x = ld16(v.x, c);
         const Pack<T> r = ld16(v.r, c), d = ld16(v.dinv, c);
 #pragma unroll
-        for (int k = 0; k < Pack<T>::W; k++) p.e[k] = r.e[k] * d.e[k] + b * p.e[k];
-        st16(pn, c, p);
+        for (int k = 0; k < Pack<T>::W; k++) {
+          x.e[k] = x.e[k] + a * p.e[k];
+          p.e[k] = r.e[k] * d.e[k] + b * p.e[k];
+        }
+        st16(v.x, c, x);
+        st16(v.p, c, p);
       },
-      [&](int64_t i) { pn[i] = v.r[i] * v.dinv[i] + b * pc[i]; });
+      [&](int64_t i) {
+        v.x[i] = v.x[i] + a * v.p[i];
+        v.p[i] = v.r[i] * v.dinv[i] + b * v.p[i];
+      });
 }
 
-// x += xalpha p (the step the fused mode still owes x after the last iteration).
+// The step of the iteration that stopped the solve (its cg_p_kernel did not run):
+// x += xalpha p; nothing after an indefinite p.w (xalpha = 0) or while the solve is
+// still going (a watchdog stop between iterations: every step has reached x).
 template <typename T>
-__global__ void cg_finish_x_kernel(CGVecs<T> v, const T* __restrict__ pl, const CGState* st) {
+__global__ void cg_finish_x_kernel(CGVecs<T> v, const CGState* st) {
+  if (!st->done) return;
   const double alpha = st->xalpha;
   if (alpha == 0.) return;
   const T a = (T)alpha;
@@ -339,12 +321,12 @@ __global__ void cg_finish_x_kernel(CGVecs<T> v, const T* __restrict__ pl, const 
       v.n,
       [&](int64_t c) {
         Pack<T> x = ld16(v.x, c);
-        const Pack<T> p = ld16(pl, c);
+        const Pack<T> p = ld16(v.p, c);
 #pragma unroll
         for (int k = 0; k < Pack<T>::W; k++) x.e[k] = x.e[k] + a * p.e[k];
         st16(v.x, c, x);
       },
-      [&](int64_t i) { v.x[i] = v.x[i] + a * pl[i]; });
+      [&](int64_t i) { v.x[i] = v.x[i] + a * v.p[i]; });
 }
 
 // ---- generic vector kernels ----
@@ -522,19 +504,17 @@ cudaError_t cg_init(const CGVecs<T>& v, CGState* st, double* partial, double rto
 }
 
 template <typename T> static bool aligned16(const CGVecs<T>& v) {
-  const void* ps[] = {v.x, v.r, v.p, v.w, v.dinv, v.p2};
+  const void* ps[] = {v.x, v.r, v.p, v.w, v.dinv};
   for (const void* p : ps)
     if (reinterpret_cast<uintptr_t>(p) % 16) return false;
   return true;
 }
 
 template <typename T>
-cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s,
-                           int parity) {
+cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cudaStream_t s) {
   if (!aligned16(v)) return cudaErrorMisalignedAddress;  // caught on the host, nothing launched
-  T* const pc = v.pcur(parity);
   if (!v.dotp) {  // the apply did not accumulate p.w: a separate pass into partial[2R, 3R)
-    cg_pw_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, pc, st, partial + 2 * RED_BLOCKS);
+    cg_pw_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial + 2 * RED_BLOCKS);
     CGVecs<T> u = v;
     u.dotp = partial + 2 * RED_BLOCKS;
     u.ndot = RED_BLOCKS;
@@ -543,15 +523,14 @@ cudaError_t cg_after_apply(const CGVecs<T>& v, CGState* st, double* partial, cud
     if (v.ndot <= 0) return cudaErrorInvalidValue;
     cg_update_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st, partial);
   }
-  cg_p_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, pc, v.pother(parity), st);
+  cg_p_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st);
   return cudaGetLastError();
 }
 
 template <typename T>
-cudaError_t cg_finish_x(const CGVecs<T>& v, const CGState* st, int parity, cudaStream_t s) {
-  if (!v.p2) return cudaSuccess;
+cudaError_t cg_finish_x(const CGVecs<T>& v, const CGState* st, cudaStream_t s) {
   if (!aligned16(v)) return cudaErrorMisalignedAddress;
-  cg_finish_x_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, v.pcur(parity), st);
+  cg_finish_x_kernel<T><<<RED_BLOCKS, RED_THREADS, 0, s>>>(v, st);
   return cudaGetLastError();
 }
 
@@ -560,11 +539,10 @@ template cudaError_t cg_init<double>(const CGVecs<double>&, CGState*, double*, d
 template cudaError_t cg_init<float>(const CGVecs<float>&, CGState*, double*, double, double,
                                     double, int, cudaStream_t);
 template cudaError_t cg_after_apply<double>(const CGVecs<double>&, CGState*, double*,
-                                            cudaStream_t, int);
-template cudaError_t cg_after_apply<float>(const CGVecs<float>&, CGState*, double*, cudaStream_t,
-                                           int);
-template cudaError_t cg_finish_x<double>(const CGVecs<double>&, const CGState*, int, cudaStream_t);
-template cudaError_t cg_finish_x<float>(const CGVecs<float>&, const CGState*, int, cudaStream_t);
+                                            cudaStream_t);
+template cudaError_t cg_after_apply<float>(const CGVecs<float>&, CGState*, double*, cudaStream_t);
+template cudaError_t cg_finish_x<double>(const CGVecs<double>&, const CGState*, cudaStream_t);
+template cudaError_t cg_finish_x<float>(const CGVecs<float>&, const CGState*, cudaStream_t);
 
 template <int K>
 static void launch_dots(const double* const* a, const double* const* b, int64_t n, double* partial,

@@ -246,15 +246,11 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
   while (batch < 64 && 2 * batch <= c->cg_last_its[kind & 7]) batch *= 2;
   bool first = true;
   *timeout = false;
-  // Batches are even (4 .. 64 iterations), so iteration b of a batch has the parity of
-  // the global iteration count (the direction buffer it applies the operator to).
   auto body = [&](int nb) {
     cudaError_t eb = cudaSuccess;
     for (int b = 0; b < nb && eb == cudaSuccess; b++) {
-      const int par = b & 1;
-      eb = apply(v.pcur(par), v.w, &c->d_cg->done, const_cast<double*>(v.dotp),
-                 v.p2 ? v.x : nullptr, v.pother(par), &c->d_cg->xalpha);
-      if (eb == cudaSuccess) eb = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream, par);
+      eb = apply(v.p, v.w, &c->d_cg->done, const_cast<double*>(v.dotp));
+      if (eb == cudaSuccess) eb = cg_after_apply<T>(v, c->d_cg, c->d_red, c->stream);
     }
     return eb;
   };
@@ -273,9 +269,8 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
     cudaGraphExec_t g = c->use_graphs ? cg_graph(c, kind, batch, [&] { return body(batch); }) : nullptr;
     e = g ? cudaGraphLaunch(g, c->stream) : body(batch);
   }
-  // fused mode: the step of the last iteration has not reached x yet
-  if (e == cudaSuccess && v.p2 && c->h_cg->its > 0)
-    e = cg_finish_x<T>(v, c->d_cg, (c->h_cg->its - 1) & 1, c->stream);
+  // the step of the iteration that stopped the solve has not reached x yet
+  if (e == cudaSuccess) e = cg_finish_x<T>(v, c->d_cg, c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "CG");
   *its = c->h_cg->its;
   *reason = c->h_cg->reason;
@@ -284,29 +279,19 @@ static int run_cg(vfgpu_ctx* c, int kind, const CGVecs<T>& v, Apply apply, doubl
 }
 
 // ---------------------------------------------------------------------------- U
-// dot: if non-null the apply also writes the block partials of x.y there (the CG's p.w);
-// xacc: if non-null the apply also does xacc += *xalpha xdir (the CG's fused solution
-// update, cg.cuh)
+// dot: if non-null the apply also writes the block partials of x.y there (the CG's p.w)
 static cudaError_t u_apply64(vfgpu_ctx* c, const double* x, double* y, const int* skip,
-                             double* dot = nullptr, double* xacc = nullptr,
-                             const double* xdir = nullptr, const double* xalpha = nullptr) {
+                             double* dot = nullptr) {
   UApplyArgs<double> A = u_args<double>(c, x, c->f[VFGPU_FIELD_V], y, c->seam64, c->plan64);
   A.skip = skip;
   A.dot = dot;
-  A.xacc = xacc;
-  A.xdir = xdir;
-  A.xalpha = xalpha;
   return launch_u_apply<double>(A, c->plan64, c->layers, c->stream);
 }
 static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* skip,
-                             double* dot = nullptr, float* xacc = nullptr,
-                             const float* xdir = nullptr, const double* xalpha = nullptr) {
+                             double* dot = nullptr) {
   UApplyArgs<float> A = u_args<float>(c, x, c->V32, y, c->seam32, c->plan32);
   A.skip = skip;
   A.dot = dot;
-  A.xacc = xacc;
-  A.xdir = xdir;
-  A.xalpha = xalpha;
   return launch_u_apply<float>(A, c->plan32, c->layers, c->stream);
 }
 static int dots_of(const vfgpu_ctx* c, const TilePlan& p) { return tile_dot_count(p, c->nx, c->ny, c->nz); }
@@ -393,13 +378,11 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   const double ttol = o.snes_rtol * fnorm;
   int reason = 0;
   if (fnorm < o.snes_atol) reason = 2;  // SNES_CONVERGED_FNORM_ABS
-  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot, double* xacc,
-                     const double* xdir, const double* xalpha) {
-    return u_apply64(c, x, y, skip, dot, xacc, xdir, xalpha);
+  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot) {
+    return u_apply64(c, x, y, skip, dot);
   };
-  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot, float* xacc,
-                     const float* xdir, const double* xalpha) {
-    return u_apply32(c, x, y, skip, dot, xacc, xdir, xalpha);
+  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot) {
+    return u_apply32(c, x, y, skip, dot);
   };
   // NOCOMPRESSION: F(X) = K(V; X) X - f(X) with the sign pattern of X (flags left at X)
   auto nc_residual = [&](const double* X, double* Fout) {
@@ -428,7 +411,6 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
       tmo = w.expired();
     } else if (!mixed) {
       CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), dots_of(c, c->plan64)};
-      v.p2 = JY;  // JY is free during the solve
       rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
@@ -449,7 +431,6 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         e = dev_to_f32(R, b32, n3, c->stream);
         if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
         CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3, dot_buf(c, 2), dots_of(c, c->plan32)};
-        v.p2 = b32 + pool_stride(n3);  // the second half of P (3N + slack doubles)
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
         rc = run_cg<float>(c, 2, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
@@ -550,25 +531,17 @@ namespace vfgpu {
 
 // ---------------------------------------------------------------------------- V
 static cudaError_t v_apply64(vfgpu_ctx* c, const double* x, double* y, const uint8_t* mask,
-                             const int* skip, double* dot = nullptr, double* xacc = nullptr,
-                             const double* xdir = nullptr, const double* xalpha = nullptr) {
+                             const int* skip, double* dot = nullptr) {
   VApplyArgs<double> A = v_args<double>(c, x, y, mask, c->vmap64, c->seam64, c->vplan64);
   A.skip = skip;
   A.dot = dot;
-  A.xacc = xacc;
-  A.xdir = xdir;
-  A.xalpha = xalpha;
   return launch_v_apply<double>(A, c->vplan64, c->layers, c->stream);
 }
 static cudaError_t v_apply32(vfgpu_ctx* c, const float* x, float* y, const uint8_t* mask,
-                             const int* skip, double* dot = nullptr, float* xacc = nullptr,
-                             const float* xdir = nullptr, const double* xalpha = nullptr) {
+                             const int* skip, double* dot = nullptr) {
   VApplyArgs<float> A = v_args<float>(c, x, y, mask, c->vmap32, c->seam32, c->vplan32);
   A.skip = skip;
   A.dot = dot;
-  A.xacc = xacc;
-  A.xdir = xdir;
-  A.xalpha = xalpha;
   return launch_v_apply<float>(A, c->vplan32, c->layers, c->stream);
 }
 
@@ -630,13 +603,11 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   const double ttol = o.snes_rtol * fnorm;
   int reason = 0;
   if (fnorm < o.snes_atol) reason = 2;
-  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot, double* xacc,
-                     const double* xdir, const double* xalpha) {
-    return v_apply64(c, x, y, mask, skip, dot, xacc, xdir, xalpha);
+  auto apply64 = [&](const double* x, double* y, const int* skip, double* dot) {
+    return v_apply64(c, x, y, mask, skip, dot);
   };
-  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot, float* xacc,
-                     const float* xdir, const double* xalpha) {
-    return v_apply32(c, x, y, mask, skip, dot, xacc, xdir, xalpha);
+  auto apply32 = [&](const float* x, float* y, const int* skip, double* dot) {
+    return v_apply32(c, x, y, mask, skip, dot);
   };
   for (int it = 0; !reason && it < o.snes_maxit; it++) {
     e = dev_v_mask(F, V, lb, ub, c->f[VFGPU_FIELD_VIRREV], c->bcV_kind, c->vf.irrevtol, at2, mask, N,
@@ -646,7 +617,6 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     bool tmo = false;
     if (!mixed) {
       CGVecs<double> v{Y, R, P, Wv, dinv, F, mask, N, dot_buf(c, 3), dots_of(c, c->vplan64)};
-      v.p2 = c->p64[5];  // not used by StepV otherwise
       rc = run_cg<double>(c, 3, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
@@ -665,7 +635,6 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         e = dev_to_f32(R, b32, N, c->stream);
         if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_v");
         CGVecs<float> v{x32, r32, pp32, w32, dinv32, b32, mask, N, dot_buf(c, 4), dots_of(c, c->vplan32)};
-        v.p2 = c->p32[4] + 2 * Na;  // after dinv32 and b32 in the 3N pool
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
         rc = run_cg<float>(c, 4, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,

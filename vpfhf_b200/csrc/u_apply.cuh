@@ -43,12 +43,6 @@ template <typename T> struct UApplyArgs {
   double* __restrict__ dot;           // if non-null: per-block partials of x.y (see tile_engine.cuh)
   const uint32_t* __restrict__ cflag; // NOCOMPRESSION: per cell, bit g = tr(eps(u0)) < 0 at Gauss
                                       // point g (u_element_nc); null = the plain operator
-  // CG with the solution update fused into the apply (see cg.cuh): if xacc is non-null,
-  // every finished node also does xacc += (T)*xalpha * xdir over its dofs (skipped when
-  // *xalpha == 0)
-  T* __restrict__ xacc;
-  const T* __restrict__ xdir;
-  const double* __restrict__ xalpha;
   int nx, ny, nz;
   int ntx, nty;                       // tiles in x, y
   T ihx, ihy, ihz, vol, eta;
