@@ -297,6 +297,7 @@ def run_gpu(args):
                     zip(names, am[key]["energies"][-1], am["fp64"]["energies"][-1])}
         return rel, rel_last, float(np.abs(vfin[key] - vfin["fp64"]).max())
     rel, rel_last, v_linf = versus_fp64("mixed")
+    vs_oracle = versus_oracle(am, vfin, n, args.am_steps)
     am_c1 = gpu_am_c1(vg, barrier)
 
     serving = run_serving(args) if args.serve_problems > 0 else None
@@ -376,6 +377,7 @@ def run_gpu(args):
                                    "mg_*: multigrid-preconditioned U solve, same stopping test",
                            "steps": args.am_steps,
                            "kspU_last": {k: am[k]["last_kspU"] for k in am},
+                           "vs_fp64_oracle": vs_oracle,
                            "c1_41": am_c1},
         "clocks": clocks,
     }
@@ -387,6 +389,25 @@ def run_gpu(args):
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def versus_oracle(am, vfin, n, its):
+    """Each AM variant against the CPU oracle's FP64 run of the same 10 iterations
+    (tests/golden/penny129.npz, made by tests/golden/make_penny129.py): the largest
+    relative difference of elastic energy, pressure work, surface energy and crack
+    opening over the iterations, and the V L-inf difference after the last one."""
+    path = os.path.join(ROOT, "tests", "golden", "penny129.npz")
+    if n != 129 or its != 10 or not os.path.exists(path):
+        return None
+    fx = np.load(path)
+    rec = fx["rec"][:, :4]
+    out = {}
+    for key in am:
+        e = np.array(am[key]["energies"])
+        out[key] = {"max_rel_energy_diff": float((np.abs(e - rec) / np.abs(rec)).max()),
+                    "v_linf": float(np.abs(vfin[key] - fx["V"]).max())}
+    out["reference"] = "CPU oracle (FP64 restatement of the reference's solves), 10 AM iterations"
+    return out
 
 
 def gpu_am_c1(vg, barrier, its=3):

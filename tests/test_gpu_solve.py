@@ -267,6 +267,40 @@ def test_penny41_am_loop(cuda, precision):
     ctx.close()
 
 
+@pytest.mark.parametrize("precision,pc", [("fp64", "jacobi"), ("mixed", "jacobi"), ("mixed", "mg")])
+def test_penny129_am_loop(cuda, precision, pc):
+    """The 129^3 pressurized penny crack (eps = 2h), 10 AM iterations -- the FP64-vs-mixed
+    workload of the benchmark -- against the FP64 oracle's run of the same iterations
+    (fixture tests/golden/penny129.npz): every iteration's elastic energy, pressure
+    work, surface energy and crack opening within 1e-6 relative, V L-inf <= 1e-4."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import vpfhf_b200 as vg
+    import vforacle as vo
+    from make_penny129 import PARAMS as P
+    fx = np.load(os.path.join(HERE, "golden", "penny129.npz"))
+    rec = fx["rec"]
+    n = P["n"]
+    ov = vo.Oracle(n, P["l"], E=P["E"], nu=P["nu"], Gc=P["Gc"], epsilon=P["epsilon"],
+                   eta=P["eta"], atnum=P["atnum"])
+    v0 = ov.penny_v(P["center"], P["r"])
+    ctx = vg.VFContext(n, P["l"], dict(E=P["E"], nu=P["nu"], Gc=P["Gc"]), epsilon=P["epsilon"],
+                       eta=P["eta"], atnum=P["atnum"], pressurize=True)
+    ctx.set_bc(vg.rollers())
+    ctx.set_field("V", v0)
+    ctx.set_field("pressure", np.full(ctx.N, P["p"]))
+    ctx.time_step_prepare()
+    for it in range(P["am_its"]):
+        rc, err, su, sv = ctx.am_step(dict(precision=precision, pc=pc))
+        assert rc == 0, (su, sv)
+        el, _, pw = ctx.u_energy()
+        s, cov = ctx.v_energy(), ctx.crack_opening()
+        for got, ref in zip((el, pw, s, cov), rec[it, :4]):
+            assert got == pytest.approx(ref, rel=1e-6), (it, got, ref)
+    assert np.abs(ctx.get_field("V") - fx["V"]).max() <= 1e-4
+    ctx.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_context_reuse_across_problems(cuda, precision):
     """A context reused for a second problem (new E, nu, Gc, epsilon, AT model; the captured
