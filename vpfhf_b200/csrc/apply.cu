@@ -14,6 +14,13 @@ namespace vfgpu {
 #define VFGPU_U64_TY 8
 #endif
 constexpr int U_TY = 8, U64_TY = VFGPU_U64_TY, V_TY = kVTileY;
+// Blocks per SM of the FP64 U operator: 1 (~250 registers, two corner-contribution
+// buffers) or, as a build option, 2 (128 registers: the row closed form of the
+// non-constant elements spills; one buffer and a second barrier per layer).
+#ifndef VFGPU_U64_MINB
+#define VFGPU_U64_MINB 1
+#endif
+constexpr int U64_MINB = VFGPU_U64_MINB;
 // V tiles carry 2 stages of 27 coefficients per cell in shared memory: 75 KB (FP32,
 // 2 CTAs per SM) or 150 KB (FP64, 1 CTA per SM).
 constexpr int V64_MINB = 1, V32_MINB = 2;
@@ -30,7 +37,10 @@ constexpr int V64_MINB = 1, V32_MINB = 2;
 #endif
 constexpr bool kU32Packed = VFGPU_U32_PACKED != 0;
 constexpr int U32_TY = kU32Packed ? VFGPU_U32_PACKED_TY : U_TY;
-constexpr int U32_MINB = kU32Packed ? (VFGPU_U32_PACKED_TY == 16 ? 1 : 2) : 2;
+#ifndef VFGPU_U32_MINB
+#define VFGPU_U32_MINB 2
+#endif
+constexpr int U32_MINB = kU32Packed ? (VFGPU_U32_PACKED_TY == 16 ? 1 : 2) : VFGPU_U32_MINB;
 using U32Op = std::conditional_t<kU32Packed, UOpF2, UOp<float>>;
 using U32OpC = std::conditional_t<kU32Packed, UOpF2, UOp<float, true>>;
 
@@ -40,8 +50,8 @@ template <typename T> bool cubic(const UApplyArgs<T>& A) { return A.ihx == A.ihy
 cudaError_t apply_kernel_attributes() {
   static std::mutex m;  // contexts may be created from several threads
   std::lock_guard<std::mutex> lk(m);
-  cudaError_t e = set_tile_attributes<UOp<double>, U64_TY, 1>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U64_TY, 1>();
+  cudaError_t e = set_tile_attributes<UOp<double>, U64_TY, U64_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U64_TY, U64_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U64_TY, 1>();
@@ -109,7 +119,7 @@ cudaError_t wait_selftest(long long cycles, int complete, int* timed_out) {
 }
 
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
-  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, 1, num_sms);
+  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, U64_MINB, num_sms);
   return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
 }
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
@@ -120,8 +130,8 @@ template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
   if (A.cflag) return launch_tile_apply<UOpNC<double>, U64_TY, 1>(A, p, L, s);
-  if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, 1>(A, p, L, s);
-  return launch_tile_apply<UOp<double>, U64_TY, 1>(A, p, L, s);
+  if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
+  return launch_tile_apply<UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
 }
 template <>
 cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,

@@ -55,10 +55,15 @@ template <int TY, int EPT = 1> struct Tile {
 };
 
 // Shared memory: a ring of 3 node planes [3][NIN][BY][BX] (planes k, k+1 in use,
-// k+2 in flight) and 2 buffers of element corner contributions [2][8*NC][TY][32].
-template <class Op, int TY> constexpr size_t tile_base_bytes() {
+// k+2 in flight) and SCS buffers of element corner contributions [SCS][8*NC][TY][32]:
+// two (layer k + 1's elements are written while layer k's node sums still read) where
+// MINB blocks of that size fit an SM, else one, with a second barrier per layer.
+template <class Op, int TY, int SCS = 2> constexpr size_t tile_base_bytes() {
   using T = typename Op::T;
-  return sizeof(T) * (3 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + 2 * 8 * Op::NC * 32 * TY);
+  return sizeof(T) * (3 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 8 * Op::NC * 32 * TY);
+}
+template <class Op, int TY, int MINB> constexpr int sc_stages() {
+  return (Op::CV > 0 || MINB * (tile_base_bytes<Op, TY, 2>() + 1024) <= 228 * 1024) ? 2 : 1;
 }
 // Per-cell value stages (Op::CV > 0): [kCellStages][CV][TY][32] at a 128-byte aligned
 // offset, then one 8-byte mbarrier per stage.
@@ -67,11 +72,11 @@ template <class Op, int TY> constexpr size_t cell_off() { return (tile_base_byte
 template <class Op, int TY> constexpr size_t cell_stage_bytes() {
   return sizeof(typename Op::T) * Op::CV * TY * 32;
 }
-template <class Op, int TY> constexpr size_t tile_smem_bytes() {
+template <class Op, int TY, int MINB> constexpr size_t tile_smem_bytes() {
   if constexpr (Op::CV > 0)
     return cell_off<Op, TY>() + kCellStages * cell_stage_bytes<Op, TY>() + kCellStages * 8;
   else
-    return tile_base_bytes<Op, TY>();
+    return tile_base_bytes<Op, TY, sc_stages<Op, TY, MINB>()>();
 }
 
 // mbarrier and tensor-copy primitives (one thread issues; every thread may wait).
@@ -152,7 +157,8 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   constexpr int NC = Op::NC, NIN = Op::NIN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sx = reinterpret_cast<T*>(smem_raw);  // [3 ring][NIN][BY][BX]
-  T* sc = sx + 3 * NIN * G::BY * G::BX;    // [2][8*NC][TY][32]
+  T* sc = sx + 3 * NIN * G::BY * G::BX;    // [SCS][8*NC][TY][32]
+  constexpr int SCS = sc_stages<Op, TY, MINB>();
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
   // This block's share of the work: node planes [U b / n, U (b + 1) / n) of the
@@ -247,7 +253,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
   [[maybe_unused]] bool gave_up = false;
   for (int k = kf; k <= kl; k++) {
-    const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = (k - kf) & 1;
+    const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = SCS == 2 ? (k - kf) & 1 : 0;
     const int ex = X0 + lane;
     if constexpr (EPT == 1) {
       const int ey = Y0 + wy;
@@ -377,6 +383,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
 #pragma unroll
       for (int c = 0; c < NC; c++) carry[si][c] = p1[c];
     }
+    if constexpr (SCS == 1) __syncthreads();  // the next layer rewrites the one buffer
   }
   if (z1 == nz) {
 #pragma unroll
@@ -504,7 +511,7 @@ template <class Op, int TY, int MINB> cudaError_t set_tile_attributes() {
   if (e != cudaSuccess) return e;
   const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
   if (g_tile_attr_set<Op, TY, MINB>.load(std::memory_order_acquire) & bit) return cudaSuccess;
-  const int smem = (int)tile_smem_bytes<Op, TY>();
+  const int smem = (int)tile_smem_bytes<Op, TY, MINB>();
   e = cudaFuncSetAttribute(tile_apply_kernel<Op, TY, MINB, false>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e == cudaSuccess)
@@ -519,7 +526,7 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
                               cudaStream_t s) {
   A.ntx = p.ntx;
   A.nty = p.nty;
-  constexpr size_t smem = tile_smem_bytes<Op, TY>();
+  constexpr size_t smem = tile_smem_bytes<Op, TY, MINB>();
   cudaError_t ea = set_tile_attributes<Op, TY, MINB>();
   if (ea != cudaSuccess) return ea;
   dim3 grid(p.ncta), block(32, TY / Op::EPT);
