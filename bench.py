@@ -313,10 +313,11 @@ def run_gpu(args):
     nodes, cells = ctx.N, (n - 1) ** 3
     # algorithmic traffic per apply: read u (24 B) + v (8 B), write y (24 B) per node
     alg_bytes = 56.0 * nodes
-    # FP64 instructions per element of the modal apply, counted by ncu on this workload
+    # FP64 instructions per element of the apply on this workload (nearly every element
+    # has a constant nodal phase field and takes the fixed-weight element), counted by ncu
     # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells:
-    # profiles/u_apply_fp64_129_instructions.md); an FMA is 2 flops
-    dfma_el, dadd_el, dmul_el = 310.4, 405.6, 208.9
+    # profiles/u_apply_fp64_129.md); an FMA is 2 flops
+    dfma_el, dadd_el, dmul_el = 44.7, 163.1, 26.5
     instr_el = dfma_el + dadd_el + dmul_el
     flops_el = 2 * dfma_el + dadd_el + dmul_el
     f64_peak = fp_peak_tflops(torch, "f64")
@@ -342,10 +343,12 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (ms64 * 1e-3) / 1e9, 1),
                      "peak": hbm, "unit": "GB/s",
                      "frac": round(alg_bytes / (ms64 * 1e-3) / 1e9 / hbm, 4),
-                     "traffic": 95.3e6 if n == N_EDGE else None,
-                     "note": "FP64-pipe-bound operator (see compute_roofline); traffic: ncu "
-                             "dram read+write per launch at 129^3 (74.0 + 21.3 MB; part of the "
-                             "51.5 MB output is still in the 126 MB L2 when the launch ends)"},
+                     "traffic": 114.0e6 if n == N_EDGE else None,
+                     "note": "traffic: ncu dram read+write per launch at 129^3 (86.4 + 27.6 MB; "
+                             "part of the 51.5 MB output is still in the 126 MB L2 when the "
+                             "launch ends); the kernel is bound by neither HBM nor the FP64 pipe "
+                             "(compute_roofline) but by the latency of its tile schedule at 8 "
+                             "warps per SM (profiles/u_apply_fp64_129.md)"},
         "compute_roofline": {
             "pipe": "fp64 CUDA cores",
             "fp64_instructions_per_element": {"dfma": dfma_el, "dadd": dadd_el, "dmul": dmul_el},
