@@ -482,6 +482,30 @@ def _am_run(ctx, prob, prec, its, altmintol=0.0, reset=True, pc="jacobi"):
     return recs
 
 
+def c3_run(ctx, prob, prec, pc, args):
+    """The quasi-static poroelastic run: pressure scaled k / load_steps for k = 1 ..
+    load_steps, each step AM to ||V - Vold||_inf < 1e-3 (at most max_am iterations),
+    from U = 0 and the initial cracks.  A progress line per step goes to stderr."""
+    ctx.set_field("U", np.zeros(3 * ctx.N))
+    ctx.init_cracks(prob["pennies"])
+    pfull = prob["pressure"]
+    steps, am_total, t_total = [], 0, 0.0
+    for k in range(1, args.load_steps + 1):
+        ctx.set_field("pressure", pfull * (k / args.load_steps))
+        ctx.time_step_prepare()
+        recs = _am_run(ctx, prob, prec, args.max_am, altmintol=1e-3, reset=False, pc=pc)
+        am_total += len(recs)
+        t_total += sum(r["s"] for r in recs)
+        steps.append(dict(step=k, am_its=len(recs), last_err=recs[-1]["err"],
+                          s=round(sum(r["s"] for r in recs), 3),
+                          kspU=[r["kspU"] for r in recs], kspV=[r["kspV"] for r in recs],
+                          **_energies(ctx)))
+        print(json.dumps({"c3_progress": prec, **steps[-1]}), file=sys.stderr, flush=True)
+    return (dict(am_steps=am_total, solve_s=round(t_total, 2),
+                 am_steps_per_s=round(am_total / t_total, 4), steps=steps),
+            ctx.get_field("V"))
+
+
 def _energies(ctx):
     el, _, pw = ctx.u_energy()
     return dict(elastic=el, pressure_work=pw, surface=ctx.v_energy(), cov=ctx.crack_opening())
@@ -490,7 +514,8 @@ def _energies(ctx):
 def run_large(args):
     """The large single-GPU set-ups: `c5` (321^3, heterogeneous E, 8 cracks, 10 AM
     iterations, FP64 and mixed from the same start) and `c3` (257x257x129 poroelastic,
-    16 cracks, 20 quasi-static pressure steps in mixed precision, AM to 1e-3)."""
+    16 cracks, 20 quasi-static pressure steps, AM to 1e-3 or at most --max-am iterations
+    per step, FP64 and mixed)."""
     import torch
     import vpfhf_b200 as vg
     from vpfhf_b200 import workloads as wl
@@ -530,22 +555,19 @@ def run_large(args):
                                for k in res if k != "fp64"},
             **res})
     else:
-        pfull = prob["pressure"]
-        steps, am_total, t_total = [], 0, 0.0
-        for k in range(1, args.load_steps + 1):
-            ctx.set_field("pressure", pfull * (k / args.load_steps))
-            ctx.time_step_prepare()
-            recs = _am_run(ctx, prob, "mixed", args.max_am, altmintol=1e-3, reset=False,
-                           pc="jacobi" if args.pc == "both" else args.pc)
-            am_total += len(recs)
-            t_total += sum(r["s"] for r in recs)
-            steps.append(dict(step=k, am_its=len(recs), last_err=recs[-1]["err"],
-                              s=round(sum(r["s"] for r in recs), 3), **_energies(ctx)))
-        out.update({"precision": "mixed", "pc": "jacobi" if args.pc == "both" else args.pc,
-                    "load_steps": args.load_steps, "altmintol": 1e-3,
-                    "max_am_per_step": args.max_am, "am_steps": am_total,
-                    "am_steps_per_s": round(am_total / t_total, 4), "solve_s": round(t_total, 2),
-                    "steps": steps})
+        pc = "mg" if args.pc == "both" else args.pc
+        runs, fields = {}, {}
+        for prec in ("fp64", "mixed"):
+            runs[prec], fields[prec] = c3_run(ctx, prob, prec, pc, args)
+        ekeys = ("elastic", "pressure_work", "surface", "cov")
+        last = {p: runs[p]["steps"][-1] for p in runs}
+        out.update({"pc": pc, "load_steps": args.load_steps, "altmintol": 1e-3,
+                    "max_am_per_step": args.max_am,
+                    "am_steps_per_s": {p: runs[p]["am_steps_per_s"] for p in runs},
+                    "mixed_vs_fp64_rel_at_last_step": {
+                        e: abs(last["mixed"][e] - last["fp64"][e]) / abs(last["fp64"][e]) for e in ekeys},
+                    "mixed_vs_fp64_v_linf": float(np.abs(fields["mixed"] - fields["fp64"]).max()),
+                    **runs})
     ctx.close()
     if rank == 0:
         print(json.dumps(out))
@@ -664,9 +686,9 @@ def main():
     ap.add_argument("--load-steps", type=int, default=20, help="c3 quasi-static steps")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="c3 / c5: cells per axis scaled by this factor (1 = the full set-up)")
-    ap.add_argument("--max-am", type=int, default=25, help="c3 AM cap per load step")
+    ap.add_argument("--max-am", type=int, default=5, help="c3 AM cap per load step")
     ap.add_argument("--pc", default="both", choices=["jacobi", "mg", "both"],
-                    help="U preconditioner of the c3 / c5 runs (c3: both = jacobi)")
+                    help="U preconditioner of the c3 / c5 runs (c3: both = mg)")
     ap.add_argument("--only-am", action="store_true",
                     help="run the AM steps only, with a per-solve breakdown; the last step of "
                          "--profile-precision is bracketed by cudaProfilerStart/Stop")
