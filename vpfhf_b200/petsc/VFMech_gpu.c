@@ -144,7 +144,8 @@ static void solve_opts(vfgpu_solve_opts *o) {
   PetscOptionsGetInt(NULL, NULL, "-vfgpu_precision", &prec, &flg);
   o->precision = (int)prec;
   /* -vfgpu_pc 0 (Jacobi, the reference's KSPCG+Jacobi, default) | 1 (multigrid V-cycle;
-     same stopping test; needs an even cell count per axis) */
+     same stopping test; needs >= 9 nodes along some axis) | 2 (multigrid on grids with
+     >= 65 nodes along some axis, Jacobi below) */
   PetscOptionsGetInt(NULL, NULL, "-vfgpu_pc", &pc, &flg);
   o->pc = (int)pc;
 }
