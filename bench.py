@@ -490,7 +490,7 @@ def c3_run(ctx, prob, prec, pc, args):
     ctx.init_cracks(prob["pennies"])
     pfull = prob["pressure"]
     steps, am_total, t_total = [], 0, 0.0
-    for k in range(1, args.load_steps + 1):
+    for k in range(1, min(args.load_steps, args.c3_steps or args.load_steps) + 1):
         ctx.set_field("pressure", pfull * (k / args.load_steps))
         ctx.time_step_prepare()
         recs = _am_run(ctx, prob, prec, args.max_am, altmintol=1e-3, reset=False, pc=pc)
@@ -561,7 +561,8 @@ def run_large(args):
             runs[prec], fields[prec] = c3_run(ctx, prob, prec, pc, args)
         ekeys = ("elastic", "pressure_work", "surface", "cov")
         last = {p: runs[p]["steps"][-1] for p in runs}
-        out.update({"pc": pc, "load_steps": args.load_steps, "altmintol": 1e-3,
+        out.update({"pc": pc, "load_steps": args.load_steps,
+                    "steps_run": len(runs["fp64"]["steps"]), "altmintol": 1e-3,
                     "max_am_per_step": args.max_am,
                     "am_steps_per_s": {p: runs[p]["am_steps_per_s"] for p in runs},
                     "mixed_vs_fp64_rel_at_last_step": {
@@ -687,6 +688,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0,
                     help="c3 / c5: cells per axis scaled by this factor (1 = the full set-up)")
     ap.add_argument("--max-am", type=int, default=5, help="c3 AM cap per load step")
+    ap.add_argument("--c3-steps", type=int, default=0,
+                    help="c3: run only the first this many of the --load-steps steps (0 = all)")
     ap.add_argument("--pc", default="both", choices=["jacobi", "mg", "both"],
                     help="U preconditioner of the c3 / c5 runs (c3: both = mg)")
     ap.add_argument("--only-am", action="store_true",
