@@ -65,19 +65,33 @@ template <typename T_, bool CUBIC = false> struct UOp {
     else
       u_element<T, CUBIC>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
-  // Writes y of node n (Dirichlet rows: y = x); with DOT, returns x.y over its dofs
-  // (the launch accumulates the CG dot into A.dot).
+  // The per-node flags finish_node needs (Dirichlet bits), loaded ahead by the tiles.
+  __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
+    return A.bc ? A.bc[n] : 0u;
+  }
+  // Writes y of node n (Dirichlet rows: y = x) from the node's flags b and input
+  // values xin; with DOT, returns x.y over its dofs (the launch accumulates the CG dot
+  // into A.dot).
   template <bool DOT>
-  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
-    const unsigned b = A.bc ? A.bc[n] : 0u;
+  __device__ __forceinline__ static double finish_node_in(const Args& A, int64_t n, const T (&val)[NC],
+                                                          unsigned b, const T (&xin)[NC]) {
     double d = 0.;
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-      const T y = ((b >> c) & 1u) ? A.x[3 * n + c] : val[c];
+      const T y = ((b >> c) & 1u) ? xin[c] : val[c];
       A.y[3 * n + c] = y;
-      if constexpr (DOT) d += (double)A.x[3 * n + c] * (double)y;
+      if constexpr (DOT) d += (double)xin[c] * (double)y;
     }
     return d;
+  }
+  // The same with the flags and inputs read from global memory (the seam fix-up).
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    const unsigned b = node_flags(A, n);
+    T xin[NC];
+#pragma unroll
+    for (int c = 0; c < 3; c++) xin[c] = (DOT || ((b >> c) & 1u)) ? A.x[3 * n + c] : T(0);
+    return finish_node_in<DOT>(A, n, val, b, xin);
   }
 };
 
@@ -115,6 +129,14 @@ template <typename T_> struct UOpNC {
       mu = T(LT.mu[layer]);
     }
     u_element_nc<T>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, A.cflag[cell], out);
+  }
+  __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
+    return UOp<T>::node_flags(A, n);
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node_in(const Args& A, int64_t n, const T (&val)[NC],
+                                                          unsigned b, const T (&xin)[NC]) {
+    return UOp<T>::template finish_node_in<DOT>(A, n, val, b, xin);
   }
   template <bool DOT>
   __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
@@ -167,6 +189,14 @@ struct UOpF2 {
         out[0][a][c] = ok[0] ? y[a][c].v.x : 0.f;
         out[1][a][c] = ok[1] ? y[a][c].v.y : 0.f;
       }
+  }
+  __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
+    return UOp<float>::node_flags(A, n);
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node_in(const Args& A, int64_t n, const T (&val)[NC],
+                                                          unsigned b, const T (&xin)[NC]) {
+    return UOp<float>::finish_node_in<DOT>(A, n, val, b, xin);
   }
   template <bool DOT>
   __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
@@ -313,12 +343,21 @@ template <typename T_> struct VOp {
 #pragma unroll
     for (int a = 0; a < 8; a++) out[a][0] = yn[a];
   }
+  __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
+    return A.mask ? A.mask[n] : 0u;
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node_in(const Args& A, int64_t n, const T (&val)[NC],
+                                                          unsigned m, const T (&xin)[NC]) {
+    const T y = m ? T(0) : val[0];
+    A.y[n] = y;
+    if constexpr (DOT) return (double)xin[0] * (double)y;
+    return 0.;
+  }
   template <bool DOT>
   __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
-    const T y = (A.mask && A.mask[n]) ? T(0) : val[0];
-    A.y[n] = y;
-    if constexpr (DOT) return (double)A.x[n] * (double)y;
-    return 0.;
+    const T xin[NC] = {DOT ? A.x[n] : T(0)};
+    return finish_node_in<DOT>(A, n, val, node_flags(A, n), xin);
   }
 };
 

@@ -6,7 +6,7 @@
 // taken column by column (all planes of tile 0, then tile 1, ...), are shared evenly
 // by one wave of blocks: block b takes units [U b / n, U (b + 1) / n), cut at column
 // ends into segments.  A segment marches up its planes: per element layer, node
-// planes of the tile's 33 x (TY+1) node box stream through a 3-slot shared-memory
+// planes of the tile's 33 x (TY+1) node box stream through a 4-slot shared-memory
 // ring by asynchronous copies (cp.async, two planes ahead), each thread computes its
 // element's 8 x NC corner contributions (Op::element), those go to shared memory,
 // and node-owner threads sum the (up to 4) xy-contributions in a fixed order; the
@@ -25,7 +25,9 @@
 //   element_multi(A, L, ex, ey[EPT], ez, ok[EPT], in[EPT][8][NIN], out[EPT][8][NC])
 //   (EPT > 1; out[e] must be 0 where ok[e] is false),
 //   finish_node<DOT>(A, n, val[NC]) (writes y, applying Dirichlet rows / masks; with
-//   DOT returns the node's x.y), and an
+//   DOT returns the node's x.y), node_flags(A, n) and finish_node_in<DOT>(A, n, val,
+//   flags, xin[NC]) (the same from flags loaded ahead and the node's inputs from the
+//   plane ring), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
 //   so that a queued batch of iterations costs nothing once it is done).
 // An Op with CV > 0 per-cell values (the V operator's 27 Gauss-point coefficients)
@@ -54,13 +56,16 @@ template <int TY, int EPT = 1> struct Tile {
   static constexpr int NSLOT = (BX * BY + NT - 1) / NT;
 };
 
-// Shared memory: a ring of 3 node planes [3][NIN][BY][BX] (planes k, k+1 in use,
-// k+2 in flight) and SCS buffers of element corner contributions [SCS][8*NC][TY][32]:
+// Shared memory: a ring of 4 node planes [4][NIN][BY][BX] (during layer k: planes k,
+// k+1 read by the elements, plane k read by the node finish after the layer barrier,
+// plane k+2 landing, plane k+3 in flight into the slot plane k-1 left) and SCS buffers
+// of element corner contributions [SCS][8*NC][TY][32]:
 // two (layer k + 1's elements are written while layer k's node sums still read) where
 // MINB blocks of that size fit an SM, else one, with a second barrier per layer.
+constexpr int kRing = 4;
 template <class Op, int TY, int SCS = 2> constexpr size_t tile_base_bytes() {
   using T = typename Op::T;
-  return sizeof(T) * (3 * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 8 * Op::NC * 32 * TY);
+  return sizeof(T) * (kRing * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 8 * Op::NC * 32 * TY);
 }
 template <class Op, int TY, int MINB> constexpr int sc_stages() {
   return (Op::CV > 0 || MINB * (tile_base_bytes<Op, TY, 2>() + 1024) <= 228 * 1024) ? 2 : 1;
@@ -156,8 +161,8 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   constexpr int EPT = Op::EPT;
   constexpr int NC = Op::NC, NIN = Op::NIN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sx = reinterpret_cast<T*>(smem_raw);  // [3 ring][NIN][BY][BX]
-  T* sc = sx + 3 * NIN * G::BY * G::BX;    // [SCS][8*NC][TY][32]
+  T* sx = reinterpret_cast<T*>(smem_raw);  // [kRing][NIN][BY][BX]
+  T* sc = sx + kRing * NIN * G::BY * G::BX;  // [SCS][8*NC][TY][32]
   constexpr int SCS = sc_stages<Op, TY, MINB>();
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
@@ -202,11 +207,15 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     cp_async_commit();
   };
 
-  auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC]) {
+  // fl: the node's flags (loaded ahead), buf: the ring slot holding plane z
+  auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC], unsigned fl, int buf) {
     const bool left = (l == 0 && bx > 0), right = (l == 32 && bx < A.ntx - 1);
     const bool bot = (w == 0 && by > 0), top = (w == TY && by < A.nty - 1);
     if (!(left || right || bot || top)) {
-      dacc += Op::template finish_node<DOT>(A, node_index(X, Y, z, nx, ny), val);
+      T xin[NC];
+#pragma unroll
+      for (int c = 0; c < NC; c++) xin[c] = SXA(buf, c, w, l);
+      dacc += Op::template finish_node_in<DOT>(A, node_index(X, Y, z, nx, ny), val, fl, xin);
     } else if (left || right) {
       const int i = left ? bx : bx + 1;
       const int slot = (bot ? 2 : 0) + (left ? 1 : 0);
@@ -253,7 +262,16 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
   [[maybe_unused]] bool gave_up = false;
   for (int k = kf; k <= kl; k++) {
-    const int r0 = (k - kf) % 3, r1 = (k - kf + 1) % 3, sb = SCS == 2 ? (k - kf) & 1 : 0;
+    const int r0 = (k - kf) % kRing, r1 = (k - kf + 1) % kRing, sb = SCS == 2 ? (k - kf) & 1 : 0;
+    // the flags of the nodes this thread finishes after the layer (plane k), loaded now
+    // so that the finish does not wait for them
+    unsigned nfl[G::NSLOT];
+#pragma unroll
+    for (int si = 0; si < G::NSLOT; si++) {
+      const int s = tid + si * G::NT, l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
+      nfl[si] = (k >= z0 && s < G::BX * G::BY && X < nx && Y < ny)
+                    ? Op::node_flags(A, node_index(X, Y, k, nx, ny)) : 0u;
+    }
     const int ex = X0 + lane;
     if constexpr (EPT == 1) {
       const int ey = Y0 + wy;
@@ -347,7 +365,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     } else {
       __syncthreads();    // ... and everyone's; corner contributions of layer k visible
     }
-    if (k + 3 <= kl + 1) fetch_plane(r0, k + 3);  // plane k is no longer read
+    if (k + 3 <= kl + 1) fetch_plane((k + 3 - kf) % kRing, k + 3);  // the slot of plane k - 1
     if constexpr (Op::CV > 0)  // layer k's stage is no longer read
       if (tid == 0 && k + kCellStages <= kl) fetch_cells((k - kf) % kCellStages, k + kCellStages);
 #pragma unroll
@@ -378,7 +396,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
         T val[NC];
 #pragma unroll
         for (int c = 0; c < NC; c++) val[c] = carry[si][c] + p0[c];
-        emit(l, w, X, Y, k, val);
+        emit(l, w, X, Y, k, val, nfl[si], r0);
       }
 #pragma unroll
       for (int c = 0; c < NC; c++) carry[si][c] = p1[c];
@@ -392,7 +410,8 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       if (s >= G::BX * G::BY) continue;
       const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
       if (X >= nx || Y >= ny) continue;
-      emit(l, w, X, Y, nz - 1, carry[si]);
+      emit(l, w, X, Y, nz - 1, carry[si], Op::node_flags(A, node_index(X, Y, nz - 1, nx, ny)),
+           (nz - 1 - kf) % kRing);
     }
   }
   return true;
