@@ -211,8 +211,16 @@ __device__ __forceinline__ void node_butterfly(const T (&w)[8], int c, T (&y)[8]
 // On cubic cells (CUBIC) every 1/(4h) factor is the same, so they all fold into W
 // (W = Wr/(1024 h^2)); otherwise the gradient columns and the node values carry
 // their own ih_d/4.  All the dropped halvings are powers of two: exact.
+// VFGPU_U_GENERAL_NOINLINE (build option): the row closed form as a called function
+// rather than inlined, so that a kernel capped at fewer registers than it needs spills
+// only inside it (the fixed-weight element of the intact bulk stays spill-free).
+#ifdef VFGPU_U_GENERAL_NOINLINE
+#define VFGPU_U_GENERAL_INLINE __noinline__
+#else
+#define VFGPU_U_GENERAL_INLINE __forceinline__
+#endif
 template <typename T, bool CUBIC = false>
-__device__ __forceinline__ void u_element(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
+__device__ VFGPU_U_GENERAL_INLINE void u_element(const T (&xn)[8][3], const T (&vn)[8], T lam, T mu,
                                           T eta, T ihx, T ihy, T ihz, T vol, T (&y)[8][3]) {
   T m[3][8], mv[8];
 #pragma unroll
