@@ -565,8 +565,9 @@ def run_large(args):
                     "steps_run": len(runs["fp64"]["steps"]), "altmintol": 1e-3,
                     "max_am_per_step": args.max_am,
                     "am_steps_per_s": {p: runs[p]["am_steps_per_s"] for p in runs},
-                    "mixed_vs_fp64_rel_at_last_step": {
-                        e: abs(last["mixed"][e] - last["fp64"][e]) / abs(last["fp64"][e]) for e in ekeys},
+                    "mixed_vs_fp64_rel_at_last_step": {  # absolute where the FP64 value is 0
+                        e: abs(last["mixed"][e] - last["fp64"][e]) / (abs(last["fp64"][e]) or 1.0)
+                        for e in ekeys},
                     "mixed_vs_fp64_v_linf": float(np.abs(fields["mixed"] - fields["fp64"]).max()),
                     **runs})
     ctx.close()
