@@ -315,8 +315,8 @@ def run_gpu(args):
     alg_bytes = 56.0 * nodes
     # FP64 instructions per element of the apply on this workload (nearly every element
     # has a constant nodal phase field and takes the fixed-weight element), counted by ncu
-    # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells:
-    # profiles/u_apply_fp64_129.md); an FMA is 2 flops
+    # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells, one launch
+    # of this workload under ncu --set full); an FMA is 2 flops
     dfma_el, dadd_el, dmul_el = 44.7, 163.1, 26.5
     instr_el = dfma_el + dadd_el + dmul_el
     flops_el = 2 * dfma_el + dadd_el + dmul_el
@@ -348,7 +348,8 @@ def run_gpu(args):
                              "part of the 51.5 MB output is still in the 126 MB L2 when the "
                              "launch ends); the kernel is bound by neither HBM nor the FP64 pipe "
                              "(compute_roofline) but by the latency of its tile schedule at 8 "
-                             "warps per SM (profiles/u_apply_fp64_129.md)"},
+                             "warps per SM (ncu: FP64 pipe 23 %, top stalls fixed-latency "
+                             "dependencies, plane loads, the layer barrier)"},
         "compute_roofline": {
             "pipe": "fp64 CUDA cores",
             "fp64_instructions_per_element": {"dfma": dfma_el, "dadd": dadd_el, "dmul": dmul_el},
