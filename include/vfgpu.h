@@ -372,8 +372,8 @@ int vfgpu_u_apply_noalloc(const vfgpu_grid* grid, const vfgpu_matprop* mp, doubl
  * pointwise degradation v^2 + eta and Lame factors on the CUDA cores.  Element results
  * are summed with atomics (not bit-reproducible); Dirichlet rows y = x.  A measured
  * alternative to vfgpu_u_apply_dev's CUDA-core element, not used by the solvers;
- * UNILATERAL_NONE only.  Queued on the ctx stream; vfgpu_tc_error reports whether a
- * bounded wait inside it gave up (its results are then void). */
+ * UNILATERAL_NONE only.  Queued on the ctx stream; vfgpu_tc_error (synchronous) reports
+ * whether a bounded wait inside the last call gave up (its results are then void). */
 int vfgpu_u_apply_tc(vfgpu_ctx* ctx, const float* x, float* y);
 int vfgpu_tc_error(vfgpu_ctx* ctx, int* flagged);
 /* Host only: the two constant matrices of vfgpu_u_apply_tc for an hx x hy x hz cell,

@@ -491,6 +491,7 @@ extern "C" int vfgpu_u_apply_tc(vfgpu_ctx* c, const float* x, float* y) {
   const int grid = (int)std::min<long long>(A.ntiles, nsm);
   const int64_t n3 = 3 * (int64_t)c->N;
   e = cudaMemsetAsync(y, 0, n3 * sizeof(float), c->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_tcerr, 0, sizeof(unsigned), c->stream);  // this call's flag
   if (e == cudaSuccess) {
     tc_u_apply_kernel<<<grid, 128, TC_SMEM, c->stream>>>(A);
     e = cudaGetLastError();
