@@ -52,7 +52,7 @@ struct vfgpu_ctx {
   // scratch
   vfgpu::TilePlan plan64{}, plan32{}, vplan64{}, vplan32{};
   double* d_dot = nullptr;   // block partials of the CG's p.w written by the operator applies
-  double* seam64 = nullptr;  // U seams FP64 (V seams use the same buffer: they are smaller)
+  double* seam64 = nullptr;  // U and V seams FP64 (sized for the larger of the two plans)
   float* seam32 = nullptr;
   double *t64a = nullptr, *t64b = nullptr;
   float *t32a = nullptr, *t32b = nullptr;

@@ -806,10 +806,12 @@ int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
   const long long N = (long long)g->nx * g->ny * g->nz;
   const long long NC = (long long)(g->nx - 1) * (g->ny - 1) * (g->nz - 1);
   const TilePlan p64 = u_plan(g->nx, g->ny, g->nz, 8, 148), p32 = u_plan(g->nx, g->ny, g->nz, 4, 148);
+  const TilePlan q64 = v_plan(g->nx, g->ny, g->nz, 8, 148), q32 = v_plan(g->nx, g->ny, g->nz, 4, 148);
   long long b = 0;
   b += (2 * 3 * N + 5 * N) * 8;                          // fields U, BCU, V, VIrrev, theta, thetaRef, p
   b += N * 4 + (g->nz - 1) + 3 * N + 3 * N;              // V32, layers, BC kinds and bits
-  b += (long long)(p64.seamX + p64.seamY) * 8 + (long long)(p32.seamX + p32.seamY) * 4;
+  b += (long long)std::max(p64.seamX + p64.seamY, q64.seamX + q64.seamY) * 8 +
+       (long long)std::max(p32.seamX + p32.seamY, q32.seamX + q32.seamY) * 4;
   b += 3 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
   b += vfgpu_ctx::NP64 * (3 * N + kPoolSlack) * 8 + vfgpu_ctx::NP32 * (3 * N + kPoolSlack) * 4;
   b += vcoef_size(g->nx - 1, g->ny - 1, g->nz - 1) * 12 + N;  // V coefficient (FP64 + FP32), mask

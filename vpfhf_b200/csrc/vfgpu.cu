@@ -5,6 +5,8 @@
 #include <cstdio>
 #include <cstring>
 
+#include <algorithm>
+
 #include "abi_util.h"
 #include "ctx.h"
 #include "vec.h"
@@ -241,8 +243,12 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   ALLOC(c->bcU_bits, c->N);
   ALLOC(c->bcV_kind, c->N);
   ALLOC(c->bcV_bits, c->N);
-  ALLOC(c->seam64, std::max<size_t>(1, c->plan64.seamX + c->plan64.seamY) * sizeof(double));
-  ALLOC(c->seam32, std::max<size_t>(1, c->plan32.seamX + c->plan32.seamY) * sizeof(float));
+  // one seam buffer per precision serves the U and the V operator: the larger of the two
+  // (the U operator's unless a build gives it taller tiles than the V operator's)
+  ALLOC(c->seam64, std::max({(size_t)1, c->plan64.seamX + c->plan64.seamY,
+                             c->vplan64.seamX + c->vplan64.seamY}) * sizeof(double));
+  ALLOC(c->seam32, std::max({(size_t)1, c->plan32.seamX + c->plan32.seamY,
+                             c->vplan32.seamX + c->vplan32.seamY}) * sizeof(float));
   ALLOC(c->t64a, 3 * c->N * sizeof(double));
   ALLOC(c->t64b, 3 * c->N * sizeof(double));
   ALLOC(c->t32a, 3 * c->N * sizeof(float));
