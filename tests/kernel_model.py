@@ -336,9 +336,71 @@ def segments(ntx, nty, nz, ncta, b):
     return out
 
 
-def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, ncta=None):
+def tile_layer_const(v, n, TY):
+    """u_classify_kernel: cls[col, k] for tile col = by ntx + bx and element layer k, True
+    when the tile's elements (32 x TY, clipped to the grid) in layer k all have 8 equal
+    nodal v."""
+    nx, ny, nz = n
+    vv = v.reshape(nz, ny, nx)
+    corners = [vv[kk:nz - 1 + kk, j:ny - 1 + j, i:nx - 1 + i] for kk in (0, 1) for j in (0, 1) for i in (0, 1)]
+    const = np.all([c == corners[0] for c in corners[1:]], axis=0)  # [nez, ney, nex]
+    ntx, nty = -(-(nx - 1) // 32), -(-(ny - 1) // TY)
+    cls = np.zeros((ntx * nty, nz - 1), bool)
+    for by in range(nty):
+        for bx in range(ntx):
+            blk = const[:, by * TY:(by + 1) * TY, bx * 32:(bx + 1) * 32]
+            cls[by * ntx + bx] = blk.reshape(nz - 1, -1).all(axis=1)
+    return cls
+
+
+def unit_lists(cls, nz, ncta):
+    """unit_lists_kernel: per list l (0: both adjacent element layers constant, 1: the
+    rest) the runs (col, z0, z1, units before) in column order, the block starts (the run
+    holding unit total b / ncta) and the unit totals."""
+    runs, nez = [[], []], nz - 1
+
+    def utype(f, z):
+        below = z == 0 or f[z - 1]
+        above = z == nez or f[z]
+        return 0 if below and above else 1
+
+    tot = [0, 0]
+    for c, f in enumerate(cls):
+        z0, t0 = 0, utype(f, 0)
+        for z in range(1, nz + 1):
+            t = utype(f, z) if z < nz else -1
+            if t != t0:
+                runs[t0].append((c, z0, z, tot[t0]))
+                tot[t0] += z - z0
+                z0, t0 = z, t
+    start = [[0] * ncta, [0] * ncta]
+    for l in (0, 1):
+        for b in range(ncta):
+            ub = tot[l] * b // ncta
+            cand = [i for i, r in enumerate(runs[l]) if r[3] <= ub]
+            start[l][b] = cand[-1] if cand else 0
+    return runs, start, tot
+
+
+def list_segments(runs, start, total, ncta, b, ntx):
+    """Block b's (bx, by, z0, z1) segments of one unit list (tile_apply_kernel, list
+    mode)."""
+    u, u1 = total * b // ncta, total * (b + 1) // ncta
+    r, out = start[b], []
+    while u < u1:
+        col, rz0, rz1, w = runs[r]
+        r += 1
+        z0, z1 = rz0 + (u - w), min(rz1, rz0 + (u1 - w))
+        out.append((col % ntx, col // ntx, z0, z1))
+        u += z1 - z0
+    return out
+
+
+def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, ncta=None,
+                  chunks=None):
     """Replays u_apply_kernel + u_seam_fixup_kernel; returns y (3N).  ncta: the kernel's
-    balanced segments over ncta blocks instead of z-chunks of zc planes."""
+    balanced segments over ncta blocks instead of z-chunks of zc planes; chunks: given
+    (bx, by, z0, z1, element) segments."""
     nx, ny, nz = n
     nex, ney = nx - 1, ny - 1
     P = plan(nx, ny, nz, TY, zc)
@@ -356,12 +418,14 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, nc
         assert 0 <= i < nx and 0 <= j < ny and 0 <= k < nz
         return (k * ny + j) * nx + i
 
-    if ncta is None:  # z-chunks of zc planes per xy tile
-        chunks = [(bx, by, bz * zc, min(bz * zc + zc, nz)) for bz in range(P["nzc"])
+    if chunks is not None:
+        pass
+    elif ncta is None:  # z-chunks of zc planes per xy tile
+        chunks = [(bx, by, bz * zc, min(bz * zc + zc, nz), el_fn) for bz in range(P["nzc"])
                   for by in range(nty) for bx in range(ntx) if bz * zc < nz]
     else:  # the kernel's balanced segments
-        chunks = [c for b in range(ncta) for c in segments(ntx, nty, nz, ncta, b)]
-    for bx, by, z0, z1 in chunks:
+        chunks = [c + (el_fn,) for b in range(ncta) for c in segments(ntx, nty, nz, ncta, b)]
+    for bx, by, z0, z1, seg_el in chunks:
         X0, Y0 = 32 * bx, TY * by
         kf, kl = max(z0 - 1, 0), min(z1, nz - 1) - 1
         carry = np.zeros((32 * TY, nslot, 3))
@@ -415,7 +479,7 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, nc
                                     a = i + 2 * j + 4 * kk
                                     xn[a] = buf[k + kk][0:3, wy + j, lane + i]
                                     vn[a] = buf[k + kk][3, wy + j, lane + i]
-                        yc = el_fn(xn, vn)
+                        yc = seg_el(xn, vn)
                         sc[:, wy, lane] = yc.reshape(24)
             for tid in range(32 * TY):
                 for si in range(nslot):

@@ -119,3 +119,43 @@ def test_u_apply_constant_phase_field_elements(cuda, oracle_mod, n, l, cellE):
     y32 = ctx.u_apply(x, vg.MIXED)
     assert np.linalg.norm(y32 - yref) <= 2e-6 * np.linalg.norm(yref)
     ctx.close()
+
+
+@pytest.mark.parametrize("n,l", [((66, 40, 35), (2.0, 1.3, 1.1)), ((23, 19, 45), (1.0, 0.8, 2.0))])
+def test_unit_lists_split(cuda, oracle_mod, n, l):
+    """The ctx's U applies split the (tile, plane) units by phase field over the
+    fixed-weight kernel and the general one (unit lists rebuilt when v changes):
+    bit-identical to the plain split of vfgpu_u_apply_noalloc and of the host slab
+    pipeline (sub-grids, no lists), and following each change of v (intact field with a
+    cracked blob, random, intact, blob again); FP32 at 2e-6 against the oracle."""
+    import ctypes as C
+
+    import vpfhf_b200 as vg
+    from vpfhf_b200 import _abi
+    torch = cuda
+    E, nu, eta = 1e10, 0.25, 1e-8
+    o, ctx, _, x, mask = _setup(oracle_mod, n, l, 9)
+    rng = np.random.default_rng(10)
+    blob = np.ones(o.N)
+    bb = blob.reshape(n[2], n[1], n[0])
+    bb[n[2] // 3: n[2] // 2, n[1] // 4: n[1] // 2, 5: 40] = rng.uniform(0, 1, bb[n[2] // 3: n[2] // 2, n[1] // 4: n[1] // 2, 5: 40].shape)
+    bb[-4:, :9, :] = 0.3
+    bits = torch.from_numpy((mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)).cuda()
+    grid, mp, L = _abi.Grid(*n, *l), _abi.MatProp(E, nu, 0.0, 0.0, 1.0), _abi.lib()
+    xd = torch.from_numpy(x).cuda()
+    for v in (blob, rng.uniform(0, 1, o.N), np.ones(o.N), blob):
+        ctx.set_field("V", v)
+        y = ctx.u_apply(xd, vg.FP64).cpu().numpy()
+        assert np.array_equal(ctx.u_apply(x, vg.FP64), y)
+        vd, yna = torch.from_numpy(v).cuda(), torch.full_like(xd, float("nan"))
+        torch.cuda.synchronize()
+        rc = L.vfgpu_u_apply_noalloc(C.byref(grid), C.byref(mp), eta, vd.data_ptr(), bits.data_ptr(),
+                                     xd.data_ptr(), yna.data_ptr(), None)
+        assert rc == 0, L.vfgpu_last_error().decode()
+        torch.cuda.synchronize()
+        assert np.array_equal(yna.cpu().numpy(), y)
+        yref = o.u_apply(v, x, mask)
+        assert np.abs(y - yref).max() <= 1e-12 * np.abs(yref).max()
+        y32 = ctx.u_apply(x, vg.MIXED)
+        assert np.linalg.norm(y32 - yref) <= 2e-6 * np.linalg.norm(yref)
+    ctx.close()

@@ -99,3 +99,44 @@ def test_modal_v_element_matches_gauss_sum(oracle_mod):
         K = np.einsum("g,adg,bdg->ab", w * aeps, dphi, dphi) + np.einsum("g,ag,bg->ab", cg, phi, phi)
         y = km.v_element(x, cg, aeps, h)
         assert np.abs(y - K @ x).max() <= 1e-13 * np.abs(K @ x).max()
+
+
+@pytest.mark.parametrize("n,TY,ncta", [((37, 21, 13), 8, 7), ((70, 19, 11), 8, 5), ((37, 21, 13), 4, 3),
+                                       ((37, 35, 9), 16, 4), ((3, 2, 4), 8, 3)])
+def test_unit_lists_split_matches_plain(oracle_mod, n, TY, ncta):
+    """The U apply split over unit lists (list 0: units whose adjacent element layers are
+    constant-phase-field throughout the tile, on the fixed-weight kernel; list 1: the
+    rest): the lists cover every (tile, plane) unit once, each block's list segments
+    feed the fixed-weight operator only constant elements, and the two waves together
+    give the plain balanced split's y bit for bit."""
+    rng = np.random.default_rng(sum(n) + TY)
+    o = oracle_mod.Oracle(n, (1.1, 0.9, 0.7), E=3.0, nu=0.2, eta=1e-2)
+    lam, mu = 3.0 * 0.2 / 1.2 / 0.6, 3.0 / 1.2 * 0.5
+    v = np.ones(o.N)
+    vv = v.reshape(n[2], n[1], n[0])
+    vv[n[2] // 2: n[2] // 2 + 2, : n[1] // 2, 3:] = rng.uniform(0, 1, vv[n[2] // 2: n[2] // 2 + 2, : n[1] // 2, 3:].shape)
+    vv[:2] = 0.25
+    x = rng.standard_normal(3 * o.N)
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    bits = (mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)
+    h = tuple(L / (k - 1) for L, k in zip((1.1, 0.9, 0.7), n))
+    ntx, nty = -(-(n[0] - 1) // 32), -(-(n[1] - 1) // TY)
+    runs, start, tot = km.unit_lists(km.tile_layer_const(v, n, TY), n[2], ncta)
+    segs = [[s for b in range(ncta) for s in km.list_segments(runs[l], start[l], tot[l], ncta, b, ntx)]
+            for l in (0, 1)]
+    units = sorted((bx, by, z) for l in (0, 1) for bx, by, z0, z1 in segs[l] for z in range(z0, z1))
+    assert units == sorted((bx, by, z) for bx in range(ntx) for by in range(nty) for z in range(n[2]))
+    assert tot[0] > 0 and tot[1] > 0
+
+    def general(xn, vn):
+        return km.u_element(xn, vn, lam, mu, 1e-2, h)
+
+    def fixed_weight(xn, vn):
+        assert (vn == vn[0]).all()
+        return general(xn, vn)
+
+    chunks = [s + (fixed_weight,) for s in segs[0]] + [s + (general,) for s in segs[1]]
+    ys = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, chunks=chunks)
+    yp = km.u_apply_tiled(x, v, bits, n, h, lam, mu, 1e-2, TY=TY, ncta=ncta)
+    assert np.array_equal(ys, yp)
+    assert np.abs(ys - o.u_apply(v, x, mask)).max() <= 1e-13 * np.abs(ys).max()

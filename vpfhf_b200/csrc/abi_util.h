@@ -40,4 +40,10 @@ void free_mg(vfgpu_ctx* c);
 long long mg_memory_bytes(int nx, int ny, int nz, int bytes);
 template <typename T>
 UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const TilePlan& p);
+// Rebuilds the U unit lists (which u_args passes) from the FP64 v on the ctx stream if
+// v changed since they were built: every entry that applies U calls it first.
+cudaError_t u_lists_refresh(vfgpu_ctx* c);
+// Whether the ctx's U applies in this precision (8 or 4 bytes) take the unit lists (and
+// write the second wave's x.y partials).
+bool u_lists_on(const vfgpu_ctx* c, int prec_bytes);
 }  // namespace vfgpu

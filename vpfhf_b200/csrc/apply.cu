@@ -52,6 +52,12 @@ cudaError_t apply_kernel_attributes() {
   std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U64_TY, U64_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U64_TY, U64_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double>, U64_TY, U64_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double, true>, U64_TY, U64_MINB>();
+  if constexpr (!kU32Packed) {
+    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float>, U32_TY, U32_MINB>();
+    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float, true>, U32_TY, U32_MINB>();
+  }
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpNC<double>, U64_TY, 1>();
@@ -118,6 +124,210 @@ cudaError_t wait_selftest(long long cycles, int complete, int* timed_out) {
   return e;
 }
 
+// ------------------------------------------------------------------ unit lists
+// cls[(by ntx + bx) (nz - 1) + k] = 1 when every element of tile (bx, by) (32 x TY
+// elements) in element layer k has 8 equal nodal v (elements beyond the grid count as
+// equal).  One block per tile and run of kClsLayers layers: each thread loads its
+// element column's 2 x 2 node quads of the run's kClsLayers + 1 planes at once, then
+// votes per layer.
+constexpr int kClsLayers = 8;
+template <int TY>
+__global__ void __launch_bounds__(32 * TY) u_classify_kernel(const double* __restrict__ v,
+                                                              uint8_t* __restrict__ cls, int nx,
+                                                              int ny, int nez) {
+  __shared__ int all[kClsLayers];
+  const int tid = threadIdx.y * 32 + threadIdx.x;
+  if (tid < kClsLayers) all[tid] = 1;
+  const int ex = blockIdx.x * 32 + threadIdx.x, ey = blockIdx.y * TY + threadIdx.y;
+  const int k0 = blockIdx.z * kClsLayers;
+  const bool in = ex < nx - 1 && ey < ny - 1;
+  const int64_t pl = (int64_t)nx * ny;
+  const double* w = v + (in ? (int64_t)k0 * pl + (int64_t)ey * nx + ex : 0);
+  double q[kClsLayers + 1][4];
+#pragma unroll
+  for (int i = 0; i <= kClsLayers; i++) {
+    const bool ld = in && k0 + i <= nez;
+    q[i][0] = ld ? w[i * pl] : 0.;
+    q[i][1] = ld ? w[i * pl + 1] : 0.;
+    q[i][2] = ld ? w[i * pl + nx] : 0.;
+    q[i][3] = ld ? w[i * pl + nx + 1] : 0.;
+  }
+  __syncthreads();  // all[] initialised
+#pragma unroll
+  for (int i = 0; i < kClsLayers; i++) {
+    const double a = q[i][0];
+    const bool c = !in || (q[i][1] == a && q[i][2] == a && q[i][3] == a && q[i + 1][0] == a &&
+                           q[i + 1][1] == a && q[i + 1][2] == a && q[i + 1][3] == a);
+    if (!__all_sync(0xffffffffu, c) && threadIdx.x == 0) all[i] = 0;
+  }
+  __syncthreads();
+  if (tid < kClsLayers && k0 + tid < nez)
+    cls[(int64_t)(blockIdx.y * gridDim.x + blockIdx.x) * nez + k0 + tid] = all[tid] ? 1 : 0;
+}
+
+// Exclusive prefix sum of a[0, n) in shared memory over the whole block (blockDim.x a
+// multiple of 32, at most 1024); returns the total.  wsum: 32 ints of shared scratch.
+__device__ int block_scan_excl(int* a, int n, int* wsum) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int per = (n + blockDim.x - 1) / blockDim.x;
+  const int b0 = min((int)threadIdx.x * per, n), b1 = min(b0 + per, n);
+  int sum = 0;
+  for (int i = b0; i < b1; i++) sum += a[i];
+  int x = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = lane < nw ? wsum[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  int run = x - sum + (warp ? wsum[warp - 1] : 0);
+  const int total = wsum[nw - 1];
+  for (int i = b0; i < b1; i++) {
+    const int t = a[i];
+    a[i] = run;
+    run += t;
+  }
+  __syncthreads();  // wsum is reused by the next scan
+  return total;
+}
+
+// Unit type of node plane z of a tile column from its layer flags f[0, nz - 1):
+// 0 when the element layers below and above are constant (or absent), else 1.
+__device__ __forceinline__ int unit_type(const uint8_t* f, int z, int nez) {
+  const bool below = z == 0 || f[z - 1], above = z == nez || f[z];
+  return below && above ? 0 : 1;
+}
+
+// One block of 1024 threads builds both unit lists of a plan from its layer flags:
+// per tile column (one thread each) the runs of equal unit type up its nz planes,
+// counted, offset by prefix sums over the columns in tile order, written; then, per
+// list and block b of the apply launch, the run holding the list's unit U b / ncta
+// (binary search on the runs' unit offsets).
+__global__ void __launch_bounds__(1024) unit_lists_kernel(const uint8_t* __restrict__ cls, int nz,
+                                                          int ncol, int ncta, int4* __restrict__ runs0,
+                                                          int4* __restrict__ runs1, int* __restrict__ start0,
+                                                          int* __restrict__ start1, int* __restrict__ total) {
+  extern __shared__ int sh[];  // [4][ncol] counts, then 32 ints of scan scratch
+  int* cnt = sh;
+  int* wsum = sh + 4 * ncol;
+  const int nez = nz - 1;
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    const uint8_t* f = cls + (int64_t)c * nez;
+    int nr[2] = {0, 0}, nu[2] = {0, 0}, prev = -1;
+    for (int z = 0; z < nz; z++) {
+      const int t = unit_type(f, z, nez);
+      nu[t]++;
+      if (t != prev) nr[t]++;
+      prev = t;
+    }
+    cnt[c] = nr[0];
+    cnt[ncol + c] = nr[1];
+    cnt[2 * ncol + c] = nu[0];
+    cnt[3 * ncol + c] = nu[1];
+  }
+  __syncthreads();
+  int tot[4];
+#pragma unroll
+  for (int a = 0; a < 4; a++) tot[a] = block_scan_excl(cnt + a * ncol, ncol, wsum);
+  int4* runs[2] = {runs0, runs1};
+  for (int c = threadIdx.x; c < ncol; c += blockDim.x) {
+    const uint8_t* f = cls + (int64_t)c * nez;
+    int r[2] = {cnt[c], cnt[ncol + c]}, u[2] = {cnt[2 * ncol + c], cnt[3 * ncol + c]};
+    int z0 = 0, t0 = unit_type(f, 0, nez);
+    for (int z = 1; z <= nz; z++) {
+      const int t = z < nz ? unit_type(f, z, nez) : -1;
+      if (t != t0) {
+        runs[t0][r[t0]++] = make_int4(c, z0, z, u[t0]);
+        u[t0] += z - z0;
+        z0 = z;
+        t0 = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 2 * ncta; i += blockDim.x) {
+    const int l = i / ncta, b = i % ncta, nrun = tot[l];
+    const int64_t ub = (int64_t)tot[2 + l] * b / ncta;
+    int lo = 0, hi = nrun - 1;
+    while (lo < hi) {  // the last run whose first unit is <= ub
+      const int mid = (lo + hi + 1) / 2;
+      if (runs[l][mid].w <= ub) lo = mid; else hi = mid - 1;
+    }
+    (l ? start1 : start0)[b] = nrun > 0 ? lo : 0;
+  }
+  if (threadIdx.x == 0) {
+    total[0] = tot[2];
+    total[1] = tot[3];
+  }
+}
+
+constexpr int kMaxListCols = 2048;  // tile columns the one-block list builder takes
+
+size_t unit_lists_bytes(const TilePlan& p, int nz) {
+  const int64_t ncol = (int64_t)p.ntx * p.nty;
+  if (nz < 2 || ncol > kMaxListCols) return 0;
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  return up(ncol * (nz - 1)) + 2 * up(ncol * nz * sizeof(int4)) + 2 * up(p.ncta * sizeof(int)) +
+         up(2 * sizeof(int));
+}
+
+UnitLists unit_lists_carve(void* base, const TilePlan& p, int nz) {
+  UnitLists L;
+  if (!base || !unit_lists_bytes(p, nz)) return L;
+  const size_t ncol = (size_t)p.ntx * p.nty;
+  auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+  char* q = static_cast<char*>(base);
+  L.cls = reinterpret_cast<uint8_t*>(q);
+  q += up(ncol * (nz - 1));
+  for (int l = 0; l < 2; l++) {
+    L.runs[l] = reinterpret_cast<int4*>(q);
+    q += up(ncol * nz * sizeof(int4));
+  }
+  for (int l = 0; l < 2; l++) {
+    L.start[l] = reinterpret_cast<int*>(q);
+    q += up(p.ncta * sizeof(int));
+  }
+  L.total = reinterpret_cast<int*>(q);
+  return L;
+}
+
+template <int TY>
+static cudaError_t classify(const double* v, uint8_t* cls, int nx, int ny, int nz, const TilePlan& p,
+                            cudaStream_t s) {
+  const int runs = (nz - 1 + kClsLayers - 1) / kClsLayers;
+  if (runs > 65535 || p.nty > 65535) return cudaErrorInvalidValue;
+  u_classify_kernel<TY><<<dim3(p.ntx, p.nty, runs), dim3(32, TY), 0, s>>>(v, cls, nx, ny, nz - 1);
+  return cudaGetLastError();
+}
+
+cudaError_t build_unit_lists(const double* v, int nx, int ny, int nz, const TilePlan& p,
+                             const UnitLists& L, cudaStream_t s) {
+  if (!L.cls) return cudaSuccess;
+  cudaError_t e;
+  switch (p.ty) {
+    case 4: e = classify<4>(v, L.cls, nx, ny, nz, p, s); break;
+    case 8: e = classify<8>(v, L.cls, nx, ny, nz, p, s); break;
+    case 16: e = classify<16>(v, L.cls, nx, ny, nz, p, s); break;
+    default: return cudaErrorInvalidValue;
+  }
+  if (e != cudaSuccess) return e;
+  const int ncol = p.ntx * p.nty;
+  unit_lists_kernel<<<1, 1024, (4 * ncol + 32) * sizeof(int), s>>>(
+      L.cls, nz, ncol, p.ncta, L.runs[0], L.runs[1], L.start[0], L.start[1], L.total);
+  return cudaGetLastError();
+}
+
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, U64_MINB, num_sms);
   return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
@@ -130,6 +340,11 @@ template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
   if (A.cflag) return launch_tile_apply<UOpNC<double>, U64_TY, 1>(A, p, L, s);
+  if (A.ur[0] && A.ur[1]) {
+    if (cubic(A))
+      return launch_tile_apply_split<UOpConst<double, true>, UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
+    return launch_tile_apply_split<UOpConst<double>, UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
+  }
   if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
   return launch_tile_apply<UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
 }
@@ -139,6 +354,13 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
   // NOCOMPRESSION needs the scalar layout: its plan is the FP32 plan only with the
   // scalar tile (the packed build option keeps the plain operator packed)
   if (A.cflag) return launch_tile_apply<UOpNC<float>, U_TY, 2>(A, p, L, s);
+  if constexpr (!kU32Packed) {
+    if (A.ur[0] && A.ur[1]) {
+      if (cubic(A))
+        return launch_tile_apply_split<UOpConst<float, true>, U32OpC, U32_TY, U32_MINB>(A, p, L, s);
+      return launch_tile_apply_split<UOpConst<float>, U32Op, U32_TY, U32_MINB>(A, p, L, s);
+    }
+  }
   if (cubic(A)) return launch_tile_apply<U32OpC, U32_TY, U32_MINB>(A, p, L, s);
   return launch_tile_apply<U32Op, U32_TY, U32_MINB>(A, p, L, s);
 }

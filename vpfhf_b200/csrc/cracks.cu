@@ -181,6 +181,7 @@ extern "C" int vfgpu_init_cracks(vfgpu_ctx* c, int npenny, const vfgpu_penny* pe
   const int blocks = (int)std::min<int64_t>((c->N + 255) / 256, (int64_t)c->nsm * 8);
   int ip = 0, ir = 0;
   B.first = 1;
+  c->v32_stale = c->ul_stale = true;  // V changes from here on, also on an error return
   cudaError_t e = cudaSuccess;
   do {  // at least one pass, so that no cracks gives V = VIrrev = 1
     B.np = std::min(kBatch, npenny - ip);
@@ -195,6 +196,5 @@ extern "C" int vfgpu_init_cracks(vfgpu_ctx* c, int npenny, const vfgpu_penny* pe
   } while (e == cudaSuccess && (ip < npenny || ir < nrect));
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_init_cracks");
-  c->v32_stale = true;
   return VFGPU_OK;
 }

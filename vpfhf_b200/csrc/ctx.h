@@ -21,6 +21,12 @@ struct vfgpu_ctx {
   int nlayer = 0;
   vfgpu::LayerTable layers{};
   uint8_t* d_elayer = nullptr;  // nz-1
+  // U unit lists of plan64 / plan32 (UnitLists::cls null: the grid takes none), in one
+  // allocation; rebuilt from the FP64 v by u_lists_refresh when ul_stale (set with
+  // v32_stale wherever v changes)
+  void* d_ul = nullptr;
+  vfgpu::UnitLists ul64, ul32;
+  bool ul_stale = true;
   vfgpu::DevParams* d_params = nullptr;  // device copy of layers / eta / aeps
   float* d_cellE = nullptr;     // NC or null
   bool have_mat = false;
@@ -47,7 +53,7 @@ struct vfgpu_ctx {
   // fields (FP64, resident)
   double* f[7] = {nullptr};
   float* V32 = nullptr;  // FP32 copy of V for the mixed-precision operator
-  bool v32_stale = true;
+  bool v32_stale = true;  // (with ul_stale)
 
   // scratch
   vfgpu::TilePlan plan64{}, plan32{}, vplan64{}, vplan32{};

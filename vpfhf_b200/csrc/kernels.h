@@ -20,6 +20,29 @@ cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int 
 // wait on a phase that never completes (complete = 0) gave up after `cycles`.
 cudaError_t wait_selftest(long long cycles, int complete, int* timed_out);
 
+// The U operator's unit lists for one tile plan (UApplyArgs::ur): the per-(tile,
+// element layer) constant-phase-field flags and the two lists built from them.
+struct UnitLists {
+  uint8_t* cls = nullptr;  // [ntx nty][nz - 1]; null: no lists for this plan
+  int4* runs[2] = {};      // [ntx nty nz] each
+  int* start[2] = {};      // [ncta] each
+  int* total = nullptr;    // [2]
+};
+// Device bytes of a plan's unit lists; 0 when the grid has more tile columns than the
+// one-block list builder takes (its applies then split all units).
+size_t unit_lists_bytes(const TilePlan& p, int nz);
+UnitLists unit_lists_carve(void* base, const TilePlan& p, int nz);
+// Rebuilds the lists from the FP64 phase field v (two launches on s).
+cudaError_t build_unit_lists(const double* v, int nx, int ny, int nz, const TilePlan& p,
+                             const UnitLists& L, cudaStream_t s);
+template <typename T> void use_unit_lists(UApplyArgs<T>& A, const UnitLists& L) {
+  for (int l = 0; l < 2; l++) {
+    A.ur[l] = L.cls ? L.runs[l] : nullptr;
+    A.ustart[l] = L.cls ? L.start[l] : nullptr;
+  }
+  A.utotal = L.cls ? L.total : nullptr;
+}
+
 template <typename T>
 cudaError_t launch_u_apply(const UApplyArgs<T>& A, const TilePlan& p, const LayerTable& L,
                            cudaStream_t s);

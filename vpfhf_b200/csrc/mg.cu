@@ -598,6 +598,7 @@ template <typename T> struct LevelT {
   const float* cellE;
   const T* dinv;
   const uint32_t* cflag;  // fine level under NOCOMPRESSION: the Jacobian's bits
+  vfgpu::UnitLists ul;    // fine level: the ctx's unit lists of its plan (else none)
   T *x, *b, *r, *d, *t;
   double* coef;
   int64_t n3;
@@ -637,6 +638,7 @@ template <typename T> LevelT<T> view(vfgpu_ctx* c, int l) {
     V.cellE = c->d_cellE;
     V.dinv = (const T*)c->mg_dinv0;
     V.cflag = c->unilateral ? c->d_cflag : nullptr;
+    V.ul = u_lists_on(c, (int)sizeof(T)) ? (sizeof(T) == 8 ? c->ul64 : c->ul32) : UnitLists{};
     V.n3 = 3 * c->N;
   } else {
     V.nx = L.nx;
@@ -653,6 +655,7 @@ template <typename T> LevelT<T> view(vfgpu_ctx* c, int l) {
     V.cellE = L.cellE;
     V.dinv = (const T*)L.dinv;
     V.cflag = nullptr;
+    V.ul = UnitLists{};
     V.n3 = 3 * L.N;
   }
   return V;
@@ -678,6 +681,7 @@ template <typename T> UApplyArgs<T> level_args(vfgpu_ctx* c, const LevelT<T>& V,
   A.eta = T(c->vf.eta);
   A.P = c->d_params;
   A.cflag = V.cflag;
+  use_unit_lists(A, V.ul);
   return A;
 }
 

@@ -25,12 +25,28 @@ template <typename T_, bool CUBIC = false> struct UOp {
   using T = T_;
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
+  static constexpr int LIST = 1;  // the unit list this operator takes in a split launch
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + 3 * n;
     src[1] = A.x + 3 * n + 1;
     src[2] = A.x + 3 * n + 2;
     src[3] = A.v + n;
   }
+  // The cell's Lame coefficients (material layer table, or per-cell modulus).
+  __device__ __forceinline__ static void lame(const Args& A, const LayerTable& L, int ex, int ey,
+                                              int ez, T& lam, T& mu) {
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    const LayerTable& LT = A.P ? A.P->L : L;
+    if (A.cellE) {
+      const T E = T(A.cellE[((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex]);
+      lam = E * T(LT.lamfac[layer]);
+      mu = E * T(LT.mufac[layer]);
+    } else {
+      lam = T(LT.lambda[layer]);
+      mu = T(LT.mu[layer]);
+    }
+  }
+  __device__ __forceinline__ static T eta_of(const Args& A) { return A.P ? T(A.P->eta) : A.eta; }
   __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
                                                  int ey, int ez, const T (&in)[8][NIN],
                                                  T (&out)[8][NC]) {
@@ -42,18 +58,9 @@ template <typename T_, bool CUBIC = false> struct UOp {
       xn[a][2] = in[a][2];
       vn[a] = in[a][3];
     }
-    const int layer = A.elayer ? A.elayer[ez] : 0;
-    const LayerTable& LT = A.P ? A.P->L : L;
-    const T eta = A.P ? T(A.P->eta) : A.eta;
     T lam, mu;
-    if (A.cellE) {
-      const T E = T(A.cellE[((int64_t)ez * (A.ny - 1) + ey) * (A.nx - 1) + ex]);
-      lam = E * T(LT.lamfac[layer]);
-      mu = E * T(LT.mufac[layer]);
-    } else {
-      lam = T(LT.lambda[layer]);
-      mu = T(LT.mu[layer]);
-    }
+    lame(A, L, ex, ey, ez, lam, mu);
+    const T eta = eta_of(A);
     // an element whose nodal phase field is constant (the intact bulk, v = 1) takes the
     // fixed-weight form; the rest the row closed form
     const T v0 = vn[0];
@@ -64,6 +71,23 @@ template <typename T_, bool CUBIC = false> struct UOp {
       u_element_const<T, CUBIC>(xn, fma(v0, v0, eta), lam, mu, A.ihx, A.ihy, A.ihz, A.vol, out);
     else
       u_element<T, CUBIC>(xn, vn, lam, mu, eta, A.ihx, A.ihy, A.ihz, A.vol, out);
+  }
+  // The same for an element known to have a constant nodal phase field (the choice
+  // element makes for it, without the general form in the code path).
+  __device__ __forceinline__ static void element_const(const Args& A, const LayerTable& L, int ex,
+                                                       int ey, int ez, const T (&in)[8][NIN],
+                                                       T (&out)[8][NC]) {
+    T xn[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; a++) {
+      xn[a][0] = in[a][0];
+      xn[a][1] = in[a][1];
+      xn[a][2] = in[a][2];
+    }
+    T lam, mu;
+    lame(A, L, ex, ey, ez, lam, mu);
+    const T v0 = in[0][3];
+    u_element_const<T, CUBIC>(xn, fma(v0, v0, eta_of(A)), lam, mu, A.ihx, A.ihy, A.ihz, A.vol, out);
   }
   // The per-node flags finish_node needs (Dirichlet bits), loaded ahead by the tiles.
   __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
@@ -95,12 +119,28 @@ template <typename T_, bool CUBIC = false> struct UOp {
   }
 };
 
+// UOp for the units of unit list 0, whose elements all have a constant nodal phase
+// field: the fixed-weight element alone (the choice UOp::element makes for them, with
+// the same arithmetic), compiled without the general element.
+template <typename T_, bool CUBIC = false> struct UOpConst : UOp<T_, CUBIC> {
+  using Base = UOp<T_, CUBIC>;
+  using T = T_;
+  using Args = UApplyArgs<T>;
+  static constexpr int LIST = 0;
+  __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
+                                                 int ey, int ez, const T (&in)[8][Base::NIN],
+                                                 T (&out)[8][Base::NC]) {
+    Base::element_const(A, L, ex, ey, ez, in, out);
+  }
+};
+
 // The NOCOMPRESSION U operator: UOp with the per-point element u_element_nc and the
 // per-cell compression bits A.cflag.
 template <typename T_> struct UOpNC {
   using T = T_;
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
+  static constexpr int LIST = -1;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<T>::node_src(A, n, src);
   }
@@ -151,6 +191,7 @@ struct UOpF2 {
   using T = float;
   using Args = UApplyArgs<float>;
   static constexpr int NC = 3, NIN = 4, EPT = 2, CV = 0;
+  static constexpr int LIST = -1;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<float>::node_src(A, n, src);
   }
@@ -325,6 +366,7 @@ template <typename T_> struct VOp {
   using T = T_;
   using Args = VApplyArgs<T>;
   static constexpr int NC = 1, NIN = 1, EPT = 1;
+  static constexpr int LIST = -1;
   static constexpr int CV = 27;  // per-cell values staged by the engine (the coefficient)
   __device__ __forceinline__ static const CUtensorMap* cell_map(const Args& A) { return &A.cmap; }
   __device__ __forceinline__ static unsigned* cell_err(const Args& A) { return A.cerr; }

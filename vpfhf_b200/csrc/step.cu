@@ -295,6 +295,10 @@ static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* 
   return launch_u_apply<float>(A, c->plan32, c->layers, c->stream);
 }
 static int dots_of(const vfgpu_ctx* c, const TilePlan& p) { return tile_dot_count(p, c->nx, c->ny, c->nz); }
+// The U applies of a split launch (unit lists) write a second wave's partials.
+static int u_dots_of(const vfgpu_ctx* c, const TilePlan& p, int prec_bytes) {
+  return dots_of(c, p) + (u_lists_on(c, prec_bytes) ? p.ncta : 0);
+}
 
 // Which CG call sites let the operator apply accumulate p.w (bit k-1 for call site k:
 // 1 U FP64, 2 U FP32, 3 V FP64, 4 V FP32); the others use a separate p.w pass.  The
@@ -362,7 +366,8 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   const bool mixed = o.precision == VFGPU_MIXED;
   ElemArgs E = elem_args(c);
   const bool nc = c->unilateral != 0;
-  cudaError_t e = nc_flags(c, U);
+  cudaError_t e = u_lists_refresh(c);  // v is fixed for the whole solve
+  if (e == cudaSuccess) e = nc_flags(c, U);
   if (e == cudaSuccess) e = u_load(c, E, f, U);
   if (e == cudaSuccess) e = launch_u_diag(E, c->f[VFGPU_FIELD_V], c->bcU_bits, JY, c->stream, U);
   if (e == cudaSuccess) e = dev_inv(JY, dinv, mixed ? c->p32[4] : nullptr, n3, c->stream);
@@ -410,7 +415,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
       S.ksp_its += kits;
       tmo = w.expired();
     } else if (!mixed) {
-      CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), dots_of(c, c->plan64)};
+      CGVecs<double> v{Y, R, P, W, dinv, F, nullptr, n3, dot_buf(c, 1), u_dots_of(c, c->plan64, 8)};
       rc = run_cg<double>(c, 1, v, apply64, o.ksp_rtol, o.ksp_atol, o.ksp_dtol, o.ksp_maxit, w, &kits,
                           &kreason, &tmo);
       if (rc) return rc;
@@ -430,7 +435,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
         float* b32 = reinterpret_cast<float*>(P);  // FP32 right-hand side staged in P
         e = dev_to_f32(R, b32, n3, c->stream);
         if (e != cudaSuccess) return cuda_fail(e, "vfgpu_step_u");
-        CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3, dot_buf(c, 2), dots_of(c, c->plan32)};
+        CGVecs<float> v{x32, r32, pp32, w32, c->p32[4], b32, nullptr, n3, dot_buf(c, 2), u_dots_of(c, c->plan32, 4)};
         const double in_rtol = std::max(o.inner_rtol, 0.5 * target / zr);
         int its32 = 0, r32reason = 0;
         rc = run_cg<float>(c, 2, v, apply32, in_rtol, 0.0, o.ksp_dtol, o.ksp_maxit, w, &its32,
@@ -587,6 +592,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
   double* V = c->f[VFGPU_FIELD_V];
   uint8_t* mask = c->vmask;
   ElemArgs E = elem_args(c);
+  c->v32_stale = c->ul_stale = true;  // V changes from here on, also on an error return
   cudaError_t e = dev_v_bounds(c->f[VFGPU_FIELD_VIRREV], c->vf.atnum == 1, lb, ub, V, N, c->stream);
   if (e == cudaSuccess)
     e = launch_v_coef(E, c->f[VFGPU_FIELD_U], c->f[VFGPU_FIELD_THETA], c->f[VFGPU_FIELD_THETAREF],
@@ -699,7 +705,7 @@ int vfgpu_step_v(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     if (w.expired() && !reason) reason = -100;
   }
   if (!reason) reason = -5;
-  c->v32_stale = true;
+  c->v32_stale = c->ul_stale = true;
   if (int rc2 = check_cell_copies(c)) return rc2;
   S.reason = reason;
   S.fnorm = fnorm;
@@ -718,13 +724,13 @@ int vfgpu_time_step_prepare(vfgpu_ctx* c) {
   // the multigrid eigenvalue estimates restart from their seed at each time step, so a
   // time step's results do not depend on the problems a pooled ctx solved before
   c->mg_ev = false;
+  c->v32_stale = c->ul_stale = true;
   cudaError_t e = cudaMemcpyAsync(c->f[VFGPU_FIELD_VIRREV], c->f[VFGPU_FIELD_V], c->N * sizeof(double),
                                   cudaMemcpyDeviceToDevice, c->stream);
   if (e == cudaSuccess) e = dev_apply_bc(c->f[VFGPU_FIELD_U], c->bcU_kind, c->f[VFGPU_FIELD_BCU], 3 * c->N, c->stream);
   if (e == cudaSuccess) e = dev_apply_bc(c->f[VFGPU_FIELD_V], c->bcV_kind, nullptr, c->N, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_time_step_prepare");
-  c->v32_stale = true;
   return VFGPU_OK;
 }
 
@@ -810,6 +816,7 @@ int vfgpu_memory_estimate(const vfgpu_grid* g, long long* bytes) {
   long long b = 0;
   b += (2 * 3 * N + 5 * N) * 8;                          // fields U, BCU, V, VIrrev, theta, thetaRef, p
   b += N * 4 + (g->nz - 1) + 3 * N + 3 * N;              // V32, layers, BC kinds and bits
+  b += (long long)(unit_lists_bytes(p64, g->nz) + unit_lists_bytes(p32, g->nz));  // U unit lists
   b += (long long)std::max(p64.seamX + p64.seamY, q64.seamX + q64.seamY) * 8 +
        (long long)std::max(p32.seamX + p32.seamY, q32.seamX + q32.seamY) * 4;
   b += 3 * 3 * N * 8 + 2 * 3 * N * 4;                    // staging vectors
@@ -828,7 +835,8 @@ int vfgpu_u_residual(vfgpu_ctx* c, double* F) {
   if (rc) return rc;
   ElemArgs E = elem_args(c);
   double *f = c->p64[0], *tmp = c->p64[1], *Fd = c->p64[2];
-  cudaError_t e = nc_flags(c, c->f[VFGPU_FIELD_U]);
+  cudaError_t e = u_lists_refresh(c);
+  if (e == cudaSuccess) e = nc_flags(c, c->f[VFGPU_FIELD_U]);
   if (e == cudaSuccess) e = u_load(c, E, f, c->f[VFGPU_FIELD_U]);
   if (e == cudaSuccess) e = u_residual(c, c->f[VFGPU_FIELD_U], f, tmp, Fd);
   if (e == cudaSuccess) e = copy_out(c, F, Fd, 3 * c->N);

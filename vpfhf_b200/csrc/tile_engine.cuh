@@ -29,7 +29,10 @@
 //   flags, xin[NC]) (the same from flags loaded ahead and the node's inputs from the
 //   plane ring), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
-//   so that a queued batch of iterations costs nothing once it is done).
+//   so that a queued batch of iterations costs nothing once it is done), and LIST:
+//   -1, or the unit list (A.ur, A.ustart, A.utotal) the operator's launches take when
+//   the list is given -- the U operator's units split by phase field over two
+//   launches, each with its own wave of blocks (unit lists 0 and 1).
 // An Op with CV > 0 per-cell values (the V operator's 27 Gauss-point coefficients)
 //   supplies cell_map(A) (a 3-D tensor map, box 32 x TY x CV over (ex, ey, CV ez + g))
 //   and cell_err(A), and element(..., cc, cs) reads its cell's values from shared
@@ -169,8 +172,15 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   // This block's share of the work: node planes [U b / n, U (b + 1) / n) of the
   // U = ntx nty nz (xy tile, node plane) units taken column by column, cut at column
   // ends into segments (a segment recomputes the element layer below its first plane,
-  // so the result does not depend on the split).
-  const int64_t U = (int64_t)A.ntx * A.nty * nz;
+  // so the result does not depend on the split) -- or, with unit list Op::LIST, of the
+  // U units of the list's runs, cut at run ends.
+  [[maybe_unused]] const int4* runs = nullptr;
+  [[maybe_unused]] int run = 0;
+  int64_t U = (int64_t)A.ntx * A.nty * nz;
+  if constexpr (Op::LIST >= 0) {
+    runs = A.ur[Op::LIST];
+    if (runs) U = A.utotal[Op::LIST];
+  }
   const int64_t u_begin = U * blockIdx.x / gridDim.x, u_end = U * (blockIdx.x + 1) / gridDim.x;
   if (u_begin >= u_end) {
     if (DOT && threadIdx.x + threadIdx.y == 0) A.dot[blockIdx.x] = 0.;
@@ -417,10 +427,21 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   return true;
   };  // run_segment
 
+  if constexpr (Op::LIST >= 0)
+    if (runs) run = A.ustart[Op::LIST][blockIdx.x];
   for (int64_t u = u_begin; u < u_end;) {
-    const int col = (int)(u / nz), z0 = (int)(u % nz);
-    const int64_t left = u_end - u;
-    const int z1 = left < (int64_t)(nz - z0) ? z0 + (int)left : nz;
+    int col, z0, z1;
+    if (runs) {
+      const int4 R = runs[run++];  // the run holding unit u
+      col = R.x;
+      z0 = R.y + (int)(u - R.w);
+      z1 = (int)std::min<int64_t>(R.z, R.y + (u_end - R.w));
+    } else {
+      col = (int)(u / nz);
+      z0 = (int)(u % nz);
+      const int64_t left = u_end - u;
+      z1 = left < (int64_t)(nz - z0) ? z0 + (int)left : nz;
+    }
     if (!run_segment(col % A.ntx, col / A.ntx, z0, z1)) break;  // block-uniform
     u += z1 - z0;
     if (u < u_end) {
@@ -556,6 +577,37 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
   } else {
     tile_apply_kernel<Op, TY, MINB, false><<<grid, block, smem, s>>>(A, L);
     if (sblocks > 0) seam_fixup_kernel<Op, false><<<sblocks, 256, 0, s>>>(A, TY, base);
+  }
+  return cudaGetLastError();
+}
+
+
+// An operator split over unit lists 0 (OpF) and 1 (OpG, which also finishes the seams):
+// one wave of blocks for each list in turn, then the seam fix-up.  With A.dot the x.y
+// block partials go to A.dot[0, ncta) (OpF), [ncta, 2 ncta) (OpG) and from 2 ncta on
+// (seams): tile_dot_count + ncta of them.
+template <class OpF, class OpG, int TY, int MINB>
+cudaError_t launch_tile_apply_split(typename OpG::Args A, const TilePlan& p, const LayerTable& L,
+                                    cudaStream_t s) {
+  static_assert(OpF::LIST == 0 && OpG::LIST == 1 && OpF::EPT == 1 && OpG::EPT == 1, "unit lists 0, 1");
+  A.ntx = p.ntx;
+  A.nty = p.nty;
+  constexpr size_t smemF = tile_smem_bytes<OpF, TY, MINB>(), smemG = tile_smem_bytes<OpG, TY, MINB>();
+  cudaError_t ea = set_tile_attributes<OpF, TY, MINB>();
+  if (ea == cudaSuccess) ea = set_tile_attributes<OpG, TY, MINB>();
+  if (ea != cudaSuccess) return ea;
+  dim3 grid(p.ncta), block(32, TY);
+  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = 2 * p.ncta;
+  typename OpG::Args AG = A;
+  if (AG.dot) AG.dot += p.ncta;
+  if (A.dot) {
+    tile_apply_kernel<OpF, TY, MINB, true><<<grid, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpG, TY, MINB, true><<<grid, block, smemG, s>>>(AG, L);
+    if (sblocks > 0) seam_fixup_kernel<OpG, true><<<sblocks, 256, 0, s>>>(A, TY, base);
+  } else {
+    tile_apply_kernel<OpF, TY, MINB, false><<<grid, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpG, TY, MINB, false><<<grid, block, smemG, s>>>(AG, L);
+    if (sblocks > 0) seam_fixup_kernel<OpG, false><<<sblocks, 256, 0, s>>>(A, TY, base);
   }
   return cudaGetLastError();
 }

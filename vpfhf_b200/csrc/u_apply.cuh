@@ -43,6 +43,14 @@ template <typename T> struct UApplyArgs {
   double* __restrict__ dot;           // if non-null: per-block partials of x.y (see tile_engine.cuh)
   const uint32_t* __restrict__ cflag; // NOCOMPRESSION: per cell, bit g = tr(eps(u0)) < 0 at Gauss
                                       // point g (u_element_nc); null = the plain operator
+  // Unit lists (null ur[l]: the launch splits all (tile, node plane) units): list 0 holds
+  // the units whose two adjacent element layers have a constant nodal v throughout the
+  // tile (the fixed-weight operator UOpConst), list 1 the rest (UOp).  The launch's
+  // blocks share the utotal[l] units of runs ur[l] (x: tile column, y: first plane, z: end
+  // plane, w: units before the run) evenly; block b starts in run ustart[l][b].
+  const int4* __restrict__ ur[2];
+  const int* __restrict__ ustart[2];
+  const int* __restrict__ utotal;
   int nx, ny, nz;
   int ntx, nty;                       // tiles in x, y
   T ihx, ihy, ihz, vol, eta;

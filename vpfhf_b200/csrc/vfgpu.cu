@@ -138,8 +138,23 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   A.eta = T(c->vf.eta);
   A.P = c->d_params;
   A.cflag = c->unilateral ? c->d_cflag : nullptr;
+  use_unit_lists(A, sizeof(T) == 8 ? c->ul64 : c->ul32);
+  if (A.cflag) use_unit_lists(A, UnitLists{});  // NOCOMPRESSION takes the plain split
   return A;
 }
+cudaError_t u_lists_refresh(vfgpu_ctx* c) {
+  if (!c->ul_stale) return cudaSuccess;
+  const double* v = c->f[VFGPU_FIELD_V];
+  cudaError_t e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan64, c->ul64, c->stream);
+  if (e == cudaSuccess) e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan32, c->ul32, c->stream);
+  if (e == cudaSuccess) c->ul_stale = false;
+  return e;
+}
+
+bool u_lists_on(const vfgpu_ctx* c, int prec_bytes) {
+  return !c->unilateral && (prec_bytes == 8 ? c->ul64.cls : c->ul32.cls) != nullptr;
+}
+
 template UApplyArgs<double> u_args<double>(vfgpu_ctx*, const double*, const double*, double*,
                                            double*, const TilePlan&);
 template UApplyArgs<float> u_args<float>(vfgpu_ctx*, const float*, const float*, float*, float*,
@@ -171,7 +186,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   cudaFree(c->t64c);
-  void* bufs[] = {c->d_tcB, c->d_tcerr, c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_tcB, c->d_tcerr, c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_ul, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -232,11 +247,19 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   for (int fi = 0; fi < 7; fi++) ALLOC(c->f[fi], field_len(c, fi) * sizeof(double));
   ALLOC(c->V32, c->N * sizeof(float));
   ALLOC(c->d_elayer, std::max(1, c->nz - 1));
+  {
+    const size_t b64 = unit_lists_bytes(c->plan64, c->nz), b32 = unit_lists_bytes(c->plan32, c->nz);
+    if (b64 + b32 > 0) {
+      ALLOC(c->d_ul, b64 + b32);
+      c->ul64 = unit_lists_carve(b64 ? c->d_ul : nullptr, c->plan64, c->nz);
+      c->ul32 = unit_lists_carve(b32 ? static_cast<char*>(c->d_ul) + b64 : nullptr, c->plan32, c->nz);
+    }
+  }
   ALLOC(c->d_params, sizeof(DevParams));
   {
     int nd = 1;
     for (const TilePlan* p : {&c->plan64, &c->plan32, &c->vplan64, &c->vplan32})
-      nd = std::max(nd, tile_dot_count(*p, c->nx, c->ny, c->nz));
+      nd = std::max(nd, tile_dot_count(*p, c->nx, c->ny, c->nz) + p->ncta);  // U: split launch
     ALLOC(c->d_dot, (size_t)nd * sizeof(double));
   }
   ALLOC(c->bcU_kind, 3 * c->N);
@@ -421,10 +444,10 @@ int vfgpu_set_field(vfgpu_ctx* c, int field, const double* data) {
   if (!c || !data) return fail(VFGPU_ERR_INVALID, "vfgpu_set_field: null argument");
   if (field < 0 || field > 6) return fail(VFGPU_ERR_INVALID, "vfgpu_set_field: bad field %d", field);
   cudaSetDevice(c->dev);
+  if (field == VFGPU_FIELD_V) c->v32_stale = c->ul_stale = true;
   cudaError_t e = copy_in(c, c->f[field], data, field_len(c, field));
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_set_field");
-  if (field == VFGPU_FIELD_V) c->v32_stale = true;
   return VFGPU_OK;
 }
 
@@ -493,6 +516,7 @@ cudaError_t u_apply_host_pipelined(vfgpu_ctx* c, const double* x, double* y) {
       A.nz = nzs;
       A.bc = c->bcU_bits + lo * plane;
       A.elayer = c->d_elayer + lo;
+      use_unit_lists(A, UnitLists{});  // a sub-grid: the whole grid's lists do not apply
       if (A.cellE) A.cellE += lo * cplane;
       if (A.cflag) A.cflag += lo * cplane;
       e = launch_u_apply<double>(A, p, c->layers, c->stream);
@@ -521,7 +545,8 @@ int vfgpu_u_apply(vfgpu_ctx* c, int precision, const double* x, double* y) {
   cudaSetDevice(c->dev);
   const int64_t n3 = 3 * c->N;
   const bool xdev = is_device_ptr(x), ydev = is_device_ptr(y);
-  cudaError_t e = cudaSuccess;
+  cudaError_t e = u_lists_refresh(c);
+  if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply");
   if (precision == VFGPU_FP64 && !xdev && !ydev && c->nz >= 8) {
     e = u_apply_host_pipelined(c, x, y);
     if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply");
@@ -562,7 +587,8 @@ int vfgpu_u_apply_dev(vfgpu_ctx* c, int precision, const void* x, void* y) {
   if (!is_device_ptr(x) || !is_device_ptr(y))
     return fail(VFGPU_ERR_INVALID, "vfgpu_u_apply_dev: x and y must be device pointers");
   cudaSetDevice(c->dev);
-  cudaError_t e = c->unilateral ? nc_flags(c, c->f[VFGPU_FIELD_U]) : cudaSuccess;
+  cudaError_t e = u_lists_refresh(c);
+  if (e == cudaSuccess && c->unilateral) e = nc_flags(c, c->f[VFGPU_FIELD_U]);
   if (e != cudaSuccess) return cuda_fail(e, "vfgpu_u_apply_dev");
   if (precision == VFGPU_FP64) {
     e = launch_u_apply<double>(u_args<double>(c, (const double*)x, c->f[VFGPU_FIELD_V], (double*)y,
