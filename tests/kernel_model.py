@@ -492,16 +492,18 @@ def u_apply_tiled(x, v, bcbits, n, h, lam, mu, eta, TY=8, zc=5, element=None, nc
                         continue
                     p0 = np.zeros(3)
                     p1 = np.zeros(3)
-                    for dw in range(2):
+                    for dw in range(2):  # x-sums (left element's corner + own) per row
                         ew, j = w - 1 + dw, 1 - dw
                         if ew < 0 or ew >= TY:
                             continue
-                        for dl in range(2):
-                            el, i = l - 1 + dl, 1 - dl
-                            if el < 0 or el >= 32:
-                                continue
-                            p0 += sc[(i + 2 * j) * 3:(i + 2 * j) * 3 + 3, ew, el]
-                            p1 += sc[(i + 2 * j + 4) * 3:(i + 2 * j + 4) * 3 + 3, ew, el]
+                        for kk, acc in ((0, p0), (1, p1)):
+                            xs = np.zeros(3)
+                            for dl in range(2):
+                                el, i = l - 1 + dl, 1 - dl
+                                if 0 <= el < 32:
+                                    a = i + 2 * j + 4 * kk
+                                    xs = xs + sc[a * 3:a * 3 + 3, ew, el]
+                            acc += xs
                     if k >= z0:
                         emit(l, w, X, Y, k, carry[tid, si] + p0)
                     carry[tid, si] = p1

@@ -21,6 +21,17 @@ constexpr int U_TY = 8, U64_TY = VFGPU_U64_TY, V_TY = kVTileY;
 #define VFGPU_U64_MINB 1
 #endif
 constexpr int U64_MINB = VFGPU_U64_MINB;
+// The fixed-weight U kernel of a split launch (UOpConst: fewer registers, and the x-summed
+// corner buffers leave room for both stages) takes more blocks per SM than the general
+// one: 2 (FP64) and 3 (FP32) measured 0.117 / 0.089 ms at 129^3 on the penny field against
+// 0.134 / 0.091 ms with the general kernel's 1 and 2.
+#ifndef VFGPU_U64C_MINB
+#define VFGPU_U64C_MINB 2
+#endif
+#ifndef VFGPU_U32C_MINB
+#define VFGPU_U32C_MINB 3
+#endif
+constexpr int U64C_MINB = VFGPU_U64C_MINB, U32C_MINB = VFGPU_U32C_MINB;
 // V tiles carry 2 stages of 27 coefficients per cell in shared memory: 75 KB (FP32,
 // 2 CTAs per SM) or 150 KB (FP64, 1 CTA per SM).
 constexpr int V64_MINB = 1, V32_MINB = 2;
@@ -52,11 +63,11 @@ cudaError_t apply_kernel_attributes() {
   std::lock_guard<std::mutex> lk(m);
   cudaError_t e = set_tile_attributes<UOp<double>, U64_TY, U64_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOp<double, true>, U64_TY, U64_MINB>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double>, U64_TY, U64_MINB>();
-  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double, true>, U64_TY, U64_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double>, U64_TY, U64C_MINB>();
+  if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double, true>, U64_TY, U64C_MINB>();
   if constexpr (!kU32Packed) {
-    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float>, U32_TY, U32_MINB>();
-    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float, true>, U32_TY, U32_MINB>();
+    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float>, U32_TY, U32C_MINB>();
+    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float, true>, U32_TY, U32C_MINB>();
   }
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
@@ -212,10 +223,10 @@ __device__ __forceinline__ int unit_type(const uint8_t* f, int z, int nez) {
 // One block of 1024 threads builds both unit lists of a plan from its layer flags:
 // per tile column (one thread each) the runs of equal unit type up its nz planes,
 // counted, offset by prefix sums over the columns in tile order, written; then, per
-// list and block b of the apply launch, the run holding the list's unit U b / ncta
-// (binary search on the runs' unit offsets).
+// list l and block b of its wave of ncta_l blocks, the run holding the list's unit
+// U b / ncta_l (binary search on the runs' unit offsets).
 __global__ void __launch_bounds__(1024) unit_lists_kernel(const uint8_t* __restrict__ cls, int nz,
-                                                          int ncol, int ncta, int4* __restrict__ runs0,
+                                                          int ncol, int ncta0, int ncta1, int4* __restrict__ runs0,
                                                           int4* __restrict__ runs1, int* __restrict__ start0,
                                                           int* __restrict__ start1, int* __restrict__ total) {
   extern __shared__ int sh[];  // [4][ncol] counts, then 32 ints of scan scratch
@@ -256,8 +267,8 @@ __global__ void __launch_bounds__(1024) unit_lists_kernel(const uint8_t* __restr
     }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < 2 * ncta; i += blockDim.x) {
-    const int l = i / ncta, b = i % ncta, nrun = tot[l];
+  for (int i = threadIdx.x; i < ncta0 + ncta1; i += blockDim.x) {
+    const int l = i < ncta0 ? 0 : 1, b = l ? i - ncta0 : i, ncta = l ? ncta1 : ncta0, nrun = tot[l];
     const int64_t ub = (int64_t)tot[2 + l] * b / ncta;
     int lo = 0, hi = nrun - 1;
     while (lo < hi) {  // the last run whose first unit is <= ub
@@ -278,8 +289,8 @@ size_t unit_lists_bytes(const TilePlan& p, int nz) {
   const int64_t ncol = (int64_t)p.ntx * p.nty;
   if (nz < 2 || ncol > kMaxListCols) return 0;
   auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
-  return up(ncol * (nz - 1)) + 2 * up(ncol * nz * sizeof(int4)) + 2 * up(p.ncta * sizeof(int)) +
-         up(2 * sizeof(int));
+  return up(ncol * (nz - 1)) + 2 * up(ncol * nz * sizeof(int4)) + up(p.ncta0 * sizeof(int)) +
+         up(p.ncta * sizeof(int)) + up(2 * sizeof(int));
 }
 
 UnitLists unit_lists_carve(void* base, const TilePlan& p, int nz) {
@@ -296,7 +307,7 @@ UnitLists unit_lists_carve(void* base, const TilePlan& p, int nz) {
   }
   for (int l = 0; l < 2; l++) {
     L.start[l] = reinterpret_cast<int*>(q);
-    q += up(p.ncta * sizeof(int));
+    q += up((l ? p.ncta : p.ncta0) * sizeof(int));
   }
   L.total = reinterpret_cast<int*>(q);
   return L;
@@ -324,13 +335,16 @@ cudaError_t build_unit_lists(const double* v, int nx, int ny, int nz, const Tile
   if (e != cudaSuccess) return e;
   const int ncol = p.ntx * p.nty;
   unit_lists_kernel<<<1, 1024, (4 * ncol + 32) * sizeof(int), s>>>(
-      L.cls, nz, ncol, p.ncta, L.runs[0], L.runs[1], L.start[0], L.start[1], L.total);
+      L.cls, nz, ncol, p.ncta0, p.ncta, L.runs[0], L.runs[1], L.start[0], L.start[1], L.total);
   return cudaGetLastError();
 }
 
 TilePlan u_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
-  if (prec_bytes == 8) return tile_plan(nx, ny, nz, U64_TY, 3, U64_MINB, num_sms);
-  return tile_plan(nx, ny, nz, U32_TY, 3, U32_MINB, num_sms);
+  TilePlan p = tile_plan(nx, ny, nz, prec_bytes == 8 ? U64_TY : U32_TY, 3,
+                         prec_bytes == 8 ? U64_MINB : U32_MINB, num_sms);
+  const TilePlan q = tile_plan(nx, ny, nz, p.ty, 3, prec_bytes == 8 ? U64C_MINB : U32C_MINB, num_sms);
+  p.ncta0 = q.ncta;
+  return p;
 }
 TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   return tile_plan(nx, ny, nz, V_TY, 1, prec_bytes == 8 ? V64_MINB : V32_MINB, num_sms);
@@ -342,8 +356,9 @@ cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& 
   if (A.cflag) return launch_tile_apply<UOpNC<double>, U64_TY, 1>(A, p, L, s);
   if (A.ur[0] && A.ur[1]) {
     if (cubic(A))
-      return launch_tile_apply_split<UOpConst<double, true>, UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
-    return launch_tile_apply_split<UOpConst<double>, UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
+      return launch_tile_apply_split<UOpConst<double, true>, UOp<double, true>, U64_TY, U64C_MINB, U64_MINB>(
+          A, p, L, s);
+    return launch_tile_apply_split<UOpConst<double>, UOp<double>, U64_TY, U64C_MINB, U64_MINB>(A, p, L, s);
   }
   if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
   return launch_tile_apply<UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
@@ -357,8 +372,8 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
   if constexpr (!kU32Packed) {
     if (A.ur[0] && A.ur[1]) {
       if (cubic(A))
-        return launch_tile_apply_split<UOpConst<float, true>, U32OpC, U32_TY, U32_MINB>(A, p, L, s);
-      return launch_tile_apply_split<UOpConst<float>, U32Op, U32_TY, U32_MINB>(A, p, L, s);
+        return launch_tile_apply_split<UOpConst<float, true>, U32OpC, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
+      return launch_tile_apply_split<UOpConst<float>, U32Op, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
     }
   }
   if (cubic(A)) return launch_tile_apply<U32OpC, U32_TY, U32_MINB>(A, p, L, s);

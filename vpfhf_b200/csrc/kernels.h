@@ -25,7 +25,7 @@ cudaError_t wait_selftest(long long cycles, int complete, int* timed_out);
 struct UnitLists {
   uint8_t* cls = nullptr;  // [ntx nty][nz - 1]; null: no lists for this plan
   int4* runs[2] = {};      // [ntx nty nz] each
-  int* start[2] = {};      // [ncta] each
+  int* start[2] = {};      // [ncta0], [ncta]
   int* total = nullptr;    // [2]
 };
 // Device bytes of a plan's unit lists; 0 when the grid has more tile columns than the

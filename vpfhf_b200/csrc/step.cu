@@ -297,7 +297,7 @@ static cudaError_t u_apply32(vfgpu_ctx* c, const float* x, float* y, const int* 
 static int dots_of(const vfgpu_ctx* c, const TilePlan& p) { return tile_dot_count(p, c->nx, c->ny, c->nz); }
 // The U applies of a split launch (unit lists) write a second wave's partials.
 static int u_dots_of(const vfgpu_ctx* c, const TilePlan& p, int prec_bytes) {
-  return dots_of(c, p) + (u_lists_on(c, prec_bytes) ? p.ncta : 0);
+  return dots_of(c, p) + (u_lists_on(c, prec_bytes) ? p.ncta0 : 0);
 }
 
 // Which CG call sites let the operator apply accumulate p.w (bit k-1 for call site k:

@@ -62,13 +62,15 @@ template <int TY, int EPT = 1> struct Tile {
 // Shared memory: a ring of 4 node planes [4][NIN][BY][BX] (during layer k: planes k,
 // k+1 read by the elements, plane k read by the node finish after the layer barrier,
 // plane k+2 landing, plane k+3 in flight into the slot plane k-1 left) and SCS buffers
-// of element corner contributions [SCS][8*NC][TY][32]:
+// of element corner contributions summed along x [SCS][4*NC][TY][33] (corner pair
+// j + 2 kk of element row w at node column l: the i = 1 corner of element l - 1 plus the
+// i = 0 corner of element l, added in registers after a warp shuffle):
 // two (layer k + 1's elements are written while layer k's node sums still read) where
 // MINB blocks of that size fit an SM, else one, with a second barrier per layer.
 constexpr int kRing = 4;
 template <class Op, int TY, int SCS = 2> constexpr size_t tile_base_bytes() {
   using T = typename Op::T;
-  return sizeof(T) * (kRing * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 8 * Op::NC * 32 * TY);
+  return sizeof(T) * (kRing * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 4 * Op::NC * 33 * TY);
 }
 template <class Op, int TY, int MINB> constexpr int sc_stages() {
   return (Op::CV > 0 || MINB * (tile_base_bytes<Op, TY, 2>() + 1024) <= 228 * 1024) ? 2 : 1;
@@ -165,7 +167,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   constexpr int NC = Op::NC, NIN = Op::NIN;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sx = reinterpret_cast<T*>(smem_raw);  // [kRing][NIN][BY][BX]
-  T* sc = sx + kRing * NIN * G::BY * G::BX;  // [SCS][8*NC][TY][32]
+  T* sc = sx + kRing * NIN * G::BY * G::BX;  // [SCS][4*NC][TY][33]
   constexpr int SCS = sc_stages<Op, TY, MINB>();
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
@@ -202,7 +204,22 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   const int kf = max(z0 - 1, 0), kl = min(z1, nz - 1) - 1;
 
 #define SXA(buf, comp, w, l) sx[(((buf) * NIN + (comp)) * G::BY + (w)) * G::BX + (l)]
-#define SCA(b, q, w, l) sc[(((b) * 8 * NC + (q)) * TY + (w)) * 32 + (l)]
+#define SCA(b, q, w, l) sc[(((b) * 4 * NC + (q)) * TY + (w)) * 33 + (l)]
+
+  // The x-sums of element row w's corner contributions yc[a], a = i + 2 j + 4 kk, into
+  // corner-pair rows q = j + 2 kk: node column lane gets (element lane - 1, i = 1) +
+  // (element lane, i = 0), column 32 the i = 1 corners of element 31 (whole warp).
+  auto store_xsums = [&](int sbuf, int w, const T (&yc)[8][NC]) {
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int c = 0; c < NC; c++) {
+        const T own = yc[2 * q][c], rt = yc[2 * q + 1][c];
+        const T left = __shfl_up_sync(0xffffffffu, rt, 1);
+        SCA(sbuf, q * NC + c, w, lane) = lane > 0 ? left + own : own;
+        if (lane == 31) SCA(sbuf, q * NC + c, w, 32) = rt;
+      }
+  };
 
   // issue the asynchronous copies of node plane kz into ring slot buf (one group)
   auto fetch_plane = [&](int buf, int kz) {
@@ -312,10 +329,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
 #pragma unroll
           for (int c = 0; c < NC; c++) yc[a][c] = T(0);
       }
-#pragma unroll
-      for (int a = 0; a < 8; a++)
-#pragma unroll
-        for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, wy, lane) = yc[a][c];
+      store_xsums(sb, wy, yc);
     } else {
       // element rows EPT*wy + e, e < EPT (node rows EPT*wy .. EPT*wy + EPT)
       int ey[EPT];
@@ -351,11 +365,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
             for (int c = 0; c < NC; c++) yc[e][a][c] = T(0);
       }
 #pragma unroll
-      for (int e = 0; e < EPT; e++)
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-#pragma unroll
-          for (int c = 0; c < NC; c++) SCA(sb, a * NC + c, EPT * wy + e, lane) = yc[e][a][c];
+      for (int e = 0; e < EPT; e++) store_xsums(sb, EPT * wy + e, yc[e]);
     }
     cp_async_wait_all();  // this thread's copies of plane k+2 have landed
     if constexpr (Op::CV > 0) {
@@ -392,14 +402,9 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
         const int ew = w - 1 + dw, j = 1 - dw;
         if (ew < 0 || ew >= TY) continue;
 #pragma unroll
-        for (int dl = 0; dl < 2; dl++) {
-          const int el = l - 1 + dl, i = 1 - dl;
-          if (el < 0 || el >= 32) continue;
-#pragma unroll
-          for (int c = 0; c < NC; c++) {
-            p0[c] += SCA(sb, (i + 2 * j) * NC + c, ew, el);
-            p1[c] += SCA(sb, (i + 2 * j + 4) * NC + c, ew, el);
-          }
+        for (int c = 0; c < NC; c++) {
+          p0[c] += SCA(sb, j * NC + c, ew, l);
+          p1[c] += SCA(sb, (j + 2) * NC + c, ew, l);
         }
       }
       if (k >= z0) {
@@ -513,6 +518,8 @@ __global__ void __launch_bounds__(256) seam_fixup_kernel(const typename Op::Args
 struct TilePlan {
   int ty, ntx, nty;
   int ncta;
+  int ncta0;  // the wave of a split launch's unit list 0 (UOpConst), which may take more
+              // blocks per SM; = ncta otherwise
   size_t seamX, seamY;
 };
 
@@ -524,6 +531,7 @@ inline TilePlan tile_plan(int nx, int ny, int nz, int ty, int nc, int ctas_per_s
   const int slots = num_sms * ctas_per_sm, tiles = p.ntx * p.nty;
   const int64_t units = (int64_t)tiles * nz;
   p.ncta = (int)std::max<int64_t>(1, std::min<int64_t>(slots, units));
+  p.ncta0 = p.ncta;
   p.seamX = (size_t)(p.ntx - 1) * nz * ny * 4 * nc;
   p.seamY = (size_t)(p.nty - 1) * nz * nx * 2 * nc;
   return p;
@@ -582,31 +590,32 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
 }
 
 
-// An operator split over unit lists 0 (OpF) and 1 (OpG, which also finishes the seams):
-// one wave of blocks for each list in turn, then the seam fix-up.  With A.dot the x.y
-// block partials go to A.dot[0, ncta) (OpF), [ncta, 2 ncta) (OpG) and from 2 ncta on
-// (seams): tile_dot_count + ncta of them.
-template <class OpF, class OpG, int TY, int MINB>
+// An operator split over unit lists 0 (OpF, MINBF blocks per SM, a wave of p.ncta0) and 1
+// (OpG, MINB, a wave of p.ncta; it also finishes the seams): the two waves in turn, then
+// the seam fix-up.  With A.dot the x.y block partials go to A.dot[0, ncta0) (OpF),
+// [ncta0, ncta0 + ncta) (OpG) and from ncta0 + ncta on (seams): tile_dot_count + ncta0
+// of them.
+template <class OpF, class OpG, int TY, int MINBF, int MINB>
 cudaError_t launch_tile_apply_split(typename OpG::Args A, const TilePlan& p, const LayerTable& L,
                                     cudaStream_t s) {
   static_assert(OpF::LIST == 0 && OpG::LIST == 1 && OpF::EPT == 1 && OpG::EPT == 1, "unit lists 0, 1");
   A.ntx = p.ntx;
   A.nty = p.nty;
-  constexpr size_t smemF = tile_smem_bytes<OpF, TY, MINB>(), smemG = tile_smem_bytes<OpG, TY, MINB>();
-  cudaError_t ea = set_tile_attributes<OpF, TY, MINB>();
+  constexpr size_t smemF = tile_smem_bytes<OpF, TY, MINBF>(), smemG = tile_smem_bytes<OpG, TY, MINB>();
+  cudaError_t ea = set_tile_attributes<OpF, TY, MINBF>();
   if (ea == cudaSuccess) ea = set_tile_attributes<OpG, TY, MINB>();
   if (ea != cudaSuccess) return ea;
-  dim3 grid(p.ncta), block(32, TY);
-  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = 2 * p.ncta;
+  const dim3 block(32, TY);
+  const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = p.ncta0 + p.ncta;
   typename OpG::Args AG = A;
-  if (AG.dot) AG.dot += p.ncta;
+  if (AG.dot) AG.dot += p.ncta0;
   if (A.dot) {
-    tile_apply_kernel<OpF, TY, MINB, true><<<grid, block, smemF, s>>>(A, L);
-    tile_apply_kernel<OpG, TY, MINB, true><<<grid, block, smemG, s>>>(AG, L);
+    tile_apply_kernel<OpF, TY, MINBF, true><<<p.ncta0, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpG, TY, MINB, true><<<p.ncta, block, smemG, s>>>(AG, L);
     if (sblocks > 0) seam_fixup_kernel<OpG, true><<<sblocks, 256, 0, s>>>(A, TY, base);
   } else {
-    tile_apply_kernel<OpF, TY, MINB, false><<<grid, block, smemF, s>>>(A, L);
-    tile_apply_kernel<OpG, TY, MINB, false><<<grid, block, smemG, s>>>(AG, L);
+    tile_apply_kernel<OpF, TY, MINBF, false><<<p.ncta0, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpG, TY, MINB, false><<<p.ncta, block, smemG, s>>>(AG, L);
     if (sblocks > 0) seam_fixup_kernel<OpG, false><<<sblocks, 256, 0, s>>>(A, TY, base);
   }
   return cudaGetLastError();

@@ -259,7 +259,7 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   {
     int nd = 1;
     for (const TilePlan* p : {&c->plan64, &c->plan32, &c->vplan64, &c->vplan32})
-      nd = std::max(nd, tile_dot_count(*p, c->nx, c->ny, c->nz) + p->ncta);  // U: split launch
+      nd = std::max(nd, tile_dot_count(*p, c->nx, c->ny, c->nz) + p->ncta0);  // U: split launch
     ALLOC(c->d_dot, (size_t)nd * sizeof(double));
   }
   ALLOC(c->bcU_kind, 3 * c->N);
