@@ -315,9 +315,9 @@ def run_gpu(args):
     alg_bytes = 56.0 * nodes
     # FP64 instructions per element of the apply on this workload (nearly every element
     # has a constant nodal phase field and takes the fixed-weight element), counted by ncu
-    # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells, one launch
-    # of this workload under ncu --set full); an FMA is 2 flops
-    dfma_el, dadd_el, dmul_el = 44.7, 163.1, 26.5
+    # (smsp__sass_thread_inst_executed_op_{dfma,dadd,dmul}_pred_on / cells, the
+    # fixed-weight launch of this workload under ncu --set full); an FMA is 2 flops
+    dfma_el, dadd_el, dmul_el = 44.1, 163.7, 25.6
     instr_el = dfma_el + dadd_el + dmul_el
     flops_el = 2 * dfma_el + dadd_el + dmul_el
     f64_peak = fp_peak_tflops(torch, "f64")
@@ -339,17 +339,20 @@ def run_gpu(args):
                    "parallelism": f"replicas x{world}", "l2": "flushed between timed steps"},
         "e2e": {"value": round(N3 * world / (e2e_ms * 1e-3) / 1e9, 3), "unit": "GDOF/s",
                 "h2d_bytes_per_step": N3 * 8, "d2h_bytes_per_step": N3 * 8},
-        "gpu_launches": 2 * args.steps,
+        "gpu_launches": 3 * args.steps,  # per apply: the two unit-list waves and the seam fix-up
         "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (ms64 * 1e-3) / 1e9, 1),
                      "peak": hbm, "unit": "GB/s",
                      "frac": round(alg_bytes / (ms64 * 1e-3) / 1e9 / hbm, 4),
-                     "traffic": 114.0e6 if n == N_EDGE else None,
-                     "note": "traffic: ncu dram read+write per launch at 129^3 (86.4 + 27.6 MB; "
-                             "part of the 51.5 MB output is still in the 126 MB L2 when the "
-                             "launch ends); the kernel is bound by neither HBM nor the FP64 pipe "
-                             "(compute_roofline) but by the latency of its tile schedule at 8 "
-                             "warps per SM (ncu: FP64 pipe 23 %, top stalls fixed-latency "
-                             "dependencies, plane loads, the layer barrier)"},
+                     "traffic": 108.7e6 if n == N_EDGE else None,
+                     "note": "achieved: algorithmic bytes over the whole apply (three launches: "
+                             "the fixed-weight wave over the intact (tile, plane) units, the "
+                             "general wave over the rest, the seam fix-up); traffic: ncu dram "
+                             "read+write of the fixed-weight launch at 129^3 (84.3 + 24.4 MB; "
+                             "part of the output is still in the 126 MB L2 when it ends).  The "
+                             "kernel is bound by neither HBM nor the FP64 pipe "
+                             "(compute_roofline) but by the latency of its tile schedule "
+                             "(ncu: 16 warps per SM, issue active 54 %, FP64 pipe 34 %, top "
+                             "stalls fixed-latency dependencies)"},
         "compute_roofline": {
             "pipe": "fp64 CUDA cores",
             "fp64_instructions_per_element": {"dfma": dfma_el, "dadd": dadd_el, "dmul": dmul_el},
@@ -438,12 +441,14 @@ def run_serving(args):
     {17, 33, 65, 97}, 1-4 random penny cracks, E ~ U[5,30] GPa, nu ~ U[0.15,0.35], AT1/AT2,
     5 AM iterations each, multigrid U solve on the two larger grids) through the library's
     request loop.  The FP64 capacity is
-    measured closed-loop on the first 128 problems; the full stream then arrives as a
+    measured closed-loop on the whole stream; the stream then arrives as a
     seeded Poisson process at 0.8x that capacity, once in FP64 and once mixed (same
     arrival times).  Latency = completion - arrival."""
     from vpfhf_b200.serve import poisson_arrivals, run_stream, serving_stream
     count, workers = args.serve_problems, args.serve_workers
-    cal = serving_stream(count=min(128, count), precision="fp64")
+    # capacity closed-loop on the whole stream: a sample's random mix of grid sizes moved
+    # it by +-10 %, and the open-loop latencies at 0.8x with it
+    cal = serving_stream(count=count, precision="fp64")
     _, cap = run_stream(cal, None, workers=workers)
     rate = 0.8 * cap["throughput"]
     arr = poisson_arrivals(count, rate)

@@ -160,6 +160,17 @@ int vfgpu_set_bc(vfgpu_ctx* ctx, const vfgpu_bc bcU[3], const vfgpu_bc* bcV);
 #define VFGPU_UNILATERAL_NOCOMPRESSION 1
 int vfgpu_set_unilateral(vfgpu_ctx* ctx, int type);
 
+/* How the ctx's U applies split their work (no reference counterpart: a launch-shape
+ * choice with bit-identical results).  ON: two waves -- the (tile, plane) units whose
+ * elements all have a constant nodal phase field on a kernel with the fixed-weight element
+ * alone, the rest on the general one; OFF: one wave over all units; AUTO (the default):
+ * ON from a grid size per precision where it measured faster.  Grids with more than 2048
+ * 32 x 8 element tiles per plane and NOCOMPRESSION always take one wave. */
+#define VFGPU_U_SPLIT_AUTO 0
+#define VFGPU_U_SPLIT_OFF 1
+#define VFGPU_U_SPLIT_ON 2
+int vfgpu_set_u_split(vfgpu_ctx* ctx, int mode);
+
 /* In-situ stresses (-insitumin / -insitumax, VFCommon.c:132-149): Voigt
  * (s11, s22, s33, s23, s13, s12) at z = 0 and z = lz, linear in z between;
  * insitumax NULL = insitumin; insitumin NULL switches them off (hasInsitu).

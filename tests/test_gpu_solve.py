@@ -234,10 +234,12 @@ def test_runtest1_on_gpu(cuda, precision):
             assert m["surface"] == pytest.approx(r["surface"], rel=post), t
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_penny41_am_loop(cuda, precision):
+@pytest.mark.parametrize("precision,split", [("fp64", "auto"), ("mixed", "auto"), ("fp64", "on"),
+                                             ("mixed", "on")])
+def test_penny41_am_loop(cuda, precision, split):
     """5 AM iterations of the 41^3 pressurized penny crack against the oracle fixture:
-    relative energy error <= 1e-6 and v L-inf <= 1e-4 (the parity bar)."""
+    relative energy error <= 1e-6 and v L-inf <= 1e-4 (the parity bar); with the U
+    applies in one wave (auto at this size) and split by phase field (on)."""
     import sys
     sys.path.insert(0, os.path.join(HERE, "golden"))
     import vpfhf_b200 as vg
@@ -253,6 +255,7 @@ def test_penny41_am_loop(cuda, precision):
     ctx = vg.VFContext(n, P["l"], dict(E=P["E"], nu=P["nu"], Gc=P["Gc"]), epsilon=P["epsilon"],
                        eta=P["eta"], atnum=P["atnum"], pressurize=True)
     ctx.set_bc(vg.rollers())
+    ctx.set_u_split(split)
     ctx.set_field("V", v0)
     ctx.set_field("pressure", np.full(ctx.N, P["p"]))
     ctx.time_step_prepare()

@@ -123,11 +123,11 @@ def test_u_apply_constant_phase_field_elements(cuda, oracle_mod, n, l, cellE):
 
 @pytest.mark.parametrize("n,l", [((66, 40, 35), (2.0, 1.3, 1.1)), ((23, 19, 45), (1.0, 0.8, 2.0))])
 def test_unit_lists_split(cuda, oracle_mod, n, l):
-    """The ctx's U applies split the (tile, plane) units by phase field over the
-    fixed-weight kernel and the general one (unit lists rebuilt when v changes):
-    bit-identical to the plain split of vfgpu_u_apply_noalloc and of the host slab
-    pipeline (sub-grids, no lists), and following each change of v (intact field with a
-    cracked blob, random, intact, blob again); FP32 at 2e-6 against the oracle."""
+    """U applies split by phase field (vfgpu_set_u_split on: the (tile, plane) units over
+    the fixed-weight kernel and the general one, unit lists rebuilt when v changes):
+    bit-identical to one wave (split off, FP64 and FP32), to vfgpu_u_apply_noalloc and to
+    the host slab pipeline (sub-grids, one wave), following each change of v (intact field
+    with a cracked blob, random, intact, blob again); FP32 at 2e-6 against the oracle."""
     import ctypes as C
 
     import vpfhf_b200 as vg
@@ -145,7 +145,12 @@ def test_unit_lists_split(cuda, oracle_mod, n, l):
     xd = torch.from_numpy(x).cuda()
     for v in (blob, rng.uniform(0, 1, o.N), np.ones(o.N), blob):
         ctx.set_field("V", v)
+        ctx.set_u_split("off")
+        y1, y1_32 = ctx.u_apply(xd, vg.FP64).cpu().numpy(), ctx.u_apply(x, vg.MIXED)
+        ctx.set_u_split("on")
         y = ctx.u_apply(xd, vg.FP64).cpu().numpy()
+        assert np.array_equal(y, y1)
+        assert np.array_equal(ctx.u_apply(x, vg.MIXED), y1_32)
         assert np.array_equal(ctx.u_apply(x, vg.FP64), y)
         vd, yna = torch.from_numpy(v).cuda(), torch.full_like(xd, float("nan"))
         torch.cuda.synchronize()

@@ -117,6 +117,13 @@ class VFContext:
             kind = {"none": 0, "nocompression": 1}[kind.lower()]
         _abi.check(self.L.vfgpu_set_unilateral(self.h, int(kind)), "vfgpu_set_unilateral")
 
+    def set_u_split(self, mode):
+        """How U applies split their work: "auto" (default), "off" (one wave) or "on"
+        (fixed-weight wave over the intact units, general wave over the rest)."""
+        if isinstance(mode, str):
+            mode = {"auto": 0, "off": 1, "on": 2}[mode.lower()]
+        _abi.check(self.L.vfgpu_set_u_split(self.h, int(mode)), "vfgpu_set_u_split")
+
     def set_insitu(self, smin, smax=None):
         """In-situ stresses (Voigt s11 s22 s33 s23 s13 s12) at z = 0 and z = lz
         (-insitumin / -insitumax); None switches them off."""

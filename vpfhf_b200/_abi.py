@@ -134,6 +134,7 @@ _SIGS = {
     "vfgpu_set_bc": [C.c_void_p, C.POINTER(BC), C.POINTER(BC)],
     "vfgpu_set_insitu": [C.c_void_p, C.c_void_p, C.c_void_p],
     "vfgpu_set_unilateral": [C.c_void_p, C.c_int],
+    "vfgpu_set_u_split": [C.c_void_p, C.c_int],
     "vfgpu_set_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_get_field": [C.c_void_p, C.c_int, C.c_void_p],
     "vfgpu_u_apply": [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p],

@@ -284,6 +284,23 @@ __global__ void __launch_bounds__(1024) unit_lists_kernel(const uint8_t* __restr
 }
 
 constexpr int kMaxListCols = 2048;  // tile columns the one-block list builder takes
+// Grids below this many (tile, plane) units keep the plain split: there the general
+// wave's latency (about one segment) and the list build cost more than the fixed-weight
+// kernel saves.  Measured on the penny field, split against plain, us per apply FP64 /
+// FP32: 41^3 35.8 / 29.7 against 25.7 / 23.6; 65^3 44.1 / 35.9 against 44.0 / 29.5;
+// 81^3 54.3 / 46.0 against 60.4 / 42.1; 97^3 64.5 / 56.3 against 72.7 / 52.2; 113^3
+// 93.3 / 72.8 against 109.6 / 74.8; 161^3 189.4 / 140.3 against 247.0 / 154.7.
+#ifndef VFGPU_U64_LISTS_MIN_UNITS
+#define VFGPU_U64_LISTS_MIN_UNITS 2000
+#endif
+#ifndef VFGPU_U32_LISTS_MIN_UNITS
+#define VFGPU_U32_LISTS_MIN_UNITS 6000
+#endif
+
+bool unit_lists_pay(const TilePlan& p, int nz, int prec_bytes) {
+  const int64_t min_units = prec_bytes == 8 ? VFGPU_U64_LISTS_MIN_UNITS : VFGPU_U32_LISTS_MIN_UNITS;
+  return (int64_t)p.ntx * p.nty * nz >= min_units;
+}
 
 size_t unit_lists_bytes(const TilePlan& p, int nz) {
   const int64_t ncol = (int64_t)p.ntx * p.nty;

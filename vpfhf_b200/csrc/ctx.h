@@ -27,6 +27,7 @@ struct vfgpu_ctx {
   void* d_ul = nullptr;
   vfgpu::UnitLists ul64, ul32;
   bool ul_stale = true;
+  int u_split = VFGPU_U_SPLIT_AUTO;
   vfgpu::DevParams* d_params = nullptr;  // device copy of layers / eta / aeps
   float* d_cellE = nullptr;     // NC or null
   bool have_mat = false;

@@ -32,6 +32,9 @@ struct UnitLists {
 // one-block list builder takes (its applies then split all units).
 size_t unit_lists_bytes(const TilePlan& p, int nz);
 UnitLists unit_lists_carve(void* base, const TilePlan& p, int nz);
+// Whether the split measured faster than one wave at this plan's size in precision
+// prec_bytes (8 or 4): the VFGPU_U_SPLIT_AUTO rule.
+bool unit_lists_pay(const TilePlan& p, int nz, int prec_bytes);
 // Rebuilds the lists from the FP64 phase field v (two launches on s).
 cudaError_t build_unit_lists(const double* v, int nx, int ny, int nz, const TilePlan& p,
                              const UnitLists& L, cudaStream_t s);

@@ -138,21 +138,30 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   A.eta = T(c->vf.eta);
   A.P = c->d_params;
   A.cflag = c->unilateral ? c->d_cflag : nullptr;
-  use_unit_lists(A, sizeof(T) == 8 ? c->ul64 : c->ul32);
-  if (A.cflag) use_unit_lists(A, UnitLists{});  // NOCOMPRESSION takes the plain split
+  use_unit_lists(A, u_lists_on(c, (int)sizeof(T)) ? (sizeof(T) == 8 ? c->ul64 : c->ul32) : UnitLists{});
   return A;
 }
+// The split mode and the grid call for the lists in this precision (NOCOMPRESSION aside).
+static bool u_lists_wanted(const vfgpu_ctx* c, int prec_bytes) {
+  const TilePlan& p = prec_bytes == 8 ? c->plan64 : c->plan32;
+  if (!(prec_bytes == 8 ? c->ul64.cls : c->ul32.cls)) return false;
+  if (c->u_split == VFGPU_U_SPLIT_ON) return true;
+  return c->u_split == VFGPU_U_SPLIT_AUTO && unit_lists_pay(p, c->nz, prec_bytes);
+}
+
 cudaError_t u_lists_refresh(vfgpu_ctx* c) {
   if (!c->ul_stale) return cudaSuccess;
   const double* v = c->f[VFGPU_FIELD_V];
-  cudaError_t e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan64, c->ul64, c->stream);
-  if (e == cudaSuccess) e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan32, c->ul32, c->stream);
+  cudaError_t e = cudaSuccess;
+  if (u_lists_wanted(c, 8)) e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan64, c->ul64, c->stream);
+  if (e == cudaSuccess && u_lists_wanted(c, 4))
+    e = build_unit_lists(v, c->nx, c->ny, c->nz, c->plan32, c->ul32, c->stream);
   if (e == cudaSuccess) c->ul_stale = false;
   return e;
 }
 
 bool u_lists_on(const vfgpu_ctx* c, int prec_bytes) {
-  return !c->unilateral && (prec_bytes == 8 ? c->ul64.cls : c->ul32.cls) != nullptr;
+  return !c->unilateral && u_lists_wanted(c, prec_bytes);
 }
 
 template UApplyArgs<double> u_args<double>(vfgpu_ctx*, const double*, const double*, double*,
@@ -395,6 +404,18 @@ int vfgpu_set_unilateral(vfgpu_ctx* c, int type) {
   }
   if (type != c->unilateral) c->gen++;  // captured CG graphs launch the other operator kernel
   c->unilateral = type;
+  return VFGPU_OK;
+}
+
+int vfgpu_set_u_split(vfgpu_ctx* c, int mode) {
+  if (!c) return fail(VFGPU_ERR_INVALID, "vfgpu_set_u_split: null ctx");
+  if (mode != VFGPU_U_SPLIT_AUTO && mode != VFGPU_U_SPLIT_OFF && mode != VFGPU_U_SPLIT_ON)
+    return fail(VFGPU_ERR_INVALID, "vfgpu_set_u_split: bad mode %d", mode);
+  if (mode != c->u_split) {
+    c->u_split = mode;
+    c->ul_stale = true;  // lists of a precision that was off were not kept up to date
+    c->gen++;            // captured CG graphs launch the other kernels
+  }
   return VFGPU_OK;
 }
 
