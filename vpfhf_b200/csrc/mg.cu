@@ -1048,6 +1048,7 @@ int mgcg(vfgpu_ctx* c, const double* b, double* x, double* r, double* p, double*
   outer.elayer = c->d_elayer;
   outer.cellE = c->d_cellE;
   outer.cflag = c->unilateral ? c->d_cflag : nullptr;
+  outer.ul = u_lists_on(c, 8) ? c->ul64 : UnitLists{};
   while (!*reason && e == cudaSuccess) {
     e = level_apply<double>(c, outer, p, w);
     const double* pa[1] = {p};
