@@ -93,6 +93,18 @@ __device__ __forceinline__ void pack_loop(int64_t n, FP fp, FT ft) {
   for (int64_t c = t0; c < np; c += st) fp(c);
   for (int64_t i = np * W + t0; i < n; i += st) ft(i);
 }
+// The same packs visited from the end of the vectors back (for an elementwise kernel
+// that follows a forward pass over some of the same vectors: it starts on the lines that
+// pass left in L2).
+template <typename T, class FP, class FT>
+__device__ __forceinline__ void pack_loop_rev(int64_t n, FP fp, FT ft) {
+  constexpr int W = Pack<T>::W;
+  const int64_t np = n / W;
+  const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t st = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = np * W + t0; i < n; i += st) ft(i);
+  for (int64_t c = t0; c < np; c += st) fp(np - 1 - c);
+}
 
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) cg_init_kernel(CGVecs<T> v, double* partial) {
@@ -284,12 +296,14 @@ __global__ void __launch_bounds__(RED_THREADS) cg_update_kernel(CGVecs<T> v, CGS
   }
 }
 
-// x += alpha p and p = z + beta p in one pass (the iteration went on: not done).
+// x += alpha p and p = z + beta p in one pass (the iteration went on: not done),
+// back from the end of the vectors: the update kernel's forward pass left the tail of r
+// and dinv in L2.
 template <typename T>
 __global__ void cg_p_kernel(CGVecs<T> v, const CGState* st) {
   if (st->done) return;
   const T a = (T)st->alpha, b = (T)st->beta;
-  pack_loop<T>(
+  pack_loop_rev<T>(
       v.n,
       [&](int64_t c) {
         Pack<T> p = ld16(v.p, c), x = ld16(v.x, c);
