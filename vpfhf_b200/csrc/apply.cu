@@ -31,7 +31,22 @@ constexpr int U64_MINB = VFGPU_U64_MINB;
 #ifndef VFGPU_U32C_MINB
 #define VFGPU_U32C_MINB 3
 #endif
-constexpr int U64C_MINB = VFGPU_U64C_MINB, U32C_MINB = VFGPU_U32C_MINB;
+// The FP32 fixed-weight wave on packed two-lane FP32 (UOpF2Const: two element rows per
+// thread, 4 warps per block; the same bits as the scalar UOpConst<float>) or scalar.
+// Measured at 129^3 on the penny field, whole FP32 apply: packed at 4 blocks per SM
+// (118-126 registers) 0.0855 ms, at 3 0.0905, at 5 (spilling) 0.0879, at 2 0.0981;
+// scalar at 3 blocks per SM 0.0900 ms.
+#ifndef VFGPU_U32C_PACKED
+#define VFGPU_U32C_PACKED 1
+#endif
+#ifndef VFGPU_U32C2_MINB
+#define VFGPU_U32C2_MINB 4
+#endif
+constexpr bool kU32CPacked = VFGPU_U32C_PACKED != 0;
+constexpr int U64C_MINB = VFGPU_U64C_MINB,
+              U32C_MINB = kU32CPacked ? VFGPU_U32C2_MINB : VFGPU_U32C_MINB;
+using U32COp = std::conditional_t<kU32CPacked, UOpF2Const<false>, UOpConst<float>>;
+using U32COpC = std::conditional_t<kU32CPacked, UOpF2Const<true>, UOpConst<float, true>>;
 // V tiles carry 2 stages of 27 coefficients per cell in shared memory: 75 KB (FP32,
 // 2 CTAs per SM) or 150 KB (FP64, 1 CTA per SM).
 constexpr int V64_MINB = 1, V32_MINB = 2;
@@ -66,8 +81,8 @@ cudaError_t apply_kernel_attributes() {
   if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double>, U64_TY, U64C_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<UOpConst<double, true>, U64_TY, U64C_MINB>();
   if constexpr (!kU32Packed) {
-    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float>, U32_TY, U32C_MINB>();
-    if (e == cudaSuccess) e = set_tile_attributes<UOpConst<float, true>, U32_TY, U32C_MINB>();
+    if (e == cudaSuccess) e = set_tile_attributes<U32COp, U32_TY, U32C_MINB>();
+    if (e == cudaSuccess) e = set_tile_attributes<U32COpC, U32_TY, U32C_MINB>();
   }
   if (e == cudaSuccess) e = set_tile_attributes<U32Op, U32_TY, U32_MINB>();
   if (e == cudaSuccess) e = set_tile_attributes<U32OpC, U32_TY, U32_MINB>();
@@ -389,8 +404,8 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
   if constexpr (!kU32Packed) {
     if (A.ur[0] && A.ur[1]) {
       if (cubic(A))
-        return launch_tile_apply_split<UOpConst<float, true>, U32OpC, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
-      return launch_tile_apply_split<UOpConst<float>, U32Op, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
+        return launch_tile_apply_split<U32COpC, U32OpC, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
+      return launch_tile_apply_split<U32COp, U32Op, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
     }
   }
   if (cubic(A)) return launch_tile_apply<U32OpC, U32_TY, U32_MINB>(A, p, L, s);

@@ -35,5 +35,10 @@ __device__ __forceinline__ f2 operator-(f2 a) { return f2(make_float2(-a.v.x, -a
 __device__ __forceinline__ f2& operator+=(f2& a, f2 b) { return a = a + b; }
 __device__ __forceinline__ f2& operator-=(f2& a, f2 b) { return a = a - b; }
 __device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return f2(__ffma2_rn(a.v, b.v, c.v)); }
+// a product kept apart from later adds: formed by a fused multiply-add with zero, which
+// nothing can fuse further (a zero product may come out +0 where the multiply gives -0)
+__device__ __forceinline__ f2 mul_rn(f2 a, f2 b) {
+  return f2(__ffma2_rn(a.v, b.v, make_float2(0.f, 0.f)));
+}
 
 }  // namespace vfgpu

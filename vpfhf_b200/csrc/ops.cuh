@@ -245,6 +245,67 @@ struct UOpF2 {
   }
 };
 
+// UOpConst<float, CUBIC> on two y-adjacent elements per thread, one per lane of the
+// packed FP32 instructions (f2): unit list 0 of the FP32 split.  u_element_const has no
+// contractible multiply-add, so each lane gives the scalar kernel's bits.
+template <bool CUBIC = false> struct UOpF2Const {
+  using T = float;
+  using Args = UApplyArgs<float>;
+  static constexpr int NC = 3, NIN = 4, EPT = 2, CV = 0;
+  static constexpr int LIST = 0;
+  __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
+    UOp<float>::node_src(A, n, src);
+  }
+  __device__ __forceinline__ static void element_multi(const Args& A, const LayerTable& L, int ex,
+                                                       const int (&ey)[2], int ez, const bool (&ok)[2],
+                                                       const T (&in)[2][8][NIN], T (&out)[2][8][NC]) {
+    f2 xn[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) xn[a][c] = f2(in[0][a][c], in[1][a][c]);
+    const int layer = A.elayer ? A.elayer[ez] : 0;
+    const LayerTable& LT = A.P ? A.P->L : L;
+    const float eta = A.P ? float(A.P->eta) : A.eta;
+    f2 lam, mu;
+    if (A.cellE) {
+      float E[2];
+#pragma unroll
+      for (int e = 0; e < 2; e++)
+        E[e] = ok[e] ? A.cellE[((int64_t)ez * (A.ny - 1) + ey[e]) * (A.nx - 1) + ex] : 0.f;
+      const f2 Ep(E[0], E[1]);
+      lam = Ep * f2(float(LT.lamfac[layer]));
+      mu = Ep * f2(float(LT.mufac[layer]));
+    } else {
+      lam = f2(float(LT.lambda[layer]));
+      mu = f2(float(LT.mu[layer]));
+    }
+    const f2 v0(in[0][0][3], in[1][0][3]);
+    f2 y[8][3];
+    u_element_const<f2, CUBIC>(xn, fma(v0, v0, f2(eta)), lam, mu, f2(A.ihx), f2(A.ihy), f2(A.ihz),
+                               f2(A.vol), y);
+#pragma unroll
+    for (int a = 0; a < 8; a++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        out[0][a][c] = ok[0] ? y[a][c].v.x : 0.f;
+        out[1][a][c] = ok[1] ? y[a][c].v.y : 0.f;
+      }
+  }
+  __device__ __forceinline__ static unsigned node_flags(const Args& A, int64_t n) {
+    return UOp<float>::node_flags(A, n);
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node_in(const Args& A, int64_t n, const T (&val)[NC],
+                                                          unsigned b, const T (&xin)[NC]) {
+    return UOp<float>::template finish_node_in<DOT>(A, n, val, b, xin);
+  }
+  template <bool DOT>
+  __device__ __forceinline__ static double finish_node(const Args& A, int64_t n, const T (&val)[NC]) {
+    return UOp<float>::template finish_node<DOT>(A, n, val);
+  }
+};
+
 template <typename T> struct VApplyArgs {
   CUtensorMap cmap;                   // the coefficient as a 3-D tensor (ex, ey, 27 ez + g),
                                       // box 32 x TY x 27 (vcoef_index layout)

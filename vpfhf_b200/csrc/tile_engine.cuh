@@ -598,23 +598,23 @@ cudaError_t launch_tile_apply(typename Op::Args A, const TilePlan& p, const Laye
 template <class OpF, class OpG, int TY, int MINBF, int MINB>
 cudaError_t launch_tile_apply_split(typename OpG::Args A, const TilePlan& p, const LayerTable& L,
                                     cudaStream_t s) {
-  static_assert(OpF::LIST == 0 && OpG::LIST == 1 && OpF::EPT == 1 && OpG::EPT == 1, "unit lists 0, 1");
+  static_assert(OpF::LIST == 0 && OpG::LIST == 1 && OpG::EPT == 1, "unit lists 0, 1");
   A.ntx = p.ntx;
   A.nty = p.nty;
   constexpr size_t smemF = tile_smem_bytes<OpF, TY, MINBF>(), smemG = tile_smem_bytes<OpG, TY, MINB>();
   cudaError_t ea = set_tile_attributes<OpF, TY, MINBF>();
   if (ea == cudaSuccess) ea = set_tile_attributes<OpG, TY, MINB>();
   if (ea != cudaSuccess) return ea;
-  const dim3 block(32, TY);
+  const dim3 blockF(32, TY / OpF::EPT), block(32, TY);
   const int sblocks = seam_blocks(p, A.nx, A.ny, A.nz), base = p.ncta0 + p.ncta;
   typename OpG::Args AG = A;
   if (AG.dot) AG.dot += p.ncta0;
   if (A.dot) {
-    tile_apply_kernel<OpF, TY, MINBF, true><<<p.ncta0, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpF, TY, MINBF, true><<<p.ncta0, blockF, smemF, s>>>(A, L);
     tile_apply_kernel<OpG, TY, MINB, true><<<p.ncta, block, smemG, s>>>(AG, L);
     if (sblocks > 0) seam_fixup_kernel<OpG, true><<<sblocks, 256, 0, s>>>(A, TY, base);
   } else {
-    tile_apply_kernel<OpF, TY, MINBF, false><<<p.ncta0, block, smemF, s>>>(A, L);
+    tile_apply_kernel<OpF, TY, MINBF, false><<<p.ncta0, blockF, smemF, s>>>(A, L);
     tile_apply_kernel<OpG, TY, MINB, false><<<p.ncta, block, smemG, s>>>(AG, L);
     if (sblocks > 0) seam_fixup_kernel<OpG, false><<<sblocks, 256, 0, s>>>(A, TY, base);
   }

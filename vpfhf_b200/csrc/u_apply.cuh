@@ -396,6 +396,10 @@ __device__ VFGPU_U_GENERAL_INLINE void u_element(const T (&xn)[8][3], const T (&
 // R[c][d][p - d] for the monomial p (the same signed butterfly as u_element).  On cubic
 // cells every k folds into the weight.  About 240 operations per element against ~925 for
 // u_element; equal to it up to rounding.
+// A product the compiler may not contract into a later add (f2's overload is in f2.cuh).
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+
 template <typename T, bool CUBIC = false>
 __device__ __forceinline__ void u_element_const(const T (&xn)[8][3], T S, T lam, T mu, T ihx,
                                                 T ihy, T ihz, T vol, T (&y)[8][3]) {
@@ -408,8 +412,13 @@ __device__ __forceinline__ void u_element_const(const T (&xn)[8][3], T S, T lam,
     modal8s(f, m[c]);
   }
   const T k[3] = {T(0.25) * ihx, T(0.25) * ihy, T(0.25) * ihz};
-  // gradient coefficient of component c, direction d, monomial B
-  auto G = [&](int c, int d, int B) -> T { return CUBIC ? m[c][B | (1 << d)] : m[c][B | (1 << d)] * k[d]; };
+  // gradient coefficient of component c, direction d, monomial B (as m * k unless CUBIC)
+  auto gm = [&](int c, int d, int B) -> T { return m[c][B | (1 << d)]; };
+  auto G = [&](int c, int d, int B) -> T { return CUBIC ? gm(c, d, B) : gm(c, d, B) * k[d]; };
+  // Every multiply that feeds an add is an explicit fma, or a product the compiler may
+  // not fuse (mul_rn: it reaches the adds below and the node butterfly's), so nothing is
+  // left to contract: the scalar and the packed two-lane (f2) builds of this element give
+  // the same bits per lane.
   T tr[7];
 #pragma unroll
   for (int B = 0; B < 7; B++) {
@@ -418,7 +427,8 @@ __device__ __forceinline__ void u_element_const(const T (&xn)[8][3], T S, T lam,
 #pragma unroll
     for (int e = 0; e < 3; e++)
       if (!((B >> e) & 1)) {
-        t = first ? G(e, e, B) : t + G(e, e, B);
+        if (CUBIC) t = first ? gm(e, e, B) : t + gm(e, e, B);
+        else t = first ? gm(e, e, B) * k[e] : fma(gm(e, e, B), k[e], t);
         first = false;
       }
     tr[B] = t;
@@ -439,14 +449,18 @@ __device__ __forceinline__ void u_element_const(const T (&xn)[8][3], T S, T lam,
         const int B = p & ~(1 << d);
         const int nb = (B & 1) + ((B >> 1) & 1) + ((B >> 2) & 1);
         const T Wd = CUBIC ? Wn[nb] : Wn[nb] * k[d];
-        T R;
-        if (c == d)
-          R = fma(T(2) * mu * Wd, G(c, c, B), (lam * Wd) * tr[B]);
-        else if (!((B >> c) & 1))
-          R = (mu * Wd) * (G(c, d, B) + G(d, c, B));
-        else
-          R = (mu * Wd) * G(c, d, B);
-        acc = first ? R : acc + R;
+        if (c == d) {
+          const T R = fma(T(2) * mu * Wd, G(c, c, B), (lam * Wd) * tr[B]);
+          acc = first ? R : acc + R;
+        } else {
+          T g;  // the symmetric gradient pair, or the one coefficient present
+          if (!((B >> c) & 1))
+            g = CUBIC ? gm(c, d, B) + gm(d, c, B) : fma(gm(d, c, B), k[c], gm(c, d, B) * k[d]);
+          else
+            g = G(c, d, B);
+          const T s = mu * Wd;
+          acc = first ? mul_rn(s, g) : fma(s, g, acc);
+        }
         first = false;
       }
       w[p] = acc;
