@@ -56,11 +56,15 @@ def test_mg_matches_oracle_step_u(cuda, oracle_mod, precision):
     ctx.close()
 
 
-@pytest.mark.parametrize("hetero,precision", [(False, "fp64"), (True, "fp64"), (True, "mixed")])
-def test_mg_matches_jacobi_65(cuda, hetero, precision):
+@pytest.mark.parametrize("hetero,precision,split", [(False, "fp64", "auto"), (True, "fp64", "auto"),
+                                                   (True, "mixed", "auto"), (True, "fp64", "on"),
+                                                   (True, "mixed", "on")])
+def test_mg_matches_jacobi_65(cuda, hetero, precision, split):
     """65^3 inclined penny, uniform or log-normal per-cell modulus: the multigrid (FP64 or
     FP32 V-cycle) and the FP64 Jacobi StepU reach the same U, the multigrid in a tenth of
-    the Krylov iterations."""
+    the Krylov iterations; with the U applies in one wave (auto at this size) and split
+    by phase field (on: the Jacobi CG's fused p.w, the V-cycle's fine level and the
+    multigrid's outer FP64 applies on the two waves)."""
     n = 65
     cellE = None
     if hetero:
@@ -69,6 +73,7 @@ def test_mg_matches_jacobi_65(cuda, hetero, precision):
     res = {}
     for pc in ("jacobi", "mg"):
         ctx = _penny_ctx(n, cellE=cellE)
+        ctx.set_u_split(split)
         rc, st = ctx.step_u(dict(pc=pc, precision=precision if pc == "mg" else "fp64"))
         assert rc == 0 and st["reason"] > 0, (pc, st)
         res[pc] = (ctx.get_field("U"), st, ctx.u_energy())

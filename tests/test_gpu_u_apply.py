@@ -95,16 +95,20 @@ def test_u_apply_host_pipeline_matches_device(cuda, oracle_mod, unilateral):
     ctx.close()
 
 
-@pytest.mark.parametrize("n,l,cellE", [((41, 41, 41), (4.0, 4.0, 4.0), False),
-                                       ((41, 41, 41), (4.0, 4.0, 4.0), True),
-                                       ((37, 21, 13), (1.1, 0.9, 0.7), False)])
-def test_u_apply_constant_phase_field_elements(cuda, oracle_mod, n, l, cellE):
+@pytest.mark.parametrize("n,l,cellE,split", [((41, 41, 41), (4.0, 4.0, 4.0), False, "auto"),
+                                             ((41, 41, 41), (4.0, 4.0, 4.0), True, "auto"),
+                                             ((37, 21, 13), (1.1, 0.9, 0.7), False, "auto"),
+                                             ((41, 41, 41), (4.0, 4.0, 4.0), True, "on"),
+                                             ((37, 21, 13), (1.1, 0.9, 0.7), False, "on")])
+def test_u_apply_constant_phase_field_elements(cuda, oracle_mod, n, l, cellE, split):
     """Mostly intact phase field (v = 1 away from a penny crack, a block of a constant
     v = 0.4 and a random block): elements whose 8 nodal v are equal take the
     fixed-weight element, the rest the row closed form; FP64 at 1e-12 and FP32 at
-    2e-6 normwise against the oracle, on cubic and non-cubic cells."""
+    2e-6 normwise against the oracle, on cubic and non-cubic cells, with per-cell
+    modulus, in one wave and split by phase field."""
     import vpfhf_b200 as vg
     o, ctx, _, x, mask = _setup(oracle_mod, n, l, 5, cellE=cellE)
+    ctx.set_u_split(split)
     rng = np.random.default_rng(6)
     pen = oracle_mod.Oracle(n, l, epsilon=2 * max(li / (ni - 1) for li, ni in zip(l, n)))
     v = pen.penny_v(tuple(li / 2 for li in l), 0.25 * min(l))
