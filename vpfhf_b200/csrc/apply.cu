@@ -93,19 +93,25 @@ cudaError_t apply_kernel_attributes() {
   return e;
 }
 
-cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int nex, int ney, int nez) {
-  using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                              const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
-                              CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
-                              CUtensorMapFloatOOBfill);
-  static const Encode encode = []() -> Encode {
-    void* fn = nullptr;
+using TensorEncode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                  CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+// cuTensorMapEncodeTiled from the driver (null if it has none)
+static TensorEncode tensor_encode() {
+  static const TensorEncode fn = []() -> TensorEncode {
+    void* f = nullptr;
     cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
         q != cudaDriverEntryPointSuccess)
       return nullptr;
-    return reinterpret_cast<Encode>(fn);
+    return reinterpret_cast<TensorEncode>(f);
   }();
+  return fn;
+}
+
+cudaError_t vcoef_tensor_map(CUtensorMap* map, const void* coef, int bytes, int nex, int ney, int nez) {
+  const TensorEncode encode = tensor_encode();
   if (!encode) return cudaErrorNotSupported;
   const int pitch = vcoef_pitch(nex);
   const cuuint64_t dims[3] = {(cuuint64_t)nex, (cuuint64_t)ney, (cuuint64_t)27 * nez};
@@ -382,15 +388,46 @@ TilePlan v_plan(int nx, int ny, int nz, int prec_bytes, int num_sms) {
   return tile_plan(nx, ny, nz, V_TY, 1, prec_bytes == 8 ? V64_MINB : V32_MINB, num_sms);
 }
 
+// The 1-D tensor maps of x (3N values) and v (N) that the fixed-weight wave copies its node
+// planes with (PlaneBox boxes, zeros beyond the ends); false where they cannot be made:
+// a pointer not 16-byte aligned, 3N past the 32-bit coordinates, no encoder.
+template <typename T> static bool u_plane_maps(UApplyArgs<T>& A) {
+  const int64_t N = (int64_t)A.nx * A.ny * A.nz;
+  const TensorEncode encode = tensor_encode();
+  if (!encode || 3 * N >= (int64_t)INT32_MAX || ((uintptr_t)A.x & 15) || ((uintptr_t)A.v & 15)) return false;
+  const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const cuuint64_t dx[1] = {(cuuint64_t)(3 * N)}, dv[1] = {(cuuint64_t)N}, none[1] = {0};
+  const cuuint32_t bx[1] = {(cuuint32_t)PlaneBox<T>::XBOX}, bv[1] = {(cuuint32_t)PlaneBox<T>::VBOX}, es[1] = {1};
+  const CUresult r1 = encode(&A.xmap, dt, 1, const_cast<T*>(A.x), dx, none, bx, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  const CUresult r2 = encode(&A.vmap, dt, 1, const_cast<T*>(A.v), dv, none, bv, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r1 == CUDA_SUCCESS && r2 == CUDA_SUCCESS;
+}
+
+// A split launch's operands (with the VFGPU_U_PLANES_TMA build option, the plane maps), or
+// false: then the apply runs one wave, with the second wave's x.y partials zeroed for a
+// caller that counts them.
+template <typename T> static bool split_args(const UApplyArgs<T>& A, const TilePlan& p, UApplyArgs<T>& B,
+                                             cudaStream_t s) {
+  B = A;
+  if (!VFGPU_U_PLANES_TMA || u_plane_maps(B)) return true;
+  if (A.dot) cudaMemsetAsync(A.dot + p.ncta + seam_blocks(p, A.nx, A.ny, A.nz), 0, p.ncta0 * sizeof(double), s);
+  return false;
+}
+
 template <>
 cudaError_t launch_u_apply<double>(const UApplyArgs<double>& A, const TilePlan& p,
                                    const LayerTable& L, cudaStream_t s) {
   if (A.cflag) return launch_tile_apply<UOpNC<double>, U64_TY, 1>(A, p, L, s);
-  if (A.ur[0] && A.ur[1]) {
+  UApplyArgs<double> B;
+  if (A.ur[0] && A.ur[1] && split_args(A, p, B, s)) {
     if (cubic(A))
       return launch_tile_apply_split<UOpConst<double, true>, UOp<double, true>, U64_TY, U64C_MINB, U64_MINB>(
-          A, p, L, s);
-    return launch_tile_apply_split<UOpConst<double>, UOp<double>, U64_TY, U64C_MINB, U64_MINB>(A, p, L, s);
+          B, p, L, s);
+    return launch_tile_apply_split<UOpConst<double>, UOp<double>, U64_TY, U64C_MINB, U64_MINB>(B, p, L, s);
   }
   if (cubic(A)) return launch_tile_apply<UOp<double, true>, U64_TY, U64_MINB>(A, p, L, s);
   return launch_tile_apply<UOp<double>, U64_TY, U64_MINB>(A, p, L, s);
@@ -402,10 +439,11 @@ cudaError_t launch_u_apply<float>(const UApplyArgs<float>& A, const TilePlan& p,
   // scalar tile (the packed build option keeps the plain operator packed)
   if (A.cflag) return launch_tile_apply<UOpNC<float>, U_TY, 2>(A, p, L, s);
   if constexpr (!kU32Packed) {
-    if (A.ur[0] && A.ur[1]) {
+    UApplyArgs<float> B;
+    if (A.ur[0] && A.ur[1] && split_args(A, p, B, s)) {
       if (cubic(A))
-        return launch_tile_apply_split<U32COpC, U32OpC, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
-      return launch_tile_apply_split<U32COp, U32Op, U32_TY, U32C_MINB, U32_MINB>(A, p, L, s);
+        return launch_tile_apply_split<U32COpC, U32OpC, U32_TY, U32C_MINB, U32_MINB>(B, p, L, s);
+      return launch_tile_apply_split<U32COp, U32Op, U32_TY, U32C_MINB, U32_MINB>(B, p, L, s);
     }
   }
   if (cubic(A)) return launch_tile_apply<U32OpC, U32_TY, U32_MINB>(A, p, L, s);

@@ -71,7 +71,8 @@ struct vfgpu_ctx {
   double* coef64 = nullptr;       // 27 per cell: V coupling coefficient (vcoef_index layout)
   float* coef32 = nullptr;
   CUtensorMap vmap64{}, vmap32{}; // coef64 / coef32 as the V apply's tensor copies see them
-  unsigned* d_cerr = nullptr;     // set by a V apply whose coefficient copy timed out
+  unsigned* d_cerr = nullptr;     // set by an apply whose bounded wait on a tensor copy (V
+                                  // coefficients, U node planes) gave up; held for the ctx's life
   uint8_t* vmask = nullptr;       // N
   vfgpu::ETab h_tab{};            // element tables of the uniform element (kernel parameter)
   vfgpu::CGState* d_cg = nullptr; // device CG scalars

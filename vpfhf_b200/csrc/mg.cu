@@ -682,6 +682,7 @@ template <typename T> UApplyArgs<T> level_args(vfgpu_ctx* c, const LevelT<T>& V,
   A.P = c->d_params;
   A.cflag = V.cflag;
   use_unit_lists(A, V.ul);
+  A.plane_err = c->d_cerr;
   return A;
 }
 

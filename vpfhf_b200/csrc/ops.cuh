@@ -18,6 +18,14 @@
 #include "tile_engine.cuh"
 #include "u_apply.cuh"
 
+// Build option: the fixed-weight U wave copies its node planes with 1-D tensor copies, two
+// per tile row (PlaneBox), instead of one cp.async per value.  Bit-identical; measured
+// slower on B200 at 129^3 on the penny field (FP64 apply 0.1223 ms against 0.1167, FP32
+// 0.0872 against 0.0855; with one thread waiting on each plane's mbarrier 0.1236 ms).
+#ifndef VFGPU_U_PLANES_TMA
+#define VFGPU_U_PLANES_TMA 0
+#endif
+
 namespace vfgpu {
 
 // CUBIC: hx = hy = hz, every 1/h factor folds into the row weight (u_element).
@@ -26,6 +34,7 @@ template <typename T_, bool CUBIC = false> struct UOp {
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
   static constexpr int LIST = 1;  // the unit list this operator takes in a split launch
+  static constexpr bool PLANES_TMA = false;  // node planes by cp.async values
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     src[0] = A.x + 3 * n;
     src[1] = A.x + 3 * n + 1;
@@ -127,6 +136,7 @@ template <typename T_, bool CUBIC = false> struct UOpConst : UOp<T_, CUBIC> {
   using T = T_;
   using Args = UApplyArgs<T>;
   static constexpr int LIST = 0;
+  static constexpr bool PLANES_TMA = VFGPU_U_PLANES_TMA != 0;  // node planes by tensor copies
   __device__ __forceinline__ static void element(const Args& A, const LayerTable& L, int ex,
                                                  int ey, int ez, const T (&in)[8][Base::NIN],
                                                  T (&out)[8][Base::NC]) {
@@ -141,6 +151,7 @@ template <typename T_> struct UOpNC {
   using Args = UApplyArgs<T>;
   static constexpr int NC = 3, NIN = 4, EPT = 1, CV = 0;
   static constexpr int LIST = -1;
+  static constexpr bool PLANES_TMA = false;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<T>::node_src(A, n, src);
   }
@@ -192,6 +203,7 @@ struct UOpF2 {
   using Args = UApplyArgs<float>;
   static constexpr int NC = 3, NIN = 4, EPT = 2, CV = 0;
   static constexpr int LIST = -1;
+  static constexpr bool PLANES_TMA = false;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<float>::node_src(A, n, src);
   }
@@ -253,6 +265,7 @@ template <bool CUBIC = false> struct UOpF2Const {
   using Args = UApplyArgs<float>;
   static constexpr int NC = 3, NIN = 4, EPT = 2, CV = 0;
   static constexpr int LIST = 0;
+  static constexpr bool PLANES_TMA = VFGPU_U_PLANES_TMA != 0;
   __device__ __forceinline__ static void node_src(const Args& A, int64_t n, const T* (&src)[NIN]) {
     UOp<float>::node_src(A, n, src);
   }
@@ -428,6 +441,7 @@ template <typename T_> struct VOp {
   using Args = VApplyArgs<T>;
   static constexpr int NC = 1, NIN = 1, EPT = 1;
   static constexpr int LIST = -1;
+  static constexpr bool PLANES_TMA = false;
   static constexpr int CV = 27;  // per-cell values staged by the engine (the coefficient)
   __device__ __forceinline__ static const CUtensorMap* cell_map(const Args& A) { return &A.cmap; }
   __device__ __forceinline__ static unsigned* cell_err(const Args& A) { return A.cerr; }

@@ -17,8 +17,6 @@ void free_solver(vfgpu_ctx* c) {
   for (auto& p : c->p32) cudaFree(p), p = nullptr;
   cudaFree(c->coef64);
   cudaFree(c->coef32);
-  cudaFree(c->d_cerr);
-  c->d_cerr = nullptr;
   cudaFree(c->vmask);
   cudaFree(c->d_cg);
   cudaFree(c->d_red);
@@ -51,8 +49,6 @@ static int solve_buffers(vfgpu_ctx* c) {
   // row padding is copied but never used; keep it defined
   if (e == cudaSuccess) e = cudaMemsetAsync(c->coef64, 0, ncoef * sizeof(double), c->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->coef32, 0, ncoef * sizeof(float), c->stream);
-  if (e == cudaSuccess) e = cudaMalloc((void**)&c->d_cerr, sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
   if (e == cudaSuccess)
     e = vcoef_tensor_map(&c->vmap64, c->coef64, 8, c->nx - 1, c->ny - 1, c->nz - 1);
   if (e == cudaSuccess)
@@ -160,7 +156,8 @@ static int check_cell_copies(vfgpu_ctx* c) {
   if (e != cudaSuccess) return cuda_fail(e, "V apply");
   if (!flag) return VFGPU_OK;
   cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
-  return fail(VFGPU_ERR_CUDA, "V apply: a coefficient tensor copy did not complete in time");
+  return fail(VFGPU_ERR_CUDA, "operator apply: a tensor copy (V coefficients or U node planes) did not "
+                              "complete in time");
 }
 
 // Reads n doubles of d_out into h_out (synchronising the stream).
@@ -521,6 +518,7 @@ int vfgpu_step_u(vfgpu_ctx* c, const vfgpu_solve_opts* o_, vfgpu_solve_stats* st
     if (w.expired() && !reason) reason = -100;
   }
   if (!reason) reason = -5;  // SNES_DIVERGED_MAX_IT
+  if (int rc2 = check_cell_copies(c)) return rc2;
   S.reason = reason;
   S.fnorm = fnorm;
   S.seconds = w.seconds();

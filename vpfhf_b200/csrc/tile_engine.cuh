@@ -68,9 +68,29 @@ template <int TY, int EPT = 1> struct Tile {
 // two (layer k + 1's elements are written while layer k's node sums still read) where
 // MINB blocks of that size fit an SM, else one, with a second barrier per layer.
 constexpr int kRing = 4;
-template <class Op, int TY, int SCS = 2> constexpr size_t tile_base_bytes() {
+// Tensor-copied node planes (Op::PLANES_TMA: the interlaced x, 3 values per node, and v):
+// a ring slot holds BY rows of x, then BY rows of v; each row is one 1-D tensor box that
+// starts at the row's first value rounded down to 16 bytes (A values), so XBOX / VBOX
+// values cover the row's 33 nodes after that shift, at 128-byte row pitches XP / VP.
+template <typename T> struct PlaneBox {
+  static constexpr int A = 16 / (int)sizeof(T);
+  static constexpr int XBOX = (99 + A - 1 + A - 1) / A * A, VBOX = (33 + A - 1 + A - 1) / A * A;
+  static constexpr int XP = (XBOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+  static constexpr int VP = (VBOX * (int)sizeof(T) + 127) / 128 * 128 / (int)sizeof(T);
+};
+template <class Op, int TY> constexpr size_t ring_bytes() {
   using T = typename Op::T;
-  return sizeof(T) * (kRing * Op::NIN * Tile<TY>::BX * Tile<TY>::BY + SCS * 4 * Op::NC * 33 * TY);
+  if constexpr (Op::PLANES_TMA)
+    return sizeof(T) * kRing * Tile<TY>::BY * (PlaneBox<T>::XP + PlaneBox<T>::VP);
+  else
+    return sizeof(T) * kRing * Op::NIN * Tile<TY>::BX * Tile<TY>::BY;
+}
+template <class Op, int TY, int SCS = 2> constexpr size_t sc_bytes() {
+  return sizeof(typename Op::T) * SCS * 4 * Op::NC * 33 * TY;
+}
+// ring, corner buffers and (PLANES_TMA) one mbarrier per ring slot
+template <class Op, int TY, int SCS = 2> constexpr size_t tile_base_bytes() {
+  return ring_bytes<Op, TY>() + sc_bytes<Op, TY, SCS>() + (Op::PLANES_TMA ? 8 * kRing : 0);
 }
 template <class Op, int TY, int MINB> constexpr int sc_stages() {
   return (Op::CV > 0 || MINB * (tile_base_bytes<Op, TY, 2>() + 1024) <= 228 * 1024) ? 2 : 1;
@@ -140,6 +160,16 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, i
       : "memory");
 }
 
+// 1-D tiled tensor copy global -> shared (no multicast), completion on bar; x: the first
+// element of the box (its byte offset a multiple of 16).
+__device__ __forceinline__ void tma_load_1d(void* dst, const CUtensorMap* map, int x, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.1d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2}], [%3];\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+      "l"(map), "r"(x), "r"((unsigned)__cvta_generic_to_shared(bar))
+      : "memory");
+}
+
 // Asynchronous global -> shared copy of one 4- or 8-byte value (LDGSTS); with
 // valid == false nothing is read and the destination is zero-filled.
 template <typename T>
@@ -165,10 +195,13 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   using G = Tile<TY, Op::EPT>;
   constexpr int EPT = Op::EPT;
   constexpr int NC = Op::NC, NIN = Op::NIN;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* sx = reinterpret_cast<T*>(smem_raw);  // [kRing][NIN][BY][BX]
-  T* sc = sx + kRing * NIN * G::BY * G::BX;  // [SCS][4*NC][TY][33]
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   constexpr int SCS = sc_stages<Op, TY, MINB>();
+  T* sx = reinterpret_cast<T*>(smem_raw);  // [kRing][NIN][BY][BX], or the PlaneBox rows
+  T* sc = reinterpret_cast<T*>(smem_raw + ring_bytes<Op, TY>());  // [SCS][4*NC][TY][33]
+  [[maybe_unused]] uint64_t* pbar = nullptr;  // PLANES_TMA: one mbarrier per ring slot
+  if constexpr (Op::PLANES_TMA)
+    pbar = reinterpret_cast<uint64_t*>(smem_raw + ring_bytes<Op, TY>() + sc_bytes<Op, TY, SCS>());
   const int lane = threadIdx.x, wy = threadIdx.y, tid = wy * 32 + lane;
   const int nx = A.nx, ny = A.ny, nz = A.nz, nex = nx - 1, ney = ny - 1;
   // This block's share of the work: node planes [U b / n, U (b + 1) / n) of the
@@ -221,18 +254,53 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       }
   };
 
-  // issue the asynchronous copies of node plane kz into ring slot buf (one group)
-  auto fetch_plane = [&](int buf, int kz) {
-    for (int s = tid; s < G::BX * G::BY; s += G::NT) {
-      const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
-      const bool in = X < nx && Y < ny;
-      const T* src[NIN];
-      Op::node_src(A, in ? node_index(X, Y, kz, nx, ny) : 0, src);
-#pragma unroll
-      for (int q = 0; q < NIN; q++) cp_async_val(&SXA(buf, q, w, l), src[q], in);
+  // input q of the node in tile row w, column l of plane kz, from ring slot buf (with
+  // PLANES_TMA: x component q < 3 or v, at the row's 16-byte shift, which only the low
+  // bits of the row's first node index decide)
+  auto rv = [&](int buf, int kz, int q, int w, int l) -> T {
+    if constexpr (Op::PLANES_TMA) {
+      using PB = PlaneBox<T>;
+      const unsigned n0 = ((unsigned)kz * (unsigned)ny + (unsigned)(Y0 + w)) * (unsigned)nx + (unsigned)X0;
+      if (q < 3) return sx[(buf * G::BY + w) * PB::XP + 3 * l + q + (int)((3u * n0) & (PB::A - 1))];
+      return sx[kRing * G::BY * PB::XP + (buf * G::BY + w) * PB::VP + l + (int)(n0 & (PB::A - 1))];
+    } else {
+      return SXA(buf, q, w, l);
     }
-    cp_async_commit();
   };
+
+  // issue the copies of node plane kz into ring slot buf: one cp.async group, or
+  // (PLANES_TMA) two tensor copies per tile row from warp 0, completing on pbar[buf]
+  auto fetch_plane = [&](int buf, int kz) {
+    if constexpr (Op::PLANES_TMA) {
+      using PB = PlaneBox<T>;
+      if (wy == 0) {
+        const int rows = min(G::BY, ny - Y0);
+        if (lane == 0)
+          mbar_expect_tx(&pbar[buf], (unsigned)(rows * (PB::XBOX + PB::VBOX) * sizeof(T)));
+        __syncwarp();
+        if (lane < rows) {
+          const int64_t n0 = ((int64_t)kz * ny + Y0 + lane) * nx + X0, e0 = 3 * n0;
+          tma_load_1d(sx + (buf * G::BY + lane) * PB::XP, &A.xmap, (int)(e0 - (e0 & (PB::A - 1))),
+                      &pbar[buf]);
+          tma_load_1d(sx + kRing * G::BY * PB::XP + (buf * G::BY + lane) * PB::VP, &A.vmap,
+                      (int)(n0 - (n0 & (PB::A - 1))), &pbar[buf]);
+        }
+      }
+    } else {
+      for (int s = tid; s < G::BX * G::BY; s += G::NT) {
+        const int l = s % G::BX, w = s / G::BX, X = X0 + l, Y = Y0 + w;
+        const bool in = X < nx && Y < ny;
+        const T* src[NIN];
+        Op::node_src(A, in ? node_index(X, Y, kz, nx, ny) : 0, src);
+#pragma unroll
+        for (int q = 0; q < NIN; q++) cp_async_val(&SXA(buf, q, w, l), src[q], in);
+      }
+      cp_async_commit();
+    }
+  };
+  // PLANES_TMA: the slot and phase parity of plane kz's copy in this segment
+  [[maybe_unused]] auto pslot = [&](int kz) { return (kz - kf) % kRing; };
+  [[maybe_unused]] auto pphase = [&](int kz) { return (unsigned)(((kz - kf) / kRing) & 1); };
 
   // fl: the node's flags (loaded ahead), buf: the ring slot holding plane z
   auto emit = [&](int l, int w, int X, int Y, int z, const T (&val)[NC], unsigned fl, int buf) {
@@ -241,7 +309,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
     if (!(left || right || bot || top)) {
       T xin[NC];
 #pragma unroll
-      for (int c = 0; c < NC; c++) xin[c] = SXA(buf, c, w, l);
+      for (int c = 0; c < NC; c++) xin[c] = rv(buf, z, c, w, l);
       dacc += Op::template finish_node_in<DOT>(A, node_index(X, Y, z, nx, ny), val, fl, xin);
     } else if (left || right) {
       const int i = left ? bx : bx + 1;
@@ -266,6 +334,14 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
   // Pipeline: planes kf, kf+1 resident before the first layer; during layer k the
   // copy of plane k+2 is in flight; one barrier per layer publishes plane k+2 and
   // the corner contributions of layer k together.
+  [[maybe_unused]] bool gave_up = false;
+  if constexpr (Op::PLANES_TMA) {
+    if (tid == 0) {
+      for (int st = 0; st < kRing; st++) mbar_init(&pbar[st], 1);
+      mbar_fence_init();
+    }
+    __syncthreads();  // initialised before any copy or wait
+  }
   fetch_plane(0, kf);
   fetch_plane(1, kf + 1);
   // per-cell values of layers kf, kf + 1 (CV > 0): issued before the first barrier,
@@ -284,10 +360,23 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
         if (kf + st <= kl) fetch_cells(st, kf + st);
     }
   }
-  cp_async_wait_all();
-  __syncthreads();
+  if constexpr (Op::PLANES_TMA) {
+    // bounded waits; if one gives up the block stops (thread 0 first waits, bounded again,
+    // for the copies in flight into slots 0 and 1) and the launch's results are void
+    gave_up = !mbar_wait(&pbar[0], 0u, A.plane_err);
+    gave_up = !mbar_wait(&pbar[1], 0u, A.plane_err) || gave_up;
+    if (__syncthreads_or(gave_up)) {
+      if (tid == 0) {
+        mbar_wait(&pbar[0], 0u, nullptr);
+        mbar_wait(&pbar[1], 0u, nullptr);
+      }
+      return false;
+    }
+  } else {
+    cp_async_wait_all();
+    __syncthreads();
+  }
   if (kf + 2 <= kl + 1) fetch_plane(2, kf + 2);
-  [[maybe_unused]] bool gave_up = false;
   for (int k = kf; k <= kl; k++) {
     const int r0 = (k - kf) % kRing, r1 = (k - kf + 1) % kRing, sb = SCS == 2 ? (k - kf) & 1 : 0;
     // the flags of the nodes this thread finishes after the layer (plane k), loaded now
@@ -315,7 +404,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
             for (int i = 0; i < 2; i++) {
               const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
 #pragma unroll
-              for (int q = 0; q < NIN; q++) in[a][q] = SXA(buf, q, wy + j, lane + i);
+              for (int q = 0; q < NIN; q++) in[a][q] = rv(buf, k + kk, q, wy + j, lane + i);
             }
         if constexpr (Op::CV > 0)
           Op::element(A, L, ex, ey, k, in, yc,
@@ -353,7 +442,7 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
               for (int i = 0; i < 2; i++) {
                 const int a = i + 2 * j + 4 * kk, buf = kk ? r1 : r0;
 #pragma unroll
-                for (int q = 0; q < NIN; q++) in[e][a][q] = SXA(buf, q, EPT * wy + e + j, lane + i);
+                for (int q = 0; q < NIN; q++) in[e][a][q] = rv(buf, k + kk, q, EPT * wy + e + j, lane + i);
               }
         Op::element_multi(A, L, ex, ey, k, ok, in, yc);
       } else {
@@ -367,7 +456,11 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
 #pragma unroll
       for (int e = 0; e < EPT; e++) store_xsums(sb, EPT * wy + e, yc[e]);
     }
-    cp_async_wait_all();  // this thread's copies of plane k+2 have landed
+    if constexpr (Op::PLANES_TMA) {  // plane k+2 has landed (bounded)
+      if (k + 2 <= kl + 1 && !mbar_wait(&pbar[pslot(k + 2)], pphase(k + 2), A.plane_err)) gave_up = true;
+    } else {
+      cp_async_wait_all();  // this thread's copies of plane k+2 have landed
+    }
     if constexpr (Op::CV > 0) {
       // ... and everyone's; corner contributions of layer k visible.  If any thread's
       // wait on layer k's values gave up, the whole block stops here: no further copy
@@ -380,6 +473,13 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
           if (k + 1 <= kl)
             mbar_wait(&cbar[(k + 1 - kf) % kCellStages], ((k + 1 - kf) / kCellStages) & 1, nullptr);
         }
+        return false;
+      }
+    } else if constexpr (Op::PLANES_TMA) {
+      // ... corner contributions of layer k visible; if a wait on plane k+2 gave up the
+      // block stops, thread 0 waiting (bounded) for that plane's copies in flight
+      if (__syncthreads_or(gave_up)) {
+        if (tid == 0 && k + 2 <= kl + 1) mbar_wait(&pbar[pslot(k + 2)], pphase(k + 2), nullptr);
         return false;
       }
     } else {
@@ -454,6 +554,9 @@ __global__ void __launch_bounds__(32 * TY / Op::EPT, MINB)
       if constexpr (Op::CV > 0)  // every phase of the stages completed: re-armed by the next init
         if (tid == 0)
           for (int st = 0; st < kCellStages; st++) mbar_inval(&cbar[st]);
+      if constexpr (Op::PLANES_TMA)  // every plane copied was waited for
+        if (tid == 0)
+          for (int st = 0; st < kRing; st++) mbar_inval(&pbar[st]);
     }
   }
   if constexpr (DOT) {

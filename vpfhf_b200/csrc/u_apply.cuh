@@ -30,6 +30,8 @@
 namespace vfgpu {
 
 template <typename T> struct UApplyArgs {
+  CUtensorMap xmap, vmap;             // 1-D tensor maps of x (3N) and v (N) for the operators that
+                                      // copy node planes by tensor copies (Op::PLANES_TMA)
   const T* __restrict__ x;            // 3N interlaced input
   const T* __restrict__ v;            // N phase field
   T* __restrict__ y;                  // 3N output
@@ -51,6 +53,7 @@ template <typename T> struct UApplyArgs {
   const int4* __restrict__ ur[2];
   const int* __restrict__ ustart[2];
   const int* __restrict__ utotal;
+  unsigned* __restrict__ plane_err;   // set when a bounded wait on a plane copy gave up
   int nx, ny, nz;
   int ntx, nty;                       // tiles in x, y
   T ihx, ihy, ihz, vol, eta;

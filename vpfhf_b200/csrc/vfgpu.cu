@@ -139,6 +139,7 @@ UApplyArgs<T> u_args(vfgpu_ctx* c, const T* x, const T* v, T* y, T* seam, const 
   A.P = c->d_params;
   A.cflag = c->unilateral ? c->d_cflag : nullptr;
   use_unit_lists(A, u_lists_on(c, (int)sizeof(T)) ? (sizeof(T) == 8 ? c->ul64 : c->ul32) : UnitLists{});
+  A.plane_err = c->d_cerr;
   return A;
 }
 // The split mode and the grid call for the lists in this precision (NOCOMPRESSION aside).
@@ -195,7 +196,7 @@ int vfgpu_destroy(vfgpu_ctx* c) {
   if (c->s_in) cudaStreamDestroy(c->s_in);
   if (c->s_out) cudaStreamDestroy(c->s_out);
   cudaFree(c->t64c);
-  void* bufs[] = {c->d_tcB, c->d_tcerr, c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_ul, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
+  void* bufs[] = {c->d_tcB, c->d_tcerr, c->d_widthc, c->d_pmult, c->d_width, c->d_wpart, c->d_wstall, c->d_cflag, c->d_params, c->d_dot, c->d_elayer, c->d_ul, c->d_cerr, c->d_cellE, c->bcU_kind, c->bcU_bits, c->bcV_kind, c->bcV_bits,
                   c->V32, c->seam64, c->seam32, c->t64a, c->t64b, c->t32a, c->t32b};
   for (void* p : bufs) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -265,6 +266,7 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
     }
   }
   ALLOC(c->d_params, sizeof(DevParams));
+  ALLOC(c->d_cerr, sizeof(unsigned));
   {
     int nd = 1;
     for (const TilePlan* p : {&c->plan64, &c->plan32, &c->vplan64, &c->vplan32})
@@ -287,6 +289,7 @@ int vfgpu_create(const vfgpu_grid* g, vfgpu_ctx** out) {
   ALLOC(c->t32b, 3 * c->N * sizeof(float));
 #undef ALLOC
   cudaMemsetAsync(c->d_elayer, 0, std::max(1, c->nz - 1), c->stream);
+  cudaMemsetAsync(c->d_cerr, 0, sizeof(unsigned), c->stream);
   cudaMemsetAsync(c->bcU_kind, 0, 3 * c->N, c->stream);
   cudaMemsetAsync(c->bcU_bits, 0, c->N, c->stream);
   cudaMemsetAsync(c->bcV_kind, 0, c->N, c->stream);
