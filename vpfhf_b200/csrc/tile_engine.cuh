@@ -29,10 +29,14 @@
 //   flags, xin[NC]) (the same from flags loaded ahead and the node's inputs from the
 //   plane ring), and an
 //   optional A.skip flag that turns a launch into a no-op (set by a converged CG,
-//   so that a queued batch of iterations costs nothing once it is done), and LIST:
+//   so that a queued batch of iterations costs nothing once it is done), LIST:
 //   -1, or the unit list (A.ur, A.ustart, A.utotal) the operator's launches take when
 //   the list is given -- the U operator's units split by phase field over two
-//   launches, each with its own wave of blocks (unit lists 0 and 1).
+//   launches, each with its own wave of blocks (unit lists 0 and 1) -- and PLANES_TMA:
+//   node planes by cp.async values (false) or, for an operator with the U inputs
+//   (interlaced x, v) and tensor maps A.xmap / A.vmap, by 1-D tensor copies per tile
+//   row (PlaneBox), completion on one mbarrier per ring slot (bounded waits,
+//   A.plane_err).
 // An Op with CV > 0 per-cell values (the V operator's 27 Gauss-point coefficients)
 //   supplies cell_map(A) (a 3-D tensor map, box 32 x TY x CV over (ex, ey, CV ez + g))
 //   and cell_err(A), and element(..., cc, cs) reads its cell's values from shared
