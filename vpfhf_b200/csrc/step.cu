@@ -298,12 +298,15 @@ static int u_dots_of(const vfgpu_ctx* c, const TilePlan& p, int prec_bytes) {
 }
 
 // Which CG call sites let the operator apply accumulate p.w (bit k-1 for call site k:
-// 1 U FP64, 2 U FP32, 3 V FP64, 4 V FP32); the others use a separate p.w pass.  The
-// FP64 sites only: in the FP32 U kernel the accumulator costs a register spill, and
-// the 129^3 AM step measured U FP32 0.064 s fused-off against 0.066 s fused-on
-// (FP64 U: 0.0957 s fused, 0.0972 s separate).
+// 1 U FP64, 2 U FP32, 3 V FP64, 4 V FP32); the others use a separate p.w pass.  U in
+// both precisions and V in FP64: the 129^3 mixed StepU measured 37.07 ms with the FP32
+// U apply accumulating p.w (the packed FP32 fixed-weight wave has the registers for it)
+// against 37.78 ms with the separate pass; with the earlier single-wave FP32 kernel the
+// accumulator spilled (U FP32 0.064 s fused-off against 0.066 s fused-on; FP64 U 0.0957 s
+// fused, 0.0972 s separate).  V FP32 fused as well measured 6.44 against 6.50 ms per
+// mixed StepV: not taken.
 #ifndef VFGPU_FUSE_DOT_MASK
-#define VFGPU_FUSE_DOT_MASK 5
+#define VFGPU_FUSE_DOT_MASK 7
 #endif
 static double* dot_buf(vfgpu_ctx* c, int kind) {
   return ((VFGPU_FUSE_DOT_MASK >> (kind - 1)) & 1) ? c->d_dot : nullptr;
