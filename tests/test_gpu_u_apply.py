@@ -168,3 +168,41 @@ def test_unit_lists_split(cuda, oracle_mod, n, l):
         y32 = ctx.u_apply(x, vg.MIXED)
         assert np.linalg.norm(y32 - yref) <= 2e-6 * np.linalg.norm(yref)
     ctx.close()
+
+
+def test_u_operator_properties_161(cuda, oracle_mod):
+    """161^3 (16.7M U dofs: past the oracle's sizes) with a penny crack, a constant block
+    and a random block of v, the applies split by phase field (AUTO at this size):
+    on vectors that vanish on the Dirichlet dofs the operator is symmetric (1e-12) and
+    positive, it is linear (1e-13), one wave gives the same bits, and FP32 stays within
+    2e-6 of FP64 normwise."""
+    import vpfhf_b200 as vg
+    torch = cuda
+    n, l = (161, 161, 161), (4.0, 4.0, 4.0)
+    o = oracle_mod.Oracle(n, l, epsilon=2 * 4.0 / 160)
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    free = mask == 0
+    v = o.penny_v((2.0, 2.0, 2.0), 0.8)
+    vv = v.reshape(n[2], n[1], n[0])
+    rng = np.random.default_rng(12)
+    vv[:20, :20, :20] = 0.4
+    vv[-12:, -12:, -12:] = rng.uniform(0, 1, (12, 12, 12))
+    ctx = vg.VFContext(n, l, dict(E=1e10, nu=0.25), eta=1e-8)
+    ctx.set_bc(vg.rollers())
+    ctx.set_field("V", vv.reshape(-1).copy())
+    x, y = (rng.standard_normal(3 * o.N) * free for _ in range(2))
+    xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+    ax = ctx.u_apply(xd, vg.FP64)
+    ay = ctx.u_apply(yd, vg.FP64)
+    axy = ctx.u_apply(2.0 * xd - 3.0 * yd, vg.FP64)
+    xay, yax = float(torch.dot(xd, ay)), float(torch.dot(yd, ax))
+    assert abs(xay - yax) <= 1e-12 * max(abs(xay), abs(yax))
+    assert float(torch.dot(xd, ax)) > 0 and float(torch.dot(yd, ay)) > 0
+    lin = axy - (2.0 * ax - 3.0 * ay)
+    assert float(lin.norm()) <= 1e-13 * float(axy.norm())
+    ctx.set_u_split("off")
+    assert torch.equal(ctx.u_apply(xd, vg.FP64), ax)
+    ctx.set_u_split("auto")
+    a32 = ctx.u_apply(xd, vg.MIXED)
+    assert float((a32 - ax).norm()) <= 2e-6 * float(ax.norm())
+    ctx.close()
