@@ -146,6 +146,7 @@ def test_unit_lists_split(cuda, oracle_mod, n, l):
     bb[-4:, :9, :] = 0.3
     bits = torch.from_numpy((mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)).cuda()
     grid, mp, L = _abi.Grid(*n, *l), _abi.MatProp(E, nu, 0.0, 0.0, 1.0), _abi.lib()
+    assert L.vfgpu_set_u_split(ctx.h, 7) != 0  # not a mode
     xd = torch.from_numpy(x).cuda()
     for v in (blob, rng.uniform(0, 1, o.N), np.ones(o.N), blob):
         ctx.set_field("V", v)
