@@ -413,3 +413,35 @@ def test_insitu_tractions_match_oracle(cuda, oracle_mod):
     assert el == pytest.approx(el_o, rel=1e-7)
     assert iw == pytest.approx(o.insitu_work(uo), rel=1e-7)
     ctx.close()
+
+
+def test_v_operator_properties_161(cuda):
+    """161^3 (past the oracle's sizes), AT1 with a random displacement (so the per-point
+    coefficient c = 2 W(u) varies), no V boundary condition and VIrrev = 1 (no pinned
+    dof): the V residual F(v) = K_V v - b is affine, and K_V = F(.) - F(0) is symmetric
+    (1e-12) and linear (1e-13)."""
+    import vpfhf_b200 as vg
+    n, L = 161, 4.0
+    h = L / (n - 1)
+    ctx = vg.VFContext((n, n, n), (L, L, L), dict(E=1e10, nu=0.25, Gc=100.0), epsilon=2 * h,
+                       eta=1e-8, atnum=1, pressurize=True)
+    ctx.set_bc(vg.rollers())
+    N = ctx.N
+    rng = np.random.default_rng(13)
+    ctx.set_field("U", rng.standard_normal(3 * N) * 1e-4)
+    ctx.set_field("pressure", np.full(N, 1e6))
+    ctx.set_field("VIrrev", np.ones(N))
+
+    def F(v):
+        ctx.set_field("V", v)
+        return ctx.v_residual()
+
+    f0 = F(np.zeros(N))
+    x, y = rng.uniform(0, 1, N), rng.uniform(0, 1, N)
+    kx, ky = F(x) - f0, F(y) - f0
+    xky, ykx = float(x @ ky), float(y @ kx)
+    assert abs(xky - ykx) <= 1e-12 * max(abs(xky), abs(ykx))
+    assert float(x @ kx) > 0
+    kz = F(2.0 * x - 3.0 * y) - f0
+    assert np.linalg.norm(kz - (2.0 * kx - 3.0 * ky)) <= 1e-13 * np.linalg.norm(kz)
+    ctx.close()
