@@ -207,3 +207,35 @@ def test_u_operator_properties_161(cuda, oracle_mod):
     a32 = ctx.u_apply(xd, vg.MIXED)
     assert float((a32 - ax).norm()) <= 2e-6 * float(ax.norm())
     ctx.close()
+
+
+def test_layered_material_split(cuda, oracle_mod):
+    """Three material layers across z (per-element-layer Lame coefficients in the device
+    parameter block) with a mostly intact phase field: the applies split by phase field
+    and in one wave give the same bits, FP64 at 1e-12 and FP32 at 2e-6 against the
+    oracle."""
+    import vpfhf_b200 as vg
+    n, l = (45, 37, 33), (2.0, 1.6, 1.4)
+    E, nu = [1e10, 3e10, 0.6e10], [0.25, 0.3, 0.2]
+    layer = np.array([0] * 10 + [1] * 12 + [2] * 10, np.int32)  # nz - 1 element layers
+    o = oracle_mod.Oracle(n, l, E=E, nu=nu, eta=1e-8, layer=layer)
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    rng = np.random.default_rng(14)
+    v = np.ones(o.N)
+    vv = v.reshape(n[2], n[1], n[0])
+    vv[12:20, 5:20, 3:30] = rng.uniform(0, 1, vv[12:20, 5:20, 3:30].shape)
+    vv[25:, :, :] = 0.5
+    ctx = vg.VFContext(n, l, [dict(E=e, nu=p) for e, p in zip(E, nu)], eta=1e-8, layer=layer)
+    ctx.set_bc(vg.rollers())
+    ctx.set_field("V", v)
+    x = rng.standard_normal(3 * o.N) * 1e-3
+    xd = cuda.from_numpy(x).cuda()
+    yref = o.u_apply(v, x, mask)
+    ys = {}
+    for split in ("off", "on"):
+        ctx.set_u_split(split)
+        ys[split] = (ctx.u_apply(xd, vg.FP64).cpu().numpy(), ctx.u_apply(x, vg.MIXED))
+    assert np.array_equal(ys["on"][0], ys["off"][0]) and np.array_equal(ys["on"][1], ys["off"][1])
+    assert np.abs(ys["on"][0] - yref).max() <= 1e-12 * np.abs(yref).max()
+    assert np.linalg.norm(ys["on"][1] - yref) <= 2e-6 * np.linalg.norm(yref)
+    ctx.close()
