@@ -171,6 +171,56 @@ def test_unit_lists_split(cuda, oracle_mod, n, l):
     ctx.close()
 
 
+@pytest.mark.parametrize("n,l", [((1025, 513, 3), (4.0, 2.0, 2.0 / 256)),   # cubic cells
+                                 ((1025, 1041, 3), (4.0, 3.0, 0.05))])
+def test_unit_lists_column_limit(cuda, oracle_mod, n, l):
+    """The one-block list builder takes up to 2048 tile columns per plan.  At 1025 x 513 x 3
+    the FP64 plan (32 x 8 element tiles) has exactly 2048 columns and the FP32 one (32 x 16)
+    1024: both split.  At 1025 x 1041 x 3 both are past the limit (4160 / 2080 columns) and
+    keep one wave although the split is asked for.  Either way: the bits of one wave (FP64
+    and FP32) and of the fixed-scratch apply, and the oracle's values (FP64 1e-12, FP32
+    2e-6), on a field with intact, constant-damage and random regions."""
+    import ctypes as C
+
+    import vpfhf_b200 as vg
+    from vpfhf_b200 import _abi
+    torch = cuda
+    E, nu, eta = 1e10, 0.25, 1e-8
+    o = oracle_mod.Oracle(n, l, E=E, nu=nu, eta=eta)
+    ctx = vg.VFContext(n, l, dict(E=E, nu=nu), eta=eta)
+    ctx.set_bc(vg.rollers())
+    mask, _ = o.bc(oracle_mod.rollers_face())
+    rng = np.random.default_rng(11)
+    v = np.ones(o.N)
+    vv = v.reshape(n[2], n[1], n[0])
+    y0, y1 = n[1] // 5, n[1] // 3
+    vv[:, y0:y1, 300:520] = rng.uniform(0, 1, (n[2], y1 - y0, 220))
+    vv[1:, -n[1] // 4:, :40] = 0.3
+    ctx.set_field("V", v)
+    x = rng.standard_normal(3 * o.N) * 1e-3
+    xd = torch.from_numpy(x).cuda()
+    ctx.set_u_split("off")
+    y_one, y_one32 = ctx.u_apply(xd, vg.FP64).cpu().numpy(), ctx.u_apply(x, vg.MIXED)
+    ctx.set_u_split("on")
+    y = ctx.u_apply(xd, vg.FP64).cpu().numpy()
+    assert np.array_equal(y, y_one)
+    y32 = ctx.u_apply(x, vg.MIXED)
+    assert np.array_equal(y32, y_one32)
+    bits = torch.from_numpy((mask.reshape(o.N, 3) * np.array([1, 2, 4])).sum(1).astype(np.uint8)).cuda()
+    vd, yna = torch.from_numpy(v).cuda(), torch.full_like(xd, float("nan"))
+    L = _abi.lib()
+    torch.cuda.synchronize()
+    rc = L.vfgpu_u_apply_noalloc(C.byref(_abi.Grid(*n, *l)), C.byref(_abi.MatProp(E, nu, 0.0, 0.0, 1.0)), eta,
+                                 vd.data_ptr(), bits.data_ptr(), xd.data_ptr(), yna.data_ptr(), None)
+    assert rc == 0, L.vfgpu_last_error().decode()
+    torch.cuda.synchronize()
+    assert np.array_equal(yna.cpu().numpy(), y)
+    yref = o.u_apply(v, x, mask)
+    assert np.abs(y - yref).max() <= 1e-12 * np.abs(yref).max()
+    assert np.linalg.norm(y32 - yref) <= 2e-6 * np.linalg.norm(yref)
+    ctx.close()
+
+
 def test_u_operator_properties_161(cuda, oracle_mod):
     """161^3 (16.7M U dofs: past the oracle's sizes) with a penny crack, a constant block
     and a random block of v, the applies split by phase field (AUTO at this size):
